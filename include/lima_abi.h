@@ -1,0 +1,254 @@
+/*
+ * lima_abi.h — C-ABI of the B200-native LIMA_MD step engine (quantom_b200).
+ *
+ * The reference (DanielRJohansen/Quantom, "LIMA_MD") has no plugin or FFI
+ * interface: its per-step path sits behind the C++ class Engine
+ * (Quantom/Quantom/Engine.cuh:109-208) operating on a Box in CUDA managed
+ * memory (Quantom/Quantom/Simulation.cuh:35-92), driven by
+ * Environment::run (Quantom/Quantom/Environment.cpp:100-122).  This header is
+ * the boundary that replaces it: plain C, plain pointers and sizes, status
+ * codes instead of exit(), caller-owned host buffers, library-owned device
+ * memory.  The structs below are byte-compatible with the reference's own
+ * (sizes in comments; tests/test_layout.py checks them against a build of
+ * the reference), so the reference's Box arrays can be passed unchanged.
+ *
+ * Units are the reference's: positions nm, time ns, mass kg/mol, energy J/mol,
+ * force J/(mol nm).
+ */
+#ifndef LIMA_ABI_H
+#define LIMA_ABI_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ */
+/* Reference layout (Quantom/Quantom/Bodies.cuh, QuantomTypes.cuh,      */
+/* Forcefield.cuh).  Capacities are the reference's constants.          */
+/* ------------------------------------------------------------------ */
+#define LIMA_MAX_COMPOUND_PARTICLES 64        /* Constants.cuh:58 */
+#define LIMA_MAX_PAIRBONDS 128                /* Bodies.cuh:300 */
+#define LIMA_MAX_ANGLEBONDS 256               /* Bodies.cuh:301 */
+#define LIMA_MAX_DIHEDRALS 384                /* Bodies.cuh:302 */
+#define LIMA_LJ_IGNORES_MAX 32                /* Bodies.cuh:170 */
+#define LIMA_MAX_PARTICLES_IN_BRIDGE 32       /* Constants.cuh:110 */
+#define LIMA_MAX_SINGLEBONDS_IN_BRIDGE 32     /* Constants.cuh:111 */
+#define LIMA_MAX_ANGLEBONDS_IN_BRIDGE 32      /* Constants.cuh:112 */
+#define LIMA_MAX_DIHEDRALBONDS_IN_BRIDGE 32   /* Constants.cuh:113 */
+#define LIMA_MAX_ATOM_TYPES 32                /* Forcefield.cuh:12 */
+#define LIMA_MAX_COMPOUNDS 255                /* Constants.cuh:88: LJ_Ignores holds uint8 compound ids */
+#define LIMA_ATOMTYPE_SOL 0                   /* Forcefield.cuh:15 */
+
+typedef struct { float x, y, z; } lima_float3;                       /* Float3, 12 B */
+
+typedef struct { lima_float3 pos, pos_tsub1; } lima_solvent;          /* Solvent, 24 B */
+
+typedef struct { float b0, kb; uint32_t atom_indexes[2]; } lima_pair_bond;            /* PairBond, 16 B */
+typedef struct { float theta_0, k_theta; uint32_t atom_indexes[3]; } lima_angle_bond; /* AngleBond, 20 B */
+typedef struct { float phi_0, k_phi; uint8_t n; uint32_t atom_indexes[4]; } lima_dihedral_bond; /* DihedralBond, 28 B */
+
+typedef struct {                                                      /* LJ_Ignores, 65 B */
+    uint8_t local_ids[LIMA_LJ_IGNORES_MAX];
+    uint8_t compound_ids[LIMA_LJ_IGNORES_MAX];
+    uint8_t n_ignores;
+} lima_lj_ignores;
+
+typedef struct {                                                      /* CompoundState, 772 B */
+    lima_float3 positions[LIMA_MAX_COMPOUND_PARTICLES];
+    uint8_t n_particles;
+} lima_compound_state;
+
+typedef struct {                                                      /* Compound (LIMA_DEBUGMODE), 24,036 B */
+    uint8_t n_particles;
+    lima_float3 prev_positions[LIMA_MAX_COMPOUND_PARTICLES];
+    lima_float3 forces[LIMA_MAX_COMPOUND_PARTICLES];
+    uint8_t atom_types[LIMA_MAX_COMPOUND_PARTICLES];
+    uint8_t atom_color_types[LIMA_MAX_COMPOUND_PARTICLES];
+    lima_lj_ignores lj_ignore_list[LIMA_MAX_COMPOUND_PARTICLES];
+    uint32_t particle_global_ids[LIMA_MAX_COMPOUND_PARTICLES];
+    lima_float3 center_of_mass;
+    uint16_t n_singlebonds;
+    lima_pair_bond singlebonds[LIMA_MAX_PAIRBONDS];
+    uint16_t n_anglebonds;
+    lima_angle_bond anglebonds[LIMA_MAX_ANGLEBONDS];
+    uint16_t n_dihedrals;
+    lima_dihedral_bond dihedrals[LIMA_MAX_DIHEDRALS];
+    int32_t key_particle_index;
+    float confining_particle_sphere;
+} lima_compound;
+
+typedef struct { int32_t compound_id, local_id_compound; } lima_particle_ref_compact; /* 8 B */
+
+typedef struct {                                                      /* CompoundBridgeCompact, 2,352 B */
+    lima_particle_ref_compact particle_refs[LIMA_MAX_PARTICLES_IN_BRIDGE];
+    uint8_t atom_types[LIMA_MAX_PARTICLES_IN_BRIDGE];
+    int32_t n_particles;
+    uint16_t n_singlebonds;
+    lima_pair_bond singlebonds[LIMA_MAX_SINGLEBONDS_IN_BRIDGE];
+    uint16_t n_anglebonds;
+    lima_angle_bond anglebonds[LIMA_MAX_ANGLEBONDS_IN_BRIDGE];
+    uint16_t n_dihedrals;
+    lima_dihedral_bond dihedrals[LIMA_MAX_DIHEDRALBONDS_IN_BRIDGE];
+} lima_compound_bridge_compact;
+
+typedef struct { float mass, sigma, epsilon; } lima_particle_parameters;                  /* 12 B */
+typedef struct { lima_particle_parameters particle_parameters[LIMA_MAX_ATOM_TYPES]; } lima_forcefield; /* 384 B */
+
+/* ------------------------------------------------------------------ */
+/* Engine parameters (the reference's compile-time Constants.cuh:6-113  */
+/* and Simulation.cuh:152 become runtime values).                       */
+/* ------------------------------------------------------------------ */
+typedef enum {
+    LIMA_OK = 0,
+    LIMA_ERR_ARGUMENT = 1,     /* bad argument or size beyond a stated limit */
+    LIMA_ERR_CUDA = 2,         /* a CUDA call failed; lima_last_error has the text */
+    LIMA_ERR_CAPACITY = 3,     /* a neighbour list overflowed its capacity (reference: exit(1), Bodies.cuh:215-245) */
+    LIMA_ERR_STATE = 4,        /* call out of order (e.g. step before lima_finish_box) */
+    LIMA_ERR_NUMERIC = 5,      /* NaN position or |F| > 2e12 (reference: critical_error_encountered, Engine.cu:1050,1151) */
+    LIMA_ERR_UNSUPPORTED = 6   /* feature not available in the selected semantics */
+} lima_status;
+
+typedef enum {
+    /* The reference's own functional forms, list radii and integrator:
+       LJ over entity neighbour lists with no force cutoff and per-path mixing
+       rules, reference bonded forms, Stormer-Verlet with the reference
+       thermostat scalar (Engine.cu:461-1223). */
+    LIMA_SEMANTICS_REFERENCE = 0,
+    /* Conservative physics of the same model: Lorentz-Berthelot LJ with a
+       cutoff (+ optional potential switch) over a Verlet-buffered list,
+       harmonic bonds/angles and periodic dihedrals as gradients of their
+       energies, velocity Verlet, optional Berendsen thermostat. */
+    LIMA_SEMANTICS_PHYSICS = 1
+} lima_semantics;
+
+typedef enum {
+    LIMA_PRECISION_FP32 = 0,   /* plain FP32 state, forces and sums */
+    LIMA_PRECISION_MIXED = 1   /* FP32 forces, compensated FP32 accumulation and state updates,
+                                  FP64 energy/virial/KE reductions and thermostat scalar */
+} lima_precision;
+
+typedef enum {
+    LIMA_THERMOSTAT_NONE = 0,
+    LIMA_THERMOSTAT_REFERENCE = 1,  /* Engine::handleBoxtemp (Engine.cu:314-393): lambda = clamp(T0/T, 0.9, 1.1)
+                                       applied to the position delta for one step every thermostat_period steps */
+    LIMA_THERMOSTAT_BERENDSEN = 2   /* lambda = sqrt(1 + dt/tau (T0/T - 1)) on velocities every step */
+} lima_thermostat;
+
+typedef struct {
+    float box_len;             /* nm, cubic periodic box (reference BOX_LEN, Constants.cuh:35) */
+    float cutoff;              /* nm, physics cutoff r_c */
+    float ref_cutoff;          /* nm, the reference's CUTOFF constant (Constants.cuh:52); lists use 2*ref_cutoff.
+                                  0 = cutoff/2, so both semantics see the same list radius */
+    float skin;                /* nm, Verlet buffer of the physics list */
+    float switch_on;           /* nm, start of the potential switch (physics); >= cutoff: plain shifted cutoff */
+    double dt;                 /* ns */
+    int nlist_period;          /* steps between list rebuilds (reference: 200, Constants.cuh:71) */
+    int semantics;             /* lima_semantics */
+    int precision;             /* lima_precision */
+    int thermostat;            /* lima_thermostat */
+    double t_target;           /* K */
+    double tau_t;              /* ns, Berendsen coupling time */
+    int thermostat_period;     /* steps, reference thermostat (Constants.cuh:82) */
+    int energy_period;         /* steps between FP64 energy/virial evaluations (0 = only on lima_compute_energies) */
+    int solvent_list_capacity; /* per-solvent solvent-neighbour capacity, reference semantics (power of two) */
+    int compound_list_capacity;/* per-compound solvent-neighbour capacity, reference semantics */
+    int device;                /* CUDA device ordinal */
+    void* stream;              /* cudaStream_t to run on, or NULL for a library-owned stream */
+} lima_params;
+
+typedef struct lima_ctx lima_ctx;
+
+/* Energies, FP64, of the last evaluated step (lima_get_energies totals[]). */
+enum {
+    LIMA_E_LJ = 0, LIMA_E_BOND = 1, LIMA_E_ANGLE = 2, LIMA_E_DIHEDRAL = 3,
+    LIMA_E_KINETIC = 4, LIMA_E_VIRIAL = 5, LIMA_E_TEMPERATURE = 6, LIMA_E_TOTAL = 7,
+    LIMA_E_COUNT = 8
+};
+
+/* Neighbour-list selectors for lima_get_nlist / lima_set_nlist. */
+enum {
+    LIMA_NL_COMPOUND_COMPOUND = 0,  /* NeighborList::neighborcompound_ids of compounds */
+    LIMA_NL_COMPOUND_SOLVENT = 1,   /* NeighborList::neighborsolvent_ids of compounds */
+    LIMA_NL_SOLVENT_COMPOUND = 2,   /* NeighborList::neighborcompound_ids of solvents */
+    LIMA_NL_SOLVENT_SOLVENT = 3     /* NeighborList::neighborsolvent_ids of solvents */
+};
+
+/* Defaults: reference semantics, FP32, box 7 nm, cutoff 1.4 nm (reference
+   CUTOFF 0.7), dt 1e-7 ns, list period 200, no thermostat. */
+void lima_default_params(lima_params* p);
+
+/* Replaces Engine::Engine(Simulation*, ForceField) (Engine.cu:9-38) together
+   with lima_set_forcefield / lima_load_* / lima_finish_box. */
+lima_status lima_create(const lima_params* params, lima_ctx** out);
+void lima_destroy(lima_ctx* ctx);
+const char* lima_last_error(const lima_ctx* ctx);
+
+/* ForceField copy to the device (Engine.cu:27: cudaMemcpyToSymbol). */
+lima_status lima_set_forcefield(lima_ctx* ctx, const lima_forcefield* ff);
+
+/* Box contents (BoxBuilder::finishBox + Box::moveToDevice, BoxBuilder.cu:73-145,
+   Simulation.cuh:73-91).  The caller keeps ownership of the host arrays. */
+lima_status lima_load_compounds(lima_ctx* ctx, const lima_compound* compounds,
+                                const lima_compound_state* states, int n_compounds);
+lima_status lima_load_bridges(lima_ctx* ctx, const lima_compound_bridge_compact* bridges, int n_bridges);
+lima_status lima_load_solvents(lima_ctx* ctx, const lima_solvent* solvents, uint32_t n_solvents);
+
+/* Uploads the box and builds the first neighbour lists synchronously
+   (Engine.cu:35: handleNLISTS(simulation, false, true)). */
+lima_status lima_finish_box(lima_ctx* ctx);
+
+/* n_steps of Engine::deviceMaster + Engine::hostMaster (Engine.cu:44-75,
+   400-451): forces, integration, list rebuilds every nlist_period steps and
+   the thermostat, all on the device with no host synchronisation inside. */
+lima_status lima_step(lima_ctx* ctx, int n_steps);
+
+/* Blocks until the engine's stream is idle and reports a device-side error
+   (capacity overflow, NaN) raised since the last call. */
+lima_status lima_synchronize(lima_ctx* ctx);
+
+/* State readback in the reference layout (Box::compound_state_array,
+   Compound::prev_positions, Box::solvents). */
+lima_status lima_get_compound_states(lima_ctx* ctx, lima_compound_state* states, lima_float3* prev_positions);
+lima_status lima_get_solvents(lima_ctx* ctx, lima_solvent* solvents);
+/* Replace the positions of a loaded box in place (same layout as loading). */
+lima_status lima_set_state(lima_ctx* ctx, const lima_compound_state* states, const lima_float3* prev_positions,
+                           const lima_solvent* solvents);
+
+/* Total force each particle was integrated with in the last step:
+   compound_forces[c*64 + l], solvent_forces[s]. */
+lima_status lima_get_forces(lima_ctx* ctx, lima_float3* compound_forces, lima_float3* solvent_forces);
+
+/* FP64 energies (LIMA_E_*) and, optionally, the per-particle potE of the last
+   step in the reference's potE_buffer indexing (compound c particle l at
+   c*64+l, solvent s at n_compounds*64+s; Engine.cu:1012,1141). */
+lima_status lima_get_energies(lima_ctx* ctx, double* totals, double* potE_per_particle);
+/* Evaluates energies for the current positions without stepping. */
+lima_status lima_compute_energies(lima_ctx* ctx);
+
+/* Neighbour lists (Engine::updateNeighborLists, Engine.cu:208-287).
+   lima_build_nlist runs one update now.  lima_get_nlist writes CSR offsets
+   (n_entities+1) and ids (sorted ascending within each list); with ids NULL
+   only offsets and *total are written.  lima_set_nlist installs a previous
+   compound-compound list state, which the reference's update depends on. */
+lima_status lima_build_nlist(lima_ctx* ctx);
+lima_status lima_get_nlist(lima_ctx* ctx, int which, uint32_t* offsets, uint32_t* ids, uint32_t* total);
+lima_status lima_set_nlist(lima_ctx* ctx, int which, const uint32_t* offsets, const uint32_t* ids);
+
+/* Reference thermostat scalar for the next step (Box::thermostat_scalar,
+   Simulation.cuh:70); 1 after it has been applied once. */
+lima_status lima_set_thermostat_scalar(lima_ctx* ctx, float scalar);
+
+lima_status lima_get_step(lima_ctx* ctx, uint64_t* step);
+
+/* Device time of the last lima_step call, ms (CUDA events on the engine's
+   stream) — the reference's Engine::timings (Engine.cu:448-450). */
+lima_status lima_get_last_step_ms(lima_ctx* ctx, float* ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LIMA_ABI_H */

@@ -1,0 +1,257 @@
+"""Python host side of the B200 LIMA_MD step engine, over the C-ABI.
+
+Mirrors the reference's driver-facing interface (Quantom/Quantom/Engine.cuh:
+109-208, Environment.cpp:100-122): build an ``Engine`` for a box, call
+``deviceMaster()`` / ``hostMaster()`` (or ``step(n)``) and read back
+positions, forces, energies and neighbour lists.  Every call goes through
+``liblima_b200.so``; there is no CPU fallback — constructing an Engine without
+the built library or without a CUDA device raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+from . import layout as L
+
+_LIB = None
+LIB_PATH = Path(__file__).resolve().parent / "liblima_b200.so"
+
+OK, ERR_ARGUMENT, ERR_CUDA, ERR_CAPACITY, ERR_STATE, ERR_NUMERIC, ERR_UNSUPPORTED = range(7)
+SEMANTICS_REFERENCE, SEMANTICS_PHYSICS = 0, 1
+PRECISION_FP32, PRECISION_MIXED = 0, 1
+THERMOSTAT_NONE, THERMOSTAT_REFERENCE, THERMOSTAT_BERENDSEN = 0, 1, 2
+NL_COMPOUND_COMPOUND, NL_COMPOUND_SOLVENT, NL_SOLVENT_COMPOUND, NL_SOLVENT_SOLVENT = 0, 1, 2, 3
+E_LJ, E_BOND, E_ANGLE, E_DIHEDRAL, E_KINETIC, E_VIRIAL, E_TEMPERATURE, E_TOTAL = range(8)
+E_COUNT = 8
+
+
+class LimaError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"lima status {status}: {message}")
+        self.status = status
+
+
+class Params(ctypes.Structure):
+    """lima_params (include/lima_abi.h)."""
+    _fields_ = [("box_len", ctypes.c_float), ("cutoff", ctypes.c_float), ("ref_cutoff", ctypes.c_float),
+                ("skin", ctypes.c_float), ("switch_on", ctypes.c_float), ("dt", ctypes.c_double),
+                ("nlist_period", ctypes.c_int), ("semantics", ctypes.c_int), ("precision", ctypes.c_int),
+                ("thermostat", ctypes.c_int), ("t_target", ctypes.c_double), ("tau_t", ctypes.c_double),
+                ("thermostat_period", ctypes.c_int), ("energy_period", ctypes.c_int),
+                ("solvent_list_capacity", ctypes.c_int), ("compound_list_capacity", ctypes.c_int),
+                ("device", ctypes.c_int), ("stream", ctypes.c_void_p)]
+
+
+def load_library():
+    """Loads the in-tree liblima_b200.so (built by quantom_b200.build)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is missing; build it with `python -m quantom_b200.build`")
+    lib = ctypes.CDLL(str(LIB_PATH))
+    vp, i, u32, f, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_float, ctypes.c_double
+    sigs = {
+        "lima_default_params": (None, [vp]),
+        "lima_create": (i, [vp, ctypes.POINTER(vp)]),
+        "lima_destroy": (None, [vp]),
+        "lima_last_error": (ctypes.c_char_p, [vp]),
+        "lima_set_forcefield": (i, [vp, vp]),
+        "lima_load_compounds": (i, [vp, vp, vp, i]),
+        "lima_load_bridges": (i, [vp, vp, i]),
+        "lima_load_solvents": (i, [vp, vp, u32]),
+        "lima_finish_box": (i, [vp]),
+        "lima_step": (i, [vp, i]),
+        "lima_synchronize": (i, [vp]),
+        "lima_get_compound_states": (i, [vp, vp, vp]),
+        "lima_get_solvents": (i, [vp, vp]),
+        "lima_set_state": (i, [vp, vp, vp, vp]),
+        "lima_get_forces": (i, [vp, vp, vp]),
+        "lima_get_energies": (i, [vp, vp, vp]),
+        "lima_compute_energies": (i, [vp]),
+        "lima_build_nlist": (i, [vp]),
+        "lima_get_nlist": (i, [vp, i, vp, vp, ctypes.POINTER(u32)]),
+        "lima_set_nlist": (i, [vp, i, vp, vp]),
+        "lima_set_thermostat_scalar": (i, [vp, f]),
+        "lima_get_step": (i, [vp, ctypes.POINTER(ctypes.c_uint64)]),
+        "lima_get_last_step_ms": (i, [vp, ctypes.POINTER(f)]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name, None)
+        if fn is None:
+            continue
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib
+
+
+def default_params(**kw) -> Params:
+    lib = load_library()
+    p = Params()
+    lib.lima_default_params(ctypes.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+class Engine:
+    """Engine(Simulation*, ForceField) (Engine.cu:9-38) for a System."""
+
+    def __init__(self, system, params: Params | None = None, **kw):
+        self.lib = load_library()
+        self.system = system
+        if params is None:
+            spec = system.spec
+            params = default_params(box_len=spec.box_len, cutoff=spec.cutoff, dt=spec.dt)
+        for k, v in kw.items():
+            setattr(params, k, v)
+        self.params = params
+        h = ctypes.c_void_p()
+        st = self.lib.lima_create(ctypes.byref(params), ctypes.byref(h))
+        if st != OK:
+            raise LimaError(st, "lima_create failed")
+        self.h = h
+        try:
+            self._check(self.lib.lima_set_forcefield(self.h, _ptr(system.forcefield)))
+            if system.n_compounds:
+                self._check(self.lib.lima_load_compounds(self.h, _ptr(system.compounds), _ptr(system.states),
+                                                         system.n_compounds))
+            if len(system.bridges):
+                self._check(self.lib.lima_load_bridges(self.h, _ptr(system.bridges), len(system.bridges)))
+            self._check(self.lib.lima_load_solvents(self.h, _ptr(system.solvents), system.n_solvents))
+            self._check(self.lib.lima_finish_box(self.h))
+        except Exception:
+            self.close()
+            raise
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.lima_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st):
+        if st != OK:
+            msg = self.lib.lima_last_error(self.h)
+            raise LimaError(st, msg.decode() if msg else "")
+
+    # -- reference driver interface ----------------------------------------
+    def deviceMaster(self):
+        """One step of forces + integration (Engine::deviceMaster, Engine.cu:44-47)."""
+        self._check(self.lib.lima_step(self.h, 1))
+
+    def hostMaster(self):
+        """The reference's per-step host work (lists, thermostat) runs on the
+        device inside lima_step; this only surfaces device-side errors."""
+        self._check(self.lib.lima_synchronize(self.h))
+
+    def step(self, n: int = 1):
+        self._check(self.lib.lima_step(self.h, int(n)))
+
+    def synchronize(self):
+        self._check(self.lib.lima_synchronize(self.h))
+
+    @property
+    def current_step(self) -> int:
+        v = ctypes.c_uint64()
+        self._check(self.lib.lima_get_step(self.h, ctypes.byref(v)))
+        return int(v.value)
+
+    def last_step_ms(self) -> float:
+        v = ctypes.c_float()
+        self._check(self.lib.lima_get_last_step_ms(self.h, ctypes.byref(v)))
+        return float(v.value)
+
+    # -- state ---------------------------------------------------------------
+    def compound_states(self):
+        n = self.system.n_compounds
+        st = np.zeros(n, L.CompoundState)
+        prev = np.zeros((n, L.MAX_COMPOUND_PARTICLES, 3), np.float32)
+        if n:
+            self._check(self.lib.lima_get_compound_states(self.h, _ptr(st), _ptr(prev)))
+        return st, prev
+
+    def solvents(self):
+        s = np.zeros(self.system.n_solvents, L.Solvent)
+        if len(s):
+            self._check(self.lib.lima_get_solvents(self.h, _ptr(s)))
+        return s
+
+    def set_state(self, states, prev_positions, solvents):
+        self._check(self.lib.lima_set_state(self.h, _ptr(states), _ptr(prev_positions), _ptr(solvents)))
+
+    def forces(self):
+        nc = self.system.n_compounds
+        fc = np.zeros((nc, L.MAX_COMPOUND_PARTICLES, 3), np.float32)
+        fs = np.zeros((self.system.n_solvents, 3), np.float32)
+        self._check(self.lib.lima_get_forces(self.h, _ptr(fc) if nc else None, _ptr(fs)))
+        return fc, fs
+
+    def energies(self, per_particle: bool = False):
+        tot = np.zeros(E_COUNT, np.float64)
+        pp = None
+        if per_particle:
+            pp = np.zeros(self.system.n_compounds * L.MAX_COMPOUND_PARTICLES + self.system.n_solvents, np.float64)
+        self._check(self.lib.lima_get_energies(self.h, _ptr(tot), _ptr(pp)))
+        return (tot, pp) if per_particle else tot
+
+    def compute_energies(self):
+        self._check(self.lib.lima_compute_energies(self.h))
+        return self.energies()
+
+    def set_thermostat_scalar(self, s: float):
+        self._check(self.lib.lima_set_thermostat_scalar(self.h, float(s)))
+
+    # -- neighbour lists -------------------------------------------------------
+    def build_nlist(self):
+        self._check(self.lib.lima_build_nlist(self.h))
+
+    def nlist(self, which: int):
+        n = self.system.n_compounds if which in (NL_COMPOUND_COMPOUND, NL_COMPOUND_SOLVENT) else self.system.n_solvents
+        off = np.zeros(n + 1, np.uint32)
+        tot = ctypes.c_uint32()
+        self._check(self.lib.lima_get_nlist(self.h, which, _ptr(off), None, ctypes.byref(tot)))
+        ids = np.zeros(max(1, tot.value), np.uint32)
+        self._check(self.lib.lima_get_nlist(self.h, which, _ptr(off), _ptr(ids), ctypes.byref(tot)))
+        return off, ids[: tot.value]
+
+    def set_nlist(self, which: int, offsets, ids):
+        offsets = np.ascontiguousarray(offsets, np.uint32)
+        ids = np.ascontiguousarray(ids if len(ids) else np.zeros(1), np.uint32)
+        self._check(self.lib.lima_set_nlist(self.h, which, _ptr(offsets), _ptr(ids)))
+
+
+def cuda_available() -> bool:
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def lib_built() -> bool:
+    return LIB_PATH.exists()
+
+
+os.environ.setdefault("LIMA_B200_LIB", str(LIB_PATH))
