@@ -15,7 +15,16 @@
 #   3. Engine.cu: Engine::step (Engine.cu:400-451, CUDA launch syntax) is
 #      deleted; ref_emu.cpp defines it with emulated launches;
 #   4. Engine.cu: integratePosition (Engine.cu:849) gets one call to
-#      lima_ref_force_hook(p_index, force) as its first statement.
+#      lima_ref_force_hook(p_index, force) as its first statement;
+#   5. Engine.cu: a __syncthreads() after the shared accumulator reset at the
+#      top of computePairbondForces/AnglebondForces/DihedralForces
+#      (Engine.cu:746,779,814), and one between thread 0's applyPBC of
+#      particle 0 and the other threads' applyHyperpos to it (Engine.cu:993-996).
+#      The reference has no barrier at either point; on a GPU, warp 0 executes
+#      them in program order (every lane resets before lane 0 adds; lanes read
+#      particle 0 after lane 0 wrapped it).  The host emulator runs threads one
+#      after another, so without the barriers it would resolve both races
+#      differently from the hardware.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 REF_ROOT="${LIMA_REF_ROOT:-/root/reference}"
@@ -50,6 +59,14 @@ awk 'BEGIN{skip=0} /^void Engine::step\(\) \{/{skip=1} { if(!skip) print; else i
 n=$(grep -c '^__device__ void integratePosition(Float3\* pos, Float3\* pos_tsub1' "$TMP/Engine.cu" || true)
 [ "$n" = "1" ] || { echo "build_ref.sh: integratePosition signature not found" >&2; exit 1; }
 sed -i '/^__device__ void integratePosition(Float3\* pos, Float3\* pos_tsub1/a\	lima_ref_force_hook(p_index, force);' "$TMP/Engine.cu"
+
+# 5. barriers at the two intra-block races (see the header)
+n=$(grep -cE '^[[:space:]]*utility_buffer\[threadIdx\.x\] = Float3\((0\.f|0, 0, 0)\);[[:space:]]*$' "$TMP/Engine.cu" || true)
+[ "$n" = "3" ] || { echo "build_ref.sh: expected 3 bonded accumulator resets, found $n" >&2; exit 1; }
+sed -i -E '/^[[:space:]]*utility_buffer\[threadIdx\.x\] = Float3\((0\.f|0, 0, 0)\);[[:space:]]*$/a\	__syncthreads();' "$TMP/Engine.cu"
+n=$(grep -c 'applyHyperpos(&compound_state.positions\[0\], &compound_state.positions\[threadIdx.x\]);.*So all particles follows p0' "$TMP/Engine.cu" || true)
+[ "$n" = "1" ] || { echo "build_ref.sh: PBC hyperpos line not found" >&2; exit 1; }
+sed -i '/applyHyperpos(&compound_state.positions\[0\], &compound_state.positions\[threadIdx.x\]);.*So all particles follows p0/i\	__syncthreads();' "$TMP/Engine.cu"
 
 CXX="${CXX:-g++}"
 "$CXX" -std=c++17 -O3 -march=x86-64-v3 -ffp-contract=off -fno-fast-math -pthread -fPIC -shared -w \

@@ -246,7 +246,7 @@ int orc_ref_nlist(float L, float C, int n_c, const lima_compound* comps, const l
     }
     /* solvent-solvent (Engine.cu:191-205, 256-275): the pair is tested from
        the lower id, with the same float expression as the add loop. */
-    for (int i = 0; i < n_s; i++) {
+    for (int i = 0; i < n_s && ss_cap > 0; i++) {   /* ss_cap == 0: caller uses orc_ref_nlist_ss_cells */
         for (int j = i + 1; j < n_s; j++) {
             if (within(&sols[i].pos, &sols[j].pos, C, C, L, Lh)) {
                 if (ss_cnt[i] >= ss_cap || ss_cnt[j] >= ss_cap) { rc = -1; continue; }
@@ -359,9 +359,9 @@ int orc_ref_step(float L, float C, double dt, float lambda, const lima_forcefiel
     /* compoundKernel reads compound_state_array (current); keep a copy so
        the per-compound updates below read pre-step positions. */
     lima_compound_state* cur = (lima_compound_state*)malloc(sizeof(lima_compound_state) * (n_c > 0 ? n_c : 1));
-    if (n_c) memcpy(cur, states, sizeof(lima_compound_state) * n_c);
+    if (n_c > 0) memcpy(cur, states, sizeof(lima_compound_state) * (size_t)n_c);
     lima_solvent* scur = (lima_solvent*)malloc(sizeof(lima_solvent) * (n_s > 0 ? n_s : 1));
-    if (n_s) memcpy(scur, sols, sizeof(lima_solvent) * n_s);
+    if (n_s > 0) memcpy(scur, sols, sizeof(lima_solvent) * (size_t)n_s);
 
     /* --- compoundKernel (Engine.cu:880-1057) --- */
     for (int c = 0; c < n_c; c++) {

@@ -1,0 +1,826 @@
+// Host engine and C-ABI (include/lima_abi.h) of the B200 LIMA_MD step path.
+//
+// Replaces the reference's Engine (Quantom/Quantom/Engine.cuh:109-208,
+// Engine.cu:9-451) and the Box set-up it relies on
+// (BoxBuilder::finishBox, BoxBuilder.cu:73-145):
+//   * no managed memory: the box is uploaded once into device buffers laid
+//     out for coalesced access (refdev.cuh / physdev.cuh);
+//   * the per-step host work of Engine::hostMaster (neighbour lists on a
+//     detached std::thread every 200 steps, thermostat every 40) runs on the
+//     device in stream order, so lima_step never synchronises with the host;
+//   * a plain step is captured once into a CUDA graph per buffer parity and
+//     replayed;
+//   * errors come back as status codes, never exit() (Engine.cuh:47-55,
+//     Bodies.cuh:243).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "lima_abi.h"
+#include "physdev.cuh"
+#include "refdev.cuh"
+
+namespace {
+
+struct LimaFail {
+    lima_status st;
+    std::string msg;
+};
+
+[[noreturn]] void fail(lima_status st, const std::string& msg) { throw LimaFail{st, msg}; }
+
+void cuda_ok(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) fail(LIMA_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+}  // namespace
+
+struct lima_ctx {
+    lima_params p{};
+    std::string err;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    // host copies of the box (the caller keeps its own arrays)
+    lima_forcefield ff{};
+    bool ff_set = false;
+    std::vector<lima_compound> comps;
+    std::vector<lima_compound_state> states;
+    std::vector<lima_compound_bridge_compact> bridges;
+    std::vector<lima_solvent> sols;
+    bool finished = false;
+    uint64_t step = 0;
+    uint64_t last_nlist_step = 0;
+    int cur = 0;
+    int n_particles_total = 0;
+    std::vector<void*> dallocs;
+    lima::RefDev ref{};
+    lima::PhysDev phys{};
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool timed = false;
+    bool lambda_pending_reset = false;
+    float ref_temperature = 0.f;
+
+    template <typename T>
+    T* dalloc(size_t n) {
+        void* ptr = nullptr;
+        cuda_ok(cudaMalloc(&ptr, std::max<size_t>(n, 1) * sizeof(T)), "cudaMalloc");
+        dallocs.push_back(ptr);
+        return static_cast<T*>(ptr);
+    }
+    ~lima_ctx() {
+        for (auto& g : graph)
+            if (g) cudaGraphExecDestroy(g);
+        for (void* ptr : dallocs) cudaFree(ptr);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (own_stream && stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+template <typename F>
+lima_status guarded(lima_ctx* c, F&& f) {
+    if (!c) return LIMA_ERR_ARGUMENT;
+    try {
+        f();
+        return LIMA_OK;
+    } catch (const LimaFail& e) {
+        c->err = e.msg;
+        return e.st;
+    } catch (const std::exception& e) {
+        c->err = e.what();
+        return LIMA_ERR_ARGUMENT;
+    }
+}
+
+void need(bool cond, lima_status st, const std::string& msg) {
+    if (!cond) fail(st, msg);
+}
+
+float4 f4(const lima_float3& v) { return make_float4(v.x, v.y, v.z, 0.f); }
+
+// ---------------------------------------------------------------------------
+// validation of the reference layout the caller hands over
+void validate_box(lima_ctx* c) {
+    need(c->ff_set, LIMA_ERR_STATE, "lima_set_forcefield must come before lima_finish_box");
+    const int nc = static_cast<int>(c->comps.size());
+    need(nc <= LIMA_MAX_COMPOUNDS, LIMA_ERR_ARGUMENT, "more than 255 compounds (LJ_Ignores stores uint8 compound ids)");
+    for (int i = 0; i < nc; i++) {
+        const lima_compound& cp = c->comps[i];
+        const int n = cp.n_particles;
+        need(n >= 1 && n <= LIMA_MAX_COMPOUND_PARTICLES, LIMA_ERR_ARGUMENT, "compound n_particles outside 1..64");
+        need(c->states[i].n_particles == cp.n_particles, LIMA_ERR_ARGUMENT, "CompoundState.n_particles != Compound.n_particles");
+        need(cp.n_singlebonds <= LIMA_MAX_PAIRBONDS && cp.n_anglebonds <= LIMA_MAX_ANGLEBONDS &&
+                 cp.n_dihedrals <= LIMA_MAX_DIHEDRALS,
+             LIMA_ERR_ARGUMENT, "bonded term count beyond the Compound capacity");
+        need(cp.key_particle_index >= 0 && cp.key_particle_index < n, LIMA_ERR_ARGUMENT, "key_particle_index out of range");
+        for (int t = 0; t < n; t++) {
+            need(cp.atom_types[t] < LIMA_MAX_ATOM_TYPES, LIMA_ERR_ARGUMENT, "atom type >= 32");
+            need(cp.lj_ignore_list[t].n_ignores <= LIMA_LJ_IGNORES_MAX, LIMA_ERR_ARGUMENT, "LJ_Ignores.n_ignores > 32");
+        }
+        for (int b = 0; b < cp.n_singlebonds; b++)
+            for (int k = 0; k < 2; k++) need(cp.singlebonds[b].atom_indexes[k] < (uint32_t)n, LIMA_ERR_ARGUMENT, "bond atom index out of range");
+        for (int b = 0; b < cp.n_anglebonds; b++)
+            for (int k = 0; k < 3; k++) need(cp.anglebonds[b].atom_indexes[k] < (uint32_t)n, LIMA_ERR_ARGUMENT, "angle atom index out of range");
+        for (int b = 0; b < cp.n_dihedrals; b++)
+            for (int k = 0; k < 4; k++) need(cp.dihedrals[b].atom_indexes[k] < (uint32_t)n, LIMA_ERR_ARGUMENT, "dihedral atom index out of range");
+    }
+    for (const auto& br : c->bridges) {
+        need(br.n_particles >= 0 && br.n_particles <= LIMA_MAX_PARTICLES_IN_BRIDGE, LIMA_ERR_ARGUMENT, "bridge n_particles outside 0..32");
+        need(br.n_singlebonds <= LIMA_MAX_SINGLEBONDS_IN_BRIDGE && br.n_anglebonds <= LIMA_MAX_ANGLEBONDS_IN_BRIDGE &&
+                 br.n_dihedrals <= LIMA_MAX_DIHEDRALBONDS_IN_BRIDGE,
+             LIMA_ERR_ARGUMENT, "bridge term count beyond capacity");
+        for (int t = 0; t < br.n_particles; t++) {
+            const auto& r = br.particle_refs[t];
+            need(r.compound_id >= 0 && r.compound_id < nc, LIMA_ERR_ARGUMENT, "bridge compound id out of range");
+            need(r.local_id_compound >= 0 && r.local_id_compound < c->comps[r.compound_id].n_particles,
+                 LIMA_ERR_ARGUMENT, "bridge local id out of range");
+        }
+        for (int b = 0; b < br.n_singlebonds; b++)
+            for (int k = 0; k < 2; k++) need(br.singlebonds[b].atom_indexes[k] < (uint32_t)br.n_particles, LIMA_ERR_ARGUMENT, "bridge bond index out of range");
+        for (int b = 0; b < br.n_anglebonds; b++)
+            for (int k = 0; k < 3; k++) need(br.anglebonds[b].atom_indexes[k] < (uint32_t)br.n_particles, LIMA_ERR_ARGUMENT, "bridge angle index out of range");
+        for (int b = 0; b < br.n_dihedrals; b++)
+            for (int k = 0; k < 4; k++) need(br.dihedrals[b].atom_indexes[k] < (uint32_t)br.n_particles, LIMA_ERR_ARGUMENT, "bridge dihedral index out of range");
+    }
+    for (const auto& s : c->sols) {
+        const float L = c->p.box_len;
+        need(s.pos.x >= 0.f && s.pos.x <= L && s.pos.y >= 0.f && s.pos.y <= L && s.pos.z >= 0.f && s.pos.z <= L,
+             LIMA_ERR_ARGUMENT, "solvent position outside [0, box_len]");
+    }
+}
+
+// ---------------------------------------------------------------------------
+// reference semantics
+void ref_setup(lima_ctx* c) {
+    lima::RefDev& d = c->ref;
+    const int nc = static_cast<int>(c->comps.size()), ns = static_cast<int>(c->sols.size());
+    const int nb = static_cast<int>(c->bridges.size());
+    d.n_c = nc;
+    d.n_s = ns;
+    d.n_b = nb;
+    d.L = c->p.box_len;
+    d.Lh = c->p.box_len / 2.f;
+    d.C = c->p.ref_cutoff > 0.f ? c->p.ref_cutoff : c->p.cutoff / 2.f;
+    d.dt = c->p.dt;
+    cudaStream_t s = c->stream;
+    auto up = [&](void* dst, const void* src, size_t bytes) {
+        if (bytes) cuda_ok(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s), "upload");
+    };
+    lima_compound* dcomps = c->dalloc<lima_compound>(nc);
+    up(dcomps, c->comps.data(), sizeof(lima_compound) * nc);
+    d.comps = dcomps;
+    lima_compound_bridge_compact* dbr = c->dalloc<lima_compound_bridge_compact>(nb);
+    up(dbr, c->bridges.data(), sizeof(lima_compound_bridge_compact) * nb);
+    d.bridges = dbr;
+    lima_particle_parameters* dpp = c->dalloc<lima_particle_parameters>(LIMA_MAX_ATOM_TYPES);
+    up(dpp, c->ff.particle_parameters, sizeof(lima_forcefield));
+    d.pp = dpp;
+
+    const size_t ncp = static_cast<size_t>(nc) * lima::kMaxCP;
+    std::vector<float4> hpos(ncp, make_float4(0, 0, 0, 0)), hprev(ncp, make_float4(0, 0, 0, 0)),
+        hbr(ncp, make_float4(0, 0, 0, 0));
+    for (int i = 0; i < nc; i++)
+        for (int t = 0; t < c->comps[i].n_particles; t++) {
+            hpos[i * lima::kMaxCP + t] = f4(c->states[i].positions[t]);
+            hprev[i * lima::kMaxCP + t] = f4(c->comps[i].prev_positions[t]);
+            hbr[i * lima::kMaxCP + t] = f4(c->comps[i].forces[t]);
+        }
+    for (int b = 0; b < 2; b++) {
+        d.cpos[b] = c->dalloc<float4>(ncp);
+        up(d.cpos[b], hpos.data(), sizeof(float4) * ncp);
+    }
+    d.cprev = c->dalloc<float4>(ncp);
+    up(d.cprev, hprev.data(), sizeof(float4) * ncp);
+    d.cbridge = c->dalloc<float4>(ncp);
+    up(d.cbridge, hbr.data(), sizeof(float4) * ncp);
+    std::vector<float4> sp(ns), spr(ns);
+    for (int i = 0; i < ns; i++) {
+        sp[i] = f4(c->sols[i].pos);
+        spr[i] = f4(c->sols[i].pos_tsub1);
+    }
+    for (int b = 0; b < 2; b++) {
+        d.spos[b] = c->dalloc<float4>(ns);
+        d.sprev[b] = c->dalloc<float4>(ns);
+        up(d.spos[b], sp.data(), sizeof(float4) * ns);
+        up(d.sprev[b], spr.data(), sizeof(float4) * ns);
+    }
+    d.ss_cap = c->p.solvent_list_capacity;
+    d.cs_cap = c->p.compound_list_capacity;
+    d.ss_ids = c->dalloc<uint32_t>(static_cast<size_t>(ns) * d.ss_cap);
+    d.ss_cnt = c->dalloc<uint32_t>(ns);
+    d.cs_ids = c->dalloc<uint32_t>(static_cast<size_t>(nc) * d.cs_cap);
+    d.cs_cnt = c->dalloc<uint32_t>(nc);
+    d.cc_ids = c->dalloc<uint32_t>(ncp);
+    d.cc_cnt = c->dalloc<uint32_t>(nc);
+    d.cc_prev = c->dalloc<uint8_t>(static_cast<size_t>(nc) * nc);
+    cuda_ok(cudaMemsetAsync(d.ss_cnt, 0, sizeof(uint32_t) * std::max(ns, 1), s), "memset");
+    cuda_ok(cudaMemsetAsync(d.cs_cnt, 0, sizeof(uint32_t) * std::max(nc, 1), s), "memset");
+    cuda_ok(cudaMemsetAsync(d.cc_cnt, 0, sizeof(uint32_t) * std::max(nc, 1), s), "memset");
+    cuda_ok(cudaMemsetAsync(d.cc_prev, 0, std::max<size_t>(1, static_cast<size_t>(nc) * nc), s), "memset");
+    const float radius = d.C + d.C;
+    int m = static_cast<int>(std::floor(d.L / (radius * 1.0001f)));
+    if (m < 3) m = 1;
+    while (m > 1 && d.L / static_cast<float>(m) < radius) m--;
+    if (m < 3) m = 1;
+    d.m = m;
+    d.cell = d.L / static_cast<float>(m);
+    const size_t ncell = static_cast<size_t>(m) * m * m;
+    d.cell_count = c->dalloc<uint32_t>(ncell);
+    d.cell_start = c->dalloc<uint32_t>(ncell);
+    d.cell_fill = c->dalloc<uint32_t>(ncell);
+    d.cell_items = c->dalloc<uint32_t>(ns);
+    d.sol_cell = c->dalloc<uint32_t>(ns);
+    d.n_chunks = (d.cs_cap + lima::kCsChunk - 1) / lima::kCsChunk;
+    d.cs_partial = c->dalloc<float4>(static_cast<size_t>(nc) * d.n_chunks * lima::kMaxCP);
+    d.force_c = c->dalloc<float4>(ncp);
+    d.force_s = c->dalloc<float4>(ns);
+    d.potE = c->dalloc<double>(ncp);
+    cuda_ok(cudaMemsetAsync(d.force_c, 0, sizeof(float4) * std::max<size_t>(ncp, 1), s), "memset");
+    cuda_ok(cudaMemsetAsync(d.force_s, 0, sizeof(float4) * std::max(ns, 1), s), "memset");
+    cuda_ok(cudaMemsetAsync(d.potE, 0, sizeof(double) * std::max<size_t>(ncp, 1), s), "memset");
+    d.lambda = c->dalloc<float>(1);
+    lima::set_device_float(d.lambda, 1.f, s);
+    d.err = c->dalloc<int>(1);
+    cuda_ok(cudaMemsetAsync(d.err, 0, sizeof(int), s), "memset");
+    d.csnap = c->dalloc<float4>(ncp);
+    d.ssnap = c->dalloc<float4>(ns);
+    d.ke_accum = c->dalloc<double>(1);
+    c->n_particles_total = ns;
+    for (const auto& cp : c->comps) c->n_particles_total += cp.n_particles;
+}
+
+void capture_graphs(lima_ctx* c, void (*launch)(lima_ctx*, int)) {
+    for (int parity = 0; parity < 2; parity++) {
+        cudaGraph_t g = nullptr;
+        if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+        launch(c, parity);
+        if (cudaStreamEndCapture(c->stream, &g) != cudaSuccess || !g) {
+            cudaGetLastError();
+            return;
+        }
+        if (cudaGraphInstantiate(&c->graph[parity], g, 0) != cudaSuccess) {
+            cudaGetLastError();
+            c->graph[parity] = nullptr;
+        }
+        cudaGraphDestroy(g);
+    }
+}
+
+void ref_launch_step(lima_ctx* c, int parity) { lima::ref_step_kernels(c->ref, parity, c->stream); }
+void phys_launch_step(lima_ctx* c, int parity) { lima::phys_step_kernels(c->phys, parity, c->stream); }
+
+void check_device_errors(lima_ctx* c) {
+    int* err_ptr = c->p.semantics == LIMA_SEMANTICS_REFERENCE ? c->ref.err : c->phys.err;
+    int h = 0;
+    cuda_ok(cudaMemcpyAsync(&h, err_ptr, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "read error flags");
+    cuda_ok(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+    if (h) {
+        cuda_ok(cudaMemsetAsync(err_ptr, 0, sizeof(int), c->stream), "memset");
+        cuda_ok(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+        std::string m;
+        if (h & lima::ERR_BIT_SS_OVERFLOW) m += "solvent-solvent list overflow; ";
+        if (h & lima::ERR_BIT_CS_OVERFLOW) m += "compound-solvent list overflow; ";
+        if (h & lima::ERR_BIT_CC_OVERFLOW) m += "compound-compound list overflow; ";
+        if (h & lima::ERR_BIT_PHYS_LIST_OVERFLOW) m += "pair list overflow; ";
+        if (h & lima::ERR_BIT_NAN) m += "NaN position; ";
+        if (h & lima::ERR_BIT_CRITICAL_FORCE) m += "critical force (|F| > 2e12); ";
+        const bool cap = h & (lima::ERR_BIT_SS_OVERFLOW | lima::ERR_BIT_CS_OVERFLOW | lima::ERR_BIT_CC_OVERFLOW |
+                              lima::ERR_BIT_PHYS_LIST_OVERFLOW);
+        fail(cap ? LIMA_ERR_CAPACITY : LIMA_ERR_NUMERIC, m);
+    }
+}
+
+void sync_checked(lima_ctx* c) {
+    cuda_ok(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+    cuda_ok(cudaGetLastError(), "kernel launch");
+    check_device_errors(c);
+}
+
+void ref_nlist_now(lima_ctx* c) {
+    lima::ref_build_nlists(c->ref, c->cur, c->stream);
+    c->last_nlist_step = c->step;
+}
+
+void ref_one_step(lima_ctx* c) {
+    lima::RefDev& d = c->ref;
+    const int period = std::max(1, c->p.nlist_period);
+    if (c->step > 0 && c->step - c->last_nlist_step >= static_cast<uint64_t>(period)) ref_nlist_now(c);
+    if (c->graph[c->cur])
+        cuda_ok(cudaGraphLaunch(c->graph[c->cur], c->stream), "cudaGraphLaunch");
+    else
+        ref_launch_step(c, c->cur);
+    c->cur ^= 1;
+    c->step++;
+    if (c->lambda_pending_reset) {
+        lima::set_device_float(d.lambda, 1.f, c->stream);
+        c->lambda_pending_reset = false;
+    }
+    if (c->p.thermostat == LIMA_THERMOSTAT_REFERENCE) {
+        const int tp = std::max(3, c->p.thermostat_period);
+        const uint64_t k = c->step % tp;
+        if (k == static_cast<uint64_t>(tp - 2)) lima::ref_thermostat_snapshot(d, c->cur, c->stream);
+        if (k == 0 && c->step >= 2) {
+            lima::ref_thermostat_update(d, c->cur, c->n_particles_total, static_cast<float>(c->p.t_target),
+                                        c->step > 20, c->stream);
+            c->lambda_pending_reset = true;   // applied for one step (Engine.cu:67-69)
+        }
+    }
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+void lima_default_params(lima_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->box_len = 7.f;
+    p->cutoff = 1.4f;
+    p->ref_cutoff = 0.f;
+    p->skin = 0.1f;
+    p->switch_on = 1.0f;
+    p->dt = 1e-7;
+    p->nlist_period = 200;
+    p->semantics = LIMA_SEMANTICS_REFERENCE;
+    p->precision = LIMA_PRECISION_FP32;
+    p->thermostat = LIMA_THERMOSTAT_NONE;
+    p->t_target = 310.0;
+    p->tau_t = 1e-4;
+    p->thermostat_period = 40;
+    p->energy_period = 0;
+    p->solvent_list_capacity = 512;
+    p->compound_list_capacity = 8192;
+    p->device = 0;
+    p->stream = nullptr;
+}
+
+lima_status lima_create(const lima_params* params, lima_ctx** out) {
+    if (!params || !out) return LIMA_ERR_ARGUMENT;
+    *out = nullptr;
+    auto* c = new lima_ctx();
+    c->p = *params;
+    lima_status st = guarded(c, [&] {
+        const lima_params& p = c->p;
+        need(p.box_len > 0.f, LIMA_ERR_ARGUMENT, "box_len must be positive");
+        need(p.dt > 0.0, LIMA_ERR_ARGUMENT, "dt must be positive");
+        need(p.semantics == LIMA_SEMANTICS_REFERENCE || p.semantics == LIMA_SEMANTICS_PHYSICS, LIMA_ERR_ARGUMENT,
+             "unknown semantics");
+        need(p.precision == LIMA_PRECISION_FP32 || p.precision == LIMA_PRECISION_MIXED, LIMA_ERR_ARGUMENT,
+             "unknown precision");
+        need(p.thermostat >= 0 && p.thermostat <= 2, LIMA_ERR_ARGUMENT, "unknown thermostat");
+        need(p.solvent_list_capacity >= 32 && p.solvent_list_capacity <= 2048, LIMA_ERR_ARGUMENT,
+             "solvent_list_capacity outside 32..2048");
+        need(p.compound_list_capacity >= 64 && p.compound_list_capacity <= (1 << 20), LIMA_ERR_ARGUMENT,
+             "compound_list_capacity outside 64..2^20");
+        need(p.cutoff > 0.f || p.ref_cutoff > 0.f, LIMA_ERR_ARGUMENT, "cutoff must be positive");
+        if (p.semantics == LIMA_SEMANTICS_PHYSICS) {
+            need(p.cutoff > 0.f && p.skin >= 0.f && 2.f * (p.cutoff + p.skin) <= p.box_len, LIMA_ERR_ARGUMENT,
+                 "physics semantics needs 2*(cutoff+skin) <= box_len");
+        }
+        int ndev = 0;
+        cuda_ok(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+        need(p.device >= 0 && p.device < ndev, LIMA_ERR_ARGUMENT, "no such CUDA device");
+        cuda_ok(cudaSetDevice(p.device), "cudaSetDevice");
+        if (p.stream) {
+            c->stream = static_cast<cudaStream_t>(p.stream);
+        } else {
+            cuda_ok(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+            c->own_stream = true;
+        }
+        cuda_ok(cudaEventCreate(&c->ev0), "cudaEventCreate");
+        cuda_ok(cudaEventCreate(&c->ev1), "cudaEventCreate");
+    });
+    if (st != LIMA_OK) {
+        fprintf(stderr, "lima_create: %s\n", c->err.c_str());
+        delete c;
+        return st;
+    }
+    *out = c;
+    return LIMA_OK;
+}
+
+void lima_destroy(lima_ctx* ctx) {
+    if (!ctx) return;
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    delete ctx;
+}
+
+const char* lima_last_error(const lima_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+lima_status lima_set_forcefield(lima_ctx* c, const lima_forcefield* ff) {
+    return guarded(c, [&] {
+        need(ff != nullptr, LIMA_ERR_ARGUMENT, "null forcefield");
+        need(!c->finished, LIMA_ERR_STATE, "box already finished");
+        c->ff = *ff;
+        c->ff_set = true;
+    });
+}
+
+lima_status lima_load_compounds(lima_ctx* c, const lima_compound* compounds, const lima_compound_state* states,
+                                int n) {
+    return guarded(c, [&] {
+        need(!c->finished, LIMA_ERR_STATE, "box already finished");
+        need(n >= 0 && n <= LIMA_MAX_COMPOUNDS, LIMA_ERR_ARGUMENT, "n_compounds outside 0..255");
+        need(n == 0 || (compounds && states), LIMA_ERR_ARGUMENT, "null compound arrays");
+        c->comps.assign(compounds, compounds + n);
+        c->states.assign(states, states + n);
+    });
+}
+
+lima_status lima_load_bridges(lima_ctx* c, const lima_compound_bridge_compact* bridges, int n) {
+    return guarded(c, [&] {
+        need(!c->finished, LIMA_ERR_STATE, "box already finished");
+        need(n >= 0 && n <= 4 * LIMA_MAX_COMPOUNDS, LIMA_ERR_ARGUMENT, "n_bridges out of range");
+        need(n == 0 || bridges, LIMA_ERR_ARGUMENT, "null bridge array");
+        c->bridges.assign(bridges, bridges + n);
+    });
+}
+
+lima_status lima_load_solvents(lima_ctx* c, const lima_solvent* solvents, uint32_t n) {
+    return guarded(c, [&] {
+        need(!c->finished, LIMA_ERR_STATE, "box already finished");
+        need(n == 0 || solvents, LIMA_ERR_ARGUMENT, "null solvent array");
+        need(n <= (1u << 26), LIMA_ERR_ARGUMENT, "more than 2^26 solvents");
+        c->sols.assign(solvents, solvents + n);
+    });
+}
+
+lima_status lima_finish_box(lima_ctx* c) {
+    return guarded(c, [&] {
+        need(!c->finished, LIMA_ERR_STATE, "box already finished");
+        validate_box(c);
+        cuda_ok(cudaSetDevice(c->p.device), "cudaSetDevice");
+        if (c->p.semantics == LIMA_SEMANTICS_REFERENCE) {
+            ref_setup(c);
+            ref_nlist_now(c);
+            sync_checked(c);
+            capture_graphs(c, ref_launch_step);
+        } else {
+            lima::PhysHost h;
+            h.params = &c->p;
+            h.ff = &c->ff;
+            h.comps = c->comps.data();
+            h.states = c->states.data();
+            h.n_c = static_cast<int>(c->comps.size());
+            h.bridges = c->bridges.data();
+            h.n_b = static_cast<int>(c->bridges.size());
+            h.sols = c->sols.data();
+            h.n_s = static_cast<int>(c->sols.size());
+            std::string msg;
+            const int rc = lima::phys_setup(h, c->phys, c->stream, c->dallocs, msg);
+            if (rc != 0) fail(static_cast<lima_status>(rc), msg);
+            lima::phys_rebuild(c->phys, c->cur, c->stream);
+            lima::phys_prime(c->phys, c->cur, c->stream);
+            sync_checked(c);
+            capture_graphs(c, phys_launch_step);
+            c->n_particles_total = c->phys.n;
+        }
+        sync_checked(c);
+        c->finished = true;
+    });
+}
+
+lima_status lima_step(lima_ctx* c, int n_steps) {
+    return guarded(c, [&] {
+        need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
+        need(n_steps >= 0, LIMA_ERR_ARGUMENT, "negative step count");
+        cuda_ok(cudaEventRecord(c->ev0, c->stream), "cudaEventRecord");
+        for (int i = 0; i < n_steps; i++) {
+            if (c->p.semantics == LIMA_SEMANTICS_REFERENCE) {
+                ref_one_step(c);
+            } else {
+                const int period = std::max(1, c->p.nlist_period);
+                if (c->step > 0 && c->step - c->last_nlist_step >= static_cast<uint64_t>(period)) {
+                    lima::phys_rebuild(c->phys, c->cur, c->stream);
+                    c->last_nlist_step = c->step;
+                }
+                const bool energy = c->p.energy_period > 0 && (c->step % c->p.energy_period) == 0;
+                if (energy || !c->graph[c->cur]) {
+                    lima::phys_step_kernels(c->phys, c->cur, c->stream, energy);
+                } else {
+                    cuda_ok(cudaGraphLaunch(c->graph[c->cur], c->stream), "cudaGraphLaunch");
+                }
+                c->cur ^= 1;
+                c->step++;
+            }
+        }
+        cuda_ok(cudaEventRecord(c->ev1, c->stream), "cudaEventRecord");
+        cuda_ok(cudaGetLastError(), "kernel launch");
+        c->timed = true;
+    });
+}
+
+lima_status lima_synchronize(lima_ctx* c) {
+    return guarded(c, [&] { sync_checked(c); });
+}
+
+lima_status lima_get_step(lima_ctx* c, uint64_t* step) {
+    return guarded(c, [&] {
+        need(step != nullptr, LIMA_ERR_ARGUMENT, "null step");
+        *step = c->step;
+    });
+}
+
+lima_status lima_get_last_step_ms(lima_ctx* c, float* ms) {
+    return guarded(c, [&] {
+        need(ms != nullptr, LIMA_ERR_ARGUMENT, "null ms");
+        need(c->timed, LIMA_ERR_STATE, "no lima_step has run");
+        cuda_ok(cudaEventSynchronize(c->ev1), "cudaEventSynchronize");
+        cuda_ok(cudaEventElapsedTime(ms, c->ev0, c->ev1), "cudaEventElapsedTime");
+    });
+}
+
+lima_status lima_set_thermostat_scalar(lima_ctx* c, float scalar) {
+    return guarded(c, [&] {
+        need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
+        need(c->p.semantics == LIMA_SEMANTICS_REFERENCE, LIMA_ERR_UNSUPPORTED,
+             "the thermostat scalar belongs to reference semantics");
+        need(std::isfinite(scalar) && scalar > 0.f, LIMA_ERR_ARGUMENT, "thermostat scalar must be finite and positive");
+        lima::set_device_float(c->ref.lambda, scalar, c->stream);
+        c->lambda_pending_reset = true;
+    });
+}
+
+lima_status lima_get_compound_states(lima_ctx* c, lima_compound_state* states, lima_float3* prev) {
+    return guarded(c, [&] {
+        need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
+        sync_checked(c);
+        const int nc = static_cast<int>(c->comps.size());
+        const size_t ncp = static_cast<size_t>(nc) * lima::kMaxCP;
+        std::vector<float4> hp(ncp), hq(ncp);
+        if (c->p.semantics == LIMA_SEMANTICS_REFERENCE) {
+            cuda_ok(cudaMemcpy(hp.data(), c->ref.cpos[c->cur], sizeof(float4) * ncp, cudaMemcpyDeviceToHost), "D2H");
+            cuda_ok(cudaMemcpy(hq.data(), c->ref.cprev, sizeof(float4) * ncp, cudaMemcpyDeviceToHost), "D2H");
+        } else {
+            lima::phys_read_compounds(c->phys, c->cur, c->comps.data(), hp.data(), hq.data());
+        }
+        for (int i = 0; i < nc; i++) {
+            if (states) {
+                std::memset(&states[i], 0, sizeof(lima_compound_state));
+                states[i].n_particles = c->comps[i].n_particles;
+            }
+            for (int t = 0; t < c->comps[i].n_particles; t++) {
+                const float4 a = hp[i * lima::kMaxCP + t], b = hq[i * lima::kMaxCP + t];
+                if (states) states[i].positions[t] = lima_float3{a.x, a.y, a.z};
+                if (prev) prev[i * lima::kMaxCP + t] = lima_float3{b.x, b.y, b.z};
+            }
+        }
+    });
+}
+
+lima_status lima_get_solvents(lima_ctx* c, lima_solvent* sols) {
+    return guarded(c, [&] {
+        need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
+        need(sols != nullptr || c->sols.empty(), LIMA_ERR_ARGUMENT, "null solvent array");
+        sync_checked(c);
+        const int ns = static_cast<int>(c->sols.size());
+        std::vector<float4> a(ns), b(ns);
+        if (c->p.semantics == LIMA_SEMANTICS_REFERENCE) {
+            cuda_ok(cudaMemcpy(a.data(), c->ref.spos[c->cur], sizeof(float4) * ns, cudaMemcpyDeviceToHost), "D2H");
+            cuda_ok(cudaMemcpy(b.data(), c->ref.sprev[c->cur], sizeof(float4) * ns, cudaMemcpyDeviceToHost), "D2H");
+        } else {
+            lima::phys_read_solvents(c->phys, c->cur, a.data(), b.data());
+        }
+        for (int i = 0; i < ns; i++) {
+            sols[i].pos = lima_float3{a[i].x, a[i].y, a[i].z};
+            sols[i].pos_tsub1 = lima_float3{b[i].x, b[i].y, b[i].z};
+        }
+    });
+}
+
+lima_status lima_set_state(lima_ctx* c, const lima_compound_state* states, const lima_float3* prev,
+                           const lima_solvent* sols) {
+    return guarded(c, [&] {
+        need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
+        sync_checked(c);
+        const int nc = static_cast<int>(c->comps.size()), ns = static_cast<int>(c->sols.size());
+        for (int i = 0; i < nc; i++) {
+            if (states) c->states[i] = states[i];
+            if (prev)
+                for (int t = 0; t < c->comps[i].n_particles; t++) c->comps[i].prev_positions[t] = prev[i * lima::kMaxCP + t];
+        }
+        if (sols) std::memcpy(c->sols.data(), sols, sizeof(lima_solvent) * ns);
+        if (c->p.semantics == LIMA_SEMANTICS_REFERENCE) {
+            const size_t ncp = static_cast<size_t>(nc) * lima::kMaxCP;
+            std::vector<float4> hp(ncp, make_float4(0, 0, 0, 0)), hq(ncp, make_float4(0, 0, 0, 0));
+            for (int i = 0; i < nc; i++)
+                for (int t = 0; t < c->comps[i].n_particles; t++) {
+                    hp[i * lima::kMaxCP + t] = f4(c->states[i].positions[t]);
+                    hq[i * lima::kMaxCP + t] = f4(c->comps[i].prev_positions[t]);
+                }
+            std::vector<float4> sp(ns), spr(ns);
+            for (int i = 0; i < ns; i++) {
+                sp[i] = f4(c->sols[i].pos);
+                spr[i] = f4(c->sols[i].pos_tsub1);
+            }
+            cuda_ok(cudaMemcpy(c->ref.cpos[c->cur], hp.data(), sizeof(float4) * ncp, cudaMemcpyHostToDevice), "H2D");
+            cuda_ok(cudaMemcpy(c->ref.cprev, hq.data(), sizeof(float4) * ncp, cudaMemcpyHostToDevice), "H2D");
+            cuda_ok(cudaMemcpy(c->ref.spos[c->cur], sp.data(), sizeof(float4) * ns, cudaMemcpyHostToDevice), "H2D");
+            cuda_ok(cudaMemcpy(c->ref.sprev[c->cur], spr.data(), sizeof(float4) * ns, cudaMemcpyHostToDevice), "H2D");
+        } else {
+            lima::PhysHost h;
+            h.params = &c->p;
+            h.ff = &c->ff;
+            h.comps = c->comps.data();
+            h.states = c->states.data();
+            h.n_c = nc;
+            h.bridges = c->bridges.data();
+            h.n_b = static_cast<int>(c->bridges.size());
+            h.sols = c->sols.data();
+            h.n_s = ns;
+            lima::phys_upload_state(h, c->phys, c->cur, c->stream);
+            lima::phys_rebuild(c->phys, c->cur, c->stream);
+            lima::phys_prime(c->phys, c->cur, c->stream);
+            c->last_nlist_step = c->step;
+        }
+        sync_checked(c);
+    });
+}
+
+lima_status lima_get_forces(lima_ctx* c, lima_float3* fc, lima_float3* fs) {
+    return guarded(c, [&] {
+        need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
+        sync_checked(c);
+        const int nc = static_cast<int>(c->comps.size()), ns = static_cast<int>(c->sols.size());
+        const size_t ncp = static_cast<size_t>(nc) * lima::kMaxCP;
+        std::vector<float4> a(ncp), b(ns);
+        if (c->p.semantics == LIMA_SEMANTICS_REFERENCE) {
+            cuda_ok(cudaMemcpy(a.data(), c->ref.force_c, sizeof(float4) * ncp, cudaMemcpyDeviceToHost), "D2H");
+            cuda_ok(cudaMemcpy(b.data(), c->ref.force_s, sizeof(float4) * ns, cudaMemcpyDeviceToHost), "D2H");
+        } else {
+            lima::phys_read_forces(c->phys, c->comps.data(), a.data(), b.data());
+        }
+        if (fc)
+            for (size_t i = 0; i < ncp; i++) fc[i] = lima_float3{a[i].x, a[i].y, a[i].z};
+        if (fs)
+            for (int i = 0; i < ns; i++) fs[i] = lima_float3{b[i].x, b[i].y, b[i].z};
+    });
+}
+
+lima_status lima_compute_energies(lima_ctx* c) {
+    return guarded(c, [&] {
+        need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
+        need(c->p.semantics == LIMA_SEMANTICS_PHYSICS, LIMA_ERR_UNSUPPORTED,
+             "the reference computes no LJ energy; reference semantics report potE of the last step");
+        lima::phys_energy_now(c->phys, c->cur, c->stream);
+        sync_checked(c);
+    });
+}
+
+lima_status lima_get_energies(lima_ctx* c, double* totals, double* per_particle) {
+    return guarded(c, [&] {
+        need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
+        sync_checked(c);
+        const int nc = static_cast<int>(c->comps.size()), ns = static_cast<int>(c->sols.size());
+        const size_t ncp = static_cast<size_t>(nc) * lima::kMaxCP;
+        if (c->p.semantics == LIMA_SEMANTICS_REFERENCE) {
+            std::vector<double> pe(ncp);
+            cuda_ok(cudaMemcpy(pe.data(), c->ref.potE, sizeof(double) * ncp, cudaMemcpyDeviceToHost), "D2H");
+            if (per_particle) {
+                std::memcpy(per_particle, pe.data(), sizeof(double) * ncp);
+                std::memset(per_particle + ncp, 0, sizeof(double) * ns);
+            }
+            if (totals) {
+                std::memset(totals, 0, sizeof(double) * LIMA_E_COUNT);
+                double sum = 0;
+                for (int i = 0; i < nc; i++)
+                    for (int t = 0; t < lima::kMaxCP; t++) sum += pe[i * lima::kMaxCP + t];
+                totals[LIMA_E_BOND] = sum;   // the reference's bonded potE (its only energy)
+                totals[LIMA_E_TOTAL] = sum;
+                double temp = 0;
+                cuda_ok(cudaMemcpy(&temp, c->ref.ke_accum, sizeof(double), cudaMemcpyDeviceToHost), "D2H");
+                totals[LIMA_E_TEMPERATURE] = temp;
+            }
+        } else {
+            lima::phys_read_energies(c->phys, totals, per_particle, c->comps.data(), nc, ns);
+        }
+    });
+}
+
+lima_status lima_build_nlist(lima_ctx* c) {
+    return guarded(c, [&] {
+        need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
+        if (c->p.semantics == LIMA_SEMANTICS_REFERENCE) {
+            ref_nlist_now(c);
+        } else {
+            lima::phys_rebuild(c->phys, c->cur, c->stream);
+            c->last_nlist_step = c->step;
+        }
+        sync_checked(c);
+    });
+}
+
+lima_status lima_get_nlist(lima_ctx* c, int which, uint32_t* offsets, uint32_t* ids, uint32_t* total) {
+    return guarded(c, [&] {
+        need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
+        need(c->p.semantics == LIMA_SEMANTICS_REFERENCE, LIMA_ERR_UNSUPPORTED,
+             "entity neighbour lists exist in reference semantics; physics uses a cluster-pair list");
+        need(which >= 0 && which <= 3, LIMA_ERR_ARGUMENT, "unknown list selector");
+        need(offsets != nullptr, LIMA_ERR_ARGUMENT, "null offsets");
+        sync_checked(c);
+        const lima::RefDev& d = c->ref;
+        const int nc = d.n_c, ns = d.n_s;
+        std::vector<uint32_t> cnt, rows;
+        auto fetch = [&](const uint32_t* dcnt, const uint32_t* dids, int n, size_t cap, bool colmajor) {
+            cnt.resize(n);
+            rows.resize(static_cast<size_t>(n) * cap);
+            if (n) {
+                cuda_ok(cudaMemcpy(cnt.data(), dcnt, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost), "D2H");
+                cuda_ok(cudaMemcpy(rows.data(), dids, sizeof(uint32_t) * n * cap, cudaMemcpyDeviceToHost), "D2H");
+            }
+            (void)colmajor;
+        };
+        uint32_t pos = 0;
+        if (which == LIMA_NL_COMPOUND_COMPOUND || which == LIMA_NL_COMPOUND_SOLVENT) {
+            const bool cc = which == LIMA_NL_COMPOUND_COMPOUND;
+            const size_t cap = cc ? lima::kMaxCP : d.cs_cap;
+            fetch(cc ? d.cc_cnt : d.cs_cnt, cc ? d.cc_ids : d.cs_ids, nc, cap, false);
+            for (int i = 0; i < nc; i++) {
+                offsets[i] = pos;
+                if (ids)
+                    for (uint32_t k = 0; k < cnt[i]; k++) ids[pos + k] = rows[i * cap + k];
+                pos += cnt[i];
+            }
+            offsets[nc] = pos;
+        } else if (which == LIMA_NL_SOLVENT_SOLVENT) {
+            fetch(d.ss_cnt, d.ss_ids, ns, d.ss_cap, true);
+            for (int i = 0; i < ns; i++) {
+                offsets[i] = pos;
+                if (ids)
+                    for (uint32_t k = 0; k < cnt[i]; k++) ids[pos + k] = rows[static_cast<size_t>(k) * ns + i];
+                pos += cnt[i];
+            }
+            offsets[ns] = pos;
+        } else {   // solvent -> compound: the transpose of compound -> solvent
+            fetch(d.cs_cnt, d.cs_ids, nc, d.cs_cap, false);
+            std::vector<std::vector<uint32_t>> tr(ns);
+            for (int cidx = 0; cidx < nc; cidx++)
+                for (uint32_t k = 0; k < cnt[cidx]; k++) tr[rows[static_cast<size_t>(cidx) * d.cs_cap + k]].push_back(cidx);
+            for (int i = 0; i < ns; i++) {
+                offsets[i] = pos;
+                if (ids)
+                    for (size_t k = 0; k < tr[i].size(); k++) ids[pos + k] = tr[i][k];
+                pos += static_cast<uint32_t>(tr[i].size());
+            }
+            offsets[ns] = pos;
+        }
+        if (total) *total = pos;
+    });
+}
+
+lima_status lima_set_nlist(lima_ctx* c, int which, const uint32_t* offsets, const uint32_t* ids) {
+    return guarded(c, [&] {
+        need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
+        need(c->p.semantics == LIMA_SEMANTICS_REFERENCE, LIMA_ERR_UNSUPPORTED, "lists can be set in reference semantics only");
+        need(offsets != nullptr && ids != nullptr, LIMA_ERR_ARGUMENT, "null list arrays");
+        need(which != LIMA_NL_SOLVENT_COMPOUND, LIMA_ERR_UNSUPPORTED, "solvent->compound lists are derived from compound->solvent");
+        sync_checked(c);
+        lima::RefDev& d = c->ref;
+        const int n = (which == LIMA_NL_SOLVENT_SOLVENT) ? d.n_s : d.n_c;
+        const int idmax = (which == LIMA_NL_COMPOUND_SOLVENT || which == LIMA_NL_SOLVENT_SOLVENT) ? d.n_s : d.n_c;
+        const size_t cap = which == LIMA_NL_COMPOUND_COMPOUND ? lima::kMaxCP
+                                                              : (which == LIMA_NL_COMPOUND_SOLVENT ? d.cs_cap : d.ss_cap);
+        std::vector<uint32_t> cnt(n), rows(static_cast<size_t>(n) * cap, 0);
+        for (int i = 0; i < n; i++) {
+            need(offsets[i + 1] >= offsets[i], LIMA_ERR_ARGUMENT, "offsets not monotone");
+            const uint32_t k = offsets[i + 1] - offsets[i];
+            need(k <= cap, LIMA_ERR_CAPACITY, "list longer than its capacity");
+            cnt[i] = k;
+            for (uint32_t q = 0; q < k; q++) {
+                const uint32_t id = ids[offsets[i] + q];
+                need(id < static_cast<uint32_t>(idmax), LIMA_ERR_ARGUMENT, "list id out of range");
+                if (which == LIMA_NL_SOLVENT_SOLVENT)
+                    rows[static_cast<size_t>(q) * n + i] = id;
+                else
+                    rows[i * cap + q] = id;
+            }
+        }
+        uint32_t* dcnt = which == LIMA_NL_COMPOUND_COMPOUND ? d.cc_cnt : (which == LIMA_NL_COMPOUND_SOLVENT ? d.cs_cnt : d.ss_cnt);
+        uint32_t* dids = which == LIMA_NL_COMPOUND_COMPOUND ? d.cc_ids : (which == LIMA_NL_COMPOUND_SOLVENT ? d.cs_ids : d.ss_ids);
+        if (n) {
+            cuda_ok(cudaMemcpy(dcnt, cnt.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice), "H2D");
+            cuda_ok(cudaMemcpy(dids, rows.data(), sizeof(uint32_t) * rows.size(), cudaMemcpyHostToDevice), "H2D");
+        }
+        if (which == LIMA_NL_COMPOUND_COMPOUND && n) {
+            std::vector<uint8_t> bm(static_cast<size_t>(n) * n, 0);
+            for (int i = 0; i < n; i++)
+                for (uint32_t q = 0; q < cnt[i]; q++) bm[static_cast<size_t>(i) * n + rows[i * cap + q]] = 1;
+            cuda_ok(cudaMemcpy(d.cc_prev, bm.data(), bm.size(), cudaMemcpyHostToDevice), "H2D");
+        }
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,353 @@
+// One step of the reference's own physics on the device (compiled with
+// -fmad=false; float operation order as the reference's device functions).
+//
+// The reference runs three kernels per step with a device sync between each
+// (Engine::step, Quantom/Quantom/Engine.cu:400-451): compoundBridgeKernel
+// (:1168-1223), compoundKernel (:880-1057) and solventForceKernel
+// (:1070-1161).  Its compoundKernel uses one 64-thread block per compound for
+// everything — bonded terms accumulated one thread at a time behind 64
+// __syncthreads per term type, and ~3,000 compound<-solvent pairs per particle
+// — so a 16-compound box keeps 16 of 148 SMs busy.  Here:
+//   k_bridge        one 32-thread block per bridge, as the reference;
+//   k_cs_partial    compound<-solvent LJ split over (compound, 256-neighbour
+//                   chunk) blocks, solvent positions staged in shared memory;
+//   k_compound      bonded terms computed one thread per term into shared
+//                   memory and summed per atom in term order (the order the
+//                   reference's serialised loop produces), intra- and
+//                   inter-compound LJ, the chunk partials, Stormer-Verlet,
+//                   PBC;
+//   k_solvent       one thread per solvent: all compound particles (staged
+//                   16 compounds at a time) + the solvent list, read
+//                   column-major so each warp's list reads coalesce.
+// k_solvent is independent of k_cs_partial/k_compound (both read the current
+// buffers and write the next ones).
+#include "refdev.cuh"
+#include "refmath.cuh"
+
+namespace lima {
+using namespace refm;
+
+namespace {
+
+__device__ __forceinline__ void flag_nan(const RefDev& d, const F3& p) {
+    if (p.x != p.x || p.y != p.y || p.z != p.z) atomicOr(d.err, ERR_BIT_NAN);
+}
+
+// Bonded forces of one entity with per-atom sums in term-index order and
+// per-thread potE over terms t, t+NT, ... (Engine.cu:744-847).
+template <int NT, int MAXB, int MAXA, int MAXD>
+struct BondedScratch {
+    F3 rb[MAXB][2];
+    F3 ra[MAXA][3];
+    F3 rd[MAXD][4];
+};
+
+template <int NT, int MAXB, int MAXA, int MAXD>
+__device__ void bonded_entity(const F3* pos, int nb, const lima_pair_bond* bonds, int na,
+                              const lima_angle_bond* angles, int nd, const lima_dihedral_bond* dihs,
+                              BondedScratch<NT, MAXB, MAXA, MAXD>& sc, F3& force, float& potE) {
+    const int t = threadIdx.x;
+    for (int b = t; b < nb; b += NT) {
+        const lima_pair_bond& pb = bonds[b];
+        pairbond(pos[pb.atom_indexes[0]], pos[pb.atom_indexes[1]], pb.b0, pb.kb, sc.rb[b], potE);
+    }
+    __syncthreads();
+    F3 acc = mk(0.f, 0.f, 0.f);
+    for (int b = 0; b < nb; b++) {
+        if ((int)bonds[b].atom_indexes[0] == t) acc = add(acc, sc.rb[b][0]);
+        if ((int)bonds[b].atom_indexes[1] == t) acc = add(acc, sc.rb[b][1]);
+    }
+    force = add(force, acc);
+    for (int a = t; a < na; a += NT) {
+        const lima_angle_bond& ab = angles[a];
+        anglebond(pos[ab.atom_indexes[0]], pos[ab.atom_indexes[1]], pos[ab.atom_indexes[2]], ab.theta_0, ab.k_theta,
+                  sc.ra[a], potE);
+    }
+    __syncthreads();
+    acc = mk(0.f, 0.f, 0.f);
+    for (int a = 0; a < na; a++)
+        for (int k = 0; k < 3; k++)
+            if ((int)angles[a].atom_indexes[k] == t) acc = add(acc, sc.ra[a][k]);
+    force = add(force, acc);
+    for (int q = t; q < nd; q += NT) {
+        const lima_dihedral_bond& db = dihs[q];
+        dihedral(pos[db.atom_indexes[0]], pos[db.atom_indexes[1]], pos[db.atom_indexes[2]], pos[db.atom_indexes[3]],
+                 db.phi_0, db.k_phi, db.n, sc.rd[q], potE);
+    }
+    __syncthreads();
+    acc = mk(0.f, 0.f, 0.f);
+    for (int q = 0; q < nd; q++)
+        for (int k = 0; k < 4; k++)
+            if ((int)dihs[q].atom_indexes[k] == t) acc = add(acc, sc.rd[q][k]);
+    force = add(force, acc);
+}
+
+__global__ void __launch_bounds__(32) k_bridge(RefDev d, int cur) {
+    __shared__ F3 pos[LIMA_MAX_PARTICLES_IN_BRIDGE];
+    __shared__ BondedScratch<32, LIMA_MAX_SINGLEBONDS_IN_BRIDGE, LIMA_MAX_ANGLEBONDS_IN_BRIDGE,
+                             LIMA_MAX_DIHEDRALBONDS_IN_BRIDGE> sc;
+    const lima_compound_bridge_compact& br = d.bridges[blockIdx.x];
+    const int t = threadIdx.x;
+    const int n = br.n_particles;
+    pos[t] = mk(0.f, 0.f, 0.f);
+    if (t < n) pos[t] = mk4(d.cpos[cur][br.particle_refs[t].compound_id * kMaxCP + br.particle_refs[t].local_id_compound]);
+    __syncthreads();
+    F3 p0 = pos[0];
+    if (t > 0) hyperpos(p0, pos[t], d.L, d.Lh);
+    __syncthreads();
+    F3 force = mk(0.f, 0.f, 0.f);
+    float potE = 0.f;
+    bonded_entity<32>(pos, br.n_singlebonds, br.singlebonds, br.n_anglebonds, br.anglebonds, br.n_dihedrals,
+                      br.dihedrals, sc, force, potE);
+    if (t < n) d.cbridge[br.particle_refs[t].compound_id * kMaxCP + br.particle_refs[t].local_id_compound] = to4(force);
+}
+
+// compound <- solvent LJ over one chunk of the compound's solvent list
+// (computeSolventToCompoundLJForces, Engine.cu:721-730, 965-973).
+__global__ void __launch_bounds__(64) k_cs_partial(RefDev d, int cur) {
+    __shared__ F3 buf[kCsChunk];
+    const int c = blockIdx.y, k = blockIdx.x, t = threadIdx.x;
+    const int cnt = d.cs_cnt[c];
+    const int begin = k * kCsChunk;
+    if (begin >= cnt) return;
+    const int len_ = min(kCsChunk, cnt - begin);
+    const F3 p0 = mk4(d.cpos[cur][c * kMaxCP]);
+    for (int q = t; q < len_; q += 64) {
+        F3 v = mk4(d.spos[cur][d.cs_ids[(size_t)c * d.cs_cap + begin + q]]);
+        hyperpos(p0, v, d.L, d.Lh);
+        buf[q] = v;
+    }
+    __syncthreads();
+    const lima_compound& cp = d.comps[c];
+    if (t >= cp.n_particles) return;
+    F3 pt = mk4(d.cpos[cur][c * kMaxCP + t]);
+    if (t > 0) hyperpos(p0, pt, d.L, d.Lh);
+    const lima_particle_parameters a = d.pp[cp.atom_types[t]];
+    const lima_particle_parameters sol = d.pp[LIMA_ATOMTYPE_SOL];
+    const float sg = mix_sigma(a.sigma, sol.sigma), ep = eps_geo(a.epsilon, sol.epsilon);
+    F3 acc = mk(0.f, 0.f, 0.f);
+    for (int q = 0; q < len_; q++) acc = add(acc, lj_force(pt, buf[q], sg, ep));
+    d.cs_partial[((size_t)c * d.n_chunks + k) * kMaxCP + t] = to4(acc);
+}
+
+__global__ void __launch_bounds__(64) k_compound(RefDev d, int cur) {
+    __shared__ F3 pos[kMaxCP];
+    __shared__ F3 nbuf[kMaxCP];
+    __shared__ BondedScratch<64, LIMA_MAX_PAIRBONDS, LIMA_MAX_ANGLEBONDS, LIMA_MAX_DIHEDRALS> sc;
+    const int c = blockIdx.x, t = threadIdx.x;
+    const lima_compound& cp = d.comps[c];
+    const int n = cp.n_particles;
+    pos[t] = t < n ? mk4(d.cpos[cur][c * kMaxCP + t]) : mk(0.f, 0.f, 0.f);
+    F3 force = mk(0.f, 0.f, 0.f);
+    if (t < n) {   // Compound::loadData takes the bridge forces and zeroes them (Bodies.cuh:437-438)
+        force = mk4(d.cbridge[c * kMaxCP + t]);
+        d.cbridge[c * kMaxCP + t] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    __syncthreads();
+    const F3 p0 = pos[0];
+    if (t > 0 && t < n) hyperpos(p0, pos[t], d.L, d.Lh);
+    __syncthreads();
+    float potE = 0.f;
+    bonded_entity<64>(pos, cp.n_singlebonds, cp.singlebonds, cp.n_anglebonds, cp.anglebonds, cp.n_dihedrals,
+                      cp.dihedrals, sc, force, potE);
+    const lima_particle_parameters a = d.pp[t < n ? cp.atom_types[t] : 0];
+    // computeIntramolecularLJForces (Engine.cu:678-700)
+    if (t < n) {
+        F3 acc = mk(0.f, 0.f, 0.f);
+        for (int i = 0; i < n; i++) {
+            if (i == t || ignored(cp.lj_ignore_list[t], i, c)) continue;
+            const lima_particle_parameters o = d.pp[cp.atom_types[i]];
+            acc = add(acc, lj_force(pos[t], pos[i], mix_sigma(a.sigma, o.sigma), eps_geo(a.epsilon, o.epsilon)));
+        }
+        force = add(force, acc);
+    }
+    // computerIntermolecularLJForces over the compound list (Engine.cu:653-676, 939-958)
+    const int ncc = d.cc_cnt[c];
+    for (int k = 0; k < ncc; k++) {
+        const int nb = d.cc_ids[c * kMaxCP + k];
+        const lima_compound& ncp = d.comps[nb];
+        const int nn = ncp.n_particles;
+        __syncthreads();
+        if (t < nn) {
+            F3 v = mk4(d.cpos[cur][nb * kMaxCP + t]);
+            hyperpos(p0, v, d.L, d.Lh);
+            nbuf[t] = v;
+        }
+        __syncthreads();
+        if (t < n) {
+            F3 acc = mk(0.f, 0.f, 0.f);
+            for (int j = 0; j < nn; j++) {
+                if (ignored(cp.lj_ignore_list[t], j, nb)) continue;
+                const lima_particle_parameters o = d.pp[ncp.atom_types[j]];
+                acc = add(acc, lj_force(pos[t], nbuf[j], mix_sigma(a.sigma, o.sigma), eps_arith(a.epsilon, o.epsilon)));
+            }
+            force = add(force, acc);
+        }
+    }
+    // compound <- solvent partial sums, in chunk order
+    if (t < n) {
+        const int nch = (d.cs_cnt[c] + kCsChunk - 1) / kCsChunk;
+        F3 acc = mk(0.f, 0.f, 0.f);
+        for (int k = 0; k < nch; k++) acc = add(acc, mk4(d.cs_partial[((size_t)c * d.n_chunks + k) * kMaxCP + t]));
+        force = add(force, acc);
+    }
+    __syncthreads();
+    // integratePosition (Engine.cu:981-984)
+    if (t < n) {
+        F3 prev = mk4(d.cprev[c * kMaxCP + t]);
+        integrate(pos[t], prev, force, (double)a.mass, d.dt, *d.lambda, d.L, d.Lh);
+        d.cprev[c * kMaxCP + t] = to4(prev);
+        d.force_c[c * kMaxCP + t] = to4(force);
+        if (len(force) > 2e12f) atomicOr(d.err, ERR_BIT_CRITICAL_FORCE);
+    }
+    __syncthreads();
+    if (t == 0) apply_pbc(pos[0], d.L);   // Engine.cu:993-996
+    __syncthreads();
+    if (t < n) {
+        F3 p = pos[t];
+        if (t > 0) hyperpos(pos[0], p, d.L, d.Lh);
+        flag_nan(d, p);
+        d.cpos[cur ^ 1][c * kMaxCP + t] = to4(p);
+    }
+    d.potE[c * kMaxCP + t] = (double)potE;   // potE_buffer write for all 64 threads (Engine.cu:1009-1013)
+}
+
+constexpr int kSolBlock = 128;
+constexpr int kStageCompounds = 16;
+
+__global__ void __launch_bounds__(kSolBlock) k_solvent(RefDev d, int cur) {
+    __shared__ F3 cbuf[kStageCompounds * kMaxCP];
+    __shared__ lima_particle_parameters cpar[kStageCompounds * kMaxCP];
+    __shared__ int cn[kStageCompounds];
+    const int s = blockIdx.x * kSolBlock + threadIdx.x;
+    const bool active = s < d.n_s;
+    F3 pos = mk(0.f, 0.f, 0.f), prev = pos;
+    if (active) {
+        pos = mk4(d.spos[cur][s]);
+        prev = mk4(d.sprev[cur][s]);
+    }
+    const lima_particle_parameters sol = d.pp[LIMA_ATOMTYPE_SOL];
+    F3 force = mk(0.f, 0.f, 0.f);
+    // solvent <- every compound particle, no list (computeLJForces, Engine.cu:1099-1117)
+    for (int c0 = 0; c0 < d.n_c; c0 += kStageCompounds) {
+        const int nst = min(kStageCompounds, d.n_c - c0);
+        __syncthreads();
+        for (int q = threadIdx.x; q < nst * kMaxCP; q += kSolBlock) {
+            const int c = c0 + q / kMaxCP, l = q % kMaxCP;
+            const lima_compound& cp = d.comps[c];
+            if (l < cp.n_particles) {
+                cbuf[q] = mk4(d.cpos[cur][c * kMaxCP + l]);
+                cpar[q] = d.pp[cp.atom_types[l]];
+            }
+            if (l == 0) cn[q / kMaxCP] = cp.n_particles;
+        }
+        __syncthreads();
+        if (active) {
+            for (int cc = 0; cc < nst; cc++) {
+                const F3* P = &cbuf[cc * kMaxCP];
+                hyperpos(P[0], pos, d.L, d.Lh);
+                F3 acc = mk(0.f, 0.f, 0.f);
+                const int nn = cn[cc];
+                for (int i = 0; i < nn; i++) {
+                    const lima_particle_parameters o = cpar[cc * kMaxCP + i];
+                    acc = add(acc, lj_force(pos, P[i], mix_sigma(sol.sigma, o.sigma), eps_arith(sol.epsilon, o.epsilon)));
+                }
+                force = add(force, acc);
+            }
+        }
+    }
+    if (!active) return;
+    // computeSolventToSolventLJForces (Engine.cu:706-720): self moves to each neighbour's image
+    {
+        F3 acc = mk(0.f, 0.f, 0.f);
+        const int cnt = d.ss_cnt[s];
+        const float sg = sol.sigma, ep = sol.epsilon;
+        for (int k = 0; k < cnt; k++) {
+            const uint32_t j = d.ss_ids[(size_t)k * d.n_s + s];
+            const F3 nb = mk4(__ldg(&d.spos[cur][j]));
+            hyperpos(nb, pos, d.L, d.Lh);
+            acc = add(acc, lj_force(pos, nb, sg, ep));
+        }
+        force = add(force, acc);
+    }
+    integrate(pos, prev, force, (double)sol.mass, d.dt, *d.lambda, d.L, d.Lh);
+    apply_pbc(pos, d.L);
+    flag_nan(d, pos);
+    d.spos[cur ^ 1][s] = to4(pos);
+    d.sprev[cur ^ 1][s] = to4(prev);
+    d.force_s[s] = to4(force);
+}
+
+// Engine::getBoxTemperature's KE term (LIMAENG::calcKineticEnergy,
+// Engine.cuh:32-45): positions two steps apart, central-difference speed.
+__global__ void k_ref_ke(RefDev d, int cur) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n_cp = d.n_c * kMaxCP;
+    double ke = 0.0;
+    if (i < n_cp) {
+        const int c = i / kMaxCP, l = i % kMaxCP;
+        const lima_compound& cp = d.comps[c];
+        if (l < cp.n_particles) {
+            F3 a = mk4(d.cpos[cur][i]), b = mk4(d.csnap[i]);
+            hyperpos(a, b, d.L, d.Lh);
+            float vel = (float)((double)(len(sub(a, b)) * 0.5f) / d.dt);
+            ke = (double)(float)(0.5 * (double)d.pp[cp.atom_types[l]].mass * vel * vel);
+        }
+    } else if (i < n_cp + d.n_s) {
+        const int s = i - n_cp;
+        F3 a = mk4(d.spos[cur][s]), b = mk4(d.ssnap[s]);
+        hyperpos(a, b, d.L, d.Lh);
+        float vel = (float)((double)(len(sub(a, b)) * 0.5f) / d.dt);
+        ke = (double)(float)(0.5 * (double)d.pp[LIMA_ATOMTYPE_SOL].mass * vel * vel);
+    }
+    for (int o = 16; o > 0; o >>= 1) ke += __shfl_down_sync(0xffffffffu, ke, o);
+    if ((threadIdx.x & 31) == 0 && ke != 0.0) atomicAdd(d.ke_accum, ke);
+}
+
+// Engine::handleBoxtemp (Engine.cu:362-393): lambda = clamp(T0/T, 0.9, 1.1).
+__global__ void k_ref_lambda(RefDev d, int n_particles, float t_target, int apply) {
+    double avg = *d.ke_accum / (double)n_particles;
+    float temp = (float)(avg * 2.0 / (3.0 * 8.3145));
+    temp = temp == 0.f ? 1.f : temp;
+    float sc = t_target / temp;
+    sc = fminf(sc, 1.1f);
+    sc = fmaxf(sc, 0.9f);
+    if (apply) *d.lambda = sc;
+    *d.ke_accum = (double)temp;   // keep the temperature for readback
+}
+
+__global__ void k_snapshot(RefDev d, int cur) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < d.n_c * kMaxCP) d.csnap[i] = d.cpos[cur][i];
+    if (i < d.n_s) d.ssnap[i] = d.spos[cur][i];
+}
+
+}  // namespace
+
+void ref_step_kernels(const RefDev& d, int cur, cudaStream_t s) {
+    if (d.n_b > 0) k_bridge<<<d.n_b, 32, 0, s>>>(d, cur);
+    if (d.n_c > 0) {
+        if (d.n_s > 0) k_cs_partial<<<dim3(d.n_chunks, d.n_c), 64, 0, s>>>(d, cur);
+        k_compound<<<d.n_c, 64, 0, s>>>(d, cur);
+    }
+    if (d.n_s > 0) k_solvent<<<(d.n_s + kSolBlock - 1) / kSolBlock, kSolBlock, 0, s>>>(d, cur);
+}
+
+void ref_thermostat_snapshot(const RefDev& d, int cur, cudaStream_t s) {
+    const int n = max(d.n_c * kMaxCP, d.n_s);
+    if (n > 0) k_snapshot<<<(n + 255) / 256, 256, 0, s>>>(d, cur);
+}
+
+// n_particles: Simulation::total_particles (compound particles present + solvents)
+void ref_thermostat_update(const RefDev& d, int cur, int n_particles, float t_target, bool apply, cudaStream_t s) {
+    cudaMemsetAsync(d.ke_accum, 0, sizeof(double), s);
+    const int n = d.n_c * kMaxCP + d.n_s;
+    if (n > 0) k_ref_ke<<<(n + 255) / 256, 256, 0, s>>>(d, cur);
+    k_ref_lambda<<<1, 1, 0, s>>>(d, n_particles, t_target, apply ? 1 : 0);
+}
+
+__global__ void k_set_float(float* p, float v) { *p = v; }
+
+void set_device_float(float* p, float v, cudaStream_t s) { k_set_float<<<1, 1, 0, s>>>(p, v); }
+
+}  // namespace lima

@@ -1,0 +1,105 @@
+// Physics-semantics path: conservative forces of the LIMA_MD model on one
+// unified particle array, laid out for throughput.
+//
+// Particle ids: "orig" = compound particles compound by compound (c, l) ->
+// base[c] + l, then solvents (n_cp + s).  "slot" = position in the spatially
+// sorted order used by every per-step array; re-sorted at each list rebuild.
+//
+// HBM layout (float3 quantities widened to float4, one 16-byte access each):
+//   pos[2][n_pad]   x, y, z in [0, L), w = type index (bit-cast)   (read by all, double-buffered)
+//   vel[n_pad]      half-step velocity, w = 1/m                  (own slot only)
+//   posc/velc       low parts of pos/vel (mixed precision)       (own slot only)
+//   xref[n_pad]     positions at the last rebuild (list validity check)
+//   force[n_pad]    total force of the last evaluation, w = per-particle LJ energy
+//   nl[cap][n_pad]  Verlet list, column-major (entry k of slot i at k*n_pad + i)
+//                   so that the k-th loads of a warp are one 128-byte line
+//   term_force      one float4 per (term, atom) of every bonded term; gathered
+//                   per particle through bterm_off/bterm_slot (CSR over orig)
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "lima_abi.h"
+
+namespace lima {
+
+struct PhysDev {
+    int n;              // particles
+    int n_pad;          // n rounded up to 32
+    int n_cp;           // compound particles
+    int n_c, n_s;
+    float L, invL, rc, rc2, rlist, rlist2, ron2, inv_sw_den, half_skin2;
+    int use_switch;
+    double dt;
+    int precision;      // lima_precision
+    int thermostat;     // lima_thermostat
+    double t_target, tau_t;
+    int n_types;
+    float4* pos[2];
+    float4* vel;
+    float4* posc;
+    float4* velc;
+    float4* xref;
+    float4* force;
+    uint32_t* orig_of_sorted;   // [n]
+    uint32_t* sorted_of_orig;   // [n]
+    float2* lj_table;           // [n_types^2] (sigma^2, 4 eps), Lorentz-Berthelot
+    // sort grid: coarse cells >= rlist, each split 4x4x4 for locality
+    int m;
+    float coarse;
+    uint32_t* keys[2];
+    uint32_t* vals[2];
+    void* sort_tmp; size_t sort_tmp_bytes;
+    uint32_t* cstart; uint32_t* cend;
+    float4* pos_tmp; float4* vel_tmp; float4* posc_tmp; float4* velc_tmp; uint32_t* orig_tmp;
+    // Verlet list
+    uint32_t* nl; uint32_t* nl_cnt; int nl_cap;
+    // exclusions (CSR over orig ids)
+    uint32_t* excl_off; uint32_t* excl_ids;
+    // bonded terms (orig ids)
+    int n_bonds, n_angles, n_dih;
+    int4* bond_idx; float2* bond_par;          // (r0, k)
+    int4* angle_idx; float2* angle_par;        // (theta0, k)
+    int4* dih_idx; float4* dih_par;            // (phi0, k, n)
+    uint32_t* bterm_off; uint32_t* bterm_slot;
+    float4* term_force;
+    int n_term_slots;
+    // FP64 reductions: acc[LIMA_E_*] summed by the step's kernels and
+    // finalised by the last block into e_last; lambda for the next step
+    double* acc;
+    double* e_last;
+    double* t_prev;
+    float* lambda;
+    unsigned int* done;
+    int* err;
+};
+
+struct PhysHost {
+    const lima_params* params;
+    const lima_forcefield* ff;
+    const lima_compound* comps;
+    const lima_compound_state* states;
+    int n_c;
+    const lima_compound_bridge_compact* bridges;
+    int n_b;
+    const lima_solvent* sols;
+    int n_s;
+};
+
+// returns 0 or a lima_status; device buffers are appended to `allocs`
+int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>& allocs, std::string& msg);
+void phys_upload_state(const PhysHost& h, PhysDev& d, int cur, cudaStream_t s);
+void phys_rebuild(PhysDev& d, int cur, cudaStream_t s);
+void phys_prime(PhysDev& d, int cur, cudaStream_t s);
+void phys_step_kernels(const PhysDev& d, int cur, cudaStream_t s, bool energy = false);
+void phys_energy_now(PhysDev& d, int cur, cudaStream_t s);
+void phys_read_compounds(const PhysDev& d, int cur, const lima_compound* comps, float4* pos_out, float4* prev_out);
+void phys_read_solvents(const PhysDev& d, int cur, float4* pos_out, float4* prev_out);
+void phys_read_forces(const PhysDev& d, const lima_compound* comps, float4* fc, float4* fs);
+void phys_read_energies(const PhysDev& d, double* totals, double* per_particle, const lima_compound* comps, int n_c,
+                        int n_s);
+
+}  // namespace lima

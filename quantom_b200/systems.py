@@ -50,6 +50,7 @@ class ChainSpec:
     sigma_range: tuple = (0.25, 0.40)           # nm
     epsilon_range: tuple = (200.0, 1000.0)      # J/mol
     mass: float = 14.027e-3           # kg/mol (united-atom CH2)
+    compound_size: int = 64           # particles per compound (the reference packs up to 64)
 
 
 @dataclass
@@ -224,7 +225,17 @@ def make_system(name_or_spec, seed: int = 2024) -> System:
     placed = np.zeros((0, 3))
     if cs is not None:
         for _c in range(cs.n_chains):
-            pts = _grow_chain(rng, cs.chain_len, cs, box, placed, spec.min_sep)
+            # the reference keeps every compound particle at the image nearest
+            # its particle 0 (Engine.cu:996), which needs the box to exceed
+            # twice a compound's extent (Constants.cuh:35): regrow otherwise
+            for _try in range(200):
+                pts = _grow_chain(rng, cs.chain_len, cs, box, placed, spec.min_sep)
+                ext = max(np.linalg.norm(pts[k:k + cs.compound_size] - pts[k], axis=1).max()
+                          for k in range(0, cs.chain_len, cs.compound_size))
+                if ext < 0.45 * box:
+                    break
+            else:
+                raise RuntimeError("could not grow a chain that fits the reference's compound convention")
             chain_pts.append(pts)
             chain_types.append(rng.integers(1, 1 + cs.n_types, cs.chain_len))
             placed = np.concatenate([placed, pts])
@@ -259,7 +270,7 @@ def make_system(name_or_spec, seed: int = 2024) -> System:
 def _pack_chains(chain_pts, chain_types, v_chain, cs, spec, box):
     if cs is None or not chain_pts:
         return (np.zeros(0, L.Compound), np.zeros(0, L.CompoundState), np.zeros(0, L.CompoundBridgeCompact))
-    per = L.MAX_COMPOUND_PARTICLES
+    per = cs.compound_size
     comp_list, state_list, bridge_list = [], [], []
     vofs = 0
     for pts, types in zip(chain_pts, chain_types):
@@ -296,7 +307,7 @@ def _pack_chains(chain_pts, chain_types, v_chain, cs, spec, box):
         terms = ([("bond", (i, i + 1)) for i in range(n - 1)] +
                  [("angle", (i, i + 1, i + 2)) for i in range(n - 2)] +
                  [("dihedral", (i, i + 1, i + 2, i + 3)) for i in range(n - 3)])
-        bridge = None
+        bridges = {}   # one CompoundBridge per pair of compounds (CompoundBridgeBundle::addBridge)
         for kind, atoms in terms:
             cids = {int(cid[a]) for a in atoms}
             # bonded LJ exclusions (distributeLJIgnores)
@@ -328,8 +339,8 @@ def _pack_chains(chain_pts, chain_types, v_chain, cs, spec, box):
             else:
                 if len(cids) > 2:
                     raise RuntimeError("term spans more than two compounds")
-                if bridge is None:
-                    bridge = {"refs": [], "types": [], "bonds": [], "angles": [], "dihedrals": []}
+                key = tuple(sorted(cids))
+                bridge = bridges.setdefault(key, {"refs": [], "types": [], "bonds": [], "angles": [], "dihedrals": []})
                 loc = []
                 for a in atoms:
                     ref = (int(cid[a]), int(lid[a]))
@@ -338,7 +349,8 @@ def _pack_chains(chain_pts, chain_types, v_chain, cs, spec, box):
                         bridge["types"].append(int(types[a]))
                     loc.append(bridge["refs"].index(ref))
                 bridge[{"bond": "bonds", "angle": "angles", "dihedral": "dihedrals"}[kind]].append(loc)
-        if bridge is not None:
+        for key in sorted(bridges):
+            bridge = bridges[key]
             br = np.zeros(1, L.CompoundBridgeCompact)[0]
             if len(bridge["refs"]) > L.MAX_PARTICLES_IN_BRIDGE:
                 raise RuntimeError("too many particles in bridge")
@@ -360,5 +372,10 @@ def _pack_chains(chain_pts, chain_types, v_chain, cs, spec, box):
         state_list.extend(list(sts))
     if len(comp_list) > L.MAX_COMPOUNDS:
         raise RuntimeError("more compounds than the reference layout holds")
-    return (np.array(comp_list, dtype=L.Compound), np.array(state_list, dtype=L.CompoundState),
-            np.array(bridge_list, dtype=L.CompoundBridgeCompact))
+    def pack(items, dt):   # zero-initialised so padding bytes are deterministic
+        out = np.zeros(len(items), dt)
+        for i, it in enumerate(items):
+            out[i] = it
+        return out
+
+    return pack(comp_list, L.Compound), pack(state_list, L.CompoundState), pack(bridge_list, L.CompoundBridgeCompact)
