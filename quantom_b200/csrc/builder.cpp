@@ -81,8 +81,10 @@ struct CellGrid {
     }
 };
 
-// True if p is at least d_min from every particle in the grid other than `self`.
-bool is_free(const CellGrid& g, const std::vector<double>& pos, const double* p, int self, double d2min) {
+// True if p is at least d_min from every particle in the grid other than
+// `self` (and at least fixed_rmin[id] from fixed particle id, if given).
+bool is_free(const CellGrid& g, const std::vector<double>& pos, const double* p, int self, double d2min,
+             const double* fixed_rmin = nullptr, int n_fixed = 0) {
     const int m = g.m;
     const int cx = std::min(m - 1, static_cast<int>(p[0] / g.cell));
     const int cy = std::min(m - 1, static_cast<int>(p[1] / g.cell));
@@ -100,7 +102,8 @@ bool is_free(const CellGrid& g, const std::vector<double>& pos, const double* p,
                         d -= g.L * std::nearbyint(d / g.L);
                         d2 += d * d;
                     }
-                    if (d2 < d2min) return false;
+                    const double lim = (fixed_rmin && id < n_fixed) ? fixed_rmin[id] * fixed_rmin[id] : d2min;
+                    if (d2 < lim) return false;
                 }
             }
     if (m < 3) {  // tiny boxes: fall back to all particles
@@ -112,7 +115,8 @@ bool is_free(const CellGrid& g, const std::vector<double>& pos, const double* p,
                 d -= g.L * std::nearbyint(d / g.L);
                 d2 += d * d;
             }
-            if (d2 < d2min) return false;
+            const double lim = (fixed_rmin && static_cast<int>(id) < n_fixed) ? fixed_rmin[id] * fixed_rmin[id] : d2min;
+            if (d2 < lim) return false;
         }
     }
     return true;
@@ -123,19 +127,21 @@ bool is_free(const CellGrid& g, const std::vector<double>& pos, const double* p,
 extern "C" {
 
 // Places n_mobile points in the periodic cube [0, box)^3, none closer than
-// d_min to each other or to the n_fixed points in `fixed_xyz` (which must lie
-// in the box).  Writes n_mobile*3 doubles to out_xyz.  Returns the number of
-// accepted Monte Carlo moves (>= 0), or -1 if the lattice cannot hold n_mobile
-// points at this density.
-long lima_builder_pack_spheres(double box, double d_min, const double* fixed_xyz, int n_fixed, int n_mobile,
-                               unsigned long long seed, int n_sweeps, double* out_xyz) {
+// d_min to each other, nor closer than fixed_rmin[k] (or d_min when
+// fixed_rmin is NULL) to fixed point k of `fixed_xyz` (which must lie in the
+// box).  Writes n_mobile*3 doubles to out_xyz.  Returns the number of accepted
+// Monte Carlo moves (>= 0), or -1 if the lattice cannot hold n_mobile points.
+long lima_builder_pack_spheres(double box, double d_min, const double* fixed_xyz, const double* fixed_rmin,
+                               int n_fixed, int n_mobile, unsigned long long seed, int n_sweeps, double* out_xyz) {
     Rng rng(seed);
     const double d2min = d_min * d_min;
     const int n_tot = n_fixed + n_mobile;
+    double cell_min = d_min;
+    for (int i = 0; fixed_rmin && i < n_fixed; i++) cell_min = std::max(cell_min, fixed_rmin[i]);
     std::vector<double> pos(static_cast<size_t>(n_tot) * 3);
     for (int i = 0; i < 3 * n_fixed; i++) pos[i] = wrap(fixed_xyz[i], box);
     CellGrid fixed_grid;
-    fixed_grid.init(box, d_min);
+    fixed_grid.init(box, cell_min);
     for (int i = 0; i < n_fixed; i++) fixed_grid.insert(i, &pos[3 * i]);
 
     // 1. lattice sites
@@ -150,7 +156,7 @@ long lima_builder_pack_spheres(double box, double d_min, const double* fixed_xyz
                 for (int k = 0; k < M; k++)
                     for (auto& b : basis) {
                         double p[3] = {(i + b[0] + 0.25) * a, (j + b[1] + 0.25) * a, (k + b[2] + 0.25) * a};
-                        if (n_fixed == 0 || is_free(fixed_grid, pos, p, -1, d2min))
+                        if (n_fixed == 0 || is_free(fixed_grid, pos, p, -1, d2min, fixed_rmin, n_fixed))
                             sites.insert(sites.end(), p, p + 3);
                     }
         if (static_cast<int>(sites.size() / 3) >= n_mobile) break;
@@ -164,7 +170,7 @@ long lima_builder_pack_spheres(double box, double d_min, const double* fixed_xyz
         std::swap(order[i], order[j]);
     }
     CellGrid grid;
-    grid.init(box, d_min);
+    grid.init(box, cell_min);
     for (int i = 0; i < n_fixed; i++) grid.insert(i, &pos[3 * i]);
     for (int i = 0; i < n_mobile; i++) {
         double* p = &pos[3 * (n_fixed + i)];
@@ -182,7 +188,7 @@ long lima_builder_pack_spheres(double box, double d_min, const double* fixed_xyz
             double* p = &pos[3 * id];
             double trial[3];
             for (int k = 0; k < 3; k++) trial[k] = wrap(p[k] + (2.0 * rng.uniform() - 1.0) * step, box);
-            if (is_free(grid, pos, trial, id, d2min)) {
+            if (is_free(grid, pos, trial, id, d2min, fixed_rmin, n_fixed)) {
                 grid.remove(id, p);
                 std::memcpy(p, trial, sizeof(trial));
                 grid.insert(id, p);

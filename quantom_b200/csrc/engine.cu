@@ -254,6 +254,32 @@ void ref_setup(lima_ctx* c) {
     d.csnap = c->dalloc<float4>(ncp);
     d.ssnap = c->dalloc<float4>(ns);
     d.ke_accum = c->dalloc<double>(1);
+    {   // per-atom bonded contribution lists (see RefDev::bt_off)
+        std::vector<uint32_t> off(static_cast<size_t>(nc) * 65 + 1, 0);
+        std::vector<uint16_t> code;
+        for (int i = 0; i < nc; i++) {
+            const lima_compound& cp = c->comps[i];
+            for (int t = 0; t < lima::kMaxCP; t++) {
+                off[i * 65 + t] = static_cast<uint32_t>(code.size());
+                for (int b = 0; b < cp.n_singlebonds; b++)
+                    for (int k = 0; k < 2; k++)
+                        if (static_cast<int>(cp.singlebonds[b].atom_indexes[k]) == t) code.push_back((0 << 14) | (b << 2) | k);
+                for (int b = 0; b < cp.n_anglebonds; b++)
+                    for (int k = 0; k < 3; k++)
+                        if (static_cast<int>(cp.anglebonds[b].atom_indexes[k]) == t) code.push_back((1 << 14) | (b << 2) | k);
+                for (int b = 0; b < cp.n_dihedrals; b++)
+                    for (int k = 0; k < 4; k++)
+                        if (static_cast<int>(cp.dihedrals[b].atom_indexes[k]) == t) code.push_back((2 << 14) | (b << 2) | k);
+            }
+            off[i * 65 + 64] = static_cast<uint32_t>(code.size());
+        }
+        off[static_cast<size_t>(nc) * 65] = static_cast<uint32_t>(code.size());
+        d.bt_off = c->dalloc<uint32_t>(off.size());
+        d.bt_code = c->dalloc<uint16_t>(code.size());
+        up(d.bt_off, off.data(), sizeof(uint32_t) * off.size());
+        up(d.bt_code, code.data(), sizeof(uint16_t) * code.size());
+        cuda_ok(cudaStreamSynchronize(s), "upload");
+    }
     c->n_particles_total = ns;
     for (const auto& cp : c->comps) c->n_particles_total += cp.n_particles;
 }
@@ -294,6 +320,9 @@ void check_device_errors(lima_ctx* c) {
         if (h & lima::ERR_BIT_CS_OVERFLOW) m += "compound-solvent list overflow; ";
         if (h & lima::ERR_BIT_CC_OVERFLOW) m += "compound-compound list overflow; ";
         if (h & lima::ERR_BIT_PHYS_LIST_OVERFLOW) m += "pair list overflow; ";
+        if (h & lima::ERR_BIT_LIST_STALE)
+            m += "pair list went stale: a particle moved more than skin/2 between rebuilds (raise skin or lower "
+                 "nlist_period); ";
         if (h & lima::ERR_BIT_NAN) m += "NaN position; ";
         if (h & lima::ERR_BIT_CRITICAL_FORCE) m += "critical force (|F| > 2e12); ";
         const bool cap = h & (lima::ERR_BIT_SS_OVERFLOW | lima::ERR_BIT_CS_OVERFLOW | lima::ERR_BIT_CC_OVERFLOW |

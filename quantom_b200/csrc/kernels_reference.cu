@@ -148,15 +148,75 @@ __global__ void __launch_bounds__(64) k_compound(RefDev d, int cur) {
     if (t > 0 && t < n) hyperpos(p0, pos[t], d.L, d.Lh);
     __syncthreads();
     float potE = 0.f;
-    bonded_entity<64>(pos, cp.n_singlebonds, cp.singlebonds, cp.n_anglebonds, cp.anglebonds, cp.n_dihedrals,
-                      cp.dihedrals, sc, force, potE);
-    const lima_particle_parameters a = d.pp[t < n ? cp.atom_types[t] : 0];
+    // bonded terms: one thread per term, results in shared memory
+    // (calcPairbondForces / calcAnglebondForces / calcDihedralbondForces)
+    for (int b = t; b < cp.n_singlebonds; b += 64) {
+        const lima_pair_bond& pb = cp.singlebonds[b];
+        pairbond(pos[pb.atom_indexes[0]], pos[pb.atom_indexes[1]], pb.b0, pb.kb, sc.rb[b], potE);
+    }
+    for (int q = t; q < cp.n_anglebonds; q += 64) {
+        const lima_angle_bond& ab = cp.anglebonds[q];
+        anglebond(pos[ab.atom_indexes[0]], pos[ab.atom_indexes[1]], pos[ab.atom_indexes[2]], ab.theta_0, ab.k_theta,
+                  sc.ra[q], potE);
+    }
+    for (int q = t; q < cp.n_dihedrals; q += 64) {
+        const lima_dihedral_bond& db = cp.dihedrals[q];
+        dihedral(pos[db.atom_indexes[0]], pos[db.atom_indexes[1]], pos[db.atom_indexes[2]], pos[db.atom_indexes[3]],
+                 db.phi_0, db.k_phi, db.n, sc.rd[q], potE);
+    }
+    // own particle parameters, and this particle's LJ_Ignores in shared memory
+    __shared__ lima_particle_parameters spar[kMaxCP];
+    __shared__ lima_particle_parameters npar[kMaxCP];
+    __shared__ uint8_t ig_local[kMaxCP][LIMA_LJ_IGNORES_MAX];
+    __shared__ uint8_t ig_comp[kMaxCP][LIMA_LJ_IGNORES_MAX];
+    int n_ig = 0;
+    if (t < n) {
+        spar[t] = d.pp[cp.atom_types[t]];
+        const lima_lj_ignores& ig = cp.lj_ignore_list[t];
+        n_ig = ig.n_ignores;
+        for (int q = 0; q < n_ig; q++) {
+            ig_local[t][q] = ig.local_ids[q];
+            ig_comp[t][q] = ig.compound_ids[q];
+        }
+    }
+    __syncthreads();
+    // per-atom sums in the reference's order: the bonds in index order, then
+    // the angles, then the dihedrals (Engine.cu:765-771, 799-806, 834-842)
+    {
+        F3 acc = mk(0.f, 0.f, 0.f);
+        int kind = 0;
+        for (uint32_t q = d.bt_off[c * 65 + t]; q < d.bt_off[c * 65 + t + 1]; q++) {
+            const uint32_t code = d.bt_code[q];
+            const int k = (int)(code >> 14), term = (int)((code >> 2) & 0x3ff), slot = (int)(code & 3);
+            while (kind < k) {
+                force = add(force, acc);
+                acc = mk(0.f, 0.f, 0.f);
+                kind++;
+            }
+            const F3 r = k == 0 ? sc.rb[term][slot] : (k == 1 ? sc.ra[term][slot] : sc.rd[term][slot]);
+            acc = add(acc, r);
+        }
+        while (kind < 3) {
+            force = add(force, acc);
+            acc = mk(0.f, 0.f, 0.f);
+            kind++;
+        }
+    }
+    const lima_particle_parameters a = t < n ? spar[t] : d.pp[0];
+    // which particles of compound `cid` this particle ignores (LJ_Ignores::ignore, Bodies.cuh:191-197)
+    auto ignore_mask = [&](int cid) {
+        unsigned long long msk = 0ull;
+        for (int q = 0; q < n_ig; q++)
+            if (ig_comp[t][q] == (uint8_t)cid) msk |= 1ull << ig_local[t][q];
+        return msk;
+    };
     // computeIntramolecularLJForces (Engine.cu:678-700)
     if (t < n) {
+        const unsigned long long msk = ignore_mask(c);
         F3 acc = mk(0.f, 0.f, 0.f);
         for (int i = 0; i < n; i++) {
-            if (i == t || ignored(cp.lj_ignore_list[t], i, c)) continue;
-            const lima_particle_parameters o = d.pp[cp.atom_types[i]];
+            if (i == t || ((msk >> i) & 1ull)) continue;
+            const lima_particle_parameters o = spar[i];
             acc = add(acc, lj_force(pos[t], pos[i], mix_sigma(a.sigma, o.sigma), eps_geo(a.epsilon, o.epsilon)));
         }
         force = add(force, acc);
@@ -165,20 +225,21 @@ __global__ void __launch_bounds__(64) k_compound(RefDev d, int cur) {
     const int ncc = d.cc_cnt[c];
     for (int k = 0; k < ncc; k++) {
         const int nb = d.cc_ids[c * kMaxCP + k];
-        const lima_compound& ncp = d.comps[nb];
-        const int nn = ncp.n_particles;
+        const int nn = d.comps[nb].n_particles;
         __syncthreads();
         if (t < nn) {
             F3 v = mk4(d.cpos[cur][nb * kMaxCP + t]);
             hyperpos(p0, v, d.L, d.Lh);
             nbuf[t] = v;
+            npar[t] = d.pp[d.comps[nb].atom_types[t]];
         }
         __syncthreads();
         if (t < n) {
+            const unsigned long long msk = ignore_mask(nb);
             F3 acc = mk(0.f, 0.f, 0.f);
             for (int j = 0; j < nn; j++) {
-                if (ignored(cp.lj_ignore_list[t], j, nb)) continue;
-                const lima_particle_parameters o = d.pp[ncp.atom_types[j]];
+                if ((msk >> j) & 1ull) continue;
+                const lima_particle_parameters o = npar[j];
                 acc = add(acc, lj_force(pos[t], nbuf[j], mix_sigma(a.sigma, o.sigma), eps_arith(a.epsilon, o.epsilon)));
             }
             force = add(force, acc);

@@ -1,0 +1,460 @@
+// Host side of the physics-semantics path: set-up from the reference layout,
+// list rebuilds, step launches and readback (kernels in kernels_physics.cu).
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+#include <vector>
+
+#include "physdev.cuh"
+#include "physkern.cuh"
+#include "refdev.cuh"
+
+namespace lima {
+namespace {
+
+inline float host_int_as_float(int v) {
+    float f;
+    std::memcpy(&f, &v, sizeof(f));
+    return f;
+}
+
+template <typename T>
+T* dalloc(std::vector<void*>& allocs, size_t n) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) throw std::runtime_error("cudaMalloc failed");
+    allocs.push_back(p);
+    return static_cast<T*>(p);
+}
+
+}  // namespace
+
+int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>& allocs, std::string& msg) {
+    const lima_params& p = *h.params;
+    if (p.thermostat == LIMA_THERMOSTAT_REFERENCE) {
+        msg = "the reference thermostat belongs to reference semantics";
+        return LIMA_ERR_UNSUPPORTED;
+    }
+    std::memset(&d, 0, sizeof(d));
+    d.n_c = h.n_c;
+    d.n_s = h.n_s;
+    std::vector<int> base(h.n_c + 1, 0);
+    for (int c = 0; c < h.n_c; c++) base[c + 1] = base[c] + h.comps[c].n_particles;
+    d.n_cp = base[h.n_c];
+    d.n = d.n_cp + h.n_s;
+    if (d.n < 2) {
+        msg = "physics semantics needs at least two particles";
+        return LIMA_ERR_ARGUMENT;
+    }
+    d.n_pad = (d.n + 31) / 32 * 32;
+    d.L = p.box_len;
+    d.invL = 1.f / p.box_len;
+    d.rc = p.cutoff;
+    d.rc2 = p.cutoff * p.cutoff;
+    d.rlist = p.cutoff + p.skin;
+    d.rlist2 = d.rlist * d.rlist;
+    d.half_skin2 = 0.25f * p.skin * p.skin;
+    d.use_switch = p.switch_on < p.cutoff ? 1 : 0;
+    const float ron = d.use_switch ? p.switch_on : p.cutoff;
+    d.ron2 = ron * ron;
+    d.inv_sw_den = d.use_switch ? 1.f / ((d.rc2 - d.ron2) * (d.rc2 - d.ron2) * (d.rc2 - d.ron2)) : 0.f;
+    d.dt = p.dt;
+    d.precision = p.precision;
+    d.thermostat = p.thermostat;
+    d.t_target = p.t_target;
+    d.tau_t = p.tau_t;
+
+    // types and the Lorentz-Berthelot table (sigma^2, 4 eps)
+    int max_type = 0;
+    for (int c = 0; c < h.n_c; c++)
+        for (int t = 0; t < h.comps[c].n_particles; t++) max_type = std::max<int>(max_type, h.comps[c].atom_types[t]);
+    d.n_types = max_type + 1;
+    for (int t = 0; t < d.n_types; t++) {
+        const auto& pp = h.ff->particle_parameters[t];
+        const bool used = t == LIMA_ATOMTYPE_SOL ? h.n_s > 0 : true;
+        if (used && (!(pp.mass > 0.f) || !(pp.sigma > 0.f) || !(pp.epsilon >= 0.f))) {
+            msg = "force-field entry of a used type has non-positive mass/sigma or negative epsilon";
+            return LIMA_ERR_ARGUMENT;
+        }
+    }
+    std::vector<float2> tab(d.n_types * d.n_types);
+    for (int a = 0; a < d.n_types; a++)
+        for (int b = 0; b < d.n_types; b++) {
+            const auto& A = h.ff->particle_parameters[a];
+            const auto& B = h.ff->particle_parameters[b];
+            const double sg = 0.5 * ((double)A.sigma + (double)B.sigma);
+            const double ep = std::sqrt(std::max(0.0, (double)A.epsilon * (double)B.epsilon));
+            tab[a * d.n_types + b] = make_float2((float)(sg * sg), (float)(4.0 * ep));
+        }
+    // exclusions (LJ_Ignores -> orig ids)
+    std::vector<std::vector<uint32_t>> excl(d.n);
+    for (int c = 0; c < h.n_c; c++)
+        for (int t = 0; t < h.comps[c].n_particles; t++) {
+            const lima_lj_ignores& ig = h.comps[c].lj_ignore_list[t];
+            for (int q = 0; q < ig.n_ignores; q++) {
+                const int oc = ig.compound_ids[q], ol = ig.local_ids[q];
+                if (oc >= h.n_c || ol >= h.comps[oc].n_particles) {
+                    msg = "LJ_Ignores entry refers to a missing particle";
+                    return LIMA_ERR_ARGUMENT;
+                }
+                excl[base[c] + t].push_back(base[oc] + ol);
+            }
+        }
+    std::vector<uint32_t> eoff(d.n + 1, 0), eids;
+    for (int i = 0; i < d.n; i++) {
+        eoff[i + 1] = eoff[i] + (uint32_t)excl[i].size();
+        eids.insert(eids.end(), excl[i].begin(), excl[i].end());
+    }
+    // bonded terms with orig ids (compounds, then bridges)
+    std::vector<int4> bidx, aidx, didx;
+    std::vector<float2> bpar, apar;
+    std::vector<float4> dpar;
+    for (int c = 0; c < h.n_c; c++) {
+        const lima_compound& cp = h.comps[c];
+        const int o = base[c];
+        for (int b = 0; b < cp.n_singlebonds; b++) {
+            const auto& t = cp.singlebonds[b];
+            bidx.push_back(make_int4(o + t.atom_indexes[0], o + t.atom_indexes[1], 0, 0));
+            bpar.push_back(make_float2(t.b0, t.kb));
+        }
+        for (int b = 0; b < cp.n_anglebonds; b++) {
+            const auto& t = cp.anglebonds[b];
+            aidx.push_back(make_int4(o + t.atom_indexes[0], o + t.atom_indexes[1], o + t.atom_indexes[2], 0));
+            apar.push_back(make_float2(t.theta_0, t.k_theta));
+        }
+        for (int b = 0; b < cp.n_dihedrals; b++) {
+            const auto& t = cp.dihedrals[b];
+            didx.push_back(make_int4(o + t.atom_indexes[0], o + t.atom_indexes[1], o + t.atom_indexes[2],
+                                     o + t.atom_indexes[3]));
+            dpar.push_back(make_float4(t.phi_0, t.k_phi, (float)t.n, 0.f));
+        }
+    }
+    for (int b = 0; b < h.n_b; b++) {
+        const lima_compound_bridge_compact& br = h.bridges[b];
+        auto gid = [&](uint32_t local) {
+            const auto& r = br.particle_refs[local];
+            return base[r.compound_id] + r.local_id_compound;
+        };
+        for (int q = 0; q < br.n_singlebonds; q++) {
+            const auto& t = br.singlebonds[q];
+            bidx.push_back(make_int4(gid(t.atom_indexes[0]), gid(t.atom_indexes[1]), 0, 0));
+            bpar.push_back(make_float2(t.b0, t.kb));
+        }
+        for (int q = 0; q < br.n_anglebonds; q++) {
+            const auto& t = br.anglebonds[q];
+            aidx.push_back(make_int4(gid(t.atom_indexes[0]), gid(t.atom_indexes[1]), gid(t.atom_indexes[2]), 0));
+            apar.push_back(make_float2(t.theta_0, t.k_theta));
+        }
+        for (int q = 0; q < br.n_dihedrals; q++) {
+            const auto& t = br.dihedrals[q];
+            didx.push_back(make_int4(gid(t.atom_indexes[0]), gid(t.atom_indexes[1]), gid(t.atom_indexes[2]),
+                                     gid(t.atom_indexes[3])));
+            dpar.push_back(make_float4(t.phi_0, t.k_phi, (float)t.n, 0.f));
+        }
+    }
+    d.n_bonds = (int)bidx.size();
+    d.n_angles = (int)aidx.size();
+    d.n_dih = (int)didx.size();
+    d.n_term_slots = 2 * d.n_bonds + 3 * d.n_angles + 4 * d.n_dih;
+    std::vector<std::vector<uint32_t>> slots(std::max(d.n_cp, 1));
+    for (int b = 0; b < d.n_bonds; b++) {
+        slots[bidx[b].x].push_back(2 * b);
+        slots[bidx[b].y].push_back(2 * b + 1);
+    }
+    for (int a = 0; a < d.n_angles; a++) {
+        const int b0 = 2 * d.n_bonds + 3 * a;
+        slots[aidx[a].x].push_back(b0);
+        slots[aidx[a].y].push_back(b0 + 1);
+        slots[aidx[a].z].push_back(b0 + 2);
+    }
+    for (int q = 0; q < d.n_dih; q++) {
+        const int b0 = 2 * d.n_bonds + 3 * d.n_angles + 4 * q;
+        slots[didx[q].x].push_back(b0);
+        slots[didx[q].y].push_back(b0 + 1);
+        slots[didx[q].z].push_back(b0 + 2);
+        slots[didx[q].w].push_back(b0 + 3);
+    }
+    std::vector<uint32_t> boff(d.n_cp + 1, 0), bslot;
+    for (int i = 0; i < d.n_cp; i++) {
+        boff[i + 1] = boff[i] + (uint32_t)slots[i].size();
+        bslot.insert(bslot.end(), slots[i].begin(), slots[i].end());
+    }
+
+    // sort grid (coarse cells >= rlist) and Verlet-list capacity
+    d.m = std::max(1, (int)std::floor(d.L / d.rlist));
+    while (d.m > 1 && d.L / d.m < d.rlist) d.m--;
+    d.coarse = d.L / d.m;
+    const double rho = d.n / ((double)d.L * d.L * d.L);
+    const double expect = 4.0 / 3.0 * M_PI * (double)d.rlist * d.rlist * d.rlist * rho;
+    d.nl_cap = std::min((d.n + kGroup - 1) / kGroup * kGroup, (int)((1.6 * expect + 96) / kGroup + 1) * kGroup);
+    d.nl_cap = std::max(d.nl_cap, 4 * kGroup);
+
+    try {
+        for (int b = 0; b < 2; b++) d.pos[b] = dalloc<float4>(allocs, d.n_pad);
+        d.vel = dalloc<float4>(allocs, d.n_pad);
+        d.posc = dalloc<float4>(allocs, d.n_pad);
+        d.velc = dalloc<float4>(allocs, d.n_pad);
+        d.xref = dalloc<float4>(allocs, d.n_pad);
+        d.force = dalloc<float4>(allocs, d.n_pad);
+        d.orig_of_sorted = dalloc<uint32_t>(allocs, d.n_pad);
+        d.sorted_of_orig = dalloc<uint32_t>(allocs, d.n);
+        d.lj_table = dalloc<float2>(allocs, tab.size());
+        for (int b = 0; b < 2; b++) {
+            d.keys[b] = dalloc<uint32_t>(allocs, d.n);
+            d.vals[b] = dalloc<uint32_t>(allocs, d.n);
+        }
+        const size_t ncell = (size_t)d.m * d.m * d.m;
+        d.cstart = dalloc<uint32_t>(allocs, ncell);
+        d.cend = dalloc<uint32_t>(allocs, ncell);
+        d.pos_tmp = dalloc<float4>(allocs, d.n);
+        d.vel_tmp = dalloc<float4>(allocs, d.n);
+        d.posc_tmp = dalloc<float4>(allocs, d.n);
+        d.velc_tmp = dalloc<float4>(allocs, d.n);
+        d.orig_tmp = dalloc<uint32_t>(allocs, d.n);
+        d.nl = dalloc<uint32_t>(allocs, (size_t)d.nl_cap * d.n_pad);
+        d.nl_cnt = dalloc<uint32_t>(allocs, d.n_pad);
+        d.excl_off = dalloc<uint32_t>(allocs, eoff.size());
+        d.excl_ids = dalloc<uint32_t>(allocs, eids.size());
+        d.bond_idx = dalloc<int4>(allocs, bidx.size());
+        d.bond_par = dalloc<float2>(allocs, bpar.size());
+        d.angle_idx = dalloc<int4>(allocs, aidx.size());
+        d.angle_par = dalloc<float2>(allocs, apar.size());
+        d.dih_idx = dalloc<int4>(allocs, didx.size());
+        d.dih_par = dalloc<float4>(allocs, dpar.size());
+        d.bterm_off = dalloc<uint32_t>(allocs, boff.size());
+        d.bterm_slot = dalloc<uint32_t>(allocs, bslot.size());
+        d.term_force = dalloc<float4>(allocs, d.n_term_slots);
+        d.acc = dalloc<double>(allocs, LIMA_E_COUNT);
+        d.e_last = dalloc<double>(allocs, LIMA_E_COUNT);
+        d.t_prev = dalloc<double>(allocs, 1);
+        d.lambda = dalloc<float>(allocs, 1);
+        d.done = dalloc<unsigned int>(allocs, 1);
+        d.err = dalloc<int>(allocs, 1);
+        cub::DeviceRadixSort::SortPairs(nullptr, d.sort_tmp_bytes, d.keys[0], d.keys[1], d.vals[0], d.vals[1], d.n, 0,
+                                        32, s);
+        d.sort_tmp = dalloc<uint8_t>(allocs, d.sort_tmp_bytes);
+    } catch (const std::exception& e) {
+        msg = std::string("device allocation failed: ") + e.what();
+        return LIMA_ERR_CUDA;
+    }
+    auto up = [&](void* dst, const void* src, size_t bytes) {
+        if (bytes) cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+    };
+    up(d.lj_table, tab.data(), sizeof(float2) * tab.size());
+    up(d.excl_off, eoff.data(), sizeof(uint32_t) * eoff.size());
+    up(d.excl_ids, eids.data(), sizeof(uint32_t) * eids.size());
+    up(d.bond_idx, bidx.data(), sizeof(int4) * bidx.size());
+    up(d.bond_par, bpar.data(), sizeof(float2) * bpar.size());
+    up(d.angle_idx, aidx.data(), sizeof(int4) * aidx.size());
+    up(d.angle_par, apar.data(), sizeof(float2) * apar.size());
+    up(d.dih_idx, didx.data(), sizeof(int4) * didx.size());
+    up(d.dih_par, dpar.data(), sizeof(float4) * dpar.size());
+    up(d.bterm_off, boff.data(), sizeof(uint32_t) * boff.size());
+    up(d.bterm_slot, bslot.data(), sizeof(uint32_t) * bslot.size());
+    cudaMemsetAsync(d.acc, 0, sizeof(double) * LIMA_E_COUNT, s);
+    cudaMemsetAsync(d.e_last, 0, sizeof(double) * LIMA_E_COUNT, s);
+    cudaMemsetAsync(d.t_prev, 0, sizeof(double), s);
+    cudaMemsetAsync(d.done, 0, sizeof(unsigned int), s);
+    cudaMemsetAsync(d.err, 0, sizeof(int), s);
+    cudaMemsetAsync(d.nl_cnt, 0, sizeof(uint32_t) * d.n_pad, s);
+    cudaMemsetAsync(d.force, 0, sizeof(float4) * d.n_pad, s);
+    set_device_float(d.lambda, 1.f, s);
+    phys_upload_state(h, d, 0, s);
+    return cudaGetLastError() == cudaSuccess ? 0 : LIMA_ERR_CUDA;
+}
+
+// Host state (reference layout) -> device, in orig order (the next rebuild
+// sorts).  Half-step velocities from the Stormer pair: v = (x - x_prev)/dt.
+void phys_upload_state(const PhysHost& h, PhysDev& d, int cur, cudaStream_t s) {
+    std::vector<float4> pos(d.n_pad), vel(d.n_pad), zero(d.n_pad, make_float4(0, 0, 0, 0));
+    std::vector<uint32_t> ident(d.n_pad);
+    const float L = d.L;
+    auto wrap = [&](double x) {
+        x = std::fmod(x, (double)L);
+        if (x < 0) x += L;
+        float f = (float)x;
+        if (f >= L) f = 0.f;
+        return f;
+    };
+    auto mimg = [&](double dd) { return dd - L * std::nearbyint(dd / L); };
+    int k = 0;
+    for (int c = 0; c < h.n_c; c++)
+        for (int t = 0; t < h.comps[c].n_particles; t++, k++) {
+            const lima_float3 x = h.states[c].positions[t], xp = h.comps[c].prev_positions[t];
+            const int type = h.comps[c].atom_types[t];
+            pos[k] = make_float4(wrap(x.x), wrap(x.y), wrap(x.z), host_int_as_float(type));
+            const float im = 1.f / h.ff->particle_parameters[type].mass;
+            vel[k] = make_float4((float)(mimg((double)x.x - xp.x) / d.dt), (float)(mimg((double)x.y - xp.y) / d.dt),
+                                 (float)(mimg((double)x.z - xp.z) / d.dt), im);
+        }
+    const float im_sol = 1.f / h.ff->particle_parameters[LIMA_ATOMTYPE_SOL].mass;
+    for (int si = 0; si < h.n_s; si++, k++) {
+        const lima_float3 x = h.sols[si].pos, xp = h.sols[si].pos_tsub1;
+        pos[k] = make_float4(wrap(x.x), wrap(x.y), wrap(x.z), host_int_as_float(LIMA_ATOMTYPE_SOL));
+        vel[k] = make_float4((float)(mimg((double)x.x - xp.x) / d.dt), (float)(mimg((double)x.y - xp.y) / d.dt),
+                             (float)(mimg((double)x.z - xp.z) / d.dt), im_sol);
+    }
+    for (int i = d.n; i < d.n_pad; i++) {
+        pos[i] = make_float4(0, 0, 0, host_int_as_float(0));
+        vel[i] = make_float4(0, 0, 0, 0);
+    }
+    for (int i = 0; i < d.n_pad; i++) ident[i] = i < d.n ? i : 0xffffffffu;
+    cudaMemcpyAsync(d.pos[cur], pos.data(), sizeof(float4) * d.n_pad, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d.vel, vel.data(), sizeof(float4) * d.n_pad, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d.posc, zero.data(), sizeof(float4) * d.n_pad, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d.velc, zero.data(), sizeof(float4) * d.n_pad, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d.orig_of_sorted, ident.data(), sizeof(uint32_t) * d.n_pad, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d.sorted_of_orig, ident.data(), sizeof(uint32_t) * d.n, cudaMemcpyHostToDevice, s);
+    set_device_float(d.lambda, 1.f, s);
+    cudaStreamSynchronize(s);
+}
+
+void phys_rebuild(PhysDev& d, int cur, cudaStream_t s) {
+    const size_t ncell = (size_t)d.m * d.m * d.m;
+    const bool mixed = d.precision == LIMA_PRECISION_MIXED;
+    launch_keys(d, cur, s);
+    size_t bytes = d.sort_tmp_bytes;
+    int end_bit = 6;
+    while ((1ull << end_bit) < (unsigned long long)ncell * 64ull) end_bit++;
+    cub::DeviceRadixSort::SortPairs(d.sort_tmp, bytes, d.keys[0], d.keys[1], d.vals[0], d.vals[1], d.n, 0, end_bit, s);
+    cudaMemsetAsync(d.cstart, 0, sizeof(uint32_t) * ncell, s);
+    cudaMemsetAsync(d.cend, 0, sizeof(uint32_t) * ncell, s);
+    launch_permute(d, cur, mixed, s);
+    cudaMemcpyAsync(d.pos[cur], d.pos_tmp, sizeof(float4) * d.n, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(d.vel, d.vel_tmp, sizeof(float4) * d.n, cudaMemcpyDeviceToDevice, s);
+    if (mixed) {
+        cudaMemcpyAsync(d.posc, d.posc_tmp, sizeof(float4) * d.n, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(d.velc, d.velc_tmp, sizeof(float4) * d.n, cudaMemcpyDeviceToDevice, s);
+    }
+    cudaMemcpyAsync(d.orig_of_sorted, d.orig_tmp, sizeof(uint32_t) * d.n, cudaMemcpyDeviceToDevice, s);
+    launch_build_list(d, cur, s);
+}
+
+void phys_prime(PhysDev&, int, cudaStream_t) {}
+
+void phys_step_kernels(const PhysDev& d, int cur, cudaStream_t s, bool energy) {
+    launch_bonded(d, cur, energy, s);
+    launch_pair(d, cur, d.precision == LIMA_PRECISION_MIXED, energy, true, s);
+}
+
+void phys_energy_now(PhysDev& d, int cur, cudaStream_t s) {
+    launch_bonded(d, cur, true, s);
+    launch_pair(d, cur, d.precision == LIMA_PRECISION_MIXED, true, false, s);
+}
+
+namespace {
+struct Snapshot {
+    std::vector<float4> pos, posc, vel, velc, force;
+    std::vector<uint32_t> orig;
+};
+Snapshot snapshot(const PhysDev& d, int cur, bool want_force) {
+    Snapshot sn;
+    sn.pos.resize(d.n);
+    sn.vel.resize(d.n);
+    sn.orig.resize(d.n);
+    cudaMemcpy(sn.pos.data(), d.pos[cur], sizeof(float4) * d.n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(sn.vel.data(), d.vel, sizeof(float4) * d.n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(sn.orig.data(), d.orig_of_sorted, sizeof(uint32_t) * d.n, cudaMemcpyDeviceToHost);
+    if (d.precision == LIMA_PRECISION_MIXED) {
+        sn.posc.resize(d.n);
+        sn.velc.resize(d.n);
+        cudaMemcpy(sn.posc.data(), d.posc, sizeof(float4) * d.n, cudaMemcpyDeviceToHost);
+        cudaMemcpy(sn.velc.data(), d.velc, sizeof(float4) * d.n, cudaMemcpyDeviceToHost);
+    }
+    if (want_force) {
+        sn.force.resize(d.n);
+        cudaMemcpy(sn.force.data(), d.force, sizeof(float4) * d.n, cudaMemcpyDeviceToHost);
+    }
+    return sn;
+}
+// per orig id: position (hi + lo) and previous position x - v dt
+void orig_state(const PhysDev& d, const Snapshot& sn, std::vector<double>& x, std::vector<double>& xp) {
+    x.assign(3 * (size_t)d.n, 0.0);
+    xp.assign(3 * (size_t)d.n, 0.0);
+    const bool mixed = !sn.posc.empty();
+    for (int k = 0; k < d.n; k++) {
+        const uint32_t o = sn.orig[k];
+        const float4 p = sn.pos[k], v = sn.vel[k];
+        double px = p.x, py = p.y, pz = p.z, vx = v.x, vy = v.y, vz = v.z;
+        if (mixed) {
+            px += sn.posc[k].x; py += sn.posc[k].y; pz += sn.posc[k].z;
+            vx += sn.velc[k].x; vy += sn.velc[k].y; vz += sn.velc[k].z;
+        }
+        x[3 * o] = px; x[3 * o + 1] = py; x[3 * o + 2] = pz;
+        xp[3 * o] = px - vx * d.dt; xp[3 * o + 1] = py - vy * d.dt; xp[3 * o + 2] = pz - vz * d.dt;
+    }
+}
+}  // namespace
+
+// compound positions in the reference's convention: particle 0 in the box,
+// the others as the image nearest to it (Engine.cu:993-996)
+void phys_read_compounds(const PhysDev& d, int cur, const lima_compound* comps, float4* pos_out, float4* prev_out) {
+    Snapshot sn = snapshot(d, cur, false);
+    std::vector<double> x, xp;
+    orig_state(d, sn, x, xp);
+    const double L = d.L;
+    int o = 0;
+    for (int c = 0; c < d.n_c; c++) {
+        const int n = comps[c].n_particles;
+        const double* p0 = &x[3 * (size_t)o];
+        for (int t = 0; t < n; t++) {
+            const double* pt = &x[3 * (size_t)(o + t)];
+            const double* qt = &xp[3 * (size_t)(o + t)];
+            double q[3], r[3];
+            for (int k = 0; k < 3; k++) {
+                double dd = pt[k] - p0[k];
+                dd -= L * std::nearbyint(dd / L);
+                q[k] = t == 0 ? pt[k] : p0[k] + dd;
+                r[k] = q[k] - (pt[k] - qt[k]);
+            }
+            pos_out[c * 64 + t] = make_float4((float)q[0], (float)q[1], (float)q[2], 0.f);
+            prev_out[c * 64 + t] = make_float4((float)r[0], (float)r[1], (float)r[2], 0.f);
+        }
+        o += n;
+    }
+}
+
+void phys_read_solvents(const PhysDev& d, int cur, float4* pos_out, float4* prev_out) {
+    Snapshot sn = snapshot(d, cur, false);
+    std::vector<double> x, xp;
+    orig_state(d, sn, x, xp);
+    for (int si = 0; si < d.n_s; si++) {
+        const size_t o = 3 * (size_t)(d.n_cp + si);
+        pos_out[si] = make_float4((float)x[o], (float)x[o + 1], (float)x[o + 2], 0.f);
+        prev_out[si] = make_float4((float)xp[o], (float)xp[o + 1], (float)xp[o + 2], 0.f);
+    }
+}
+
+void phys_read_forces(const PhysDev& d, const lima_compound* comps, float4* fc, float4* fs) {
+    Snapshot sn = snapshot(d, 0, true);
+    std::vector<float4> by_orig(d.n);
+    for (int k = 0; k < d.n; k++) by_orig[sn.orig[k]] = sn.force[k];
+    int o = 0;
+    for (int c = 0; c < d.n_c; c++) {
+        for (int t = 0; t < 64; t++) fc[c * 64 + t] = make_float4(0, 0, 0, 0);
+        for (int t = 0; t < comps[c].n_particles; t++) fc[c * 64 + t] = by_orig[o + t];
+        o += comps[c].n_particles;
+    }
+    for (int si = 0; si < d.n_s; si++) fs[si] = by_orig[d.n_cp + si];
+}
+
+void phys_read_energies(const PhysDev& d, double* totals, double* per_particle, const lima_compound* comps, int n_c,
+                        int n_s) {
+    if (totals) cudaMemcpy(totals, d.e_last, sizeof(double) * LIMA_E_COUNT, cudaMemcpyDeviceToHost);
+    if (per_particle) {
+        Snapshot sn = snapshot(d, 0, true);
+        std::vector<double> by_orig(d.n);
+        for (int k = 0; k < d.n; k++) by_orig[sn.orig[k]] = sn.force[k].w;
+        std::memset(per_particle, 0, sizeof(double) * ((size_t)n_c * 64 + n_s));
+        int o = 0;
+        for (int c = 0; c < n_c; c++) {
+            for (int t = 0; t < comps[c].n_particles; t++) per_particle[c * 64 + t] = by_orig[o + t];
+            o += comps[c].n_particles;
+        }
+        for (int si = 0; si < n_s; si++) per_particle[(size_t)n_c * 64 + si] = by_orig[d.n_cp + si];
+    }
+}
+
+}  // namespace lima

@@ -23,6 +23,7 @@ enum : int {
     ERR_BIT_NAN = 8,
     ERR_BIT_CRITICAL_FORCE = 16,
     ERR_BIT_PHYS_LIST_OVERFLOW = 32,
+    ERR_BIT_LIST_STALE = 64,      // a particle moved more than skin/2 since the last list build
 };
 
 struct RefDev {
@@ -57,6 +58,11 @@ struct RefDev {
     // reference thermostat (Engine::getBoxTemperature) scratch
     float4* csnap; float4* ssnap;   // positions two steps back
     double* ke_accum;               // [1]
+    // per compound particle, the bonded-term results it receives, in the
+    // order the reference accumulates them (bonds, then angles, then
+    // dihedrals, each by term index): CSR rows c*65+t, codes
+    // (kind << 14) | (term << 2) | slot, kind 0 bond, 1 angle, 2 dihedral
+    uint32_t* bt_off; uint16_t* bt_code;
 };
 
 // nlist_reference.cu

@@ -122,18 +122,18 @@ def _lib_builder():
     lib = load_library()
     fn = lib.lima_builder_pack_spheres
     fn.restype = ctypes.c_long
-    fn.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+    fn.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                    ctypes.c_ulonglong, ctypes.c_int, ctypes.c_void_p]
     return fn
 
 
-def _grow_chain(rng, n, spec: ChainSpec, box, placed, min_sep, max_tries=200):
+def _grow_chain(rng, n, spec: ChainSpec, box, placed, min_sep, sig, placed_sig, max_tries=200):
     """Self-avoiding chain with fixed bond length and bond angle and a uniform
     random dihedral; non-bonded beads (|i-j| >= 4, and beads of earlier
-    chains) stay >= min_sep apart under the minimum image."""
+    chains) stay at least max(min_sep, 0.95 sigma_ij) apart under the
+    minimum image (sig: per-bead sigma of this chain)."""
     theta = math.radians(spec.angle_theta0_deg)
     b = spec.bond_r0
-    d2 = min_sep * min_sep
     for _attempt in range(1000):
         pts = np.zeros((n, 3))
         pts[0] = rng.uniform(0, box, 3)
@@ -163,13 +163,16 @@ def _grow_chain(rng, n, spec: ChainSpec, box, placed, min_sep, max_tries=200):
                                       b * math.sin(theta) * math.sin(phi)])
                     cand = c_ + d_loc[0] * bc + d_loc[1] * m + d_loc[2] * nrm
                 others = [pts[: max(0, i - 3)]]
+                osig = [sig[: max(0, i - 3)]]
                 if placed is not None and len(placed):
                     others.append(placed)
-                oth = np.concatenate(others) if others else np.zeros((0, 3))
+                    osig.append(placed_sig)
+                oth = np.concatenate(others)
                 if len(oth):
                     d = oth - cand
                     d -= box * np.round(d / box)
-                    if np.min(np.einsum("ij,ij->i", d, d)) < d2:
+                    lim = np.maximum(min_sep, 0.95 * 0.5 * (np.concatenate(osig) + sig[i]))
+                    if np.any(np.einsum("ij,ij->i", d, d) < lim * lim):
                         continue
                 pts[i] = cand
                 break
@@ -220,16 +223,23 @@ def make_system(name_or_spec, seed: int = 2024) -> System:
             pp[1 + t] = (cs.mass, sig[t], eps[t])
 
     # ---- chains --------------------------------------------------------
+    # Rejection distance between two particles: the workload's 0.28 nm, or
+    # 0.95 of the pair's Lorentz-Berthelot sigma where that is larger (chain
+    # types go up to sigma 0.40 nm; a contact at 0.28 nm would start the
+    # dynamics with ~1e7 J/(mol nm) forces).
     chain_pts = []
     chain_types = []
     placed = np.zeros((0, 3))
+    placed_sig = np.zeros(0)
+    sig_of = pp["sigma"].astype(np.float64)
     if cs is not None:
         for _c in range(cs.n_chains):
+            types = rng.integers(1, 1 + cs.n_types, cs.chain_len)
             # the reference keeps every compound particle at the image nearest
             # its particle 0 (Engine.cu:996), which needs the box to exceed
             # twice a compound's extent (Constants.cuh:35): regrow otherwise
             for _try in range(200):
-                pts = _grow_chain(rng, cs.chain_len, cs, box, placed, spec.min_sep)
+                pts = _grow_chain(rng, cs.chain_len, cs, box, placed, spec.min_sep, sig_of[types], placed_sig)
                 ext = max(np.linalg.norm(pts[k:k + cs.compound_size] - pts[k], axis=1).max()
                           for k in range(0, cs.chain_len, cs.compound_size))
                 if ext < 0.45 * box:
@@ -237,15 +247,18 @@ def make_system(name_or_spec, seed: int = 2024) -> System:
             else:
                 raise RuntimeError("could not grow a chain that fits the reference's compound convention")
             chain_pts.append(pts)
-            chain_types.append(rng.integers(1, 1 + cs.n_types, cs.chain_len))
+            chain_types.append(types)
             placed = np.concatenate([placed, pts])
+            placed_sig = np.concatenate([placed_sig, sig_of[types]])
     fixed = np.mod(placed, box) if len(placed) else np.zeros((0, 3))
+    fixed_rmin = np.maximum(spec.min_sep, 0.95 * 0.5 * (placed_sig + spec.solvent_sigma))
 
     # ---- solvents --------------------------------------------------------
     out = np.zeros((spec.n_solvents, 3))
     pack = _lib_builder()
     fixed_c = np.ascontiguousarray(fixed, dtype=np.float64)
-    acc = pack(box, spec.min_sep, fixed_c.ctypes.data, len(fixed_c), spec.n_solvents,
+    fixed_r = np.ascontiguousarray(fixed_rmin if len(fixed_rmin) else np.zeros(1), dtype=np.float64)
+    acc = pack(box, spec.min_sep, fixed_c.ctypes.data, fixed_r.ctypes.data, len(fixed_c), spec.n_solvents,
                int(rng.integers(0, 2**63)), spec.mc_sweeps, out.ctypes.data)
     if acc < 0:
         raise RuntimeError("solvent packing failed")
