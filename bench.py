@@ -1,0 +1,400 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 LIMA_MD step path.
+
+Workload: the 32,024-particle solvated-chain box (16 chains x 64 particles in
+31,000 single-site solvents, 10 nm periodic box, 1.2 nm cutoff, Berendsen
+300 K, dt 2 fs), seeded synthetic input.  One "step" is one MD step (forces,
+integration, thermostat; a list rebuild every 10 steps).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line.  value = simulated ns/day of the whole job (N
+independent replicas under torchrun, one per GPU; device time, max over
+ranks), L2 flushed before every timed step.  e2e = the same metric through the
+public API from host arrays (box upload, K steps with per-step FP64 energy
+readback, final positions).  --impl reference runs the reference's own step
+code (oracle/_ref: Engine.cu built for the host) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = "solvated_chains_32k"
+NS_PER_DAY_S = 86400.0   # seconds per day
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12   # clock-derived FP32 FMA peak (no measured figure)
+FLOP_PER_PAIR = 32       # per unique pair within the cutoff (minimum image, r^2, rcp, LJ, force, both sides)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=40)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--cpu-sample-steps", type=int, default=2)
+    ap.add_argument("--mode", default="full", choices=["full", "kernels"],
+                    help="kernels: only warm-up + K plain-FP32 steps (the command profiled with ncu)")
+    ap.add_argument("--semantics", default="physics", choices=["physics", "reference"],
+                    help="semantics of --mode kernels")
+    return ap.parse_args()
+
+
+def run_kernels_only(args):
+    """The profiled command: W + K steps of one engine, nothing else."""
+    import torch
+    from quantom_b200 import engine as E
+    from quantom_b200 import systems as S
+    spec = S.CONFIGS[args.workload]
+    system = S.make_system(args.workload, seed=args.seed)
+    if args.semantics == "physics":
+        p = physics_params(E, spec, E.PRECISION_FP32, None, 0)
+    else:
+        p = E.default_params(box_len=spec.box_len, cutoff=spec.cutoff, dt=spec.dt)
+    with E.Engine(system, p) as eng:
+        eng.step(max(3, args.warmup))
+        eng.synchronize()
+        eng.step(args.steps)
+        eng.synchronize()
+        print(json.dumps({"mode": "kernels", "semantics": args.semantics, "steps": args.steps,
+                          "ms_per_step_unflushed": eng.last_step_ms() / max(1, args.steps)}), flush=True)
+
+
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        import torch
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return ws, rank, local, pg
+
+
+def max_over_ranks(x, pg, device):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        self.f.close()
+
+    def summary(self):
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax = max(smax, float(parts[2]))
+                except ValueError:
+                    continue
+                for k, nm in enumerate(names):
+                    if parts[5 + k].lower().startswith("active"):
+                        reasons.add(nm)
+        finally:
+            os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        return {}
+
+
+def ncu_traffic(kernel, workload):
+    """dram bytes per launch from the committed ncu summary, if present."""
+    p = ROOT / "profiles" / f"ncu_{kernel}_{workload}.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.strip().startswith("dram_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def physics_params(E, spec, precision, stream_handle=None, device=0):
+    p = E.default_params(box_len=spec.box_len, cutoff=spec.cutoff, dt=spec.dt, semantics=E.SEMANTICS_PHYSICS,
+                         precision=precision, skin=0.1, switch_on=1.0, nlist_period=10, t_target=spec.temperature,
+                         tau_t=spec.tau_t, device=device)
+    p.thermostat = E.THERMOSTAT_BERENDSEN if spec.thermostat == "berendsen" else E.THERMOSTAT_NONE
+    if stream_handle is not None:
+        p.stream = stream_handle
+    return p
+
+
+def timed_steps(eng, stream, n, flush):
+    """Device time of n steps, L2 flushed (untimed) before each."""
+    import torch
+    evs = []
+    for _ in range(n):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        eng.step(1)
+        b.record(stream)
+        evs.append((a, b))
+    stream.synchronize()
+    eng.synchronize()
+    return sum(a.elapsed_time(b) for a, b in evs)   # ms
+
+
+def ns_per_day(dt_ns, ms_per_step):
+    return dt_ns * NS_PER_DAY_S / (ms_per_step * 1e-3)
+
+
+# --------------------------------------------------------------- CPU side --
+def cpu_reference_rate(system, steps, threads):
+    """Seconds per step of the reference's own step code on the host cores
+    (oracle/_ref: Engine.cu kernels + host neighbour list), with its list
+    update (every 200 steps, Constants.cuh:71) amortised."""
+    from oracle import pyoracle as po
+    if po.ref_available():
+        ref = po.RefEngine(system, n_threads=threads)
+        t0 = time.perf_counter()
+        ref.update_nlists()
+        t_nl = time.perf_counter() - t0
+        ref.step(1)   # warm
+        t0 = time.perf_counter()
+        ref.step(steps)
+        t_step = (time.perf_counter() - t0) / steps
+        ref.close()
+        kind, used = "reference", threads
+    else:   # the C restatement of the same path, single-threaded
+        t0 = time.perf_counter()
+        lists = po.ref_nlist(system, cells=False, ss_cap=1024)
+        t_nl = time.perf_counter() - t0
+        s = system
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            s, _, _, _ = po.ref_step(s, lists)
+        t_step = (time.perf_counter() - t0) / steps
+        kind, used = "port", 1
+    return t_step + t_nl / 200.0, t_step, t_nl, kind, used
+
+
+def run_reference_arm(args, ws, rank):
+    if rank != 0:
+        return
+    from quantom_b200 import systems as S
+    spec = S.CONFIGS[args.workload]
+    system = S.make_system(args.workload, seed=args.seed)
+    threads = os.cpu_count() or 1
+    budget_steps = max(1, min(args.steps, 6))
+    per_step, t_step, t_nl, kind, used = cpu_reference_rate(system, budget_steps, threads)
+    v = ns_per_day(spec.dt, per_step * 1e3)
+    sample = (f"{budget_steps} reference steps of the {system.n_particles}-particle box on {used} host threads "
+              f"(+ one neighbour-list update, {t_nl:.2f} s, amortised over its 200-step period)")
+    print(json.dumps({
+        "impl": "reference", "metric": f"ns/day, {args.workload}", "value": v, "unit": "ns/day", "n_gpus": ws,
+        "steps": budget_steps, "warmup": 1, "ms_per_step": per_step * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": args.workload, "particles": system.n_particles, "semantics": "reference",
+                   "dt_fs": spec.dt * 1e6},
+        "cpu_baseline": {"value": v, "unit": "ns/day", "cores": used, "kind": kind, "sample": sample},
+        "e2e": {"value": v, "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+# ------------------------------------------------------------------ ours --
+def run_ours(args, ws, rank, local, pg):
+    import torch
+    from quantom_b200 import engine as E
+    from quantom_b200 import systems as S
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    spec = S.CONFIGS[args.workload]
+    system = S.make_system(args.workload, seed=args.seed + rank)
+    n = system.n_particles
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # > 126 MB L2
+
+    # ---- plain FP32 physics path (headline) -----------------------------
+    eng = E.Engine(system, physics_params(E, spec, E.PRECISION_FP32, stream.cuda_stream, local))
+    timed_steps(eng, stream, max(3, args.warmup), flush)
+    barrier(pg)
+    launches0 = eng.kernel_launches()
+    with ClockSampler(local) as clk:
+        ms = timed_steps(eng, stream, args.steps, flush)
+    launches = eng.kernel_launches() - launches0
+    ms_step = max_over_ranks(ms / args.steps, pg, dev)
+    clocks = clk.summary()
+    prof = eng.profile_steps(50)
+    eng.close()
+
+    # ---- mixed precision, same protocol ------------------------------------
+    engm = E.Engine(system, physics_params(E, spec, E.PRECISION_MIXED, stream.cuda_stream, local))
+    timed_steps(engm, stream, max(3, args.warmup // 2), flush)
+    ms_mixed = timed_steps(engm, stream, max(50, args.steps // 2), flush) / max(50, args.steps // 2)
+    prof_m = engm.profile_steps(50)
+    engm.close()
+
+    # ---- the reference's own semantics on the GPU, same workload ------------
+    pr = E.default_params(box_len=spec.box_len, cutoff=spec.cutoff, dt=spec.dt, device=local)
+    pr.stream = stream.cuda_stream
+    engr = E.Engine(system, pr)
+    timed_steps(engr, stream, 5, flush)
+    ms_ref_sem = timed_steps(engr, stream, 50, flush) / 50
+    engr.close()
+
+    # ---- end to end through the public API from host arrays -----------------
+    torch.cuda.synchronize(dev)
+    barrier(pg)
+    t0 = time.perf_counter()
+    e2e = E.Engine(system, physics_params(E, spec, E.PRECISION_FP32, None, local))
+    h2d = (system.compounds.nbytes + system.states.nbytes + system.solvents.nbytes + system.bridges.nbytes +
+           system.forcefield.nbytes)
+    d2h = 0
+    for _ in range(args.steps):
+        e2e.step(1)
+        tot = e2e.energies()
+        d2h += tot.nbytes
+    st, prev = e2e.compound_states()
+    sol = e2e.solvents()
+    d2h += st.nbytes + prev.nbytes + sol.nbytes
+    e2e.close()
+    t_e2e = max_over_ranks(time.perf_counter() - t0, pg, dev)
+
+    if rank != 0:
+        return
+    # ---- roofline of the dominant kernel (pair + integrate) -----------------
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs")
+    peak_src = "measured (MEASURED_PEAKS.json)"
+    if not hbm:
+        hbm, peak_src = 6650.0, "fallback"
+    rho = n / spec.box_len ** 3
+    pairs = n * (4.0 / 3.0) * math.pi * spec.cutoff ** 3 * rho / 2.0
+    t_pair = prof["pair"] * 1e-3
+    bytes_pair = n * 80.0      # read pos, vel; write pos, vel, force (16 B each)
+    flops_pair = pairs * FLOP_PER_PAIR
+    achieved = bytes_pair / t_pair / 1e9
+    traffic = ncu_traffic("k_pair_integrate", args.workload)
+    cpu = None
+    if ws == 1:
+        per_step, t_step, t_nl, kind, used = cpu_reference_rate(system, args.cpu_sample_steps, os.cpu_count() or 1)
+        cpu = {"value": ns_per_day(spec.dt, per_step * 1e3), "unit": "ns/day", "cores": used, "kind": kind,
+               "sample": f"{args.cpu_sample_steps} steps of the same {n}-particle box through the reference's own "
+                         f"Engine.cu step code (reference semantics) on {used} host threads, plus one neighbour-list "
+                         f"update ({t_nl:.2f} s) amortised over its 200-step period"}
+    value = ws * ns_per_day(spec.dt, ms_step)
+    out = {
+        "metric": f"ns/day, {args.workload} (32k particles)", "value": value, "unit": "ns/day", "n_gpus": ws,
+        "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": f"{args.workload}: 16 chains x 64 + 31,000 solvents, 10 nm box, rc 1.2 nm "
+                               f"(switch from 1.0), skin 0.1 nm, list every 10 steps, Berendsen 300 K tau 0.1 ps, "
+                               f"dt 2 fs, plain FP32", "particles": n,
+                   "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+                   "l2": "flushed before every timed step (256 MiB memset on the engine stream, outside the timed "
+                         "events)"},
+        "mixed": {"ms_per_step": ms_mixed, "ratio_to_fp32": ms_mixed / ms_step,
+                  "ns_per_day": ns_per_day(spec.dt, ms_mixed), "kernels_ms": prof_m},
+        "reference_semantics_gpu": {"ms_per_step": ms_ref_sem, "ns_per_day": ns_per_day(spec.dt, ms_ref_sem)},
+        "kernels_ms": prof,
+        "roofline": {"kernel": "k_pair_integrate", "bound": "hbm", "achieved": achieved, "peak": hbm,
+                     "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic, "peak_source": peak_src,
+                     "algorithmic_bytes_per_launch": bytes_pair, "algorithmic_flops_per_launch": flops_pair,
+                     "fp32": {"achieved_tflops": flops_pair / t_pair / 1e12, "peak_tflops": FP32_NOMINAL_TFLOPS,
+                              "frac": flops_pair / t_pair / 1e12 / FP32_NOMINAL_TFLOPS,
+                              "peak_source": "nominal 148 SMs x 128 lanes x 2 x 1.965 GHz"}},
+        "e2e": {"value": ws * ns_per_day(spec.dt, t_e2e * 1e3 / args.steps), "unit": "ns/day",
+                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+                "note": "box uploaded from host arrays inside the timed region; per-step FP64 energies read back"},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if cpu:
+        out["cpu_baseline"] = cpu
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    if args.mode == "kernels":
+        run_kernels_only(args)
+        return
+    ws, rank, local, pg = dist_setup(args) if args.impl == "ours" else (int(os.environ.get("WORLD_SIZE", "1")),
+                                                                        int(os.environ.get("RANK", "0")), 0, None)
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, ws, rank)
+        else:
+            run_ours(args, ws, rank, local, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

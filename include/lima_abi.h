@@ -247,6 +247,21 @@ lima_status lima_get_step(lima_ctx* ctx, uint64_t* step);
    stream) — the reference's Engine::timings (Engine.cu:448-450). */
 lima_status lima_get_last_step_ms(lima_ctx* ctx, float* ms);
 
+/* Per-kernel device time: runs n_steps (no graph) with CUDA events around
+   each kernel group on the engine's stream and writes the mean ms per step
+   into ms[LIMA_PROF_COUNT].  Groups: physics — neighbour rebuild (sort,
+   permute, list), bonded terms, pair+integrate; reference — rebuild,
+   bridges, compound<-solvent chunks + compound kernel, solvent kernel.
+   The reference's Engine::timings splits force/copy/list time
+   (Engine.cu:49-75, 400-451). */
+enum { LIMA_PROF_TOTAL = 0, LIMA_PROF_NLIST = 1, LIMA_PROF_BONDED = 2, LIMA_PROF_PAIR = 3, LIMA_PROF_COMPOUND = 4,
+       LIMA_PROF_COUNT = 5 };
+lima_status lima_profile_steps(lima_ctx* ctx, int n_steps, float* ms);
+
+/* Number of kernels of this library the context has launched so far
+   (graph replays count the kernels they contain). */
+lima_status lima_get_kernel_launches(lima_ctx* ctx, uint64_t* count);
+
 #ifdef __cplusplus
 }
 #endif

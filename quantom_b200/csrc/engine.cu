@@ -66,6 +66,8 @@ struct lima_ctx {
     bool timed = false;
     bool lambda_pending_reset = false;
     float ref_temperature = 0.f;
+    uint64_t launches = 0;     // kernels of this library launched by this context
+    int graph_kernels = 0;     // kernels in one replay of a step graph
 
     template <typename T>
     T* dalloc(size_t n) {
@@ -304,8 +306,10 @@ void capture_graphs(lima_ctx* c, void (*launch)(lima_ctx*, int)) {
     }
 }
 
-void ref_launch_step(lima_ctx* c, int parity) { lima::ref_step_kernels(c->ref, parity, c->stream); }
-void phys_launch_step(lima_ctx* c, int parity) { lima::phys_step_kernels(c->phys, parity, c->stream); }
+void ref_launch_step(lima_ctx* c, int parity) { c->graph_kernels = lima::ref_step_kernels(c->ref, parity, c->stream); }
+void phys_launch_step(lima_ctx* c, int parity) {
+    c->graph_kernels = lima::phys_step_kernels(c->phys, parity, c->stream);
+}
 
 void check_device_errors(lima_ctx* c) {
     int* err_ptr = c->p.semantics == LIMA_SEMANTICS_REFERENCE ? c->ref.err : c->phys.err;
@@ -323,6 +327,7 @@ void check_device_errors(lima_ctx* c) {
         if (h & lima::ERR_BIT_LIST_STALE)
             m += "pair list went stale: a particle moved more than skin/2 between rebuilds (raise skin or lower "
                  "nlist_period); ";
+        if (h & lima::ERR_BIT_TILE_TIMEOUT) m += "shared-memory staging wait timed out; ";
         if (h & lima::ERR_BIT_NAN) m += "NaN position; ";
         if (h & lima::ERR_BIT_CRITICAL_FORCE) m += "critical force (|F| > 2e12); ";
         const bool cap = h & (lima::ERR_BIT_SS_OVERFLOW | lima::ERR_BIT_CS_OVERFLOW | lima::ERR_BIT_CC_OVERFLOW |
@@ -339,32 +344,65 @@ void sync_checked(lima_ctx* c) {
 
 void ref_nlist_now(lima_ctx* c) {
     lima::ref_build_nlists(c->ref, c->cur, c->stream);
+    c->launches += (c->ref.n_s > 0 ? 4 : 0) + (c->ref.n_c > 0 ? (c->ref.n_s > 0 ? 2 : 1) : 0);
     c->last_nlist_step = c->step;
 }
 
-void ref_one_step(lima_ctx* c) {
-    lima::RefDev& d = c->ref;
+// One step.  prof (nullable): [0] before any list rebuild, [1] after it, then
+// the four per-kernel-group events of ref_step_kernels / phys_step_kernels;
+// with prof the step is launched directly instead of through the graph.
+void one_step(lima_ctx* c, cudaEvent_t* prof) {
     const int period = std::max(1, c->p.nlist_period);
-    if (c->step > 0 && c->step - c->last_nlist_step >= static_cast<uint64_t>(period)) ref_nlist_now(c);
-    if (c->graph[c->cur])
-        cuda_ok(cudaGraphLaunch(c->graph[c->cur], c->stream), "cudaGraphLaunch");
-    else
-        ref_launch_step(c, c->cur);
-    c->cur ^= 1;
-    c->step++;
-    if (c->lambda_pending_reset) {
-        lima::set_device_float(d.lambda, 1.f, c->stream);
-        c->lambda_pending_reset = false;
-    }
-    if (c->p.thermostat == LIMA_THERMOSTAT_REFERENCE) {
-        const int tp = std::max(3, c->p.thermostat_period);
-        const uint64_t k = c->step % tp;
-        if (k == static_cast<uint64_t>(tp - 2)) lima::ref_thermostat_snapshot(d, c->cur, c->stream);
-        if (k == 0 && c->step >= 2) {
-            lima::ref_thermostat_update(d, c->cur, c->n_particles_total, static_cast<float>(c->p.t_target),
-                                        c->step > 20, c->stream);
-            c->lambda_pending_reset = true;   // applied for one step (Engine.cu:67-69)
+    const bool rebuild = c->step > 0 && c->step - c->last_nlist_step >= static_cast<uint64_t>(period);
+    if (prof) cuda_ok(cudaEventRecord(prof[0], c->stream), "cudaEventRecord");
+    if (c->p.semantics == LIMA_SEMANTICS_REFERENCE) {
+        lima::RefDev& d = c->ref;
+        if (rebuild) ref_nlist_now(c);
+        if (prof) cuda_ok(cudaEventRecord(prof[1], c->stream), "cudaEventRecord");
+        if (c->graph[c->cur] && !prof) {
+            cuda_ok(cudaGraphLaunch(c->graph[c->cur], c->stream), "cudaGraphLaunch");
+            c->launches += c->graph_kernels;
+        } else {
+            c->launches += lima::ref_step_kernels(d, c->cur, c->stream, prof ? prof + 2 : nullptr);
         }
+        c->cur ^= 1;
+        c->step++;
+        if (c->lambda_pending_reset) {
+            lima::set_device_float(d.lambda, 1.f, c->stream);
+            c->launches++;
+            c->lambda_pending_reset = false;
+        }
+        if (c->p.thermostat == LIMA_THERMOSTAT_REFERENCE) {
+            const int tp = std::max(3, c->p.thermostat_period);
+            const uint64_t k = c->step % tp;
+            if (k == static_cast<uint64_t>(tp - 2)) {
+                lima::ref_thermostat_snapshot(d, c->cur, c->stream);
+                c->launches++;
+            }
+            if (k == 0 && c->step >= 2) {
+                lima::ref_thermostat_update(d, c->cur, c->n_particles_total, static_cast<float>(c->p.t_target),
+                                            c->step > 20, c->stream);
+                c->launches += 2;
+                c->lambda_pending_reset = true;   // applied for one step (Engine.cu:67-69)
+            }
+        }
+    } else {
+        if (rebuild) {
+            lima::phys_rebuild(c->phys, c->cur, c->stream);
+            c->launches += 3;
+            c->last_nlist_step = c->step;
+        }
+        if (prof) cuda_ok(cudaEventRecord(prof[1], c->stream), "cudaEventRecord");
+        const bool energy = c->p.energy_period > 0 && (c->step % c->p.energy_period) == 0;
+        if (energy || !c->graph[c->cur] || prof) {
+            c->launches += lima::phys_step_kernels(c->phys, c->cur, c->stream, energy, prof ? prof + 2 : nullptr);
+            if (prof) cuda_ok(cudaEventRecord(prof[5], c->stream), "cudaEventRecord");
+        } else {
+            cuda_ok(cudaGraphLaunch(c->graph[c->cur], c->stream), "cudaGraphLaunch");
+            c->launches += c->graph_kernels;
+        }
+        c->cur ^= 1;
+        c->step++;
     }
 }
 
@@ -527,28 +565,58 @@ lima_status lima_step(lima_ctx* c, int n_steps) {
         need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
         need(n_steps >= 0, LIMA_ERR_ARGUMENT, "negative step count");
         cuda_ok(cudaEventRecord(c->ev0, c->stream), "cudaEventRecord");
-        for (int i = 0; i < n_steps; i++) {
-            if (c->p.semantics == LIMA_SEMANTICS_REFERENCE) {
-                ref_one_step(c);
-            } else {
-                const int period = std::max(1, c->p.nlist_period);
-                if (c->step > 0 && c->step - c->last_nlist_step >= static_cast<uint64_t>(period)) {
-                    lima::phys_rebuild(c->phys, c->cur, c->stream);
-                    c->last_nlist_step = c->step;
-                }
-                const bool energy = c->p.energy_period > 0 && (c->step % c->p.energy_period) == 0;
-                if (energy || !c->graph[c->cur]) {
-                    lima::phys_step_kernels(c->phys, c->cur, c->stream, energy);
-                } else {
-                    cuda_ok(cudaGraphLaunch(c->graph[c->cur], c->stream), "cudaGraphLaunch");
-                }
-                c->cur ^= 1;
-                c->step++;
-            }
-        }
+        for (int i = 0; i < n_steps; i++) one_step(c, nullptr);
         cuda_ok(cudaEventRecord(c->ev1, c->stream), "cudaEventRecord");
         cuda_ok(cudaGetLastError(), "kernel launch");
         c->timed = true;
+    });
+}
+
+lima_status lima_profile_steps(lima_ctx* c, int n_steps, float* ms) {
+    return guarded(c, [&] {
+        need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
+        need(n_steps > 0 && ms != nullptr, LIMA_ERR_ARGUMENT, "need n_steps > 0 and an output array");
+        cudaEvent_t ev[6];
+        for (auto& e : ev) cuda_ok(cudaEventCreate(&e), "cudaEventCreate");
+        double acc[LIMA_PROF_COUNT] = {0, 0, 0, 0, 0};
+        lima_status st = LIMA_OK;
+        std::string msg;
+        try {
+            for (int i = 0; i < n_steps; i++) {
+                one_step(c, ev);
+                if (c->p.semantics == LIMA_SEMANTICS_REFERENCE)
+                    cuda_ok(cudaEventRecord(ev[5], c->stream), "cudaEventRecord");
+                cuda_ok(cudaEventSynchronize(ev[5]), "cudaEventSynchronize");
+                float t[5];
+                for (int k = 0; k < 5; k++) cuda_ok(cudaEventElapsedTime(&t[k], ev[k], ev[k + 1]), "cudaEventElapsedTime");
+                acc[LIMA_PROF_NLIST] += t[0];
+                if (c->p.semantics == LIMA_SEMANTICS_REFERENCE) {
+                    acc[LIMA_PROF_BONDED] += t[2];     // bridges
+                    acc[LIMA_PROF_COMPOUND] += t[3];   // compound<-solvent chunks + compound kernel
+                    acc[LIMA_PROF_PAIR] += t[4];       // solvent kernel
+                } else {
+                    acc[LIMA_PROF_BONDED] += t[2];
+                    acc[LIMA_PROF_PAIR] += t[3];       // pair + integrate
+                }
+                float tot = 0.f;
+                cuda_ok(cudaEventElapsedTime(&tot, ev[0], ev[5]), "cudaEventElapsedTime");
+                acc[LIMA_PROF_TOTAL] += tot;
+            }
+        } catch (const LimaFail& e) {
+            st = e.st;
+            msg = e.msg;
+        }
+        for (auto& e : ev) cudaEventDestroy(e);
+        if (st != LIMA_OK) fail(st, msg);
+        for (int k = 0; k < LIMA_PROF_COUNT; k++) ms[k] = static_cast<float>(acc[k] / n_steps);
+        sync_checked(c);
+    });
+}
+
+lima_status lima_get_kernel_launches(lima_ctx* c, uint64_t* count) {
+    return guarded(c, [&] {
+        need(count != nullptr, LIMA_ERR_ARGUMENT, "null count");
+        *count = c->launches;
     });
 }
 
@@ -734,6 +802,10 @@ lima_status lima_get_energies(lima_ctx* c, double* totals, double* per_particle)
                 totals[LIMA_E_TEMPERATURE] = temp;
             }
         } else {
+            if (c->step > 0) {   // fold the last step's FP64 accumulators
+                lima::phys_finalize(c->phys, c->cur, c->stream);
+                sync_checked(c);
+            }
             lima::phys_read_energies(c->phys, totals, per_particle, c->comps.data(), nc, ns);
         }
     });

@@ -5,20 +5,23 @@
 // lanes) and positions/velocities carry FP32 low parts; energy, virial and
 // kinetic-energy reductions and the thermostat scalar are FP64.
 //
+// Layout: particles sorted by cell (side >= r_list/2, x-major), so the
+// kGroup = 8 lanes of the 4 particles a warp handles share a cell and read
+// largely the same neighbours — the position gathers of a warp hit L1.
+//
 // Per step (two launches, captured in a CUDA graph):
-//   k_bonded          one thread per bonded term -> term_force slots (+ energies)
-//   k_pair_integrate  kGroup lanes per particle (slot order): each lane walks
-//                     every kGroup-th entry of the particle's Verlet list
-//                     (index loads coalesce: the list is blocked so that the
-//                     kGroup lanes of 4 consecutive particles read one 128-byte
-//                     line), partial forces are reduced with warp shuffles,
-//                     lane 0 gathers the bonded term forces, kicks and drifts
-//                     and adds 1/2 m v^2 to the FP64 accumulator; the last
-//                     block folds the accumulators into e_last and the next
-//                     Berendsen lambda.
-// Every nlist_period steps (physics_host.cu): sort by (coarse cell, 4x4x4
-// Morton sub-cell), permute, rebuild the Verlet list (k_build_list, kGroup
-// lanes per particle over the 27 coarse cells, ordered by candidate).
+//   k_bonded          one thread per bonded term -> term_force slots; block 0
+//                     also folds the previous step's FP64 accumulators into
+//                     e_last and the Berendsen lambda for this step
+//   k_pair_integrate  8 lanes per particle walk its Verlet list (blocked so
+//                     the lanes of consecutive particles read one line),
+//                     branch-free LJ + switch, partial forces reduced with
+//                     warp shuffles; lane 0 gathers the bonded term forces,
+//                     kicks, drifts and adds 1/2 m v^2 to the FP64 accumulator
+// Every nlist_period steps (physics_host.cu): sort, permute, k_build_list —
+// 8 lanes per particle over the 5x5x5 neighbouring cells, a cell skipped by
+// the whole warp when its box is beyond r_list of all 4 of the warp's
+// particles.
 #include "physdev.cuh"
 #include "physkern.cuh"
 #include "refdev.cuh"
@@ -54,23 +57,61 @@ __device__ __forceinline__ void block_add(double* acc, int idx, double v) {
     if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(&acc[idx], v);
 }
 
-__device__ __forceinline__ uint32_t spread2(uint32_t v) { return (v & 1u) | ((v & 2u) << 2); }
-
-__device__ __forceinline__ void cell_coords(const PhysDev& d, float4 p, int& cx, int& cy, int& cz, uint32_t& sub) {
+__device__ __forceinline__ void cell_xyz(const PhysDev& d, float4 p, int& cx, int& cy, int& cz) {
     const float inv = (float)d.m / d.L;
-    const float fx = p.x * inv, fy = p.y * inv, fz = p.z * inv;
-    cx = min(max((int)fx, 0), d.m - 1);
-    cy = min(max((int)fy, 0), d.m - 1);
-    cz = min(max((int)fz, 0), d.m - 1);
-    const uint32_t sx = (uint32_t)min(max((int)((fx - cx) * 4.f), 0), 3);
-    const uint32_t sy = (uint32_t)min(max((int)((fy - cy) * 4.f), 0), 3);
-    const uint32_t sz = (uint32_t)min(max((int)((fz - cz) * 4.f), 0), 3);
-    sub = (spread2(sx) << 2) | (spread2(sy) << 1) | spread2(sz);
+    cx = min(max((int)(p.x * inv), 0), d.m - 1);
+    cy = min(max((int)(p.y * inv), 0), d.m - 1);
+    cz = min(max((int)(p.z * inv), 0), d.m - 1);
 }
 
-// blocked Verlet-list address of entry k of slot i
-__device__ __forceinline__ size_t nl_addr(const PhysDev& d, int i, int k) {
-    return ((size_t)(k / kGroup) * d.n_pad + i) * kGroup + (k % kGroup);
+__device__ __forceinline__ uint32_t nl_index(const PhysDev& d, int i, int k) {
+    return ((uint32_t)(k / kGroup) * (uint32_t)d.n_pad + (uint32_t)i) * kGroup + (uint32_t)(k % kGroup);
+}
+
+__device__ __forceinline__ bool excluded(const PhysDev& d, uint32_t oi, uint32_t oj) {
+    for (uint32_t q = d.excl_off[oi]; q < d.excl_off[oi + 1]; q++)
+        if (d.excl_ids[q] == oj) return true;
+    return false;
+}
+
+// squared distance from p to the box of cell (x, y, z), periodic
+__device__ __forceinline__ float box_d2(const PhysDev& d, float4 p, int x, int y, int z) {
+    const float cs = d.L / (float)d.m;
+    auto axis = [&](float v, int c) {
+        const float lo = c * cs;
+        float dd = v - (lo + 0.5f * cs);
+        dd = mimg(dd, d.L, d.invL);
+        return fmaxf(fabsf(dd) - 0.5f * cs, 0.f);
+    };
+    const float ax = axis(p.x, x), ay = axis(p.y, y), az = axis(p.z, z);
+    return ax * ax + ay * ay + az * az;
+}
+
+// Fold an accumulator slot into e_last; parity slots also set the next
+// step's Berendsen lambda.  Idempotent: a folded slot reads zero.
+__device__ void fold(const PhysDev& d, int src) {
+    volatile double* a = d.acc + src * LIMA_E_COUNT;
+    const double kin = a[LIMA_E_KINETIC];
+    if (kin == 0.0) return;
+    const double temp = 2.0 * kin / (3.0 * (double)d.n * kR);
+    d.e_last[LIMA_E_KINETIC] = kin;
+    d.e_last[LIMA_E_TEMPERATURE] = temp;
+    if (d.acc_energy[src]) {
+        d.e_last[LIMA_E_LJ] = a[LIMA_E_LJ];
+        d.e_last[LIMA_E_BOND] = a[LIMA_E_BOND];
+        d.e_last[LIMA_E_ANGLE] = a[LIMA_E_ANGLE];
+        d.e_last[LIMA_E_DIHEDRAL] = a[LIMA_E_DIHEDRAL];
+        d.e_last[LIMA_E_VIRIAL] = a[LIMA_E_VIRIAL];
+        d.e_last[LIMA_E_TOTAL] = a[LIMA_E_LJ] + a[LIMA_E_BOND] + a[LIMA_E_ANGLE] + a[LIMA_E_DIHEDRAL] + kin;
+        d.acc_energy[src] = 0;
+    }
+    if (src < 2) {
+        float lam = 1.f;
+        if (d.thermostat == LIMA_THERMOSTAT_BERENDSEN && temp > 0.0)
+            lam = (float)sqrt(1.0 + d.dt / d.tau_t * (d.t_target / temp - 1.0));
+        d.lambda[src ^ 1] = lam;
+    }
+    for (int q = 0; q < LIMA_E_COUNT; q++) a[q] = 0.0;
 }
 
 }  // namespace
@@ -80,9 +121,8 @@ __global__ void k_keys(PhysDev d, int cur) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= d.n) return;
     int cx, cy, cz;
-    uint32_t sub;
-    cell_coords(d, d.pos[cur][i], cx, cy, cz, sub);
-    d.keys[0][i] = ((uint32_t)((cx * d.m + cy) * d.m + cz) << 6) | sub;
+    cell_xyz(d, d.pos[cur][i], cx, cy, cz);
+    d.keys[0][i] = (uint32_t)((cx * d.m + cy) * d.m + cz);
     d.vals[0][i] = i;
 }
 
@@ -101,75 +141,65 @@ __global__ void k_permute(PhysDev d, int cur, int mixed) {
     d.orig_tmp[k] = o;
     d.sorted_of_orig[o] = k;
     d.xref[k] = p;
-    const uint32_t c = d.keys[1][k] >> 6;
-    if (k == 0 || (d.keys[1][k - 1] >> 6) != c) d.cstart[c] = k;
-    if (k == d.n - 1 || (d.keys[1][k + 1] >> 6) != c) d.cend[c] = k + 1;
+    const uint32_t c = d.keys[1][k];
+    if (k == 0 || d.keys[1][k - 1] != c) d.cstart[c] = k;
+    if (k == d.n - 1 || d.keys[1][k + 1] != c) d.cend[c] = k + 1;
 }
 
-namespace {
-__device__ __forceinline__ bool excluded(const PhysDev& d, uint32_t oi, uint32_t oj) {
-    for (uint32_t q = d.excl_off[oi]; q < d.excl_off[oi + 1]; q++)
-        if (d.excl_ids[q] == oj) return true;
-    return false;
-}
-}  // namespace
-
-// kGroup lanes per particle; candidates are taken kGroup at a time in cell
-// order and compacted with a group ballot, so list order is deterministic.
+// kGroup lanes per particle.  Cells are visited in a fixed order and their
+// members kGroup at a time, compacted with a ballot, so the list order is
+// deterministic.  A cell is skipped when its box is beyond r_list of every
+// particle of the warp.
+// One thread per particle, no warp collectives: the thread appends its
+// neighbours in cell order (so the list order is deterministic) into the
+// blocked layout the pair kernel reads.
 __global__ void __launch_bounds__(kTB) k_build_list(PhysDev d, int cur) {
-    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = gtid / kGroup;
-    const int g = threadIdx.x % kGroup;
-    const int lane = threadIdx.x & 31;
-    const unsigned gmask = ((1u << kGroup) - 1u) << (lane & ~(kGroup - 1));
-    const bool active = i < d.n;
-    const float4 pi = active ? d.pos[cur][i] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const uint32_t oi = active ? d.orig_of_sorted[i] : 0xffffffffu;
-    const bool cpi = active && oi < (uint32_t)d.n_cp && d.excl_off[oi + 1] > d.excl_off[oi];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    const float4 pi = d.pos[cur][i];
+    const uint32_t oi = d.orig_of_sorted[i];
+    const bool cpi = oi < (uint32_t)d.n_cp && d.excl_off[oi + 1] > d.excl_off[oi];
     int cx, cy, cz;
-    uint32_t sub;
-    cell_coords(d, pi, cx, cy, cz, sub);
+    cell_xyz(d, pi, cx, cy, cz);
     const int m = d.m;
     int cnt = 0;
-    const int ncell = active ? (m >= 3 ? 27 : m * m * m) : 0;
-    for (int q = 0; q < ncell; q++) {
-        int c;
-        if (m >= 3) {
-            const int dx = q / 9 - 1, dy = (q / 3) % 3 - 1, dz = q % 3 - 1;
-            c = (((cx + dx + m) % m) * m + ((cy + dy + m) % m)) * m + ((cz + dz + m) % m);
+    for (int q = 0; q < d.nbr; q++) {
+        int x, y, z;
+        if (m >= 5) {
+            x = (cx + q / 25 - 2 + m) % m;
+            y = (cy + (q / 5) % 5 - 2 + m) % m;
+            z = (cz + q % 5 - 2 + m) % m;
         } else {
-            c = q;
+            x = q / (m * m);
+            y = (q / m) % m;
+            z = q % m;
         }
+        if (box_d2(d, pi, x, y, z) >= d.rlist2) continue;
+        const int c = (x * m + y) * m + z;
         const int b = (int)d.cstart[c], e = (int)d.cend[c];
-        for (int base = b; base < e; base += kGroup) {
-            const int j = base + g;
-            bool ok = false;
-            if (j < e && j != i) {
-                const float4 pj = d.pos[cur][j];
-                const float dx = mimg(pj.x - pi.x, d.L, d.invL);
-                const float dy = mimg(pj.y - pi.y, d.L, d.invL);
-                const float dz = mimg(pj.z - pi.z, d.L, d.invL);
-                ok = dx * dx + dy * dy + dz * dz < d.rlist2;
-                if (ok && cpi) {
-                    const uint32_t oj = d.orig_of_sorted[j];
-                    if (oj < (uint32_t)d.n_cp && excluded(d, oi, oj)) ok = false;
-                }
+        for (int j = b; j < e; j++) {
+            if (j == i) continue;
+            const float4 pj = d.pos[cur][j];
+            const float dx = mimg(pj.x - pi.x, d.L, d.invL);
+            const float dy = mimg(pj.y - pi.y, d.L, d.invL);
+            const float dz = mimg(pj.z - pi.z, d.L, d.invL);
+            if (dx * dx + dy * dy + dz * dz >= d.rlist2) continue;
+            if (cpi) {
+                const uint32_t oj = d.orig_of_sorted[j];
+                if (oj < (uint32_t)d.n_cp && excluded(d, oi, oj)) continue;
             }
-            const unsigned bal = __ballot_sync(gmask, ok) & gmask;
-            const int pos = cnt + __popc(bal & ((1u << lane) - 1u));
-            if (ok && pos < d.nl_cap) d.nl[nl_addr(d, i, pos)] = (uint32_t)j;
-            cnt += __popc(bal);
+            if (cnt < d.nl_cap) d.nl[nl_index(d, i, cnt)] = (uint32_t)j;
+            cnt++;
         }
     }
-    if (active && g == 0) {
-        d.nl_cnt[i] = min(cnt, d.nl_cap);
-        if (cnt > d.nl_cap) atomicOr(d.err, ERR_BIT_PHYS_LIST_OVERFLOW);
-    }
+    d.nl_cnt[i] = min(cnt, d.nl_cap);
+    if (cnt > d.nl_cap) atomicOr(d.err, ERR_BIT_PHYS_LIST_OVERFLOW);
 }
 
 // ----------------------------------------------------------------- bonded ---
 template <bool ENERGY>
-__global__ void __launch_bounds__(kTB) k_bonded(PhysDev d, int cur) {
+__global__ void __launch_bounds__(kTB) k_bonded(PhysDev d, int cur, int slot, int fold_src) {
+    if (fold_src >= 0 && blockIdx.x == 0 && threadIdx.x == 0) fold(d, fold_src);
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double eb = 0.0, ea = 0.0, ed = 0.0, vir = 0.0;
     const float L = d.L, iL = d.invL;
@@ -203,13 +233,13 @@ __global__ void __launch_bounds__(kTB) k_bonded(PhysDev d, int cur) {
         const float th = atan2f(sn, cs);
         const float dth = th - par.x;
         const float inuv = 1.f / (nu * nv);
-        const float c = cs * inuv;
+        const float cosv = cs * inuv;
         const float s = fmaxf(sn * inuv, 1e-6f);
         const float gk = par.y * dth / s;   // (dV/dtheta) / sin(theta)
-        const float fix = gk * (vx * inuv - c * ux / uu), fiy = gk * (vy * inuv - c * uy / uu),
-                    fiz = gk * (vz * inuv - c * uz / uu);
-        const float fkx = gk * (ux * inuv - c * vx / vv), fky = gk * (uy * inuv - c * vy / vv),
-                    fkz = gk * (uz * inuv - c * vz / vv);
+        const float fix = gk * (vx * inuv - cosv * ux / uu), fiy = gk * (vy * inuv - cosv * uy / uu),
+                    fiz = gk * (vz * inuv - cosv * uz / uu);
+        const float fkx = gk * (ux * inuv - cosv * vx / vv), fky = gk * (uy * inuv - cosv * vy / vv),
+                    fkz = gk * (uz * inuv - cosv * vz / vv);
         const int base = 2 * d.n_bonds + 3 * a_;
         d.term_force[base + 0] = make_float4(fix, fiy, fiz, 0.f);
         d.term_force[base + 1] = make_float4(-fix - fkx, -fiy - fky, -fiz - fkz, 0.f);
@@ -258,55 +288,61 @@ __global__ void __launch_bounds__(kTB) k_bonded(PhysDev d, int cur) {
         }
     }
     if (ENERGY) {
-        block_add(d.acc, LIMA_E_BOND, eb);
-        block_add(d.acc, LIMA_E_ANGLE, ea);
-        block_add(d.acc, LIMA_E_DIHEDRAL, ed);
-        block_add(d.acc, LIMA_E_VIRIAL, vir);
+        double* acc = d.acc + slot * LIMA_E_COUNT;
+        block_add(acc, LIMA_E_BOND, eb);
+        block_add(acc, LIMA_E_ANGLE, ea);
+        block_add(acc, LIMA_E_DIHEDRAL, ed);
+        block_add(acc, LIMA_E_VIRIAL, vir);
     }
 }
+
+__global__ void k_finalize(PhysDev d, int src) { fold(d, src); }
 
 // ------------------------------------------------------- pair + integrate ---
 namespace {
 
-template <bool ENERGY>
-__device__ __forceinline__ void lj_pair(const PhysDev& d, const float2* row, float4 pi, float4 pj, float& px,
-                                        float& py, float& pz, float& e_i, float& w_i) {
+// One pair, branch-free: out-of-cutoff pairs contribute zero through a
+// select, the switch is evaluated for every pair (S = 1, S' = 0 below r_on).
+template <bool ENERGY, bool SWITCH>
+__device__ __forceinline__ void lj_pair(const PhysDev& d, const float2* __restrict__ row, float4 pi, float4 pj,
+                                        float& px, float& py, float& pz, float& e_i, float& w_i) {
     const float dx = mimg(pj.x - pi.x, d.L, d.invL);
     const float dy = mimg(pj.y - pi.y, d.L, d.invL);
     const float dz = mimg(pj.z - pi.z, d.L, d.invL);
     const float r2 = dx * dx + dy * dy + dz * dz;
-    if (r2 < d.rc2) {
-        const float2 tab = row[__float_as_int(pj.w)];
-        const float inv = __frcp_rn(r2);
-        const float sr2 = tab.x * inv;
-        const float sr6 = sr2 * sr2 * sr2;
-        float fr = 6.f * tab.y * inv * sr6 * (2.f * sr6 - 1.f);   // F_j / r_vec
-        float v = 0.f;
-        if (ENERGY || d.use_switch) v = tab.y * (sr6 * sr6 - sr6);
-        if (d.use_switch && r2 > d.ron2) {
-            const float a = d.rc2 - r2;
-            const float sw = a * a * (d.rc2 + 2.f * r2 - 3.f * d.ron2) * d.inv_sw_den;
-            const float dsw = 12.f * a * (d.ron2 - r2) * d.inv_sw_den;   // (dS/dr)/r
-            fr = fr * sw - v * dsw;
-            v *= sw;
-        } else if (ENERGY && !d.use_switch) {
-            const float src2 = tab.x / d.rc2, src6 = src2 * src2 * src2;
-            v -= tab.y * (src6 * src6 - src6);
-        }
-        px -= fr * dx;
-        py -= fr * dy;
-        pz -= fr * dz;
-        if (ENERGY) {
-            e_i += 0.5f * v;
-            w_i += 0.5f * fr * r2;
-        }
+    const float2 tab = row[__float_as_int(pj.w)];
+    const float inv = __fdividef(1.f, r2);
+    const float sr2 = tab.x * inv;
+    const float sr6 = sr2 * sr2 * sr2;
+    float fr = 6.f * tab.y * inv * sr6 * (2.f * sr6 - 1.f);   // F_j / r_vec
+    float v = 0.f;
+    if (ENERGY || SWITCH) v = tab.y * (sr6 * sr6 - sr6);
+    if (SWITCH) {
+        const float a = fmaxf(d.rc2 - r2, 0.f);
+        const bool sw_on = r2 > d.ron2;
+        const float sw = sw_on ? a * a * (d.rc2 + 2.f * r2 - 3.f * d.ron2) * d.inv_sw_den : 1.f;
+        const float dsw = sw_on ? 12.f * a * (d.ron2 - r2) * d.inv_sw_den : 0.f;   // (dS/dr)/r
+        fr = fr * sw - v * dsw;
+        v *= sw;
+    } else if (ENERGY) {
+        const float src2 = tab.x / d.rc2, src6 = src2 * src2 * src2;
+        v -= tab.y * (src6 * src6 - src6);
+    }
+    const bool in = r2 < d.rc2;
+    fr = in ? fr : 0.f;
+    px -= fr * dx;
+    py -= fr * dy;
+    pz -= fr * dz;
+    if (ENERGY) {
+        e_i += in ? 0.5f * v : 0.f;
+        w_i += 0.5f * fr * r2;
     }
 }
 
 }  // namespace
 
-template <bool MIXED, bool ENERGY, bool INTEGRATE>
-__global__ void __launch_bounds__(kTB) k_pair_integrate(PhysDev d, int cur) {
+template <bool MIXED, bool ENERGY, bool INTEGRATE, bool SWITCH>
+__global__ void __launch_bounds__(kTB) k_pair_integrate(PhysDev d, int cur, int slot) {
     extern __shared__ float2 s_tab[];
     const int nt2 = d.n_types * d.n_types;
     for (int q = threadIdx.x; q < nt2; q += blockDim.x) s_tab[q] = d.lj_table[q];
@@ -315,31 +351,31 @@ __global__ void __launch_bounds__(kTB) k_pair_integrate(PhysDev d, int cur) {
     const int g = threadIdx.x % kGroup;
     const bool active = i < d.n;
     double ke = 0.0, elj = 0.0, vir = 0.0;
-    const float4 pi = active ? d.pos[cur][i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4* __restrict__ pos = d.pos[cur];
+    const float4 pi = active ? pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
     const float2* row = &s_tab[__float_as_int(pi.w) * d.n_types];
     float fx = 0.f, fy = 0.f, fz = 0.f, cxx = 0.f, cyy = 0.f, czz = 0.f;
     float e_i = 0.f, w_i = 0.f;
     const int cnt = active ? (int)d.nl_cnt[i] : 0;
-    const uint32_t* nl = d.nl + (size_t)i * kGroup + g;
-    const size_t stride = (size_t)d.n_pad * kGroup;
-    // entries g, g+kGroup, ...: row r of this lane is nl[r*stride]
-    const int rows = (cnt - g + kGroup - 1) / kGroup;
+    const uint32_t stride = (uint32_t)d.n_pad * kGroup;
+    const uint32_t* __restrict__ nl = d.nl + (uint32_t)i * kGroup + g;
+    const int rows = cnt > g ? (cnt - g + kGroup - 1) / kGroup : 0;
     int r = 0;
     while (r < rows) {
         const int rend = MIXED ? min(rows, r + 8) : rows;
         float px = 0.f, py = 0.f, pz = 0.f;
-        for (; r + 1 < rend; r += 2) {   // two gathers in flight
-            const uint32_t j0 = __ldg(&nl[(size_t)r * stride]);
-            const uint32_t j1 = __ldg(&nl[(size_t)(r + 1) * stride]);
-            const float4 p0 = d.pos[cur][j0];
-            const float4 p1 = d.pos[cur][j1];
-            lj_pair<ENERGY>(d, row, pi, p0, px, py, pz, e_i, w_i);
-            lj_pair<ENERGY>(d, row, pi, p1, px, py, pz, e_i, w_i);
+        for (; r + 3 < rend; r += 4) {   // four gathers in flight
+            const uint32_t j0 = __ldg(nl + r * stride), j1 = __ldg(nl + (r + 1) * stride);
+            const uint32_t j2 = __ldg(nl + (r + 2) * stride), j3 = __ldg(nl + (r + 3) * stride);
+            const float4 p0 = __ldg(pos + j0), p1 = __ldg(pos + j1), p2 = __ldg(pos + j2), p3 = __ldg(pos + j3);
+            lj_pair<ENERGY, SWITCH>(d, row, pi, p0, px, py, pz, e_i, w_i);
+            lj_pair<ENERGY, SWITCH>(d, row, pi, p1, px, py, pz, e_i, w_i);
+            lj_pair<ENERGY, SWITCH>(d, row, pi, p2, px, py, pz, e_i, w_i);
+            lj_pair<ENERGY, SWITCH>(d, row, pi, p3, px, py, pz, e_i, w_i);
         }
-        if (r < rend) {
-            const uint32_t j0 = __ldg(&nl[(size_t)r * stride]);
-            lj_pair<ENERGY>(d, row, pi, d.pos[cur][j0], px, py, pz, e_i, w_i);
-            r++;
+        for (; r < rend; r++) {
+            const uint32_t j0 = __ldg(nl + r * stride);
+            lj_pair<ENERGY, SWITCH>(d, row, pi, __ldg(pos + j0), px, py, pz, e_i, w_i);
         }
         if (MIXED) {
             ds_add(fx, cxx, px);
@@ -351,7 +387,7 @@ __global__ void __launch_bounds__(kTB) k_pair_integrate(PhysDev d, int cur) {
             fz += pz;
         }
     }
-    // reduce the group's partial forces (warp shuffles)
+    // reduce the kGroup lanes of this particle (warp shuffles)
 #pragma unroll
     for (int o = kGroup / 2; o > 0; o >>= 1) {
         if (MIXED) {
@@ -419,7 +455,7 @@ __global__ void __launch_bounds__(kTB) k_pair_integrate(PhysDev d, int cur) {
             const double vx = (double)vhx + vc.x, vy = (double)vhy + vc.y, vz = (double)vhz + vc.z;
             ke = 0.5 / (double)im * (vx * vx + vy * vy + vz * vz);
             if (INTEGRATE) {
-                const float lam = *d.lambda;
+                const float lam = d.lambda[slot];
                 if (lam != 1.f) {   // scale (hi, lo): keep the product's rounding error in lo
                     float p = lam * vhx; vc.x = fmaf(lam, vhx, -p) + lam * vc.x; vhx = p;
                     p = lam * vhy; vc.y = fmaf(lam, vhy, -p) + lam * vc.y; vhy = p;
@@ -431,9 +467,9 @@ __global__ void __launch_bounds__(kTB) k_pair_integrate(PhysDev d, int cur) {
                 float4 pc = d.posc[i];
                 const float dtf = (float)d.dt;
                 float x = pi.x, y = pi.y, z = pi.z;
-                float t = vhx * dtf; ds_add(x, pc.x, t); pc.x += fmaf(vhx, dtf, -t) + vc.x * dtf;
-                t = vhy * dtf; ds_add(y, pc.y, t); pc.y += fmaf(vhy, dtf, -t) + vc.y * dtf;
-                t = vhz * dtf; ds_add(z, pc.z, t); pc.z += fmaf(vhz, dtf, -t) + vc.z * dtf;
+                float tt = vhx * dtf; ds_add(x, pc.x, tt); pc.x += fmaf(vhx, dtf, -tt) + vc.x * dtf;
+                tt = vhy * dtf; ds_add(y, pc.y, tt); pc.y += fmaf(vhy, dtf, -tt) + vc.y * dtf;
+                tt = vhz * dtf; ds_add(z, pc.z, tt); pc.z += fmaf(vhz, dtf, -tt) + vc.z * dtf;
                 if (x < 0.f) ds_add(x, pc.x, L); else if (x >= L) ds_add(x, pc.x, -L);
                 if (y < 0.f) ds_add(y, pc.y, L); else if (y >= L) ds_add(y, pc.y, -L);
                 if (z < 0.f) ds_add(z, pc.z, L); else if (z >= L) ds_add(z, pc.z, -L);
@@ -453,7 +489,7 @@ __global__ void __launch_bounds__(kTB) k_pair_integrate(PhysDev d, int cur) {
             float vx = v.x + ax * h, vy = v.y + ay * h, vz = v.z + az * h;
             ke = 0.5 / (double)im * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
             if (INTEGRATE) {
-                const float lam = *d.lambda;
+                const float lam = d.lambda[slot];
                 vx = lam * vx + ax * h;
                 vy = lam * vy + ay * h;
                 vz = lam * vz + az * h;
@@ -474,46 +510,32 @@ __global__ void __launch_bounds__(kTB) k_pair_integrate(PhysDev d, int cur) {
             }
         }
     }
-    block_add(d.acc, LIMA_E_KINETIC, ke);
+    double* acc = d.acc + slot * LIMA_E_COUNT;
+    block_add(acc, LIMA_E_KINETIC, ke);
     if (ENERGY) {
-        block_add(d.acc, LIMA_E_LJ, elj);
-        block_add(d.acc, LIMA_E_VIRIAL, vir);
-    }
-    // last block: fold the FP64 accumulators, temperature, next lambda
-    __shared__ bool last;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(d.done, 1u) == gridDim.x - 1;
-    __syncthreads();
-    if (last && threadIdx.x == 0) {
-        __threadfence();
-        volatile double* acc = d.acc;
-        const double kin = acc[LIMA_E_KINETIC];
-        const double temp = 2.0 * kin / (3.0 * (double)d.n * kR);
-        d.e_last[LIMA_E_KINETIC] = kin;
-        d.e_last[LIMA_E_TEMPERATURE] = temp;
-        if (ENERGY) {
-            d.e_last[LIMA_E_LJ] = acc[LIMA_E_LJ];
-            d.e_last[LIMA_E_BOND] = acc[LIMA_E_BOND];
-            d.e_last[LIMA_E_ANGLE] = acc[LIMA_E_ANGLE];
-            d.e_last[LIMA_E_DIHEDRAL] = acc[LIMA_E_DIHEDRAL];
-            d.e_last[LIMA_E_VIRIAL] = acc[LIMA_E_VIRIAL];
-            d.e_last[LIMA_E_TOTAL] = acc[LIMA_E_LJ] + acc[LIMA_E_BOND] + acc[LIMA_E_ANGLE] + acc[LIMA_E_DIHEDRAL] + kin;
-        }
-        for (int q = 0; q < LIMA_E_COUNT; q++) acc[q] = 0.0;
-        if (INTEGRATE) {
-            float lam = 1.f;
-            if (d.thermostat == LIMA_THERMOSTAT_BERENDSEN && temp > 0.0)
-                lam = (float)sqrt(1.0 + d.dt / d.tau_t * (d.t_target / temp - 1.0));
-            *d.lambda = lam;
-            *d.t_prev = temp;
-        }
-        __threadfence();
-        *d.done = 0;
+        block_add(acc, LIMA_E_LJ, elj);
+        block_add(acc, LIMA_E_VIRIAL, vir);
+        if (blockIdx.x == 0 && threadIdx.x == 0) d.acc_energy[slot] = 1;
     }
 }
 
 // ---------------------------------------------------------------- launchers --
+namespace {
+
+template <bool MIXED, bool ENERGY, bool INTEGRATE>
+void pair_variant(const PhysDev& d, int cur, int slot, cudaStream_t s) {
+    const int nb = (int)(((size_t)d.n_pad * kGroup + kTB - 1) / kTB);
+    const size_t smem = sizeof(float2) * d.n_types * d.n_types;
+    if (d.use_switch)
+        k_pair_integrate<MIXED, ENERGY, INTEGRATE, true><<<nb, kTB, smem, s>>>(d, cur, slot);
+    else
+        k_pair_integrate<MIXED, ENERGY, INTEGRATE, false><<<nb, kTB, smem, s>>>(d, cur, slot);
+}
+
+}  // namespace
+
+void physics_kernel_attributes(const PhysDev&) {}
+
 void launch_keys(const PhysDev& d, int cur, cudaStream_t s) {
     k_keys<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d, cur);
 }
@@ -523,32 +545,30 @@ void launch_permute(const PhysDev& d, int cur, bool mixed, cudaStream_t s) {
 }
 
 void launch_build_list(const PhysDev& d, int cur, cudaStream_t s) {
-    const int nb = (int)(((size_t)d.n_pad * kGroup + kTB - 1) / kTB);
-    k_build_list<<<nb, kTB, 0, s>>>(d, cur);
+    k_build_list<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d, cur);
 }
 
-void launch_bonded(const PhysDev& d, int cur, bool energy, cudaStream_t s) {
+void launch_bonded(const PhysDev& d, int cur, bool energy, int slot, int fold_src, cudaStream_t s) {
     const int nterms = d.n_bonds + d.n_angles + d.n_dih;
-    if (nterms == 0) return;
-    const int nb = (nterms + kTB - 1) / kTB;
+    const int nb = std::max(1, (nterms + kTB - 1) / kTB);
     if (energy)
-        k_bonded<true><<<nb, kTB, 0, s>>>(d, cur);
+        k_bonded<true><<<nb, kTB, 0, s>>>(d, cur, slot, fold_src);
     else
-        k_bonded<false><<<nb, kTB, 0, s>>>(d, cur);
+        k_bonded<false><<<nb, kTB, 0, s>>>(d, cur, slot, fold_src);
 }
 
-void launch_pair(const PhysDev& d, int cur, bool mixed, bool energy, bool integrate, cudaStream_t s) {
-    const int nb = (int)(((size_t)d.n_pad * kGroup + kTB - 1) / kTB);
-    const size_t smem = sizeof(float2) * d.n_types * d.n_types;
+void launch_pair(const PhysDev& d, int cur, bool mixed, bool energy, bool integrate, int slot, cudaStream_t s) {
     if (mixed) {
-        if (!integrate) k_pair_integrate<true, true, false><<<nb, kTB, smem, s>>>(d, cur);
-        else if (energy) k_pair_integrate<true, true, true><<<nb, kTB, smem, s>>>(d, cur);
-        else k_pair_integrate<true, false, true><<<nb, kTB, smem, s>>>(d, cur);
+        if (!integrate) pair_variant<true, true, false>(d, cur, slot, s);
+        else if (energy) pair_variant<true, true, true>(d, cur, slot, s);
+        else pair_variant<true, false, true>(d, cur, slot, s);
     } else {
-        if (!integrate) k_pair_integrate<false, true, false><<<nb, kTB, smem, s>>>(d, cur);
-        else if (energy) k_pair_integrate<false, true, true><<<nb, kTB, smem, s>>>(d, cur);
-        else k_pair_integrate<false, false, true><<<nb, kTB, smem, s>>>(d, cur);
+        if (!integrate) pair_variant<false, true, false>(d, cur, slot, s);
+        else if (energy) pair_variant<false, true, true>(d, cur, slot, s);
+        else pair_variant<false, false, true>(d, cur, slot, s);
     }
 }
+
+void launch_finalize(const PhysDev& d, int src, cudaStream_t s) { k_finalize<<<1, 1, 0, s>>>(d, src); }
 
 }  // namespace lima

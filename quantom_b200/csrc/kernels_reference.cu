@@ -385,13 +385,31 @@ __global__ void k_snapshot(RefDev d, int cur) {
 
 }  // namespace
 
-void ref_step_kernels(const RefDev& d, int cur, cudaStream_t s) {
-    if (d.n_b > 0) k_bridge<<<d.n_b, 32, 0, s>>>(d, cur);
-    if (d.n_c > 0) {
-        if (d.n_s > 0) k_cs_partial<<<dim3(d.n_chunks, d.n_c), 64, 0, s>>>(d, cur);
-        k_compound<<<d.n_c, 64, 0, s>>>(d, cur);
+// ev (nullable): events recorded before the bridges, after them, after the
+// compound kernels and after the solvent kernel.  Returns kernels launched.
+int ref_step_kernels(const RefDev& d, int cur, cudaStream_t s, cudaEvent_t* ev) {
+    int launched = 0;
+    if (ev) cudaEventRecord(ev[0], s);
+    if (d.n_b > 0) {
+        k_bridge<<<d.n_b, 32, 0, s>>>(d, cur);
+        launched++;
     }
-    if (d.n_s > 0) k_solvent<<<(d.n_s + kSolBlock - 1) / kSolBlock, kSolBlock, 0, s>>>(d, cur);
+    if (ev) cudaEventRecord(ev[1], s);
+    if (d.n_c > 0) {
+        if (d.n_s > 0) {
+            k_cs_partial<<<dim3(d.n_chunks, d.n_c), 64, 0, s>>>(d, cur);
+            launched++;
+        }
+        k_compound<<<d.n_c, 64, 0, s>>>(d, cur);
+        launched++;
+    }
+    if (ev) cudaEventRecord(ev[2], s);
+    if (d.n_s > 0) {
+        k_solvent<<<(d.n_s + kSolBlock - 1) / kSolBlock, kSolBlock, 0, s>>>(d, cur);
+        launched++;
+    }
+    if (ev) cudaEventRecord(ev[3], s);
+    return launched;
 }
 
 void ref_thermostat_snapshot(const RefDev& d, int cur, cudaStream_t s) {

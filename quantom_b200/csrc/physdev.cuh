@@ -2,17 +2,24 @@
 // unified particle array, laid out for throughput.
 //
 // Particle ids: "orig" = compound particles compound by compound (c, l) ->
-// base[c] + l, then solvents (n_cp + s).  "slot" = position in the spatially
-// sorted order used by every per-step array; re-sorted at each list rebuild.
+// base[c] + l, then solvents (n_cp + s).  "slot" = position in the cell-sorted
+// order used by every per-step array; re-sorted at each list rebuild.
+//
+// Cells: a uniform grid of m^3 cells of side >= r_list/2, so every particle
+// within r_list of a cell lies in the 5x5x5 block of cells around it (all
+// m^3 cells when m < 5).  A cell's particles occupy a contiguous slot range
+// [cstart, cend), so a cell's neighbourhood ("tile") is 125 contiguous ranges
+// that the step kernels stage into shared memory with bulk copies.
 //
 // HBM layout (float3 quantities widened to float4, one 16-byte access each):
-//   pos[2][n_pad]   x, y, z in [0, L), w = type index (bit-cast)   (read by all, double-buffered)
-//   vel[n_pad]      half-step velocity, w = 1/m                  (own slot only)
-//   posc/velc       low parts of pos/vel (mixed precision)       (own slot only)
+//   pos[2][n_pad]   x, y, z in [0, L), w = type index (bit-cast)   (double-buffered)
+//   vel[n_pad]      half-step velocity, w = 1/m
+//   posc/velc       low parts of pos/vel (mixed precision)
 //   xref[n_pad]     positions at the last rebuild (list validity check)
 //   force[n_pad]    total force of the last evaluation, w = per-particle LJ energy
-//   nl[cap][n_pad]  Verlet list, column-major (entry k of slot i at k*n_pad + i)
-//                   so that the k-th loads of a warp are one 128-byte line
+//   nl[cap][n_pad]  Verlet list of 16-bit tile-local indices, blocked so that
+//                   the kGroup lanes of one particle read kGroup consecutive
+//                   entries and consecutive particles follow each other
 //   term_force      one float4 per (term, atom) of every bonded term; gathered
 //                   per particle through bterm_off/bterm_slot (CSR over orig)
 #pragma once
@@ -25,6 +32,9 @@
 #include "lima_abi.h"
 
 namespace lima {
+
+// accumulator slots: 0/1 = step parity, 2 = on-demand energy evaluation
+constexpr int kAccSlots = 3;
 
 struct PhysDev {
     int n;              // particles
@@ -47,15 +57,17 @@ struct PhysDev {
     uint32_t* orig_of_sorted;   // [n]
     uint32_t* sorted_of_orig;   // [n]
     float2* lj_table;           // [n_types^2] (sigma^2, 4 eps), Lorentz-Berthelot
-    // sort grid: coarse cells >= rlist, each split 4x4x4 for locality
-    int m;
-    float coarse;
+    // cell grid
+    int m;                      // cells per dimension
+    int n_cells;                // m^3
+    int nbr;                    // cells in a neighbourhood: 125, or m^3 when m < 5
+    int tile_cap;               // staged particles per block (shared memory capacity)
     uint32_t* keys[2];
     uint32_t* vals[2];
     void* sort_tmp; size_t sort_tmp_bytes;
     uint32_t* cstart; uint32_t* cend;
     float4* pos_tmp; float4* vel_tmp; float4* posc_tmp; float4* velc_tmp; uint32_t* orig_tmp;
-    // Verlet list
+    // Verlet list (tile-local indices)
     uint32_t* nl; uint32_t* nl_cnt; int nl_cap;
     // exclusions (CSR over orig ids)
     uint32_t* excl_off; uint32_t* excl_ids;
@@ -67,13 +79,13 @@ struct PhysDev {
     uint32_t* bterm_off; uint32_t* bterm_slot;
     float4* term_force;
     int n_term_slots;
-    // FP64 reductions: acc[LIMA_E_*] summed by the step's kernels and
-    // finalised by the last block into e_last; lambda for the next step
+    // FP64 reductions: acc[slot*8 + LIMA_E_*]; slot 0/1 are folded into e_last
+    // (and the next Berendsen lambda[1-slot]) by the first kernel of the next
+    // step or by k_finalize before a readback
     double* acc;
+    int* acc_energy;    // [kAccSlots] energies were accumulated into this slot
     double* e_last;
-    double* t_prev;
-    float* lambda;
-    unsigned int* done;
+    float* lambda;      // [2]
     int* err;
 };
 
@@ -94,8 +106,11 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
 void phys_upload_state(const PhysHost& h, PhysDev& d, int cur, cudaStream_t s);
 void phys_rebuild(PhysDev& d, int cur, cudaStream_t s);
 void phys_prime(PhysDev& d, int cur, cudaStream_t s);
-void phys_step_kernels(const PhysDev& d, int cur, cudaStream_t s, bool energy = false);
+// ev (nullable): events before the bonded kernel, after it, after the pair
+// kernel.  Returns kernels launched.
+int phys_step_kernels(const PhysDev& d, int cur, cudaStream_t s, bool energy = false, cudaEvent_t* ev = nullptr);
 void phys_energy_now(PhysDev& d, int cur, cudaStream_t s);
+void phys_finalize(const PhysDev& d, int cur, cudaStream_t s);
 void phys_read_compounds(const PhysDev& d, int cur, const lima_compound* comps, float4* pos_out, float4* prev_out);
 void phys_read_solvents(const PhysDev& d, int cur, float4* pos_out, float4* prev_out);
 void phys_read_forces(const PhysDev& d, const lima_compound* comps, float4* fc, float4* fs);

@@ -182,10 +182,21 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
         bslot.insert(bslot.end(), slots[i].begin(), slots[i].end());
     }
 
-    // sort grid (coarse cells >= rlist) and Verlet-list capacity
-    d.m = std::max(1, (int)std::floor(d.L / d.rlist));
-    while (d.m > 1 && d.L / d.m < d.rlist) d.m--;
-    d.coarse = d.L / d.m;
+    // cell grid (side >= rlist/2: the 5x5x5 neighbourhood covers rlist),
+    // shared-memory tile capacity and Verlet-list capacity
+    const float half = 0.5f * d.rlist;
+    d.m = std::max(1, (int)std::floor(d.L / half));
+    while (d.m > 1 && d.L / d.m < half) d.m--;
+    d.n_cells = d.m * d.m * d.m;
+    d.nbr = d.m >= 5 ? 125 : d.n_cells;
+    const double per_cell = (double)d.n / d.n_cells;
+    const double tile_expect = d.m >= 5 ? 125.0 * per_cell : (double)d.n;
+    d.tile_cap = d.m >= 5 ? (int)std::min<double>(d.n, tile_expect + 8.0 * std::sqrt(tile_expect) + 64) : d.n;
+    d.tile_cap = (d.tile_cap + 7) / 8 * 8;
+    if (d.tile_cap > 12288) {
+        msg = "particle density too high for the shared-memory tile (more than 12288 particles per 5x5x5 cells)";
+        return LIMA_ERR_ARGUMENT;
+    }
     const double rho = d.n / ((double)d.L * d.L * d.L);
     const double expect = 4.0 / 3.0 * M_PI * (double)d.rlist * d.rlist * d.rlist * rho;
     d.nl_cap = std::min((d.n + kGroup - 1) / kGroup * kGroup, (int)((1.6 * expect + 96) / kGroup + 1) * kGroup);
@@ -205,9 +216,8 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
             d.keys[b] = dalloc<uint32_t>(allocs, d.n);
             d.vals[b] = dalloc<uint32_t>(allocs, d.n);
         }
-        const size_t ncell = (size_t)d.m * d.m * d.m;
-        d.cstart = dalloc<uint32_t>(allocs, ncell);
-        d.cend = dalloc<uint32_t>(allocs, ncell);
+        d.cstart = dalloc<uint32_t>(allocs, d.n_cells);
+        d.cend = dalloc<uint32_t>(allocs, d.n_cells);
         d.pos_tmp = dalloc<float4>(allocs, d.n);
         d.vel_tmp = dalloc<float4>(allocs, d.n);
         d.posc_tmp = dalloc<float4>(allocs, d.n);
@@ -226,11 +236,10 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
         d.bterm_off = dalloc<uint32_t>(allocs, boff.size());
         d.bterm_slot = dalloc<uint32_t>(allocs, bslot.size());
         d.term_force = dalloc<float4>(allocs, d.n_term_slots);
-        d.acc = dalloc<double>(allocs, LIMA_E_COUNT);
+        d.acc = dalloc<double>(allocs, kAccSlots * LIMA_E_COUNT);
+        d.acc_energy = dalloc<int>(allocs, kAccSlots);
         d.e_last = dalloc<double>(allocs, LIMA_E_COUNT);
-        d.t_prev = dalloc<double>(allocs, 1);
-        d.lambda = dalloc<float>(allocs, 1);
-        d.done = dalloc<unsigned int>(allocs, 1);
+        d.lambda = dalloc<float>(allocs, 2);
         d.err = dalloc<int>(allocs, 1);
         cub::DeviceRadixSort::SortPairs(nullptr, d.sort_tmp_bytes, d.keys[0], d.keys[1], d.vals[0], d.vals[1], d.n, 0,
                                         32, s);
@@ -253,14 +262,13 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
     up(d.dih_par, dpar.data(), sizeof(float4) * dpar.size());
     up(d.bterm_off, boff.data(), sizeof(uint32_t) * boff.size());
     up(d.bterm_slot, bslot.data(), sizeof(uint32_t) * bslot.size());
-    cudaMemsetAsync(d.acc, 0, sizeof(double) * LIMA_E_COUNT, s);
+    cudaMemsetAsync(d.acc, 0, sizeof(double) * kAccSlots * LIMA_E_COUNT, s);
+    cudaMemsetAsync(d.acc_energy, 0, sizeof(int) * kAccSlots, s);
     cudaMemsetAsync(d.e_last, 0, sizeof(double) * LIMA_E_COUNT, s);
-    cudaMemsetAsync(d.t_prev, 0, sizeof(double), s);
-    cudaMemsetAsync(d.done, 0, sizeof(unsigned int), s);
     cudaMemsetAsync(d.err, 0, sizeof(int), s);
     cudaMemsetAsync(d.nl_cnt, 0, sizeof(uint32_t) * d.n_pad, s);
     cudaMemsetAsync(d.force, 0, sizeof(float4) * d.n_pad, s);
-    set_device_float(d.lambda, 1.f, s);
+    physics_kernel_attributes(d);
     phys_upload_state(h, d, 0, s);
     return cudaGetLastError() == cudaSuccess ? 0 : LIMA_ERR_CUDA;
 }
@@ -308,16 +316,19 @@ void phys_upload_state(const PhysHost& h, PhysDev& d, int cur, cudaStream_t s) {
     cudaMemcpyAsync(d.orig_of_sorted, ident.data(), sizeof(uint32_t) * d.n_pad, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(d.sorted_of_orig, ident.data(), sizeof(uint32_t) * d.n, cudaMemcpyHostToDevice, s);
     set_device_float(d.lambda, 1.f, s);
+    set_device_float(d.lambda + 1, 1.f, s);
+    cudaMemsetAsync(d.acc, 0, sizeof(double) * kAccSlots * LIMA_E_COUNT, s);
+    cudaMemsetAsync(d.acc_energy, 0, sizeof(int) * kAccSlots, s);
     cudaStreamSynchronize(s);
 }
 
 void phys_rebuild(PhysDev& d, int cur, cudaStream_t s) {
-    const size_t ncell = (size_t)d.m * d.m * d.m;
+    const size_t ncell = (size_t)d.n_cells;
     const bool mixed = d.precision == LIMA_PRECISION_MIXED;
     launch_keys(d, cur, s);
     size_t bytes = d.sort_tmp_bytes;
-    int end_bit = 6;
-    while ((1ull << end_bit) < (unsigned long long)ncell * 64ull) end_bit++;
+    int end_bit = 1;
+    while ((1ull << end_bit) < (unsigned long long)ncell) end_bit++;
     cub::DeviceRadixSort::SortPairs(d.sort_tmp, bytes, d.keys[0], d.keys[1], d.vals[0], d.vals[1], d.n, 0, end_bit, s);
     cudaMemsetAsync(d.cstart, 0, sizeof(uint32_t) * ncell, s);
     cudaMemsetAsync(d.cend, 0, sizeof(uint32_t) * ncell, s);
@@ -334,15 +345,24 @@ void phys_rebuild(PhysDev& d, int cur, cudaStream_t s) {
 
 void phys_prime(PhysDev&, int, cudaStream_t) {}
 
-void phys_step_kernels(const PhysDev& d, int cur, cudaStream_t s, bool energy) {
-    launch_bonded(d, cur, energy, s);
-    launch_pair(d, cur, d.precision == LIMA_PRECISION_MIXED, energy, true, s);
+// The step of parity `cur` accumulates into slot cur; its bonded kernel first
+// folds slot cur^1 (the previous step) into e_last and lambda[cur].
+int phys_step_kernels(const PhysDev& d, int cur, cudaStream_t s, bool energy, cudaEvent_t* ev) {
+    if (ev) cudaEventRecord(ev[0], s);
+    launch_bonded(d, cur, energy, cur, cur ^ 1, s);
+    if (ev) cudaEventRecord(ev[1], s);
+    launch_pair(d, cur, d.precision == LIMA_PRECISION_MIXED, energy, true, cur, s);
+    if (ev) cudaEventRecord(ev[2], s);
+    return 2;
 }
 
 void phys_energy_now(PhysDev& d, int cur, cudaStream_t s) {
-    launch_bonded(d, cur, true, s);
-    launch_pair(d, cur, d.precision == LIMA_PRECISION_MIXED, true, false, s);
+    launch_bonded(d, cur, true, 2, -1, s);
+    launch_pair(d, cur, d.precision == LIMA_PRECISION_MIXED, true, false, 2, s);
+    launch_finalize(d, 2, s);
 }
+
+void phys_finalize(const PhysDev& d, int cur, cudaStream_t s) { launch_finalize(d, cur ^ 1, s); }
 
 namespace {
 struct Snapshot {

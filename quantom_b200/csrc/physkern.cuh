@@ -1,17 +1,24 @@
 // Launchers of the physics-semantics kernels (kernels_physics.cu), called by
 // the host side in physics_host.cu.
 #pragma once
+#include <algorithm>
+
 #include "physdev.cuh"
 
 namespace lima {
 
-constexpr int kTB = 256;      // threads per block
-constexpr int kGroup = 8;     // lanes per particle in the pair and list kernels
+constexpr int kTB = 256;         // threads per block of the per-particle / per-term kernels
+constexpr int kGroup = 8;        // lanes per particle in the list and pair kernels
+constexpr int kCellBlock = 128;  // threads per cell block (16 particles per pass)
+constexpr int kMaxTypes = 32;    // LIMA_MAX_ATOM_TYPES
 
+void physics_kernel_attributes(const PhysDev& d);
 void launch_keys(const PhysDev& d, int cur, cudaStream_t s);
 void launch_permute(const PhysDev& d, int cur, bool mixed, cudaStream_t s);
 void launch_build_list(const PhysDev& d, int cur, cudaStream_t s);
-void launch_bonded(const PhysDev& d, int cur, bool energy, cudaStream_t s);
-void launch_pair(const PhysDev& d, int cur, bool mixed, bool energy, bool integrate, cudaStream_t s);
+// slot: accumulator slot to add energies to; fold_src: slot to fold first (-1: none)
+void launch_bonded(const PhysDev& d, int cur, bool energy, int slot, int fold_src, cudaStream_t s);
+void launch_pair(const PhysDev& d, int cur, bool mixed, bool energy, bool integrate, int slot, cudaStream_t s);
+void launch_finalize(const PhysDev& d, int src, cudaStream_t s);
 
 }  // namespace lima

@@ -24,6 +24,7 @@ enum : int {
     ERR_BIT_CRITICAL_FORCE = 16,
     ERR_BIT_PHYS_LIST_OVERFLOW = 32,
     ERR_BIT_LIST_STALE = 64,      // a particle moved more than skin/2 since the last list build
+    ERR_BIT_TILE_TIMEOUT = 128,   // a shared-memory staging wait ran out (bounded mbarrier wait)
 };
 
 struct RefDev {
@@ -68,7 +69,7 @@ struct RefDev {
 // nlist_reference.cu
 void ref_build_nlists(const RefDev& d, int cur, cudaStream_t s);
 // kernels_reference.cu
-void ref_step_kernels(const RefDev& d, int cur, cudaStream_t s);
+int ref_step_kernels(const RefDev& d, int cur, cudaStream_t s, cudaEvent_t* ev = nullptr);
 void ref_thermostat_snapshot(const RefDev& d, int cur, cudaStream_t s);
 void ref_thermostat_update(const RefDev& d, int cur, int n_particles, float t_target, bool apply, cudaStream_t s);
 void set_device_float(float* p, float v, cudaStream_t s);

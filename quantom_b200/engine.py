@@ -27,6 +27,8 @@ THERMOSTAT_NONE, THERMOSTAT_REFERENCE, THERMOSTAT_BERENDSEN = 0, 1, 2
 NL_COMPOUND_COMPOUND, NL_COMPOUND_SOLVENT, NL_SOLVENT_COMPOUND, NL_SOLVENT_SOLVENT = 0, 1, 2, 3
 E_LJ, E_BOND, E_ANGLE, E_DIHEDRAL, E_KINETIC, E_VIRIAL, E_TEMPERATURE, E_TOTAL = range(8)
 E_COUNT = 8
+PROF_NAMES = ("total", "nlist", "bonded", "pair", "compound")
+PROF_COUNT = len(PROF_NAMES)
 
 
 class LimaError(RuntimeError):
@@ -79,6 +81,8 @@ def load_library():
         "lima_set_thermostat_scalar": (i, [vp, f]),
         "lima_get_step": (i, [vp, ctypes.POINTER(ctypes.c_uint64)]),
         "lima_get_last_step_ms": (i, [vp, ctypes.POINTER(f)]),
+        "lima_profile_steps": (i, [vp, i, vp]),
+        "lima_get_kernel_launches": (i, [vp, ctypes.POINTER(ctypes.c_uint64)]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name, None)
@@ -182,6 +186,18 @@ class Engine:
         v = ctypes.c_float()
         self._check(self.lib.lima_get_last_step_ms(self.h, ctypes.byref(v)))
         return float(v.value)
+
+    def profile_steps(self, n: int) -> dict:
+        """Mean device ms per step of each kernel group over n steps
+        (CUDA events on the engine's stream; Engine::timings)."""
+        out = np.zeros(PROF_COUNT, np.float32)
+        self._check(self.lib.lima_profile_steps(self.h, int(n), _ptr(out)))
+        return {name: float(out[k]) for k, name in enumerate(PROF_NAMES)}
+
+    def kernel_launches(self) -> int:
+        v = ctypes.c_uint64()
+        self._check(self.lib.lima_get_kernel_launches(self.h, ctypes.byref(v)))
+        return int(v.value)
 
     # -- state ---------------------------------------------------------------
     def compound_states(self):
