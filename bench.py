@@ -22,9 +22,7 @@ import json
 import math
 import os
 import statistics
-import subprocess
 import sys
-import tempfile
 import time
 from pathlib import Path
 
@@ -34,6 +32,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 WORKLOAD = "solvated_chains_32k"
+SKIN = 0.1                # Verlet-list skin, nm
 NS_PER_DAY_S = 86400.0   # seconds per day
 FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12   # clock-derived FP32 FMA peak (no measured figure)
 FLOP_PER_PAIR = 32       # per unique pair within the cutoff (minimum image, r^2, rcp, LJ, force, both sides)
@@ -42,7 +41,7 @@ FLOP_PER_PAIR = 32       # per unique pair within the cutoff (minimum image, r^2
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--steps", type=int, default=4000)
     ap.add_argument("--warmup", type=int, default=40)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
@@ -106,57 +105,86 @@ def barrier(pg):
 
 
 class ClockSampler:
-    """nvidia-smi samples every 200 ms while the timed region runs."""
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and clock-event reasons sampled every 50 ms through NVML
+    (read-only queries) by a background thread; `window()` brackets the timed
+    region and `summary()` keeps the samples taken inside it."""
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
 
-    def __init__(self, device):
+    def __init__(self, device, period_s=0.05):
         self.device = device
-        self.proc = None
-        self.path = None
+        self.period = period_s
+        self.samples = []          # (t, sm_mhz, reasons bitmask, power W)
+        self.win = [None, None]
+        self.sm_max = None
+        self._stop = None
+        self._thr = None
+
+    def _handle(self, nv):
+        import torch
+        try:
+            pr = torch.cuda.get_device_properties(self.device)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return nv.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.device)
 
     def __enter__(self):
-        fd, self.path = tempfile.mkstemp(suffix=".csv")
-        os.close(fd)
+        import threading
         try:
-            self.f = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", str(self.device)], stdout=self.f,
-                                         stderr=subprocess.DEVNULL)
+            import pynvml as nv
+            nv.nvmlInit()
+            h = self._handle(nv)
+            self.sm_max = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
         except Exception:
-            self.proc = None
+            return self
+        self._stop = threading.Event()
+
+        def loop():
+            while not self._stop.is_set():
+                try:
+                    t = time.perf_counter()
+                    sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                    rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+                    pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                    self.samples.append((t, sm, rs, pw))
+                except Exception:
+                    pass
+                self._stop.wait(self.period)
+
+        self._thr = threading.Thread(target=loop, daemon=True)
+        self._thr.start()
         return self
 
+    def window(self):
+        s = self
+
+        class _W:
+            def __enter__(self_):
+                s.win[0] = time.perf_counter()
+
+            def __exit__(self_, *a):
+                s.win[1] = time.perf_counter()
+        return _W()
+
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
+        if self._thr is not None:
+            self._stop.set()
+            self._thr.join(timeout=5)
             try:
-                self.proc.wait(timeout=5)
+                import pynvml as nv
+                nv.nvmlShutdown()
             except Exception:
-                self.proc.kill()
-        self.f.close()
+                pass
 
     def summary(self):
-        sm, smax, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        try:
-            for line in open(self.path):
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) < 9:
-                    continue
-                try:
-                    sm.append(float(parts[1]))
-                    smax = max(smax, float(parts[2]))
-                except ValueError:
-                    continue
-                for k, nm in enumerate(names):
-                    if parts[5 + k].lower().startswith("active"):
-                        reasons.add(nm)
-        finally:
-            os.unlink(self.path)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax or None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        t0, t1 = self.win
+        inside = [x for x in self.samples if t0 is not None and t0 <= x[0] <= (t1 or t0)]
+        reasons = sorted({nm for x in inside for nm, bit in self.REASONS if x[2] & bit})
+        return {"sm_mhz": statistics.median([x[1] for x in inside]) if inside else None,
+                "sm_max_mhz": self.sm_max, "reasons": reasons, "samples": len(inside),
+                "power_w_median": statistics.median([x[3] for x in inside]) if inside else None,
+                "source": "NVML, every 50 ms during the timed steps"}
 
 
 def measured_peaks():
@@ -182,7 +210,7 @@ def ncu_traffic(kernel, workload):
 
 def physics_params(E, spec, precision, stream_handle=None, device=0):
     p = E.default_params(box_len=spec.box_len, cutoff=spec.cutoff, dt=spec.dt, semantics=E.SEMANTICS_PHYSICS,
-                         precision=precision, skin=0.1, switch_on=1.0, nlist_period=10, t_target=spec.temperature,
+                         precision=precision, skin=SKIN, switch_on=1.0, nlist_period=10, t_target=spec.temperature,
                          tau_t=spec.tau_t, device=device)
     p.thermostat = E.THERMOSTAT_BERENDSEN if spec.thermostat == "berendsen" else E.THERMOSTAT_NONE
     if stream_handle is not None:
@@ -285,7 +313,9 @@ def run_ours(args, ws, rank, local, pg):
     barrier(pg)
     launches0 = eng.kernel_launches()
     with ClockSampler(local) as clk:
-        ms = timed_steps(eng, stream, args.steps, flush)
+        time.sleep(0.2)
+        with clk.window():
+            ms = timed_steps(eng, stream, args.steps, flush)
     launches = eng.kernel_launches() - launches0
     ms_step = max_over_ranks(ms / args.steps, pg, dev)
     clocks = clk.summary()
@@ -336,7 +366,10 @@ def run_ours(args, ws, rank, local, pg):
     rho = n / spec.box_len ** 3
     pairs = n * (4.0 / 3.0) * math.pi * spec.cutoff ** 3 * rho / 2.0
     t_pair = prof["pair"] * 1e-3
-    bytes_pair = n * 80.0      # read pos, vel; write pos, vel, force (16 B each)
+
+    list_len = (4.0 / 3.0) * math.pi * (spec.cutoff + SKIN) ** 3 * rho    # expected Verlet-list entries
+    # read pos, vel, 4-byte list entries; write pos, vel, force (16 B each)
+    bytes_pair = n * (80.0 + 4.0 * list_len)
     flops_pair = pairs * FLOP_PER_PAIR
     achieved = bytes_pair / t_pair / 1e9
     traffic = ncu_traffic("k_pair_integrate", args.workload)
