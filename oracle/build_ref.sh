@@ -5,7 +5,7 @@
 # infrastructure: the product never loads this library.
 #
 # The reference sources are read from $LIMA_REF_ROOT (default /root/reference)
-# and copied to a temporary directory OUTSIDE the repository, where four
+# and copied to a temporary directory OUTSIDE the repository, where five
 # documented changes are made before compiling; only the built .so is written
 # under oracle/_ref/:
 #   1. Constants.cuh is replaced by oracle/ref_shim/Constants.cuh (runtime box
