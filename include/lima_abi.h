@@ -9,7 +9,7 @@
  * the boundary that replaces it: plain C, plain pointers and sizes, status
  * codes instead of exit(), caller-owned host buffers, library-owned device
  * memory.  The structs below are byte-compatible with the reference's own
- * (sizes in comments; tests/test_layout.py checks them against a build of
+ * (sizes in comments; tests/test_layout_and_abi.py checks them against a build of
  * the reference), so the reference's Box arrays can be passed unchanged.
  *
  * Units are the reference's: positions nm, time ns, mass kg/mol, energy J/mol,
@@ -261,6 +261,43 @@ lima_status lima_profile_steps(lima_ctx* ctx, int n_steps, float* ms);
 /* Number of kernels of this library the context has launched so far
    (graph replays count the kernels they contain). */
 lima_status lima_get_kernel_launches(lima_ctx* ctx, uint64_t* count);
+
+/* ------------------------------------------------------------------ */
+/* No counterpart in the reference.  The reference updates its lists on  */
+/* the host (Engine::updateNeighborLists, Engine.cu:208-287); this is a  */
+/* context-free, allocation-free form of the device build behind          */
+/* lima_build_nlist for the solvent-solvent list.                         */
+/* ------------------------------------------------------------------ */
+#define LIMA_NOALLOC_MAX_SOLVENTS 65536
+
+/* Solvent-solvent neighbour list of the reference semantics,
+   {i<j : within(pos_i, pos_j, cutoff + cutoff)} mirrored to both rows and
+   sorted ascending.  This is what lima_get_nlist(LIMA_NL_SOLVENT_SOLVENT)
+   returns after lima_build_nlist. It is built on caller-owned device buffers
+   and allocates no memory.  It is for callers that cannot allocate device
+   memory: memory reserved up front, or a loop that must not call
+   cudaMalloc/cudaFree, which can wait on other streams' work.  Such callers
+   cannot use lima_ctx, whose buffers lima_finish_box allocates.  The cell grid
+   and staged positions live in one fixed 1,966,080-byte device array of the
+   library.  Hence the limits:
+     n_solvents 1..LIMA_NOALLOC_MAX_SOLVENTS; capacity 32..2048
+     (LIMA_ERR_CAPACITY beyond either).
+   Buffers (device memory of the current device):
+     d_solvents  n_solvents reference Solvent records (only pos is read);
+     d_ids       capacity * n_solvents; entry k of solvent i at d_ids[k * n_solvents + i];
+     d_counts    n_solvents row lengths, clamped to capacity;
+     d_overflow  one int: zeroed by the call; nonzero once the work has run if
+                 a row held more than capacity neighbours.
+   cutoff is the reference CUTOFF (list radius 2 * cutoff).  The work is queued
+   on `stream` (a cudaStream_t; NULL is the default stream) and the call returns
+   without waiting.  The first call on a device looks up the array's address
+   there (cudaGetSymbolAddress), so make it before any stream capture on that
+   device.  Every call on a device shares the one array: calls that overlap in
+   time, from other streams or host threads, race.  err (may be NULL) receives a
+   message on failure. */
+lima_status lima_ss_nlist_noalloc(const lima_solvent* d_solvents, int n_solvents, float box_len, float cutoff,
+                                  int capacity, uint32_t* d_ids, uint32_t* d_counts, int* d_overflow, void* stream,
+                                  char* err, size_t err_len);
 
 #ifdef __cplusplus
 }

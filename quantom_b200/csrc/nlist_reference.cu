@@ -241,3 +241,153 @@ void ref_build_nlists(const RefDev& d, int cur, cudaStream_t s) {
 }
 
 }  // namespace lima
+
+// ---------------------------------------------------------------------------
+// Solvent-solvent list build that allocates no memory.
+//
+// Who needs it: a caller that owns its device memory and cannot hand the
+// library an allocation: a host that reserved the device's memory up front,
+// or a stepping loop that must not call cudaMalloc/cudaFree, which can block
+// on work queued on other streams and can fail once that memory is spoken
+// for.  Such a caller cannot create a lima_ctx, whose buffers lima_finish_box
+// allocates.  This entry point runs the same kernels as the context's build
+// (k_cell_count, k_scan, k_cell_fill, k_ss_list) on caller-owned device
+// buffers.  Its cell grid and the staged float4 positions live in
+// g_noalloc_scratch, one file-scope device array of kNaScratchBytes
+// (1,966,080 bytes): at most LIMA_NOALLOC_MAX_SOLVENTS solvents and a grid of
+// at most 32^3 cells.  A coarser grid leaves the sorted lists unchanged.
+//
+// The array is shared by every call on a device, so calls that overlap in
+// time (other streams, other host threads) race.
+#include <cmath>
+#include <cstdio>
+#include <mutex>
+
+namespace {
+constexpr int kNaMaxM = 32;
+constexpr size_t kNaPosBytes = static_cast<size_t>(LIMA_NOALLOC_MAX_SOLVENTS) * sizeof(float4);
+constexpr size_t kNaItemBytes = static_cast<size_t>(LIMA_NOALLOC_MAX_SOLVENTS) * sizeof(uint32_t);
+constexpr size_t kNaCellBytes = static_cast<size_t>(kNaMaxM) * kNaMaxM * kNaMaxM * sizeof(uint32_t);
+// regions: pos4 | cell_items | sol_cell | cell_count | cell_start | cell_fill (each a multiple of 256 B)
+constexpr size_t kNaScratchBytes = kNaPosBytes + 2 * kNaItemBytes + 3 * kNaCellBytes;
+static_assert(kNaPosBytes % 256 == 0 && kNaItemBytes % 256 == 0 && kNaCellBytes % 256 == 0, "region alignment");
+constexpr int kNaMaxDevices = 64;
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaScratchBytes];
+
+namespace lima {
+namespace {
+
+std::mutex g_na_mu;
+void* g_na_addr[kNaMaxDevices] = {};
+
+__global__ void k_na_stage(const lima_solvent* __restrict__ sol, float4* __restrict__ pos, int n) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) {
+        const lima_float3 p = sol[s].pos;
+        pos[s] = make_float4(p.x, p.y, p.z, 0.f);
+    }
+}
+
+lima_status na_fail(char* err, size_t err_len, lima_status st, const char* msg) {
+    if (err && err_len) std::snprintf(err, err_len, "%s", msg);
+    return st;
+}
+
+}  // namespace
+}  // namespace lima
+
+extern "C" lima_status lima_ss_nlist_noalloc(const lima_solvent* d_solvents, int n_solvents, float box_len,
+                                             float cutoff, int capacity, uint32_t* d_ids, uint32_t* d_counts,
+                                             int* d_overflow, void* stream, char* err, size_t err_len) {
+    using namespace lima;
+    char msg[160];
+    if (err && err_len) err[0] = '\0';
+    if (n_solvents < 1) return na_fail(err, err_len, LIMA_ERR_ARGUMENT, "n_solvents must be at least 1");
+    if (n_solvents > LIMA_NOALLOC_MAX_SOLVENTS) {
+        std::snprintf(msg, sizeof msg, "n_solvents %d exceeds the no-allocation maximum of %d", n_solvents,
+                      LIMA_NOALLOC_MAX_SOLVENTS);
+        return na_fail(err, err_len, LIMA_ERR_CAPACITY, msg);
+    }
+    if (capacity < 32 || capacity > 2048)
+        return na_fail(err, err_len, LIMA_ERR_CAPACITY, "capacity outside 32..2048");
+    if (!(box_len > 0.f) || !std::isfinite(box_len) || !(cutoff > 0.f) || !std::isfinite(cutoff))
+        return na_fail(err, err_len, LIMA_ERR_ARGUMENT, "box_len and cutoff must be positive and finite");
+    if (!d_solvents || !d_ids || !d_counts || !d_overflow)
+        return na_fail(err, err_len, LIMA_ERR_ARGUMENT, "null device buffer");
+    if ((reinterpret_cast<uintptr_t>(d_solvents) | reinterpret_cast<uintptr_t>(d_ids) |
+         reinterpret_cast<uintptr_t>(d_counts) | reinterpret_cast<uintptr_t>(d_overflow)) & 3u)
+        return na_fail(err, err_len, LIMA_ERR_ARGUMENT, "device buffers must be 4-byte aligned");
+
+    // scratch address on the current device, looked up on the first call there
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return na_fail(err, err_len, LIMA_ERR_CUDA, "cudaGetDevice failed");
+    if (dev < 0 || dev >= kNaMaxDevices) return na_fail(err, err_len, LIMA_ERR_UNSUPPORTED, "device ordinal >= 64");
+    unsigned char* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_na_mu);
+        if (!g_na_addr[dev]) {
+            void* p = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess || !p) {
+                std::snprintf(msg, sizeof msg, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+                return na_fail(err, err_len, LIMA_ERR_CUDA, msg);
+            }
+            g_na_addr[dev] = p;
+        }
+        base = static_cast<unsigned char*>(g_na_addr[dev]);
+    }
+
+    RefDev d{};
+    d.n_s = n_solvents;
+    d.L = box_len;
+    d.Lh = box_len / 2.f;
+    d.C = cutoff;
+    // the context's grid rule (cells no smaller than the list radius C + C), capped at 32 per side
+    const float radius = d.C + d.C;
+    int m = static_cast<int>(std::floor(d.L / (radius * 1.0001f)));
+    if (m < 3) m = 1;
+    while (m > 1 && d.L / static_cast<float>(m) < radius) m--;
+    if (m < 3) m = 1;
+    if (m > kNaMaxM) m = kNaMaxM;
+    d.m = m;
+    d.cell = d.L / static_cast<float>(m);
+    const int ncells = m * m * m;
+    float4* pos4 = reinterpret_cast<float4*>(base);
+    d.spos[0] = d.spos[1] = pos4;
+    d.cell_items = reinterpret_cast<uint32_t*>(base + kNaPosBytes);
+    d.sol_cell = reinterpret_cast<uint32_t*>(base + kNaPosBytes + kNaItemBytes);
+    d.cell_count = reinterpret_cast<uint32_t*>(base + kNaPosBytes + 2 * kNaItemBytes);
+    d.cell_start = reinterpret_cast<uint32_t*>(base + kNaPosBytes + 2 * kNaItemBytes + kNaCellBytes);
+    d.cell_fill = reinterpret_cast<uint32_t*>(base + kNaPosBytes + 2 * kNaItemBytes + 2 * kNaCellBytes);
+    d.ss_ids = d_ids;
+    d.ss_cnt = d_counts;
+    d.ss_cap = capacity;
+    d.err = d_overflow;
+
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // start at zero: the per-cell counters (atomic counts and fill cursors) and the overflow flag
+    cudaError_t e = cudaMemsetAsync(d.cell_count, 0, sizeof(uint32_t) * ncells, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d.cell_fill, 0, sizeof(uint32_t) * ncells, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_overflow, 0, sizeof(int), s);
+    if (e != cudaSuccess) {
+        std::snprintf(msg, sizeof msg, "cudaMemsetAsync: %s", cudaGetErrorString(e));
+        return na_fail(err, err_len, LIMA_ERR_CUDA, msg);
+    }
+    const int tb = 256, nb = (n_solvents + tb - 1) / tb;
+    k_na_stage<<<nb, tb, 0, s>>>(d_solvents, pos4, n_solvents);
+    k_cell_count<<<nb, tb, 0, s>>>(d, 0);
+    k_scan<<<1, 1024, 0, s>>>(d.cell_count, d.cell_start, ncells);
+    k_cell_fill<<<nb, tb, 0, s>>>(d);
+    int cap2 = 32;
+    while (cap2 < capacity) cap2 <<= 1;
+    constexpr int W = 4;
+    k_ss_list<W><<<(n_solvents + W - 1) / W, W * 32, W * cap2 * sizeof(uint32_t), s>>>(d, 0, cap2);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        std::snprintf(msg, sizeof msg, "kernel launch: %s", cudaGetErrorString(e));
+        return na_fail(err, err_len, LIMA_ERR_CUDA, msg);
+    }
+    return LIMA_OK;
+}
