@@ -18,10 +18,9 @@
 //                     branch-free LJ + switch, partial forces reduced with
 //                     warp shuffles; lane 0 gathers the bonded term forces,
 //                     kicks, drifts and adds 1/2 m v^2 to the FP64 accumulator
-// Every nlist_period steps (physics_host.cu): sort, permute, k_build_list —
-// 8 lanes per particle over the 5x5x5 neighbouring cells, a cell skipped by
-// the whole warp when its box is beyond r_list of all 4 of the warp's
-// particles.
+// Every nlist_period steps (physics_host.cu): k_keys, a radix sort by cell,
+// k_permute, and k_build_list — one warp per cell over the 25 columns of its
+// 5x5x5 neighbourhood.
 #include "physdev.cuh"
 #include "physkern.cuh"
 #include "refdev.cuh"
@@ -72,19 +71,6 @@ __device__ __forceinline__ bool excluded(const PhysDev& d, uint32_t oi, uint32_t
     for (uint32_t q = d.excl_off[oi]; q < d.excl_off[oi + 1]; q++)
         if (d.excl_ids[q] == oj) return true;
     return false;
-}
-
-// squared distance from p to the box of cell (x, y, z), periodic
-__device__ __forceinline__ float box_d2(const PhysDev& d, float4 p, int x, int y, int z) {
-    const float cs = d.L / (float)d.m;
-    auto axis = [&](float v, int c) {
-        const float lo = c * cs;
-        float dd = v - (lo + 0.5f * cs);
-        dd = mimg(dd, d.L, d.invL);
-        return fmaxf(fabsf(dd) - 0.5f * cs, 0.f);
-    };
-    const float ax = axis(p.x, x), ay = axis(p.y, y), az = axis(p.z, z);
-    return ax * ax + ay * ay + az * az;
 }
 
 // Fold an accumulator slot into e_last; parity slots also set the next
@@ -141,59 +127,140 @@ __global__ void k_permute(PhysDev d, int cur, int mixed) {
     d.orig_tmp[k] = o;
     d.sorted_of_orig[o] = k;
     d.xref[k] = p;
+    // cstart[c] = first sorted slot of cell c for every c in 0..n_cells (empty cells included)
     const uint32_t c = d.keys[1][k];
-    if (k == 0 || d.keys[1][k - 1] != c) d.cstart[c] = k;
-    if (k == d.n - 1 || d.keys[1][k + 1] != c) d.cend[c] = k + 1;
+    if (k == 0) {
+        for (uint32_t q = 0; q <= c; q++) d.cstart[q] = 0;
+    } else {
+        const uint32_t cp = d.keys[1][k - 1];
+        for (uint32_t q = cp + 1; q <= c; q++) d.cstart[q] = k;
+    }
+    if (k == d.n - 1)
+        for (uint32_t q = c + 1; q <= (uint32_t)d.n_cells; q++) d.cstart[q] = d.n;
 }
 
-// kGroup lanes per particle.  Cells are visited in a fixed order and their
-// members kGroup at a time, compacted with a ballot, so the list order is
-// deterministic.  A cell is skipped when its box is beyond r_list of every
-// particle of the warp.
-// One thread per particle, no warp collectives: the thread appends its
-// neighbours in cell order (so the list order is deterministic) into the
-// blocked layout the pair kernel reads.
-__global__ void __launch_bounds__(kTB) k_build_list(PhysDev d, int cur) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= d.n) return;
-    const float4 pi = d.pos[cur][i];
-    const uint32_t oi = d.orig_of_sorted[i];
-    const bool cpi = oi < (uint32_t)d.n_cp && d.excl_off[oi + 1] > d.excl_off[oi];
-    int cx, cy, cz;
-    cell_xyz(d, pi, cx, cy, cz);
+// One warp per home cell.  The home cell's particles, 32 at a time, are the
+// i side.  The candidates are the 25 columns of 5 cells along z around it:
+// cells (x, y, z..z+4) have consecutive keys, so a column is one contiguous
+// slot range of the cell-sorted order (two where it wraps around the box).
+// Lanes take 32 candidates at a time, shifted by whole box lengths into the
+// home cell's frame (no minimum image per pair), and test them against each
+// home particle whose distance to the range's box is below r_list (a ballot
+// per range picks those).  A ballot per home particle appends its hits in
+// candidate order, so every row is deterministic.  Every loop bound and every
+// collective below is warp-uniform.  Boxes with fewer than 5 cells per side
+// scan all particles with the minimum image instead.
+__global__ void __launch_bounds__(kBuildWarps * 32) k_build_list(PhysDev d, int cur) {
+    __shared__ float4 s_pi[kBuildWarps][32];
+    __shared__ uint32_t s_oi[kBuildWarps][32];   // orig id | bit 31 when the particle has exclusions
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int c = blockIdx.x * kBuildWarps + w;
+    if (c >= d.n_cells) return;   // the whole warp
+    const float4* __restrict__ pos = d.pos[cur];
     const int m = d.m;
-    int cnt = 0;
-    for (int q = 0; q < d.nbr; q++) {
-        int x, y, z;
-        if (m >= 5) {
-            x = (cx + q / 25 - 2 + m) % m;
-            y = (cy + (q / 5) % 5 - 2 + m) % m;
-            z = (cz + q % 5 - 2 + m) % m;
-        } else {
-            x = q / (m * m);
-            y = (q / m) % m;
-            z = q % m;
+    const float cs = d.L / (float)m;
+    const float lim2 = d.rlist2 * 1.001f;   // range pruning keeps a margin for cell-boundary rounding
+    const int cx = c / (m * m), cy = (c / m) % m, cz = c % m;
+    const int hb = (int)d.cstart[c], he = (int)d.cstart[c + 1];
+    const unsigned lt = (1u << lane) - 1u;
+
+    for (int i0 = hb; i0 < he; i0 += 32) {
+        const int ni = min(32, he - i0);
+        __syncwarp();
+        float4 my_p = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (lane < ni) {
+            my_p = pos[i0 + lane];
+            const uint32_t o = d.orig_of_sorted[i0 + lane];
+            const bool ex = o < (uint32_t)d.n_cp && d.excl_off[o + 1] > d.excl_off[o];
+            s_pi[w][lane] = my_p;
+            s_oi[w][lane] = o | (ex ? 0x80000000u : 0u);
         }
-        if (box_d2(d, pi, x, y, z) >= d.rlist2) continue;
-        const int c = (x * m + y) * m + z;
-        const int b = (int)d.cstart[c], e = (int)d.cend[c];
-        for (int j = b; j < e; j++) {
-            if (j == i) continue;
-            const float4 pj = d.pos[cur][j];
-            const float dx = mimg(pj.x - pi.x, d.L, d.invL);
-            const float dy = mimg(pj.y - pi.y, d.L, d.invL);
-            const float dz = mimg(pj.z - pi.z, d.L, d.invL);
-            if (dx * dx + dy * dy + dz * dz >= d.rlist2) continue;
-            if (cpi) {
-                const uint32_t oj = d.orig_of_sorted[j];
-                if (oj < (uint32_t)d.n_cp && excluded(d, oi, oj)) continue;
+        __syncwarp();
+        int my_cnt = 0;
+
+        // candidates [jb, je), shifted by (sx, sy, sz); (lo, hi) = their box in the home frame
+        auto scan = [&](int jb, int je, float sx, float sy, float sz, float3 lo, float3 hi, bool min_image) {
+            unsigned live;
+            if (min_image) {
+                live = __ballot_sync(0xffffffffu, lane < ni);
+            } else {
+                const float gx = fmaxf(fmaxf(lo.x - my_p.x, my_p.x - hi.x), 0.f);
+                const float gy = fmaxf(fmaxf(lo.y - my_p.y, my_p.y - hi.y), 0.f);
+                const float gz = fmaxf(fmaxf(lo.z - my_p.z, my_p.z - hi.z), 0.f);
+                live = __ballot_sync(0xffffffffu, lane < ni && gx * gx + gy * gy + gz * gz < lim2);
             }
-            if (cnt < d.nl_cap) d.nl[nl_index(d, i, cnt)] = (uint32_t)j;
-            cnt++;
+            if (!live) return;
+            for (int jc = jb; jc < je; jc += 32) {
+                const int j = jc + lane;
+                const bool valid = j < je;
+                float4 pj = valid ? pos[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+                pj.x += sx;
+                pj.y += sy;
+                pj.z += sz;
+                for (unsigned r = live; r; r &= r - 1u) {
+                    const int ii = __ffs(r) - 1;
+                    const float4 pi = s_pi[w][ii];
+                    float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+                    if (min_image) {
+                        dx = mimg(dx, d.L, d.invL);
+                        dy = mimg(dy, d.L, d.invL);
+                        dz = mimg(dz, d.L, d.invL);
+                    }
+                    bool hit = valid && j != i0 + ii && dx * dx + dy * dy + dz * dz < d.rlist2;
+                    const uint32_t oi = s_oi[w][ii];
+                    if (hit && (oi & 0x80000000u)) {
+                        const uint32_t oj = d.orig_of_sorted[j];
+                        if (oj < (uint32_t)d.n_cp && excluded(d, oi & 0x7fffffffu, oj)) hit = false;
+                    }
+                    const unsigned mask = __ballot_sync(0xffffffffu, hit);
+                    if (mask) {
+                        const int base = __shfl_sync(0xffffffffu, my_cnt, ii);
+                        if (hit) {
+                            const int k = base + __popc(mask & lt);
+                            if (k < d.nl_cap) d.nl[nl_index(d, i0 + ii, k)] = (uint32_t)j;
+                        }
+                        if (lane == ii) my_cnt += __popc(mask);
+                    }
+                }
+            }
+        };
+
+        if (m < 5) {
+            scan(0, d.n, 0.f, 0.f, 0.f, make_float3(0.f, 0.f, 0.f), make_float3(0.f, 0.f, 0.f), true);
+        } else {
+            for (int ox = -2; ox <= 2; ox++) {
+                int x = cx + ox;
+                float sx = 0.f;
+                if (x < 0) { x += m; sx = -d.L; } else if (x >= m) { x -= m; sx = d.L; }
+                for (int oy = -2; oy <= 2; oy++) {
+                    int y = cy + oy;
+                    float sy = 0.f;
+                    if (y < 0) { y += m; sy = -d.L; } else if (y >= m) { y -= m; sy = d.L; }
+                    const int col = (x * m + y) * m;
+                    const float x0 = (cx + ox) * cs, y0 = (cy + oy) * cs;
+                    auto run = [&](int za, int zb, float sz, int zhome) {   // cells za..zb, home-frame cell zhome
+                        scan((int)d.cstart[col + za], (int)d.cstart[col + zb + 1], sx, sy, sz,
+                             make_float3(x0, y0, zhome * cs), make_float3(x0 + cs, y0 + cs, (zhome + zb - za + 1) * cs),
+                             false);
+                    };
+                    const int z0 = cz - 2, z1 = cz + 2;
+                    if (z0 < 0) {
+                        run(z0 + m, m - 1, -d.L, z0);
+                        run(0, z1, 0.f, 0);
+                    } else if (z1 >= m) {
+                        run(z0, m - 1, 0.f, z0);
+                        run(0, z1 - m, d.L, m);
+                    } else {
+                        run(z0, z1, 0.f, z0);
+                    }
+                }
+            }
+        }
+        if (lane < ni) {
+            d.nl_cnt[i0 + lane] = (uint32_t)min(my_cnt, d.nl_cap);
+            if (my_cnt > d.nl_cap) atomicOr(d.err, ERR_BIT_PHYS_LIST_OVERFLOW);
         }
     }
-    d.nl_cnt[i] = min(cnt, d.nl_cap);
-    if (cnt > d.nl_cap) atomicOr(d.err, ERR_BIT_PHYS_LIST_OVERFLOW);
 }
 
 // ----------------------------------------------------------------- bonded ---
@@ -534,8 +601,6 @@ void pair_variant(const PhysDev& d, int cur, int slot, cudaStream_t s) {
 
 }  // namespace
 
-void physics_kernel_attributes(const PhysDev&) {}
-
 void launch_keys(const PhysDev& d, int cur, cudaStream_t s) {
     k_keys<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d, cur);
 }
@@ -545,7 +610,7 @@ void launch_permute(const PhysDev& d, int cur, bool mixed, cudaStream_t s) {
 }
 
 void launch_build_list(const PhysDev& d, int cur, cudaStream_t s) {
-    k_build_list<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d, cur);
+    k_build_list<<<(d.n_cells + kBuildWarps - 1) / kBuildWarps, kBuildWarps * 32, 0, s>>>(d, cur);
 }
 
 void launch_bonded(const PhysDev& d, int cur, bool energy, int slot, int fold_src, cudaStream_t s) {

@@ -8,8 +8,8 @@
 // Cells: a uniform grid of m^3 cells of side >= r_list/2, so every particle
 // within r_list of a cell lies in the 5x5x5 block of cells around it (all
 // m^3 cells when m < 5).  A cell's particles occupy a contiguous slot range
-// [cstart, cend), so a cell's neighbourhood ("tile") is 125 contiguous ranges
-// that the step kernels stage into shared memory with bulk copies.
+// [cstart[c], cstart[c+1]), and cells (x, y, z..z+4) are consecutive, so a
+// neighbourhood is 25 contiguous ranges (columns along z).
 //
 // HBM layout (float3 quantities widened to float4, one 16-byte access each):
 //   pos[2][n_pad]   x, y, z in [0, L), w = type index (bit-cast)   (double-buffered)
@@ -17,8 +17,9 @@
 //   posc/velc       low parts of pos/vel (mixed precision)
 //   xref[n_pad]     positions at the last rebuild (list validity check)
 //   force[n_pad]    total force of the last evaluation, w = per-particle LJ energy
-//   nl[cap][n_pad]  Verlet list of 16-bit tile-local indices, blocked so that
-//                   the kGroup lanes of one particle read kGroup consecutive
+//   nl[cap][n_pad]  Verlet list of sorted slots, entry k of particle i at
+//                   ((k / kGroup) * n_pad + i) * kGroup + k % kGroup: the
+//                   kGroup lanes of one particle read kGroup consecutive
 //                   entries and consecutive particles follow each other
 //   term_force      one float4 per (term, atom) of every bonded term; gathered
 //                   per particle through bterm_off/bterm_slot (CSR over orig)
@@ -60,12 +61,10 @@ struct PhysDev {
     // cell grid
     int m;                      // cells per dimension
     int n_cells;                // m^3
-    int nbr;                    // cells in a neighbourhood: 125, or m^3 when m < 5
-    int tile_cap;               // staged particles per block (shared memory capacity)
     uint32_t* keys[2];
     uint32_t* vals[2];
     void* sort_tmp; size_t sort_tmp_bytes;
-    uint32_t* cstart; uint32_t* cend;
+    uint32_t* cstart;           // [n_cells + 1]: cell c holds sorted slots [cstart[c], cstart[c+1])
     float4* pos_tmp; float4* vel_tmp; float4* posc_tmp; float4* velc_tmp; uint32_t* orig_tmp;
     // Verlet list (tile-local indices)
     uint32_t* nl; uint32_t* nl_cnt; int nl_cap;

@@ -182,21 +182,12 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
         bslot.insert(bslot.end(), slots[i].begin(), slots[i].end());
     }
 
-    // cell grid (side >= rlist/2: the 5x5x5 neighbourhood covers rlist),
-    // shared-memory tile capacity and Verlet-list capacity
+    // cell grid (side >= rlist/2: the 5x5x5 neighbourhood covers rlist) and
+    // Verlet-list capacity
     const float half = 0.5f * d.rlist;
     d.m = std::max(1, (int)std::floor(d.L / half));
     while (d.m > 1 && d.L / d.m < half) d.m--;
     d.n_cells = d.m * d.m * d.m;
-    d.nbr = d.m >= 5 ? 125 : d.n_cells;
-    const double per_cell = (double)d.n / d.n_cells;
-    const double tile_expect = d.m >= 5 ? 125.0 * per_cell : (double)d.n;
-    d.tile_cap = d.m >= 5 ? (int)std::min<double>(d.n, tile_expect + 8.0 * std::sqrt(tile_expect) + 64) : d.n;
-    d.tile_cap = (d.tile_cap + 7) / 8 * 8;
-    if (d.tile_cap > 12288) {
-        msg = "particle density too high for the shared-memory tile (more than 12288 particles per 5x5x5 cells)";
-        return LIMA_ERR_ARGUMENT;
-    }
     const double rho = d.n / ((double)d.L * d.L * d.L);
     const double expect = 4.0 / 3.0 * M_PI * (double)d.rlist * d.rlist * d.rlist * rho;
     d.nl_cap = std::min((d.n + kGroup - 1) / kGroup * kGroup, (int)((1.6 * expect + 96) / kGroup + 1) * kGroup);
@@ -216,8 +207,7 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
             d.keys[b] = dalloc<uint32_t>(allocs, d.n);
             d.vals[b] = dalloc<uint32_t>(allocs, d.n);
         }
-        d.cstart = dalloc<uint32_t>(allocs, d.n_cells);
-        d.cend = dalloc<uint32_t>(allocs, d.n_cells);
+        d.cstart = dalloc<uint32_t>(allocs, (size_t)d.n_cells + 1);
         d.pos_tmp = dalloc<float4>(allocs, d.n);
         d.vel_tmp = dalloc<float4>(allocs, d.n);
         d.posc_tmp = dalloc<float4>(allocs, d.n);
@@ -268,7 +258,6 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
     cudaMemsetAsync(d.err, 0, sizeof(int), s);
     cudaMemsetAsync(d.nl_cnt, 0, sizeof(uint32_t) * d.n_pad, s);
     cudaMemsetAsync(d.force, 0, sizeof(float4) * d.n_pad, s);
-    physics_kernel_attributes(d);
     phys_upload_state(h, d, 0, s);
     return cudaGetLastError() == cudaSuccess ? 0 : LIMA_ERR_CUDA;
 }
@@ -330,8 +319,6 @@ void phys_rebuild(PhysDev& d, int cur, cudaStream_t s) {
     int end_bit = 1;
     while ((1ull << end_bit) < (unsigned long long)ncell) end_bit++;
     cub::DeviceRadixSort::SortPairs(d.sort_tmp, bytes, d.keys[0], d.keys[1], d.vals[0], d.vals[1], d.n, 0, end_bit, s);
-    cudaMemsetAsync(d.cstart, 0, sizeof(uint32_t) * ncell, s);
-    cudaMemsetAsync(d.cend, 0, sizeof(uint32_t) * ncell, s);
     launch_permute(d, cur, mixed, s);
     cudaMemcpyAsync(d.pos[cur], d.pos_tmp, sizeof(float4) * d.n, cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(d.vel, d.vel_tmp, sizeof(float4) * d.n, cudaMemcpyDeviceToDevice, s);

@@ -9,10 +9,9 @@ namespace lima {
 
 constexpr int kTB = 256;         // threads per block of the per-particle / per-term kernels
 constexpr int kGroup = 8;        // lanes per particle in the list and pair kernels
-constexpr int kCellBlock = 128;  // threads per cell block (16 particles per pass)
+constexpr int kBuildWarps = 4;   // warps (home cells) per block of the list build
 constexpr int kMaxTypes = 32;    // LIMA_MAX_ATOM_TYPES
 
-void physics_kernel_attributes(const PhysDev& d);
 void launch_keys(const PhysDev& d, int cur, cudaStream_t s);
 void launch_permute(const PhysDev& d, int cur, bool mixed, cudaStream_t s);
 void launch_build_list(const PhysDev& d, int cur, cudaStream_t s);
