@@ -4,7 +4,8 @@
 Workload: the 32,024-particle solvated-chain box (16 chains x 64 particles in
 31,000 single-site solvents, 10 nm periodic box, 1.2 nm cutoff, Berendsen
 300 K, dt 2 fs), seeded synthetic input.  One "step" is one MD step (forces,
-integration, thermostat; a list rebuild every 10 steps).
+integration, thermostat; the pair list is rebuilt, inside the step's CUDA
+graph, whenever a particle has moved more than skin/2).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -47,8 +48,11 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-sample-steps", type=int, default=2)
-    ap.add_argument("--mode", default="full", choices=["full", "kernels"],
-                    help="kernels: only warm-up + K plain-FP32 steps (the command profiled with ncu)")
+    ap.add_argument("--mode", default="full", choices=["full", "kernels", "precision"],
+                    help="kernels: only warm-up + K plain-FP32 steps (the command profiled with ncu); "
+                         "precision: the NVE drift / force-error study of plain FP32 against mixed precision")
+    ap.add_argument("--nve-steps", type=int, default=50000, help="--mode precision: NVE steps per run")
+    ap.add_argument("--eq-steps", type=int, default=5000, help="--mode precision: Berendsen equilibration steps")
     ap.add_argument("--semantics", default="physics", choices=["physics", "reference"],
                     help="semantics of --mode kernels")
     return ap.parse_args()
@@ -208,9 +212,10 @@ def ncu_traffic(kernel, workload):
     return None
 
 
-def physics_params(E, spec, precision, stream_handle=None, device=0):
-    p = E.default_params(box_len=spec.box_len, cutoff=spec.cutoff, dt=spec.dt, semantics=E.SEMANTICS_PHYSICS,
-                         precision=precision, skin=SKIN, switch_on=1.0, nlist_period=10, t_target=spec.temperature,
+def physics_params(E, spec, precision, stream_handle=None, device=0, dt=None):
+    p = E.default_params(box_len=spec.box_len, cutoff=spec.cutoff, dt=spec.dt if dt is None else dt,
+                         semantics=E.SEMANTICS_PHYSICS,
+                         precision=precision, skin=SKIN, switch_on=1.0, nlist_period=0, t_target=spec.temperature,
                          tau_t=spec.tau_t, device=device)
     p.thermostat = E.THERMOSTAT_BERENDSEN if spec.thermostat == "berendsen" else E.THERMOSTAT_NONE
     if stream_handle is not None:
@@ -238,6 +243,115 @@ def timed_steps(eng, stream, n, flush):
 
 def ns_per_day(dt_ns, ms_per_step):
     return dt_ns * NS_PER_DAY_S / (ms_per_step * 1e-3)
+
+
+# ------------------------------------------------------- precision study --
+K_B = 8.314462618        # J/(mol K)
+
+
+def with_state(system, st, prev, sol):
+    """The same topology with positions/previous positions from a readback."""
+    import copy
+    s = copy.copy(system)
+    s.compounds = system.compounds.copy()
+    s.states = system.states.copy()
+    s.solvents = sol.copy()
+    for c in range(system.n_compounds):
+        s.states[c]["positions"] = st[c]["positions"]
+        s.compounds[c]["prev_positions"] = prev[c]
+    return s
+
+
+def rescale_dt(system, factor):
+    """Previous positions for a time step `factor` times the current one
+    (same velocities: x_prev' = x - factor * (x - x_prev))."""
+    import copy
+    s = copy.copy(system)
+    s.compounds = system.compounds.copy()
+    s.solvents = system.solvents.copy()
+    for c in range(system.n_compounds):
+        x = system.states[c]["positions"].astype(np.float64)
+        xp = system.compounds[c]["prev_positions"].astype(np.float64)
+        s.compounds[c]["prev_positions"] = (x - factor * (x - xp)).astype(np.float32)
+    x = system.solvents["pos"].astype(np.float64)
+    xp = system.solvents["pos_tsub1"].astype(np.float64)
+    s.solvents["pos_tsub1"] = (x - factor * (x - xp)).astype(np.float32)
+    return s
+
+
+def flat_forces(system, fc, fs):
+    parts = [fc[c, : system.compounds[c]["n_particles"]] for c in range(system.n_compounds)]
+    return np.concatenate(parts + [fs]) if parts else fs
+
+
+def run_precision(args):
+    """Config-2 study on the 32k box: Berendsen equilibration, then NVE runs
+    of plain FP32 and mixed precision at dt 2 fs and 1 fs.  Drift = slope of
+    a linear fit of the total energy, per particle, in kT per ns.  Force error
+    = relative RMS against the FP64 oracle at the same positions."""
+    from oracle import pyoracle as po
+    from quantom_b200 import engine as E
+    from quantom_b200 import systems as S
+    spec = S.CONFIGS[args.workload]
+    system = S.make_system(args.workload, seed=args.seed)
+    n = system.n_particles
+    kT = K_B * spec.temperature
+    with E.Engine(system, physics_params(E, spec, E.PRECISION_FP32)) as eq:
+        eq.step(args.eq_steps)
+        st, prev = eq.compound_states()
+        sol = eq.solvents()
+    start = with_state(system, st, prev, sol)
+
+    def force_errors(sys_x):
+        F64, _ = po.PhysSystem(sys_x, rc=spec.cutoff, r_on=1.0).forces()
+        out = {}
+        for name, prec in (("fp32", E.PRECISION_FP32), ("mixed", E.PRECISION_MIXED)):
+            p = physics_params(E, spec, prec)
+            p.thermostat = E.THERMOSTAT_NONE
+            with E.Engine(sys_x, p) as eng:
+                eng.compute_energies()
+                F = flat_forces(sys_x, *eng.forces()).astype(np.float64)
+            out[name] = float(np.sqrt(((F - F64) ** 2).sum() / (F64 ** 2).sum()))
+        return out
+
+    result = {"mode": "precision", "workload": args.workload, "particles": n, "eq_steps": args.eq_steps,
+              "nve_steps": args.nve_steps, "force_relrms_vs_fp64": {"start": force_errors(start)}, "runs": []}
+    block = 100
+    for dt_fs in (2.0, 1.0):
+        sys_dt = rescale_dt(start, dt_fs * 1e-6 / spec.dt)
+        for name, prec in (("fp32", E.PRECISION_FP32), ("mixed", E.PRECISION_MIXED)):
+            p = physics_params(E, spec, prec, dt=dt_fs * 1e-6)
+            p.thermostat = E.THERMOSTAT_NONE
+            t_ns, etot, temp = [], [], []
+            with E.Engine(sys_dt, p) as eng:
+                for b in range(args.nve_steps // block + 1):
+                    e = eng.compute_energies()
+                    t_ns.append(b * block * dt_fs * 1e-6)
+                    etot.append(e[E.E_TOTAL])
+                    temp.append(e[E.E_TEMPERATURE])
+                    if b < args.nve_steps // block:
+                        eng.step(block)
+                if dt_fs == 2.0 and name == "fp32":
+                    st2, prev2 = eng.compound_states()
+                    end = with_state(system, st2, prev2, eng.solvents())
+            t = np.asarray(t_ns)
+            et = np.asarray(etot)
+            slope = float(np.polyfit(t, et, 1)[0])            # J/mol per ns
+            resid = et - np.polyval(np.polyfit(t, et, 1), t)
+            result["runs"].append({
+                "precision": name, "dt_fs": dt_fs, "simulated_ps": float(t[-1] * 1e3),
+                "drift_kT_per_particle_per_ns": slope / (n * kT),
+                "drift_J_per_mol_per_ns": slope,
+                "etot_fluct_rms_kT_per_particle": float(resid.std() / (n * kT)),
+                "temperature_mean_K": float(np.mean(temp)), "temperature_first_last_K": [temp[0], temp[-1]],
+            })
+            print(json.dumps(result["runs"][-1]), flush=True)
+    result["force_relrms_vs_fp64"]["after_nve_fp32_2fs"] = force_errors(end)
+    for dt_fs in (2.0, 1.0):
+        r = {x["precision"]: x for x in result["runs"] if x["dt_fs"] == dt_fs}
+        result[f"drift_ratio_fp32_over_mixed_{int(dt_fs)}fs"] = (
+            abs(r["fp32"]["drift_kT_per_particle_per_ns"]) / max(abs(r["mixed"]["drift_kT_per_particle_per_ns"]), 1e-30))
+    print(json.dumps(result), flush=True)
 
 
 # --------------------------------------------------------------- CPU side --
@@ -312,21 +426,23 @@ def run_ours(args, ws, rank, local, pg):
     timed_steps(eng, stream, max(3, args.warmup), flush)
     barrier(pg)
     launches0 = eng.kernel_launches()
+    rebuilds0 = eng.rebuild_count()
     with ClockSampler(local) as clk:
         time.sleep(0.2)
         with clk.window():
             ms = timed_steps(eng, stream, args.steps, flush)
     launches = eng.kernel_launches() - launches0
+    steps_per_rebuild = args.steps / max(1, eng.rebuild_count() - rebuilds0)
     ms_step = max_over_ranks(ms / args.steps, pg, dev)
     clocks = clk.summary()
-    prof = eng.profile_steps(50)
+    prof = eng.profile_steps(200)
     eng.close()
 
     # ---- mixed precision, same protocol ------------------------------------
     engm = E.Engine(system, physics_params(E, spec, E.PRECISION_MIXED, stream.cuda_stream, local))
     timed_steps(engm, stream, max(3, args.warmup // 2), flush)
     ms_mixed = timed_steps(engm, stream, max(50, args.steps // 2), flush) / max(50, args.steps // 2)
-    prof_m = engm.profile_steps(50)
+    prof_m = engm.profile_steps(200)
     engm.close()
 
     # ---- the reference's own semantics on the GPU, same workload ------------
@@ -386,7 +502,7 @@ def run_ours(args, ws, rank, local, pg):
         "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
         "config": {"workload": f"{args.workload}: 16 chains x 64 + 31,000 solvents, 10 nm box, rc 1.2 nm "
-                               f"(switch from 1.0), skin 0.1 nm, list every 10 steps, Berendsen 300 K tau 0.1 ps, "
+                               f"(C2 switch from 1.0), skin 0.1 nm, list rebuilt when a particle moved > skin/2, Berendsen 300 K tau 0.1 ps, "
                                f"dt 2 fs, plain FP32", "particles": n,
                    "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
                    "l2": "flushed before every timed step (256 MiB memset on the engine stream, outside the timed "
@@ -405,6 +521,7 @@ def run_ours(args, ws, rank, local, pg):
                 "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                 "note": "box uploaded from host arrays inside the timed region; per-step FP64 energies read back"},
         "gpu_launches": launches,
+        "steps_per_list_rebuild": steps_per_rebuild,
         "clocks": clocks,
     }
     if cpu:
@@ -416,6 +533,9 @@ def main():
     args = parse()
     if args.mode == "kernels":
         run_kernels_only(args)
+        return
+    if args.mode == "precision":
+        run_precision(args)
         return
     ws, rank, local, pg = dist_setup(args) if args.impl == "ours" else (int(os.environ.get("WORLD_SIZE", "1")),
                                                                         int(os.environ.get("RANK", "0")), 0, None)

@@ -143,9 +143,13 @@ typedef struct {
     float ref_cutoff;          /* nm, the reference's CUTOFF constant (Constants.cuh:52); lists use 2*ref_cutoff.
                                   0 = cutoff/2, so both semantics see the same list radius */
     float skin;                /* nm, Verlet buffer of the physics list */
-    float switch_on;           /* nm, start of the potential switch (physics); >= cutoff: plain shifted cutoff */
+    float switch_on;           /* nm, start of the C2 potential switch S = t^3 (10 - 15 t + 6 t^2),
+                                  t = (cutoff^2 - r^2) / (cutoff^2 - switch_on^2) (physics); >= cutoff: plain shifted cutoff */
     double dt;                 /* ns */
-    int nlist_period;          /* steps between list rebuilds (reference: 200, Constants.cuh:71) */
+    int nlist_period;          /* steps between list rebuilds (reference: 200, Constants.cuh:71); physics
+                                  semantics: <= 0 rebuilds when a particle has moved more than skin/2
+                                  (decided on the device), > 0 rebuilds every nlist_period steps and
+                                  reports a list gone stale in between as LIMA_ERR_NUMERIC */
     int semantics;             /* lima_semantics */
     int precision;             /* lima_precision */
     int thermostat;            /* lima_thermostat */
@@ -236,6 +240,12 @@ lima_status lima_compute_energies(lima_ctx* ctx);
 lima_status lima_build_nlist(lima_ctx* ctx);
 lima_status lima_get_nlist(lima_ctx* ctx, int which, uint32_t* offsets, uint32_t* ids, uint32_t* total);
 lima_status lima_set_nlist(lima_ctx* ctx, int which, const uint32_t* offsets, const uint32_t* ids);
+
+/* Physics semantics: pair-list builds since lima_finish_box (those at creation,
+   lima_set_state and lima_build_nlist included).  With nlist_period <= 0 the
+   list is rebuilt whenever a particle has moved more than skin/2 since the
+   last build, decided on the device inside the step graph. */
+lima_status lima_get_rebuild_count(lima_ctx* ctx, uint64_t* count);
 
 /* Reference thermostat scalar for the next step (Box::thermostat_scalar,
    Simulation.cuh:70); 1 after it has been applied once. */

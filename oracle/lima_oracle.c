@@ -512,10 +512,12 @@ static void lj_pair64(const orc_phys_sys* S, double r2, double sig, double eps, 
     if (ron < rc) {
         double rc2 = rc * rc, ron2 = ron * ron;
         if (r2 > ron2) {
-            double den = (rc2 - ron2) * (rc2 - ron2) * (rc2 - ron2);
-            double a = rc2 - r2;
-            double sw = a * a * (rc2 + 2.0 * r2 - 3.0 * ron2) / den;
-            double dsw_over_r = 12.0 * a * (ron2 - r2) / den;      /* (dS/dr)/r */
+            /* C2 switch in r^2: S = t^3 (10 - 15 t + 6 t^2), t = (rc^2 - r^2) / (rc^2 - r_on^2);
+               S, S' and S'' are continuous at r_on (t = 1) and r_c (t = 0) */
+            double D = rc2 - ron2;
+            double t = r2 < rc2 ? (rc2 - r2) / D : 0.0;
+            double sw = t * t * t * (10.0 + t * (-15.0 + 6.0 * t));
+            double dsw_over_r = -60.0 * t * t * (1.0 - t) * (1.0 - t) / D;   /* (dS/dr)/r = 2 dS/d(r^2) */
             dvdr_over_r = dvdr_over_r * sw + v * dsw_over_r;
             v *= sw;
         }

@@ -62,6 +62,10 @@ struct lima_ctx {
     lima::RefDev ref{};
     lima::PhysDev phys{};
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    // physics with dynamic lists: [parity][energy] step graphs with a conditional rebuild
+    cudaGraphExec_t dgraph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    int dgraph_kernels[2] = {0, 0};
+    uint64_t host_rebuilds = 0;   // list builds launched by the host (creation, set_state, build_nlist, ...)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool timed = false;
     bool lambda_pending_reset = false;
@@ -79,6 +83,9 @@ struct lima_ctx {
     ~lima_ctx() {
         for (auto& g : graph)
             if (g) cudaGraphExecDestroy(g);
+        for (auto& row : dgraph)
+            for (auto& g : row)
+                if (g) cudaGraphExecDestroy(g);
         for (void* ptr : dallocs) cudaFree(ptr);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -354,6 +361,9 @@ void ref_nlist_now(lima_ctx* c) {
 void one_step(lima_ctx* c, cudaEvent_t* prof) {
     const int period = std::max(1, c->p.nlist_period);
     const bool rebuild = c->step > 0 && c->step - c->last_nlist_step >= static_cast<uint64_t>(period);
+    // profiling a dynamic list: the host reads the rebuild request before the first event
+    const bool dyn_rebuild = prof && c->p.semantics == LIMA_SEMANTICS_PHYSICS && c->phys.dynamic_list &&
+                             lima::phys_rebuild_pending(c->phys, c->stream);
     if (prof) cuda_ok(cudaEventRecord(prof[0], c->stream), "cudaEventRecord");
     if (c->p.semantics == LIMA_SEMANTICS_REFERENCE) {
         lima::RefDev& d = c->ref;
@@ -386,10 +396,28 @@ void one_step(lima_ctx* c, cudaEvent_t* prof) {
                 c->lambda_pending_reset = true;   // applied for one step (Engine.cu:67-69)
             }
         }
+    } else if (c->phys.dynamic_list) {
+        const bool energy = c->p.energy_period > 0 && (c->step % c->p.energy_period) == 0;
+        if (!prof) {
+            cuda_ok(cudaGraphLaunch(c->dgraph[c->cur][energy ? 1 : 0], c->stream), "cudaGraphLaunch");
+            c->launches += c->dgraph_kernels[energy ? 1 : 0];
+        } else {   // profiling: the same kernels launched directly, the rebuild decided on the host
+            if (dyn_rebuild) {
+                lima::phys_rebuild(c->phys, c->cur, c->stream);
+                c->launches += lima::kRebuildKernels;
+                c->host_rebuilds++;
+            }
+            cuda_ok(cudaEventRecord(prof[1], c->stream), "cudaEventRecord");
+            c->launches += lima::phys_step_kernels(c->phys, c->cur, c->stream, energy, prof + 2);
+            cuda_ok(cudaEventRecord(prof[5], c->stream), "cudaEventRecord");
+        }
+        c->cur ^= 1;
+        c->step++;
     } else {
         if (rebuild) {
             lima::phys_rebuild(c->phys, c->cur, c->stream);
-            c->launches += 3;
+            c->launches += lima::kRebuildKernels;
+            c->host_rebuilds++;
             c->last_nlist_step = c->step;
         }
         if (prof) cuda_ok(cudaEventRecord(prof[1], c->stream), "cudaEventRecord");
@@ -551,8 +579,20 @@ lima_status lima_finish_box(lima_ctx* c) {
             if (rc != 0) fail(static_cast<lima_status>(rc), msg);
             lima::phys_rebuild(c->phys, c->cur, c->stream);
             lima::phys_prime(c->phys, c->cur, c->stream);
+            c->host_rebuilds++;
             sync_checked(c);
-            capture_graphs(c, phys_launch_step);
+            if (c->phys.dynamic_list) {
+                for (int parity = 0; parity < 2; parity++)
+                    for (int energy = 0; energy < 2; energy++) {
+                        const int k = lima::phys_capture_dynamic(c->phys, parity, energy != 0, c->stream,
+                                                                 &c->dgraph[parity][energy]);
+                        need(k > 0, LIMA_ERR_CUDA,
+                             "dynamic pair lists need CUDA graphs with conditional nodes (CUDA 12.4+ driver)");
+                        c->dgraph_kernels[energy] = k;
+                    }
+            } else {
+                capture_graphs(c, phys_launch_step);
+            }
             c->n_particles_total = c->phys.n;
         }
         sync_checked(c);
@@ -617,6 +657,8 @@ lima_status lima_get_kernel_launches(lima_ctx* c, uint64_t* count) {
     return guarded(c, [&] {
         need(count != nullptr, LIMA_ERR_ARGUMENT, "null count");
         *count = c->launches;
+        if (c->finished && c->p.semantics == LIMA_SEMANTICS_PHYSICS && c->phys.dynamic_list)
+            *count += lima::phys_device_rebuilds(c->phys, c->stream) * lima::kRebuildKernels;
     });
 }
 
@@ -741,6 +783,8 @@ lima_status lima_set_state(lima_ctx* c, const lima_compound_state* states, const
             lima::phys_upload_state(h, c->phys, c->cur, c->stream);
             lima::phys_rebuild(c->phys, c->cur, c->stream);
             lima::phys_prime(c->phys, c->cur, c->stream);
+            c->launches += lima::kRebuildKernels;
+            c->host_rebuilds++;
             c->last_nlist_step = c->step;
         }
         sync_checked(c);
@@ -772,7 +816,13 @@ lima_status lima_compute_energies(lima_ctx* c) {
         need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
         need(c->p.semantics == LIMA_SEMANTICS_PHYSICS, LIMA_ERR_UNSUPPORTED,
              "the reference computes no LJ energy; reference semantics report potE of the last step");
+        if (c->phys.dynamic_list && lima::phys_rebuild_pending(c->phys, c->stream)) {
+            lima::phys_rebuild(c->phys, c->cur, c->stream);
+            c->launches += lima::kRebuildKernels;
+            c->host_rebuilds++;
+        }
         lima::phys_energy_now(c->phys, c->cur, c->stream);
+        c->launches += 3;
         sync_checked(c);
     });
 }
@@ -818,9 +868,21 @@ lima_status lima_build_nlist(lima_ctx* c) {
             ref_nlist_now(c);
         } else {
             lima::phys_rebuild(c->phys, c->cur, c->stream);
+            c->launches += lima::kRebuildKernels;
+            c->host_rebuilds++;
             c->last_nlist_step = c->step;
         }
         sync_checked(c);
+    });
+}
+
+lima_status lima_get_rebuild_count(lima_ctx* c, uint64_t* count) {
+    return guarded(c, [&] {
+        need(count != nullptr, LIMA_ERR_ARGUMENT, "null count");
+        need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
+        need(c->p.semantics == LIMA_SEMANTICS_PHYSICS, LIMA_ERR_UNSUPPORTED,
+             "reference semantics rebuild every nlist_period steps");
+        *count = c->host_rebuilds + (c->phys.dynamic_list ? lima::phys_device_rebuilds(c->phys, c->stream) : 0);
     });
 }
 

@@ -139,138 +139,184 @@ __global__ void k_permute(PhysDev d, int cur, int mixed) {
         for (uint32_t q = c + 1; q <= (uint32_t)d.n_cells; q++) d.cstart[q] = d.n;
 }
 
-// One warp per home cell.  The home cell's particles, 32 at a time, are the
-// i side.  The candidates are the 25 columns of 5 cells along z around it:
-// cells (x, y, z..z+4) have consecutive keys, so a column is one contiguous
-// slot range of the cell-sorted order (two where it wraps around the box).
-// Lanes take 32 candidates at a time, shifted by whole box lengths into the
-// home cell's frame (no minimum image per pair), and test them against each
-// home particle whose distance to the range's box is below r_list (a ballot
-// per range picks those).  A ballot per home particle appends its hits in
-// candidate order, so every row is deterministic.  Every loop bound and every
-// collective below is warp-uniform.  Boxes with fewer than 5 cells per side
-// scan all particles with the minimum image instead.
-__global__ void __launch_bounds__(kBuildWarps * 32) k_build_list(PhysDev d, int cur) {
-    __shared__ float4 s_pi[kBuildWarps][32];
-    __shared__ uint32_t s_oi[kBuildWarps][32];   // orig id | bit 31 when the particle has exclusions
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int c = blockIdx.x * kBuildWarps + w;
-    if (c >= d.n_cells) return;   // the whole warp
-    const float4* __restrict__ pos = d.pos[cur];
-    const int m = d.m;
-    const float cs = d.L / (float)m;
-    const float lim2 = d.rlist2 * 1.001f;   // range pruning keeps a margin for cell-boundary rounding
-    const int cx = c / (m * m), cy = (c / m) % m, cz = c % m;
-    const int hb = (int)d.cstart[c], he = (int)d.cstart[c + 1];
-    const unsigned lt = (1u << lane) - 1u;
+// Sorted copies back into the step arrays; clears the rebuild request.
+__global__ void k_copy_back(PhysDev d, int cur, int mixed) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k == 0) *d.need_rebuild = 0;
+    if (k >= d.n) return;
+    d.pos[cur][k] = d.pos_tmp[k];
+    d.vel[k] = d.vel_tmp[k];
+    if (mixed) {
+        d.posc[k] = d.posc_tmp[k];
+        d.velc[k] = d.velc_tmp[k];
+    }
+    d.orig_of_sorted[k] = d.orig_tmp[k];
+}
 
-    for (int i0 = hb; i0 < he; i0 += 32) {
-        const int ni = min(32, he - i0);
+// First node of a dynamic-list step graph: requests the conditional rebuild
+// when the previous step's pair kernel asked for one.
+__global__ void k_list_check(const int* need, unsigned long long* count, cudaGraphConditionalHandle h) {
+    const int v = *need;
+    cudaGraphSetConditional(h, v ? 1u : 0u);
+    if (v) *count += 1ull;
+}
+
+// Verlet-list build: one warp per 8 consecutive sorted particles, four lanes
+// per particle (lane = 4 * particle + slice).  The warp's particles are split
+// into groups that share a home column (cells (x, y, *)) and a z-window of at
+// most m-4 cells; particles outside the current group idle.  For a group with
+// home cells z0..z1, the candidates are the cells z0-2..z1+2 of the 25
+// columns around it (cells of side >= r_list/2, so they cover r_list), each
+// one or two contiguous slot ranges of the cell-sorted order.  Candidates
+// come through shared memory 32 at a time, shifted into the home frame by
+// whole box lengths; each lane tests every fourth candidate against its
+// particle, the four lanes' hit masks are merged with two xor-shuffles, and
+// every lane writes its own hits at their rank in the merged mask, so each
+// row lists its neighbours in candidate order (deterministic).  Collectives
+// (ballots, shuffles, __syncwarp) only occur in warp-uniform code.  Boxes
+// with fewer than 5 cells per side test all particles with the minimum image.
+namespace {
+
+struct Cand {
+    float4 p;       // shifted position
+    uint32_t j;     // slot | bit 31 when the particle is a compound particle
+};
+
+template <bool MIN_IMAGE>
+__device__ __forceinline__ void scan_range(const PhysDev& d, const float4* __restrict__ pos, Cand* sc, int jb, int je,
+                                           float sx, float sy, float sz, bool mine, int i, float4 pi, uint32_t oi,
+                                           bool ex, int lane, int sub, int& cnt) {
+    for (int jc = jb; jc < je; jc += 32) {
+        const int nv = min(32, je - jc);
         __syncwarp();
-        float4 my_p = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (lane < ni) {
-            my_p = pos[i0 + lane];
-            const uint32_t o = d.orig_of_sorted[i0 + lane];
-            const bool ex = o < (uint32_t)d.n_cp && d.excl_off[o + 1] > d.excl_off[o];
-            s_pi[w][lane] = my_p;
-            s_oi[w][lane] = o | (ex ? 0x80000000u : 0u);
+        if (lane < nv) {
+            const int j = jc + lane;
+            const float4 p = pos[j];
+            const uint32_t oj = d.orig_of_sorted[j];
+            sc[lane].p = make_float4(p.x + sx, p.y + sy, p.z + sz, 0.f);
+            sc[lane].j = (uint32_t)j | (oj < (uint32_t)d.n_cp ? 0x80000000u : 0u);
         }
         __syncwarp();
-        int my_cnt = 0;
-
-        // candidates [jb, je), shifted by (sx, sy, sz); (lo, hi) = their box in the home frame
-        auto scan = [&](int jb, int je, float sx, float sy, float sz, float3 lo, float3 hi, bool min_image) {
-            unsigned live;
-            if (min_image) {
-                live = __ballot_sync(0xffffffffu, lane < ni);
-            } else {
-                const float gx = fmaxf(fmaxf(lo.x - my_p.x, my_p.x - hi.x), 0.f);
-                const float gy = fmaxf(fmaxf(lo.y - my_p.y, my_p.y - hi.y), 0.f);
-                const float gz = fmaxf(fmaxf(lo.z - my_p.z, my_p.z - hi.z), 0.f);
-                live = __ballot_sync(0xffffffffu, lane < ni && gx * gx + gy * gy + gz * gz < lim2);
-            }
-            if (!live) return;
-            for (int jc = jb; jc < je; jc += 32) {
-                const int j = jc + lane;
-                const bool valid = j < je;
-                float4 pj = valid ? pos[j] : make_float4(0.f, 0.f, 0.f, 0.f);
-                pj.x += sx;
-                pj.y += sy;
-                pj.z += sz;
-                for (unsigned r = live; r; r &= r - 1u) {
-                    const int ii = __ffs(r) - 1;
-                    const float4 pi = s_pi[w][ii];
-                    float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
-                    if (min_image) {
+        // slice `sub` tests candidates sub, sub+4, ..., sub+28 (consecutive lanes of a
+        // particle read consecutive 32-byte records: no shared-memory bank conflicts)
+        uint32_t mine_bits = 0;
+        if (mine) {
+#pragma unroll
+            for (int t = 0; t < 8; t++) {
+                const int c = 4 * t + sub;
+                if (c < nv) {
+                    const float4 q = sc[c].p;
+                    float dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
+                    if (MIN_IMAGE) {
                         dx = mimg(dx, d.L, d.invL);
                         dy = mimg(dy, d.L, d.invL);
                         dz = mimg(dz, d.L, d.invL);
                     }
-                    bool hit = valid && j != i0 + ii && dx * dx + dy * dy + dz * dz < d.rlist2;
-                    const uint32_t oi = s_oi[w][ii];
-                    if (hit && (oi & 0x80000000u)) {
-                        const uint32_t oj = d.orig_of_sorted[j];
-                        if (oj < (uint32_t)d.n_cp && excluded(d, oi & 0x7fffffffu, oj)) hit = false;
-                    }
-                    const unsigned mask = __ballot_sync(0xffffffffu, hit);
-                    if (mask) {
-                        const int base = __shfl_sync(0xffffffffu, my_cnt, ii);
-                        if (hit) {
-                            const int k = base + __popc(mask & lt);
-                            if (k < d.nl_cap) d.nl[nl_index(d, i0 + ii, k)] = (uint32_t)j;
-                        }
-                        if (lane == ii) my_cnt += __popc(mask);
-                    }
+                    mine_bits |= (dx * dx + dy * dy + dz * dz < d.rlist2 ? 1u : 0u) << c;
                 }
             }
-        };
+            const int self = i - jc;
+            if (self >= 0 && self < 32) mine_bits &= ~(1u << self);
+            if (ex)
+                for (uint32_t b = mine_bits; b; b &= b - 1u) {
+                    const int c = __ffs(b) - 1;
+                    const uint32_t jw = sc[c].j;
+                    if ((jw >> 31) && excluded(d, oi, d.orig_of_sorted[jw & 0x7fffffffu])) mine_bits &= ~(1u << c);
+                }
+        }
+        uint32_t m32 = mine_bits;
+        m32 |= __shfl_xor_sync(0xffffffffu, m32, 1);
+        m32 |= __shfl_xor_sync(0xffffffffu, m32, 2);
+        for (uint32_t b = mine_bits; b; b &= b - 1u) {
+            const int c = __ffs(b) - 1;
+            const int k = cnt + __popc(m32 & ((1u << c) - 1u));
+            if (k < d.nl_cap) d.nl[nl_index(d, i, k)] = sc[c].j & 0x7fffffffu;
+        }
+        cnt += __popc(m32);
+    }
+}
 
-        if (m < 5) {
-            scan(0, d.n, 0.f, 0.f, 0.f, make_float3(0.f, 0.f, 0.f), make_float3(0.f, 0.f, 0.f), true);
-        } else {
+}  // namespace
+
+__global__ void __launch_bounds__(kBuildWarps * 32) k_build_list(PhysDev d, int cur) {
+    __shared__ Cand s_cand[kBuildWarps][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int pl = lane >> 2, sub = lane & 3;
+    const int base = (blockIdx.x * kBuildWarps + w) * 8;
+    if (base >= d.n) return;   // the whole warp
+    const float4* __restrict__ pos = d.pos[cur];
+    Cand* sc = s_cand[w];
+    const int i = base + pl;
+    const bool have = i < d.n;
+    const float4 pi = have ? pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const uint32_t oi = have ? d.orig_of_sorted[i] : 0u;
+    const bool ex = have && oi < (uint32_t)d.n_cp && d.excl_off[oi + 1] > d.excl_off[oi];
+    int cnt = 0;
+    const int m = d.m;
+
+    if (m < 5) {
+        scan_range<true>(d, pos, sc, 0, d.n, 0.f, 0.f, 0.f, have, i, pi, oi, ex, lane, sub, cnt);
+    } else {
+        int cx = -1, cy = -1, cz = 0;
+        if (have) cell_xyz(d, pi, cx, cy, cz);
+        // one bit per particle, at its slice-0 lane
+        unsigned todo = __ballot_sync(0xffffffffu, have && sub == 0);
+        while (todo) {   // warp-uniform: todo is the same in every lane
+            const int lead = __ffs(todo) - 1;
+            const int hx = __shfl_sync(0xffffffffu, cx, lead);
+            const int hy = __shfl_sync(0xffffffffu, cy, lead);
+            const int hz0 = __shfl_sync(0xffffffffu, cz, lead);
+            const bool mine = ((todo >> (pl * 4)) & 1u) && cx == hx && cy == hy && cz <= hz0 + (m - 5);
+            const unsigned grp = __ballot_sync(0xffffffffu, mine && sub == 0);
+            todo &= ~grp;
+            // sorted by cell: the group's last particle has its top cell
+            const int hz1 = __shfl_sync(0xffffffffu, cz, 31 - __clz(grp));
             for (int ox = -2; ox <= 2; ox++) {
-                int x = cx + ox;
+                int x = hx + ox;
                 float sx = 0.f;
                 if (x < 0) { x += m; sx = -d.L; } else if (x >= m) { x -= m; sx = d.L; }
                 for (int oy = -2; oy <= 2; oy++) {
-                    int y = cy + oy;
+                    int y = hy + oy;
                     float sy = 0.f;
                     if (y < 0) { y += m; sy = -d.L; } else if (y >= m) { y -= m; sy = d.L; }
                     const int col = (x * m + y) * m;
-                    const float x0 = (cx + ox) * cs, y0 = (cy + oy) * cs;
-                    auto run = [&](int za, int zb, float sz, int zhome) {   // cells za..zb, home-frame cell zhome
-                        scan((int)d.cstart[col + za], (int)d.cstart[col + zb + 1], sx, sy, sz,
-                             make_float3(x0, y0, zhome * cs), make_float3(x0 + cs, y0 + cs, (zhome + zb - za + 1) * cs),
-                             false);
-                    };
-                    const int z0 = cz - 2, z1 = cz + 2;
-                    if (z0 < 0) {
-                        run(z0 + m, m - 1, -d.L, z0);
-                        run(0, z1, 0.f, 0);
-                    } else if (z1 >= m) {
-                        run(z0, m - 1, 0.f, z0);
-                        run(0, z1 - m, d.L, m);
+                    // unwrapped cells u0..u1 (at most m of them) -> one or two real ranges
+                    const int u0 = hz0 - 2, u1 = hz1 + 2;
+                    if (u0 < 0) {
+                        scan_range<false>(d, pos, sc, (int)d.cstart[col + u0 + m], (int)d.cstart[col + m], sx, sy, -d.L,
+                                          mine, i, pi, oi, ex, lane, sub, cnt);
+                        scan_range<false>(d, pos, sc, (int)d.cstart[col], (int)d.cstart[col + u1 + 1], sx, sy, 0.f, mine,
+                                          i, pi, oi, ex, lane, sub, cnt);
+                    } else if (u1 >= m) {
+                        scan_range<false>(d, pos, sc, (int)d.cstart[col + u0], (int)d.cstart[col + m], sx, sy, 0.f, mine,
+                                          i, pi, oi, ex, lane, sub, cnt);
+                        scan_range<false>(d, pos, sc, (int)d.cstart[col], (int)d.cstart[col + u1 - m + 1], sx, sy, d.L,
+                                          mine, i, pi, oi, ex, lane, sub, cnt);
                     } else {
-                        run(z0, z1, 0.f, z0);
+                        scan_range<false>(d, pos, sc, (int)d.cstart[col + u0], (int)d.cstart[col + u1 + 1], sx, sy, 0.f,
+                                          mine, i, pi, oi, ex, lane, sub, cnt);
                     }
                 }
             }
         }
-        if (lane < ni) {
-            d.nl_cnt[i0 + lane] = (uint32_t)min(my_cnt, d.nl_cap);
-            if (my_cnt > d.nl_cap) atomicOr(d.err, ERR_BIT_PHYS_LIST_OVERFLOW);
-        }
+    }
+    if (have && sub == 0) {
+        d.nl_cnt[i] = (uint32_t)min(cnt, d.nl_cap);
+        if (cnt > d.nl_cap) atomicOr(d.err, ERR_BIT_PHYS_LIST_OVERFLOW);
     }
 }
 
 // ----------------------------------------------------------------- bonded ---
 template <bool ENERGY>
+// The bonded terms read the orig-ordered compound positions (pos_orig), none
+// of the arrays a list rebuild re-sorts, so a rebuild may run concurrently.
 __global__ void __launch_bounds__(kTB) k_bonded(PhysDev d, int cur, int slot, int fold_src) {
     if (fold_src >= 0 && blockIdx.x == 0 && threadIdx.x == 0) fold(d, fold_src);
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double eb = 0.0, ea = 0.0, ed = 0.0, vir = 0.0;
     const float L = d.L, iL = d.invL;
-    auto P = [&](int orig) { return d.pos[cur][d.sorted_of_orig[orig]]; };
+    const float4* __restrict__ po = d.pos_orig[cur];
+    auto P = [&](int orig) { return po[orig]; };
     if (t < d.n_bonds) {
         const int4 ix = d.bond_idx[t];
         const float2 par = d.bond_par[t];
@@ -385,23 +431,28 @@ __device__ __forceinline__ void lj_pair(const PhysDev& d, const float2* __restri
     float v = 0.f;
     if (ENERGY || SWITCH) v = tab.y * (sr6 * sr6 - sr6);
     if (SWITCH) {
-        const float a = fmaxf(d.rc2 - r2, 0.f);
-        const bool sw_on = r2 > d.ron2;
-        const float sw = sw_on ? a * a * (d.rc2 + 2.f * r2 - 3.f * d.ron2) * d.inv_sw_den : 1.f;
-        const float dsw = sw_on ? 12.f * a * (d.ron2 - r2) * d.inv_sw_den : 0.f;   // (dS/dr)/r
+        // C2 switch in r^2: S = t^3 (10 - 15 t + 6 t^2), t = sat((rc^2 - r^2) / (rc^2 - r_on^2));
+        // S = 1 below r_on and S = S' = 0 beyond r_c, so no separate cutoff select
+        const float t = __saturatef((d.rc2 - r2) * d.inv_sw_d);
+        const float t2 = t * t, omt = 1.f - t;
+        const float sw = t2 * t * fmaf(t, fmaf(6.f, t, -15.f), 10.f);
+        const float dsw = -60.f * d.inv_sw_d * t2 * omt * omt;   // (dS/dr)/r
         fr = fr * sw - v * dsw;
         v *= sw;
-    } else if (ENERGY) {
-        const float src2 = tab.x / d.rc2, src6 = src2 * src2 * src2;
-        v -= tab.y * (src6 * src6 - src6);
+    } else {
+        if (ENERGY) {
+            const float src2 = tab.x / d.rc2, src6 = src2 * src2 * src2;
+            v -= tab.y * (src6 * src6 - src6);
+        }
+        const bool in = r2 < d.rc2;
+        fr = in ? fr : 0.f;
+        v = in ? v : 0.f;
     }
-    const bool in = r2 < d.rc2;
-    fr = in ? fr : 0.f;
     px -= fr * dx;
     py -= fr * dy;
     pz -= fr * dz;
     if (ENERGY) {
-        e_i += in ? 0.5f * v : 0.f;
+        e_i += 0.5f * v;
         w_i += 0.5f * fr * r2;
     }
 }
@@ -544,12 +595,16 @@ __global__ void __launch_bounds__(kTB) k_pair_integrate(PhysDev d, int cur, int 
                 if (y >= L) y -= L;
                 if (z >= L) z -= L;
                 d.pos[cur ^ 1][i] = make_float4(x, y, z, pi.w);
+                if (oi < (uint32_t)d.n_cp) d.pos_orig[cur ^ 1][oi] = make_float4(x, y, z, pi.w);
                 d.posc[i] = pc;
                 d.vel[i] = make_float4(vhx, vhy, vhz, im);
                 d.velc[i] = vc;
                 const float4 xr = d.xref[i];
                 const float ddx = mimg(x - xr.x, L, iL), ddy = mimg(y - xr.y, L, iL), ddz = mimg(z - xr.z, L, iL);
-                if (ddx * ddx + ddy * ddy + ddz * ddz > d.half_skin2) atomicOr(d.err, ERR_BIT_LIST_STALE);
+                if (ddx * ddx + ddy * ddy + ddz * ddz > d.half_skin2) {
+                    if (d.dynamic_list) *d.need_rebuild = 1;
+                    else atomicOr(d.err, ERR_BIT_LIST_STALE);
+                }
                 if (!(x == x) || !(y == y) || !(z == z)) atomicOr(d.err, ERR_BIT_NAN);
             }
         } else {
@@ -569,10 +624,14 @@ __global__ void __launch_bounds__(kTB) k_pair_integrate(PhysDev d, int cur, int 
                 if (y >= L) y -= L;
                 if (z >= L) z -= L;
                 d.pos[cur ^ 1][i] = make_float4(x, y, z, pi.w);
+                if (oi < (uint32_t)d.n_cp) d.pos_orig[cur ^ 1][oi] = make_float4(x, y, z, pi.w);
                 d.vel[i] = make_float4(vx, vy, vz, im);
                 const float4 xr = d.xref[i];
                 const float ddx = mimg(x - xr.x, L, iL), ddy = mimg(y - xr.y, L, iL), ddz = mimg(z - xr.z, L, iL);
-                if (ddx * ddx + ddy * ddy + ddz * ddz > d.half_skin2) atomicOr(d.err, ERR_BIT_LIST_STALE);
+                if (ddx * ddx + ddy * ddy + ddz * ddz > d.half_skin2) {
+                    if (d.dynamic_list) *d.need_rebuild = 1;
+                    else atomicOr(d.err, ERR_BIT_LIST_STALE);
+                }
                 if (!(x == x) || !(y == y) || !(z == z)) atomicOr(d.err, ERR_BIT_NAN);
             }
         }
@@ -610,7 +669,16 @@ void launch_permute(const PhysDev& d, int cur, bool mixed, cudaStream_t s) {
 }
 
 void launch_build_list(const PhysDev& d, int cur, cudaStream_t s) {
-    k_build_list<<<(d.n_cells + kBuildWarps - 1) / kBuildWarps, kBuildWarps * 32, 0, s>>>(d, cur);
+    const int warps = (d.n + 7) / 8;
+    k_build_list<<<(warps + kBuildWarps - 1) / kBuildWarps, kBuildWarps * 32, 0, s>>>(d, cur);
+}
+
+void launch_copy_back(const PhysDev& d, int cur, bool mixed, cudaStream_t s) {
+    k_copy_back<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d, cur, mixed ? 1 : 0);
+}
+
+void launch_list_check(const PhysDev& d, cudaGraphConditionalHandle h, cudaStream_t s) {
+    k_list_check<<<1, 1, 0, s>>>(d.need_rebuild, d.rebuild_count, h);
 }
 
 void launch_bonded(const PhysDev& d, int cur, bool energy, int slot, int fold_src, cudaStream_t s) {

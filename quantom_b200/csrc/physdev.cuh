@@ -42,7 +42,7 @@ struct PhysDev {
     int n_pad;          // n rounded up to 32
     int n_cp;           // compound particles
     int n_c, n_s;
-    float L, invL, rc, rc2, rlist, rlist2, ron2, inv_sw_den, half_skin2;
+    float L, invL, rc, rc2, rlist, rlist2, ron2, inv_sw_d, half_skin2;   // inv_sw_d = 1/(rc^2 - r_on^2)
     int use_switch;
     double dt;
     int precision;      // lima_precision
@@ -55,6 +55,7 @@ struct PhysDev {
     float4* velc;
     float4* xref;
     float4* force;
+    float4* pos_orig[2];        // [n_cp] compound-particle positions in orig order (the bonded kernel's input)
     uint32_t* orig_of_sorted;   // [n]
     uint32_t* sorted_of_orig;   // [n]
     float2* lj_table;           // [n_types^2] (sigma^2, 4 eps), Lorentz-Berthelot
@@ -68,6 +69,13 @@ struct PhysDev {
     float4* pos_tmp; float4* vel_tmp; float4* posc_tmp; float4* velc_tmp; uint32_t* orig_tmp;
     // Verlet list (tile-local indices)
     uint32_t* nl; uint32_t* nl_cnt; int nl_cap;
+    // dynamic lists (nlist_period <= 0): the pair kernel requests a rebuild
+    // once a particle has moved more than skin/2 since the last one, and the
+    // next step rebuilds before its forces (a conditional node of the step
+    // graph); fixed period: the same test is an error (ERR_BIT_LIST_STALE)
+    int dynamic_list;
+    int* need_rebuild;
+    unsigned long long* rebuild_count;   // rebuilds decided on the device
     // exclusions (CSR over orig ids)
     uint32_t* excl_off; uint32_t* excl_ids;
     // bonded terms (orig ids)
@@ -103,8 +111,14 @@ struct PhysHost {
 // returns 0 or a lima_status; device buffers are appended to `allocs`
 int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>& allocs, std::string& msg);
 void phys_upload_state(const PhysHost& h, PhysDev& d, int cur, cudaStream_t s);
-void phys_rebuild(PhysDev& d, int cur, cudaStream_t s);
+void phys_rebuild(const PhysDev& d, int cur, cudaStream_t s);
 void phys_prime(PhysDev& d, int cur, cudaStream_t s);
+// dynamic lists: the step graph of parity `cur` ({check -> IF(rebuild)} || bonded -> pair);
+// returns the kernels of one replay without a rebuild, or -1 if the graph cannot be built
+int phys_capture_dynamic(const PhysDev& d, int cur, bool energy, cudaStream_t s, cudaGraphExec_t* out);
+bool phys_rebuild_pending(const PhysDev& d, cudaStream_t s);
+unsigned long long phys_device_rebuilds(const PhysDev& d, cudaStream_t s);
+constexpr int kRebuildKernels = 4;   // k_keys, k_permute, k_copy_back, k_build_list (plus the library sort)
 // ev (nullable): events before the bonded kernel, after it, after the pair
 // kernel.  Returns kernels launched.
 int phys_step_kernels(const PhysDev& d, int cur, cudaStream_t s, bool energy = false, cudaEvent_t* ev = nullptr);

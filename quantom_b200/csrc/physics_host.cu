@@ -56,10 +56,11 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
     d.rlist = p.cutoff + p.skin;
     d.rlist2 = d.rlist * d.rlist;
     d.half_skin2 = 0.25f * p.skin * p.skin;
+    d.dynamic_list = p.nlist_period <= 0 ? 1 : 0;
     d.use_switch = p.switch_on < p.cutoff ? 1 : 0;
     const float ron = d.use_switch ? p.switch_on : p.cutoff;
     d.ron2 = ron * ron;
-    d.inv_sw_den = d.use_switch ? 1.f / ((d.rc2 - d.ron2) * (d.rc2 - d.ron2) * (d.rc2 - d.ron2)) : 0.f;
+    d.inv_sw_d = d.use_switch ? 1.f / (d.rc2 - d.ron2) : 0.f;
     d.dt = p.dt;
     d.precision = p.precision;
     d.thermostat = p.thermostat;
@@ -200,6 +201,7 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
         d.velc = dalloc<float4>(allocs, d.n_pad);
         d.xref = dalloc<float4>(allocs, d.n_pad);
         d.force = dalloc<float4>(allocs, d.n_pad);
+        for (int b = 0; b < 2; b++) d.pos_orig[b] = dalloc<float4>(allocs, std::max(1, d.n_cp));
         d.orig_of_sorted = dalloc<uint32_t>(allocs, d.n_pad);
         d.sorted_of_orig = dalloc<uint32_t>(allocs, d.n);
         d.lj_table = dalloc<float2>(allocs, tab.size());
@@ -231,6 +233,8 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
         d.e_last = dalloc<double>(allocs, LIMA_E_COUNT);
         d.lambda = dalloc<float>(allocs, 2);
         d.err = dalloc<int>(allocs, 1);
+        d.need_rebuild = dalloc<int>(allocs, 1);
+        d.rebuild_count = dalloc<unsigned long long>(allocs, 1);
         cub::DeviceRadixSort::SortPairs(nullptr, d.sort_tmp_bytes, d.keys[0], d.keys[1], d.vals[0], d.vals[1], d.n, 0,
                                         32, s);
         d.sort_tmp = dalloc<uint8_t>(allocs, d.sort_tmp_bytes);
@@ -256,6 +260,8 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
     cudaMemsetAsync(d.acc_energy, 0, sizeof(int) * kAccSlots, s);
     cudaMemsetAsync(d.e_last, 0, sizeof(double) * LIMA_E_COUNT, s);
     cudaMemsetAsync(d.err, 0, sizeof(int), s);
+    cudaMemsetAsync(d.need_rebuild, 0, sizeof(int), s);
+    cudaMemsetAsync(d.rebuild_count, 0, sizeof(unsigned long long), s);
     cudaMemsetAsync(d.nl_cnt, 0, sizeof(uint32_t) * d.n_pad, s);
     cudaMemsetAsync(d.force, 0, sizeof(float4) * d.n_pad, s);
     phys_upload_state(h, d, 0, s);
@@ -299,6 +305,7 @@ void phys_upload_state(const PhysHost& h, PhysDev& d, int cur, cudaStream_t s) {
     }
     for (int i = 0; i < d.n_pad; i++) ident[i] = i < d.n ? i : 0xffffffffu;
     cudaMemcpyAsync(d.pos[cur], pos.data(), sizeof(float4) * d.n_pad, cudaMemcpyHostToDevice, s);
+    if (d.n_cp) cudaMemcpyAsync(d.pos_orig[cur], pos.data(), sizeof(float4) * d.n_cp, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(d.vel, vel.data(), sizeof(float4) * d.n_pad, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(d.posc, zero.data(), sizeof(float4) * d.n_pad, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(d.velc, zero.data(), sizeof(float4) * d.n_pad, cudaMemcpyHostToDevice, s);
@@ -311,7 +318,7 @@ void phys_upload_state(const PhysHost& h, PhysDev& d, int cur, cudaStream_t s) {
     cudaStreamSynchronize(s);
 }
 
-void phys_rebuild(PhysDev& d, int cur, cudaStream_t s) {
+void phys_rebuild(const PhysDev& d, int cur, cudaStream_t s) {
     const size_t ncell = (size_t)d.n_cells;
     const bool mixed = d.precision == LIMA_PRECISION_MIXED;
     launch_keys(d, cur, s);
@@ -320,17 +327,96 @@ void phys_rebuild(PhysDev& d, int cur, cudaStream_t s) {
     while ((1ull << end_bit) < (unsigned long long)ncell) end_bit++;
     cub::DeviceRadixSort::SortPairs(d.sort_tmp, bytes, d.keys[0], d.keys[1], d.vals[0], d.vals[1], d.n, 0, end_bit, s);
     launch_permute(d, cur, mixed, s);
-    cudaMemcpyAsync(d.pos[cur], d.pos_tmp, sizeof(float4) * d.n, cudaMemcpyDeviceToDevice, s);
-    cudaMemcpyAsync(d.vel, d.vel_tmp, sizeof(float4) * d.n, cudaMemcpyDeviceToDevice, s);
-    if (mixed) {
-        cudaMemcpyAsync(d.posc, d.posc_tmp, sizeof(float4) * d.n, cudaMemcpyDeviceToDevice, s);
-        cudaMemcpyAsync(d.velc, d.velc_tmp, sizeof(float4) * d.n, cudaMemcpyDeviceToDevice, s);
-    }
-    cudaMemcpyAsync(d.orig_of_sorted, d.orig_tmp, sizeof(uint32_t) * d.n, cudaMemcpyDeviceToDevice, s);
+    launch_copy_back(d, cur, mixed, s);
     launch_build_list(d, cur, s);
 }
 
 void phys_prime(PhysDev&, int, cudaStream_t) {}
+
+bool phys_rebuild_pending(const PhysDev& d, cudaStream_t s) {
+    int h = 0;
+    cudaMemcpyAsync(&h, d.need_rebuild, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    return h != 0;
+}
+
+unsigned long long phys_device_rebuilds(const PhysDev& d, cudaStream_t s) {
+    unsigned long long h = 0;
+    cudaMemcpyAsync(&h, d.rebuild_count, sizeof(h), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    return h;
+}
+
+namespace {
+// ends a capture left open by a failed step of phys_capture_dynamic
+void end_open_capture(cudaStream_t s) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(s, &g);
+        if (g) cudaGraphDestroy(g);
+    }
+    cudaGetLastError();
+}
+}  // namespace
+
+// {k_list_check -> IF(rebuild requested){ sort, permute, copy back, list }}
+// in parallel with the bonded terms, then the pair kernel after both: the
+// conditional's own latency hides behind the bonded kernel.  The conditional
+// body is captured from the same launch sequence as a host-driven rebuild, so
+// both paths run identical kernels.
+int phys_capture_dynamic(const PhysDev& d, int cur, bool energy, cudaStream_t s, cudaGraphExec_t* out) {
+    *out = nullptr;
+    cudaGraph_t g = nullptr;
+    if (cudaGraphCreate(&g, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
+    int kernels = -1;
+    do {
+        cudaGraphConditionalHandle h;
+        if (cudaGraphConditionalHandleCreate(&h, g, 0, 0) != cudaSuccess) break;
+        cudaGraph_t tmp = nullptr;
+        // two roots: the check (then the conditional rebuild) and the bonded terms
+        if (cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, mode) != cudaSuccess) break;
+        launch_list_check(d, h, s);
+        if (cudaStreamEndCapture(s, &tmp) != cudaSuccess) break;
+        cudaGraphNode_t check = nullptr;
+        size_t nn = 1;
+        if (cudaGraphGetNodes(g, &check, &nn) != cudaSuccess || nn != 1) break;
+        if (cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, mode) != cudaSuccess) break;
+        launch_bonded(d, cur, energy, cur, cur ^ 1, s);
+        if (cudaStreamEndCapture(s, &tmp) != cudaSuccess) break;
+        cudaGraphNode_t roots[2] = {nullptr, nullptr};
+        nn = 2;
+        if (cudaGraphGetNodes(g, roots, &nn) != cudaSuccess || nn != 2) break;
+        const cudaGraphNode_t bonded = roots[0] == check ? roots[1] : roots[0];
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        cudaGraphNode_t cond = nullptr;
+        if (cudaGraphAddNode(&cond, g, &check, 1, &cp) != cudaSuccess) break;
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        if (cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, mode) != cudaSuccess) break;
+        phys_rebuild(d, cur, s);
+        if (cudaStreamEndCapture(s, &tmp) != cudaSuccess) break;
+        const cudaGraphNode_t before_pair[2] = {cond, bonded};
+        if (cudaStreamBeginCaptureToGraph(s, g, before_pair, nullptr, 2, mode) != cudaSuccess) break;
+        launch_pair(d, cur, d.precision == LIMA_PRECISION_MIXED, energy, true, cur, s);
+        if (cudaStreamEndCapture(s, &tmp) != cudaSuccess) break;
+        if (cudaGraphInstantiate(out, g, 0) != cudaSuccess) {
+            *out = nullptr;
+            break;
+        }
+        kernels = 3;
+    } while (false);
+    end_open_capture(s);
+    cudaGraphDestroy(g);
+    return kernels;
+}
 
 // The step of parity `cur` accumulates into slot cur; its bonded kernel first
 // folds slot cur^1 (the previous step) into e_last and lambda[cur].

@@ -82,6 +82,7 @@ def load_library():
         "lima_get_step": (i, [vp, ctypes.POINTER(ctypes.c_uint64)]),
         "lima_get_last_step_ms": (i, [vp, ctypes.POINTER(f)]),
         "lima_profile_steps": (i, [vp, i, vp]),
+        "lima_get_rebuild_count": (i, [vp, ctypes.POINTER(ctypes.c_uint64)]),
         "lima_get_kernel_launches": (i, [vp, ctypes.POINTER(ctypes.c_uint64)]),
     }
     for name, (res, args) in sigs.items():
@@ -197,6 +198,12 @@ class Engine:
     def kernel_launches(self) -> int:
         v = ctypes.c_uint64()
         self._check(self.lib.lima_get_kernel_launches(self.h, ctypes.byref(v)))
+        return int(v.value)
+
+    def rebuild_count(self) -> int:
+        """Physics semantics: pair-list builds since creation."""
+        v = ctypes.c_uint64()
+        self._check(self.lib.lima_get_rebuild_count(self.h, ctypes.byref(v)))
         return int(v.value)
 
     # -- state ---------------------------------------------------------------

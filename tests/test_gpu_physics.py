@@ -115,3 +115,44 @@ def test_deterministic_across_runs(gpu):
             eng.step(25)
             out.append(_positions(E, eng, s))
     assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_dynamic_list_trajectory_matches_fp64(gpu, precision):
+    """nlist_period 0: rebuilds decided on the device (conditional node of the
+    step graph) leave the trajectory on the FP64 oracle's."""
+    E = gpu
+    s = S.make_system("small_chains", seed=3)
+    ps = po.PhysSystem(s, rc=s.spec.cutoff, r_on=1.0)
+    x64, _, _, _ = ps.run(s.spec.dt, 20)
+    with E.Engine(s, _params(E, s, precision=precision, nlist_period=0)) as eng:
+        eng.step(20)
+        x = _positions(E, eng, s)
+        assert eng.rebuild_count() >= 1
+    d = x - x64
+    d -= s.spec.box_len * np.round(d / s.spec.box_len)
+    assert np.abs(d).max() < 1e-5
+
+
+def test_dynamic_list_stays_valid_over_a_long_run(gpu):
+    """Small skin, 3000 steps: the list is rebuilt on demand (never a stale
+    error), and the forces at the final positions still match FP64."""
+    E = gpu
+    s = S.make_system("small_bridged", seed=4)
+    with E.Engine(s, _params(E, s, nlist_period=0, skin=0.04, thermostat=E.THERMOSTAT_BERENDSEN,
+                              t_target=300.0, tau_t=1e-4)) as eng:
+        eng.step(3000)
+        eng.synchronize()
+        n_rb = eng.rebuild_count()
+        st, prev = eng.compound_states()
+        sol = eng.solvents()
+        eng.compute_energies()
+        F = _flat(s, *eng.forces())
+        launches = eng.kernel_launches()
+    assert 10 < n_rb < 3000
+    assert launches >= 3 * 3000
+    s2 = S.System(s.spec, s.seed, s.forcefield, s.compounds.copy(), st, sol, s.bridges)
+    for c in range(s.n_compounds):
+        s2.compounds[c]["prev_positions"] = prev[c]
+    F64, _ = po.PhysSystem(s2, rc=s.spec.cutoff, r_on=1.0).forces()
+    assert relrms(F, F64) < 5e-5

@@ -61,6 +61,14 @@ def test_switch_is_continuous():
         # a jump would be O(1); continuity leaves slope * 2e-7
         assert abs(e[0] - e[1]) <= 2.5e-7 * max(abs(f[0]), abs(f[1])) + 1e-9
         assert abs(f[0] - f[1]) < 1e-3
+        # C2: the force's slope is continuous too (a C1 switch jumps by V(r) S''(r), ~1e2 here)
+        h = 1e-5   # smooth: the one-sided slopes differ by ~F'' * 1.5 h
+        fx = []
+        for r in (r0 - 2 * h, r0 - h, r0 + h, r0 + 2 * h):
+            x = np.array([[0.5, 0.5, 0.5], [0.5 + r, 0.5, 0.5]])
+            fx.append(ps.forces(x)[0][1, 0])
+        left, right = (fx[1] - fx[0]) / h, (fx[3] - fx[2]) / h
+        assert abs(left - right) < 1.0
 
 
 def test_velocity_verlet_conserves_energy_small_dt():
