@@ -48,11 +48,13 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-sample-steps", type=int, default=2)
-    ap.add_argument("--mode", default="full", choices=["full", "kernels", "precision"],
+    ap.add_argument("--mode", default="full", choices=["full", "kernels", "precision", "grad"],
                     help="kernels: only warm-up + K plain-FP32 steps (the command profiled with ncu); "
                          "precision: the NVE drift / force-error study of plain FP32 against mixed precision")
     ap.add_argument("--nve-steps", type=int, default=50000, help="--mode precision: NVE steps per run")
     ap.add_argument("--eq-steps", type=int, default=5000, help="--mode precision: Berendsen equilibration steps")
+    ap.add_argument("--fp64-fd", action="store_true",
+                    help="--mode grad: also central differences of the FP64 oracle loss (minutes of host time)")
     ap.add_argument("--semantics", default="physics", choices=["physics", "reference"],
                     help="semantics of --mode kernels")
     return ap.parse_args()
@@ -354,6 +356,104 @@ def run_precision(args):
     print(json.dumps(result), flush=True)
 
 
+# ----------------------------------------------------- parameter gradients --
+GRAD_WORKLOAD = "lj_solvent_8192"
+
+
+def grad_study(E, S, device=0, fd=True, fp64_fd=False):
+    """Config-3 gradient: 8,192 LJ particles in a 6.3 nm box, loss = <U>/N +
+    RDF-bin loss (50 bins over 0..r_max, support ending at the 1.2 nm cutoff)
+    over a 200-step NVE unroll with checkpoints every 20 steps.  Returns cost
+    and accuracy figures."""
+    import torch
+    spec = S.CONFIGS[GRAD_WORKLOAD]
+    system = S.make_system(GRAD_WORKLOAD, seed=2024)
+    nb, rmax, T, C = 50, 1.2 * 50 / 51, 200, 20
+    w_e, w_r = 1.0, 100.0
+
+    def params(thermostat):
+        p = E.default_params(box_len=spec.box_len, cutoff=spec.cutoff, dt=spec.dt, semantics=E.SEMANTICS_PHYSICS,
+                             precision=E.PRECISION_FP32, skin=0.2, switch_on=1.0, nlist_period=0,
+                             t_target=300.0, tau_t=1e-4, device=device)
+        p.thermostat = thermostat
+        return p
+
+    # equilibrate, then a target occupancy from the same box with sigma + 2 %
+    with E.Engine(system, params(E.THERMOSTAT_BERENDSEN)) as eq:
+        eq.step(3000)
+        st, prev = eq.compound_states()
+        sol = eq.solvents()
+        start = system.with_state(st, prev, sol)
+        th = eq.get_params()
+        th2 = th.copy()
+        th2[0] *= 1.02
+        eq.set_params(th2)
+        eq.step(1000)
+        target = np.zeros(nb)
+        for _ in range(10):
+            eq.step(50)
+            target += eq.rdf(nb, rmax) / 10
+    out = {"workload": f"{GRAD_WORKLOAD}: {system.n_particles} particles, {spec.box_len} nm box, rc 1.2 nm "
+                       f"(C2 switch from 1.0), skin 0.2 nm, NVE dt 2 fs, FP32",
+           "n_steps": T, "checkpoint_every": C, "n_bins": nb, "r_max_nm": rmax, "w_energy": w_e, "w_rdf": w_r,
+           "target": "RDF-bin occupancy of the same box equilibrated with sigma + 2 %"}
+    with E.Engine(start, params(E.THERMOSTAT_NONE)) as eng:
+        theta = eng.get_params()
+
+        def wall(fn, reps=3):
+            fn()
+            torch.cuda.synchronize(device)
+            ts = []
+            for _ in range(reps):
+                t0 = time.perf_counter()
+                r = fn()
+                torch.cuda.synchronize(device)
+                ts.append(time.perf_counter() - t0)
+            return r, 1e3 * min(ts)
+        L, t_loss = wall(lambda: eng.loss(T, C, nb, rmax, w_e, w_r, target))
+        (L2, g), t_grad = wall(lambda: eng.grad(T, C, nb, rmax, w_e, w_r, target))
+        (_, g1), t_grad1 = wall(lambda: eng.grad(T, T, nb, rmax, w_e, w_r, target))   # one segment: every state kept
+        out.update({"loss": L, "theta": theta.tolist(), "grad": g.tolist(), "ms_forward_loss": t_loss,
+                    "ms_grad": t_grad, "grad_over_forward": t_grad / t_loss, "ms_grad_all_states_kept": t_grad1,
+                    "grad_all_states_kept_over_forward": t_grad1 / t_loss,
+                    "loss_same_in_both_calls": abs(L2 - L) <= 1e-9 * abs(L)})
+        if fd:
+            fdv, rel = [], []
+            for k in (0, 1):   # sigma and epsilon of the one LJ type
+                h = 1e-4 * abs(theta[k])
+                tp = theta.copy()
+                tp[k] += h
+                eng.set_params(tp)
+                lp = eng.loss(T, C, nb, rmax, w_e, w_r, target)
+                tp[k] -= 2 * h
+                eng.set_params(tp)
+                lm = eng.loss(T, C, nb, rmax, w_e, w_r, target)
+                eng.set_params(theta)
+                fdv.append((lp - lm) / (2 * h))
+                rel.append(abs(g[k] - fdv[-1]) / abs(fdv[-1]))
+            out.update({"fd_fp32_gpu": fdv, "rel_err_vs_fd_fp32_gpu": rel})
+    if fp64_fd:
+        from oracle import pyoracle as po
+        ps = po.PhysSystem(start, rc=spec.cutoff, r_on=1.0)
+        th64 = ps.params()
+        fdv, rel = [], []
+        for k in (0, 1):
+            h = 1e-4 * abs(th64[k])
+            e = np.eye(len(th64))[k]
+            lp, _ = ps.with_params(th64 + h * e).loss(spec.dt, T, nb, rmax, w_e, w_r, target)
+            lm, _ = ps.with_params(th64 - h * e).loss(spec.dt, T, nb, rmax, w_e, w_r, target)
+            fdv.append((lp - lm) / (2 * h))
+            rel.append(abs(g[k] - fdv[-1]) / abs(fdv[-1]))
+        out.update({"fd_fp64_oracle": fdv, "rel_err_vs_fd_fp64": rel})
+    return out
+
+
+def run_grad(args):
+    from quantom_b200 import engine as E
+    from quantom_b200 import systems as S
+    print(json.dumps({"mode": "grad", **grad_study(E, S, fp64_fd=args.fp64_fd)}), flush=True)
+
+
 # --------------------------------------------------------------- CPU side --
 def cpu_reference_rate(system, steps, threads):
     """Seconds per step of the reference's own step code on the host cores
@@ -473,6 +573,10 @@ def run_ours(args, ws, rank, local, pg):
 
     if rank != 0:
         return
+    # ---- parameter gradients (config 3), cost relative to the forward loss ---
+    grad = grad_study(E, S, device=local, fd=True, fp64_fd=False)
+    grad = {k: grad[k] for k in ("workload", "n_steps", "checkpoint_every", "ms_forward_loss", "ms_grad",
+                                 "grad_over_forward", "grad", "fd_fp32_gpu", "rel_err_vs_fd_fp32_gpu")}
     # ---- roofline of the dominant kernel (pair + integrate) -----------------
     peaks = measured_peaks()
     hbm = peaks.get("hbm_gbs")
@@ -520,6 +624,7 @@ def run_ours(args, ws, rank, local, pg):
         "e2e": {"value": ws * ns_per_day(spec.dt, t_e2e * 1e3 / args.steps), "unit": "ns/day",
                 "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                 "note": "box uploaded from host arrays inside the timed region; per-step FP64 energies read back"},
+        "grad": grad,
         "gpu_launches": launches,
         "steps_per_list_rebuild": steps_per_rebuild,
         "clocks": clocks,
@@ -536,6 +641,9 @@ def main():
         return
     if args.mode == "precision":
         run_precision(args)
+        return
+    if args.mode == "grad":
+        run_grad(args)
         return
     ws, rank, local, pg = dist_setup(args) if args.impl == "ours" else (int(os.environ.get("WORLD_SIZE", "1")),
                                                                         int(os.environ.get("RANK", "0")), 0, None)

@@ -273,6 +273,48 @@ lima_status lima_profile_steps(lima_ctx* ctx, int n_steps, float* ms);
 lima_status lima_get_kernel_launches(lima_ctx* ctx, uint64_t* count);
 
 /* ------------------------------------------------------------------ */
+/* Parameter gradients of a trajectory loss (physics semantics).  The   */
+/* reference has no gradients: LIMA_NET learns from trajectories the    */
+/* engine writes (Environment.cpp:138-141).  Here the loss is           */
+/* differentiated through the unrolled steps by a hand-written adjoint. */
+/* ------------------------------------------------------------------ */
+#define LIMA_LOSS_MAX_BINS 128
+
+/* Parameter vector theta, n = 2 * n_types + 3 entries:
+   [sigma_0 .. sigma_{n_types-1}, epsilon_0 .. epsilon_{n_types-1}, s_bond, s_angle, s_dihedral];
+   n_types = 1 + the largest atom type in the box, sigma in nm and epsilon in J/mol
+   (Lorentz-Berthelot mixing per pair), s_* scale every bond, angle and dihedral force
+   constant as loaded (1 = as loaded). */
+lima_status lima_get_param_count(lima_ctx* ctx, int* n);
+lima_status lima_get_params(lima_ctx* ctx, double* theta);
+lima_status lima_set_params(lima_ctx* ctx, const double* theta);
+
+typedef struct {
+    int n_steps;             /* T: the loss averages over the states after steps 1..T */
+    int checkpoint_every;    /* C: the forward pass keeps every C-th state and the backward pass
+                                recomputes each C-step segment from it (C >= T: one segment) */
+    int n_bins;              /* RDF bins, 1..LIMA_LOSS_MAX_BINS */
+    float r_max;             /* nm: bins of width dr = r_max / n_bins over [0, r_max];
+                                r_max + dr <= cutoff (the B-spline support) */
+    double w_energy;         /* weight of the potential energy per particle, U / N (J/mol) */
+    double w_rdf;            /* weight of the RDF-bin term */
+    const double* rdf_target;/* n_bins target occupancies (host); may be NULL when w_rdf == 0 */
+} lima_loss_spec;
+
+/* loss = (1/T) sum_{n=1..T} [ w_energy U(x_n)/N + w_rdf sum_b (h_b(x_n) - target_b)^2 ] with
+   h_b(x) = (1/N) sum over non-excluded pairs i<j of B(r_ij/dr - b - 1/2), B the quadratic
+   B-spline (support |u| < 3/2; the bins of one distance sum to 1).  Both calls run T NVE
+   velocity-Verlet steps of the physics path from the current state (plain FP32, thermostat
+   none, potential switch on), rebuild the pair list at every checkpoint (it must stay valid
+   for C steps: LIMA_ERR_NUMERIC otherwise) and leave the state as they found it. */
+lima_status lima_loss(lima_ctx* ctx, const lima_loss_spec* spec, double* loss);
+/* The same loss and d loss / d theta (lima_get_params order), by the adjoint of the unrolled
+   steps: pair and bonded Hessian-vector products in FP32, FP64 parameter reductions. */
+lima_status lima_grad(lima_ctx* ctx, const lima_loss_spec* spec, double* loss, double* grad);
+/* h_b of the current state (definition above), e.g. to build a target. */
+lima_status lima_rdf(lima_ctx* ctx, int n_bins, float r_max, double* h);
+
+/* ------------------------------------------------------------------ */
 /* No counterpart in the reference.  The reference updates its lists on  */
 /* the host (Engine::updateNeighborLists, Engine.cu:208-287); this is a  */
 /* context-free, allocation-free form of the device build behind          */

@@ -736,6 +736,103 @@ int orc_phys_run(const orc_phys_sys* S, const double* mass, double dt, int n_ste
     return 0;
 }
 
+/*
+ * Trajectory loss of the physics semantics (the definition the GPU adjoint
+ * differentiates, include/lima_abi.h lima_loss):
+ *   loss = (1/T) sum_{n=1..T} [ w_e U(x_n)/N + w_r sum_b (h_b(x_n) - target_b)^2 ]
+ *   h_b(x) = (1/N) sum over non-excluded pairs i<j of B(r_ij/dr - b - 1/2),
+ * B the quadratic B-spline (support |u| < 3/2), dr = r_max / n_bins.
+ */
+static double bspline2(double u) {
+    u = fabs(u);
+    if (u < 0.5) return 0.75 - u * u;
+    if (u < 1.5) return 0.5 * (1.5 - u) * (1.5 - u);
+    return 0.0;
+}
+
+int orc_phys_rdf(const orc_phys_sys* S, const double* x, int n_bins, double r_max, double* h) {
+    const int n = S->n;
+    const double L = S->box, dr = r_max / n_bins, sup = r_max + dr, sup2 = sup * sup;
+    memset(h, 0, sizeof(double) * n_bins);
+    int m = (int)floor(L / sup);
+    if (m < 3) m = 1;
+    const double cell = L / m;
+    int* head = (int*)malloc(sizeof(int) * m * m * m);
+    int* next = (int*)malloc(sizeof(int) * n);
+    int* cidx = (int*)malloc(sizeof(int) * n);
+    for (int k = 0; k < m * m * m; k++) head[k] = -1;
+    for (int i = 0; i < n; i++) {
+        int c[3];
+        for (int d = 0; d < 3; d++) {
+            double w = x[3 * i + d] - L * floor(x[3 * i + d] / L);
+            c[d] = (int)(w / cell);
+            if (c[d] >= m) c[d] = m - 1;
+        }
+        cidx[i] = (c[0] * m + c[1]) * m + c[2];
+        next[i] = head[cidx[i]];
+        head[cidx[i]] = i;
+    }
+    for (int i = 0; i < n; i++) {
+        const int ci = cidx[i];
+        const int cx = ci / (m * m), cy = (ci / m) % m, cz = ci % m;
+        const int span = m >= 3 ? 1 : 0;
+        for (int dx = -span; dx <= span; dx++)
+            for (int dy = -span; dy <= span; dy++)
+                for (int dz = -span; dz <= span; dz++) {
+                    const int k = (((cx + dx + m) % m) * m + ((cy + dy + m) % m)) * m + ((cz + dz + m) % m);
+                    for (int j = head[k]; j >= 0; j = next[j]) {
+                        if (j <= i) continue;
+                        double r2 = 0;
+                        for (int d = 0; d < 3; d++) {
+                            const double q = mimg(x[3 * j + d] - x[3 * i + d], L);
+                            r2 += q * q;
+                        }
+                        if (r2 >= sup2 || excluded(S, i, j)) continue;
+                        const double u = sqrt(r2) / dr;
+                        const int b0 = (int)floor(u - 0.5) - 1;
+                        for (int b = b0; b <= b0 + 3; b++)
+                            if (b >= 0 && b < n_bins) h[b] += bspline2(u - b - 0.5);
+                    }
+                }
+    }
+    for (int b = 0; b < n_bins; b++) h[b] /= n;
+    free(head);
+    free(next);
+    free(cidx);
+    return 0;
+}
+
+/* NVE velocity Verlet (half-step velocities v) from x for n_steps; x and v
+   are advanced in place; per_step (nullable) receives l(x_n), n = 1..T. */
+double orc_phys_loss(const orc_phys_sys* S, const double* mass, double dt, int n_steps, double* x, double* v,
+                     int n_bins, double r_max, double w_e, double w_r, const double* target, double* per_step) {
+    const int n = S->n;
+    double* F = (double*)malloc(sizeof(double) * 3 * n);
+    double* h = (double*)malloc(sizeof(double) * n_bins);
+    double en[5], total = 0.0;
+    orc_phys_forces(S, x, F, en);
+    for (int step = 0; step < n_steps; step++) {
+        for (int i = 0; i < n; i++)
+            for (int d = 0; d < 3; d++) {
+                v[3 * i + d] += F[3 * i + d] / mass[i] * dt;
+                x[3 * i + d] += v[3 * i + d] * dt;
+            }
+        orc_phys_forces(S, x, F, en);
+        orc_phys_rdf(S, x, n_bins, r_max, h);
+        double r = 0.0;
+        for (int b = 0; b < n_bins; b++) {
+            const double c = h[b] - (target ? target[b] : 0.0);
+            r += c * c;
+        }
+        const double l = w_e * (en[0] + en[1] + en[2] + en[3]) / n + w_r * r;
+        if (per_step) per_step[step] = l;
+        total += l;
+    }
+    free(F);
+    free(h);
+    return total / n_steps;
+}
+
 long orc_sizeof(int which) {
     switch (which) {
         case 0: return (long)sizeof(lima_compound);

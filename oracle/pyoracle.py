@@ -48,6 +48,10 @@ def oracle_lib():
         lib.orc_phys_forces.argtypes = [vp, vp, vp, vp]
         lib.orc_phys_run.restype = i
         lib.orc_phys_run.argtypes = [vp, vp, d, i, i, d, d, vp, vp, vp, vp, vp]
+        lib.orc_phys_rdf.restype = i
+        lib.orc_phys_rdf.argtypes = [vp, vp, i, d, vp]
+        lib.orc_phys_loss.restype = d
+        lib.orc_phys_loss.argtypes = [vp, vp, d, i, vp, vp, i, d, d, d, vp, vp]
         lib.orc_sizeof.restype = ctypes.c_long
         lib.orc_sizeof.argtypes = [i]
         _orc = lib
@@ -291,6 +295,9 @@ class PhysSystem:
         self.mass = ff["mass"][types].astype(np.float64)
         self.sigma = ff["sigma"][types].astype(np.float64)
         self.epsilon = ff["epsilon"][types].astype(np.float64)
+        self.n_types = int(types.max()) + 1 if n else 1
+        self.type_sigma = ff["sigma"][: self.n_types].astype(np.float64)
+        self.type_epsilon = ff["epsilon"][: self.n_types].astype(np.float64)
         self.box = float(s.spec.box_len)
         self.rc = float(s.spec.cutoff if rc is None else rc)
         self.r_on = float(self.rc if r_on is None else r_on)
@@ -362,6 +369,44 @@ class PhysSystem:
         st = self._struct()
         oracle_lib().orc_phys_forces(ctypes.byref(st), _p(x), _p(F), _p(en))
         return F, en
+
+    # -- trajectory loss (the quantity lima_loss / lima_grad evaluate) ---------
+    def params(self):
+        """theta in lima_get_params order: per-type sigma, per-type epsilon,
+        bond / angle / dihedral scales (1 = as built)."""
+        return np.concatenate([self.type_sigma, self.type_epsilon, [1.0, 1.0, 1.0]])
+
+    def with_params(self, theta):
+        """A copy whose per-type LJ parameters and bonded constants follow theta."""
+        import copy
+        nt = self.n_types
+        q = copy.copy(self)
+        q.type_sigma = np.asarray(theta[:nt], np.float64).copy()
+        q.type_epsilon = np.asarray(theta[nt:2 * nt], np.float64).copy()
+        q.sigma = q.type_sigma[self.types]
+        q.epsilon = q.type_epsilon[self.types]
+        q.bond_k = self.bond_k * theta[2 * nt]
+        q.angle_k = self.angle_k * theta[2 * nt + 1]
+        q.dih_k = self.dih_k * theta[2 * nt + 2]
+        return q
+
+    def rdf(self, n_bins, r_max, x=None):
+        x = np.ascontiguousarray(self.x if x is None else x, np.float64)
+        h = np.zeros(n_bins)
+        st = self._struct()
+        oracle_lib().orc_phys_rdf(ctypes.byref(st), _p(x), n_bins, r_max, _p(h))
+        return h
+
+    def loss(self, dt, n_steps, n_bins, r_max, w_energy, w_rdf, target=None, x=None, v=None):
+        """FP64 loss over n_steps NVE steps from (x, v); returns (loss, per-step terms)."""
+        x = np.ascontiguousarray((self.x if x is None else x).copy(), np.float64)
+        v = np.ascontiguousarray((self.velocities(dt) if v is None else v).copy(), np.float64)
+        per = np.zeros(n_steps)
+        tg = np.ascontiguousarray(np.zeros(n_bins) if target is None else target, np.float64)
+        st = self._struct()
+        L = oracle_lib().orc_phys_loss(ctypes.byref(st), _p(np.ascontiguousarray(self.mass)), dt, n_steps, _p(x),
+                                       _p(v), n_bins, r_max, w_energy, w_rdf, _p(tg), _p(per))
+        return L, per
 
     def run(self, dt, n_steps, x=None, v=None, thermostat=0, t0=300.0, tau=1e-4, t_prev=-1.0):
         x = np.ascontiguousarray((self.x if x is None else x).copy(), np.float64)

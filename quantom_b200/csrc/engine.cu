@@ -22,6 +22,7 @@
 #include <string>
 #include <vector>
 
+#include "adjoint.cuh"
 #include "lima_abi.h"
 #include "physdev.cuh"
 #include "refdev.cuh"
@@ -66,6 +67,9 @@ struct lima_ctx {
     cudaGraphExec_t dgraph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
     int dgraph_kernels[2] = {0, 0};
     uint64_t host_rebuilds = 0;   // list builds launched by the host (creation, set_state, build_nlist, ...)
+    // physics: differentiable parameters and the loss / adjoint buffers
+    lima::PhysParams params;
+    lima::AdjBuffers adj;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool timed = false;
     bool lambda_pending_reset = false;
@@ -581,6 +585,7 @@ lima_status lima_finish_box(lima_ctx* c) {
             lima::phys_prime(c->phys, c->cur, c->stream);
             c->host_rebuilds++;
             sync_checked(c);
+            lima::phys_params_init(c->phys, c->ff, c->params, c->stream);
             if (c->phys.dynamic_list) {
                 for (int parity = 0; parity < 2; parity++)
                     for (int energy = 0; energy < 2; energy++) {
@@ -873,6 +878,89 @@ lima_status lima_build_nlist(lima_ctx* c) {
             c->last_nlist_step = c->step;
         }
         sync_checked(c);
+    });
+}
+
+namespace {
+void need_physics(lima_ctx* c) {
+    need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
+    need(c->p.semantics == LIMA_SEMANTICS_PHYSICS, LIMA_ERR_UNSUPPORTED,
+         "parameters and gradients belong to physics semantics");
+}
+void need_gradable(lima_ctx* c) {
+    need_physics(c);
+    need(c->p.precision == LIMA_PRECISION_FP32, LIMA_ERR_UNSUPPORTED, "the loss / adjoint passes run in plain FP32");
+    need(c->p.thermostat == LIMA_THERMOSTAT_NONE, LIMA_ERR_UNSUPPORTED,
+         "the loss / adjoint passes integrate NVE (thermostat none)");
+    need(c->phys.use_switch, LIMA_ERR_UNSUPPORTED, "the loss / adjoint passes need the potential switch");
+}
+}  // namespace
+
+lima_status lima_get_param_count(lima_ctx* c, int* n) {
+    return guarded(c, [&] {
+        need(n != nullptr, LIMA_ERR_ARGUMENT, "null count");
+        need_physics(c);
+        *n = 2 * c->params.n_types + lima::kParKinds;
+    });
+}
+
+lima_status lima_get_params(lima_ctx* c, double* theta) {
+    return guarded(c, [&] {
+        need(theta != nullptr, LIMA_ERR_ARGUMENT, "null parameter vector");
+        need_physics(c);
+        lima::phys_params_get(c->params, theta);
+    });
+}
+
+lima_status lima_set_params(lima_ctx* c, const double* theta) {
+    return guarded(c, [&] {
+        need(theta != nullptr, LIMA_ERR_ARGUMENT, "null parameter vector");
+        need_physics(c);
+        sync_checked(c);
+        std::string msg;
+        const int st = lima::phys_params_set(c->phys, c->params, theta, msg, c->stream);
+        if (st != LIMA_OK) fail(static_cast<lima_status>(st), msg);
+        for (int t = 0; t < c->params.n_types; t++) {
+            c->ff.particle_parameters[t].sigma = static_cast<float>(c->params.sigma[t]);
+            c->ff.particle_parameters[t].epsilon = static_cast<float>(c->params.epsilon[t]);
+        }
+    });
+}
+
+lima_status lima_loss(lima_ctx* c, const lima_loss_spec* spec, double* loss) {
+    return guarded(c, [&] {
+        need(spec != nullptr && loss != nullptr, LIMA_ERR_ARGUMENT, "null spec or output");
+        need_gradable(c);
+        sync_checked(c);
+        std::string msg;
+        const int st = lima::adj_run(c->phys, c->cur, c->params, c->adj, c->dallocs, *spec, loss, nullptr, c->stream, msg);
+        if (st != LIMA_OK) fail(static_cast<lima_status>(st), msg);
+        c->host_rebuilds += 1;
+        sync_checked(c);
+    });
+}
+
+lima_status lima_grad(lima_ctx* c, const lima_loss_spec* spec, double* loss, double* grad) {
+    return guarded(c, [&] {
+        need(spec != nullptr && loss != nullptr && grad != nullptr, LIMA_ERR_ARGUMENT, "null spec or output");
+        need_gradable(c);
+        sync_checked(c);
+        std::string msg;
+        const int st = lima::adj_run(c->phys, c->cur, c->params, c->adj, c->dallocs, *spec, loss, grad, c->stream, msg);
+        if (st != LIMA_OK) fail(static_cast<lima_status>(st), msg);
+        c->host_rebuilds += 1;
+        sync_checked(c);
+    });
+}
+
+lima_status lima_rdf(lima_ctx* c, int n_bins, float r_max, double* h) {
+    return guarded(c, [&] {
+        need(h != nullptr, LIMA_ERR_ARGUMENT, "null output");
+        need_physics(c);
+        sync_checked(c);
+        std::string msg;
+        const int st = lima::adj_rdf(c->phys, c->cur, c->adj, c->dallocs, n_bins, r_max, h, c->stream, msg);
+        if (st != LIMA_OK) fail(static_cast<lima_status>(st), msg);
     });
 }
 

@@ -37,6 +37,13 @@ class LimaError(RuntimeError):
         self.status = status
 
 
+class LossSpec(ctypes.Structure):
+    """lima_loss_spec (include/lima_abi.h)."""
+    _fields_ = [("n_steps", ctypes.c_int), ("checkpoint_every", ctypes.c_int), ("n_bins", ctypes.c_int),
+                ("r_max", ctypes.c_float), ("w_energy", ctypes.c_double), ("w_rdf", ctypes.c_double),
+                ("rdf_target", ctypes.c_void_p)]
+
+
 class Params(ctypes.Structure):
     """lima_params (include/lima_abi.h)."""
     _fields_ = [("box_len", ctypes.c_float), ("cutoff", ctypes.c_float), ("ref_cutoff", ctypes.c_float),
@@ -83,6 +90,12 @@ def load_library():
         "lima_get_last_step_ms": (i, [vp, ctypes.POINTER(f)]),
         "lima_profile_steps": (i, [vp, i, vp]),
         "lima_get_rebuild_count": (i, [vp, ctypes.POINTER(ctypes.c_uint64)]),
+        "lima_get_param_count": (i, [vp, ctypes.POINTER(i)]),
+        "lima_get_params": (i, [vp, vp]),
+        "lima_set_params": (i, [vp, vp]),
+        "lima_loss": (i, [vp, vp, ctypes.POINTER(d)]),
+        "lima_grad": (i, [vp, vp, ctypes.POINTER(d), vp]),
+        "lima_rdf": (i, [vp, i, f, vp]),
         "lima_get_kernel_launches": (i, [vp, ctypes.POINTER(ctypes.c_uint64)]),
     }
     for name, (res, args) in sigs.items():
@@ -199,6 +212,52 @@ class Engine:
         v = ctypes.c_uint64()
         self._check(self.lib.lima_get_kernel_launches(self.h, ctypes.byref(v)))
         return int(v.value)
+
+    # -- parameters, trajectory loss and its gradient (physics semantics) -----
+    def param_count(self) -> int:
+        n = ctypes.c_int()
+        self._check(self.lib.lima_get_param_count(self.h, ctypes.byref(n)))
+        return int(n.value)
+
+    def get_params(self) -> np.ndarray:
+        """theta = [sigma per type, epsilon per type, bond, angle, dihedral scales]."""
+        th = np.zeros(self.param_count(), np.float64)
+        self._check(self.lib.lima_get_params(self.h, _ptr(th)))
+        return th
+
+    def set_params(self, theta):
+        th = np.ascontiguousarray(theta, np.float64)
+        if th.shape != (self.param_count(),):
+            raise ValueError(f"expected {self.param_count()} parameters")
+        self._check(self.lib.lima_set_params(self.h, _ptr(th)))
+
+    @staticmethod
+    def loss_spec(n_steps, checkpoint_every, n_bins, r_max, w_energy, w_rdf, target=None):
+        tg = None if target is None else np.ascontiguousarray(target, np.float64)
+        spec = LossSpec(int(n_steps), int(checkpoint_every), int(n_bins), float(r_max), float(w_energy),
+                        float(w_rdf), tg.ctypes.data if tg is not None else None)
+        return spec, tg
+
+    def loss(self, n_steps, checkpoint_every, n_bins, r_max, w_energy, w_rdf, target=None) -> float:
+        spec, keep = self.loss_spec(n_steps, checkpoint_every, n_bins, r_max, w_energy, w_rdf, target)
+        out = ctypes.c_double()
+        self._check(self.lib.lima_loss(self.h, ctypes.byref(spec), ctypes.byref(out)))
+        del keep
+        return float(out.value)
+
+    def grad(self, n_steps, checkpoint_every, n_bins, r_max, w_energy, w_rdf, target=None):
+        """(loss, d loss / d theta) by the adjoint of the unrolled steps."""
+        spec, keep = self.loss_spec(n_steps, checkpoint_every, n_bins, r_max, w_energy, w_rdf, target)
+        out = ctypes.c_double()
+        g = np.zeros(self.param_count(), np.float64)
+        self._check(self.lib.lima_grad(self.h, ctypes.byref(spec), ctypes.byref(out), _ptr(g)))
+        del keep
+        return float(out.value), g
+
+    def rdf(self, n_bins, r_max) -> np.ndarray:
+        h = np.zeros(int(n_bins), np.float64)
+        self._check(self.lib.lima_rdf(self.h, int(n_bins), float(r_max), _ptr(h)))
+        return h
 
     def rebuild_count(self) -> int:
         """Physics semantics: pair-list builds since creation."""

@@ -83,6 +83,19 @@ class System:
     bridges: np.ndarray                    # CompoundBridgeCompact, (n_bridges,)
     info: dict = field(default_factory=dict)
 
+    def with_state(self, states, prev_positions, solvents) -> "System":
+        """The same topology with positions and previous positions from a
+        readback (Engine.compound_states / Engine.solvents)."""
+        import copy
+        s = copy.copy(self)
+        s.compounds = self.compounds.copy()
+        s.states = self.states.copy()
+        s.solvents = np.array(solvents, copy=True)
+        for c in range(self.n_compounds):
+            s.states[c]["positions"] = states[c]["positions"]
+            s.compounds[c]["prev_positions"] = prev_positions[c]
+        return s
+
     @property
     def n_compounds(self) -> int:
         return len(self.compounds)
