@@ -305,8 +305,9 @@ typedef struct {
    h_b(x) = (1/N) sum over non-excluded pairs i<j of B(r_ij/dr - b - 1/2), B the quadratic
    B-spline (support |u| < 3/2; the bins of one distance sum to 1).  Both calls run T NVE
    velocity-Verlet steps of the physics path from the current state (plain FP32, thermostat
-   none, potential switch on), rebuild the pair list at every checkpoint (it must stay valid
-   for C steps: LIMA_ERR_NUMERIC otherwise) and leave the state as they found it. */
+   none, potential switch on), re-sort and rebuild the pair list at every checkpoint and
+   rebuild it in place every 10 steps in between (it must stay valid for 10 steps:
+   LIMA_ERR_NUMERIC otherwise), and leave the state as they found it. */
 lima_status lima_loss(lima_ctx* ctx, const lima_loss_spec* spec, double* loss);
 /* The same loss and d loss / d theta (lima_get_params order), by the adjoint of the unrolled
    steps: pair and bonded Hessian-vector products in FP32, FP64 parameter reductions. */

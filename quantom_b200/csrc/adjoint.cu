@@ -24,6 +24,10 @@ namespace lima {
 namespace {
 
 constexpr int kAdjTB = 256;   // 32 particles x kGroup lanes
+// Inside a checkpoint segment the pair list is rebuilt in place (particle
+// order kept) every kListEpoch steps; the backward pass rebuilds the list of
+// each epoch from its first state, which reproduces the forward's lists.
+constexpr int kListEpoch = 10;
 
 __device__ __forceinline__ float mimg_a(float d, float L, float invL) { return d - L * rintf(d * invL); }
 
@@ -724,6 +728,7 @@ int adj_run(const PhysDev& d0, int cur, const PhysParams& pp, AdjBuffers& A, std
         R.restore(cur, k);
         const int n0 = k * C, len = std::min(C, T - n0);
         for (int q = 0; q < len; q++) {
+            if (q > 0 && q % kListEpoch == 0) phys_rebuild_inplace(d, d.pos[cur], s);
             phys_step_kernels(d, cur, s, false);
             cur ^= 1;
             if (!grad) R.loss_pass(cur, d.pos[cur], d.pos_orig[cur], n0 + q + 1);
@@ -758,6 +763,7 @@ int adj_run(const PhysDev& d0, int cur, const PhysParams& pp, AdjBuffers& A, std
             if (d.n_cp)
                 cudaMemcpyAsync(A.seg_xo, d.pos_orig[cur], sizeof(float4) * d.n_cp, cudaMemcpyDeviceToDevice, s);
             for (int q = 0; q < len; q++) {
+                if (q > 0 && q % kListEpoch == 0) phys_rebuild_inplace(d, d.pos[cur], s);
                 phys_step_kernels(d, cur, s, false);
                 cur ^= 1;
                 float4* xs = A.seg_x + (size_t)(q + 1) * d.n_pad;
@@ -778,7 +784,12 @@ int adj_run(const PhysDev& d0, int cur, const PhysParams& pp, AdjBuffers& A, std
                 k_adj_bonded<1><<<tbk, kAdjTB, 0, s>>>(d, xo, a, 0, nullptr);
                 k_adj_pair<false, true><<<pb, kAdjTB, 0, s>>>(d, xs, a, A.hist + (size_t)(n0 + q) * nb, A.target);
             }
+            int epoch = (len - 1) / kListEpoch;   // the list built last
             for (int q = len - 1; q >= 0; q--) {
+                if (q / kListEpoch != epoch) {
+                    epoch = q / kListEpoch;
+                    phys_rebuild_inplace(d, A.seg_x + (size_t)epoch * kListEpoch * d.n_pad, s);
+                }
                 const bool has_loss = q >= 1;
                 a.le = has_loss ? le : 0.f;
                 a.lr = has_loss ? lr : 0.f;

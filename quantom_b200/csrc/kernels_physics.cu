@@ -103,11 +103,11 @@ __device__ void fold(const PhysDev& d, int src) {
 }  // namespace
 
 // ---------------------------------------------------------------- rebuild ---
-__global__ void k_keys(PhysDev d, int cur) {
+__global__ void k_keys(PhysDev d, const float4* __restrict__ pos) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= d.n) return;
     int cx, cy, cz;
-    cell_xyz(d, d.pos[cur][i], cx, cy, cz);
+    cell_xyz(d, pos[i], cx, cy, cz);
     d.keys[0][i] = (uint32_t)((cx * d.m + cy) * d.m + cz);
     d.vals[0][i] = i;
 }
@@ -128,6 +128,23 @@ __global__ void k_permute(PhysDev d, int cur, int mixed) {
     d.sorted_of_orig[o] = k;
     d.xref[k] = p;
     // cstart[c] = first sorted slot of cell c for every c in 0..n_cells (empty cells included)
+    const uint32_t c = d.keys[1][k];
+    if (k == 0) {
+        for (uint32_t q = 0; q <= c; q++) d.cstart[q] = 0;
+    } else {
+        const uint32_t cp = d.keys[1][k - 1];
+        for (uint32_t q = cp + 1; q <= c; q++) d.cstart[q] = k;
+    }
+    if (k == d.n - 1)
+        for (uint32_t q = c + 1; q <= (uint32_t)d.n_cells; q++) d.cstart[q] = d.n;
+}
+
+// In-place rebuild: cell offsets of the sorted keys (the particles stay where
+// they are; vals[1] lists them in cell order) and the list's reference positions.
+__global__ void k_cell_offsets(PhysDev d, const float4* __restrict__ pos) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= d.n) return;
+    d.xref[k] = pos[k];
     const uint32_t c = d.keys[1][k];
     if (k == 0) {
         for (uint32_t q = 0; q <= c; q++) d.cstart[q] = 0;
@@ -175,6 +192,9 @@ __global__ void k_list_check(const int* need, unsigned long long* count, cudaGra
 // row lists its neighbours in candidate order (deterministic).  Collectives
 // (ballots, shuffles, __syncwarp) only occur in warp-uniform code.  Boxes
 // with fewer than 5 cells per side test all particles with the minimum image.
+// items (nullable): the cell order as a list of slots when the particles were
+// not moved into it (in-place rebuild); positions q of that order index cells,
+// slots index the particle data and the list rows.
 namespace {
 
 struct Cand {
@@ -183,14 +203,15 @@ struct Cand {
 };
 
 template <bool MIN_IMAGE>
-__device__ __forceinline__ void scan_range(const PhysDev& d, const float4* __restrict__ pos, Cand* sc, int jb, int je,
-                                           float sx, float sy, float sz, bool mine, int i, float4 pi, uint32_t oi,
+__device__ __forceinline__ void scan_range(const PhysDev& d, const float4* __restrict__ pos,
+                                           const uint32_t* __restrict__ items, Cand* sc, int jb, int je, float sx,
+                                           float sy, float sz, bool mine, int i, int qi, float4 pi, uint32_t oi,
                                            bool ex, int lane, int sub, int& cnt) {
     for (int jc = jb; jc < je; jc += 32) {
         const int nv = min(32, je - jc);
         __syncwarp();
         if (lane < nv) {
-            const int j = jc + lane;
+            const int j = items ? (int)items[jc + lane] : jc + lane;
             const float4 p = pos[j];
             const uint32_t oj = d.orig_of_sorted[j];
             sc[lane].p = make_float4(p.x + sx, p.y + sy, p.z + sz, 0.f);
@@ -215,7 +236,7 @@ __device__ __forceinline__ void scan_range(const PhysDev& d, const float4* __res
                     mine_bits |= (dx * dx + dy * dy + dz * dz < d.rlist2 ? 1u : 0u) << c;
                 }
             }
-            const int self = i - jc;
+            const int self = qi - jc;
             if (self >= 0 && self < 32) mine_bits &= ~(1u << self);
             if (ex)
                 for (uint32_t b = mine_bits; b; b &= b - 1u) {
@@ -238,16 +259,17 @@ __device__ __forceinline__ void scan_range(const PhysDev& d, const float4* __res
 
 }  // namespace
 
-__global__ void __launch_bounds__(kBuildWarps * 32) k_build_list(PhysDev d, int cur) {
+__global__ void __launch_bounds__(kBuildWarps * 32) k_build_list(PhysDev d, const float4* __restrict__ pos,
+                                                                 const uint32_t* __restrict__ items) {
     __shared__ Cand s_cand[kBuildWarps][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int pl = lane >> 2, sub = lane & 3;
     const int base = (blockIdx.x * kBuildWarps + w) * 8;
     if (base >= d.n) return;   // the whole warp
-    const float4* __restrict__ pos = d.pos[cur];
     Cand* sc = s_cand[w];
-    const int i = base + pl;
-    const bool have = i < d.n;
+    const int qi = base + pl;   // position in the cell order
+    const bool have = qi < d.n;
+    const int i = have ? (items ? (int)items[qi] : qi) : qi;   // slot
     const float4 pi = have ? pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
     const uint32_t oi = have ? d.orig_of_sorted[i] : 0u;
     const bool ex = have && oi < (uint32_t)d.n_cp && d.excl_off[oi + 1] > d.excl_off[oi];
@@ -255,7 +277,7 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_build_list(PhysDev d, int 
     const int m = d.m;
 
     if (m < 5) {
-        scan_range<true>(d, pos, sc, 0, d.n, 0.f, 0.f, 0.f, have, i, pi, oi, ex, lane, sub, cnt);
+        scan_range<true>(d, pos, items, sc, 0, d.n, 0.f, 0.f, 0.f, have, i, qi, pi, oi, ex, lane, sub, cnt);
     } else {
         int cx = -1, cy = -1, cz = 0;
         if (have) cell_xyz(d, pi, cx, cy, cz);
@@ -283,18 +305,18 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_build_list(PhysDev d, int 
                     // unwrapped cells u0..u1 (at most m of them) -> one or two real ranges
                     const int u0 = hz0 - 2, u1 = hz1 + 2;
                     if (u0 < 0) {
-                        scan_range<false>(d, pos, sc, (int)d.cstart[col + u0 + m], (int)d.cstart[col + m], sx, sy, -d.L,
-                                          mine, i, pi, oi, ex, lane, sub, cnt);
-                        scan_range<false>(d, pos, sc, (int)d.cstart[col], (int)d.cstart[col + u1 + 1], sx, sy, 0.f, mine,
-                                          i, pi, oi, ex, lane, sub, cnt);
+                        scan_range<false>(d, pos, items, sc, (int)d.cstart[col + u0 + m], (int)d.cstart[col + m], sx, sy, -d.L,
+                                          mine, i, qi, pi, oi, ex, lane, sub, cnt);
+                        scan_range<false>(d, pos, items, sc, (int)d.cstart[col], (int)d.cstart[col + u1 + 1], sx, sy, 0.f, mine,
+                                          i, qi, pi, oi, ex, lane, sub, cnt);
                     } else if (u1 >= m) {
-                        scan_range<false>(d, pos, sc, (int)d.cstart[col + u0], (int)d.cstart[col + m], sx, sy, 0.f, mine,
-                                          i, pi, oi, ex, lane, sub, cnt);
-                        scan_range<false>(d, pos, sc, (int)d.cstart[col], (int)d.cstart[col + u1 - m + 1], sx, sy, d.L,
-                                          mine, i, pi, oi, ex, lane, sub, cnt);
+                        scan_range<false>(d, pos, items, sc, (int)d.cstart[col + u0], (int)d.cstart[col + m], sx, sy, 0.f, mine,
+                                          i, qi, pi, oi, ex, lane, sub, cnt);
+                        scan_range<false>(d, pos, items, sc, (int)d.cstart[col], (int)d.cstart[col + u1 - m + 1], sx, sy, d.L,
+                                          mine, i, qi, pi, oi, ex, lane, sub, cnt);
                     } else {
-                        scan_range<false>(d, pos, sc, (int)d.cstart[col + u0], (int)d.cstart[col + u1 + 1], sx, sy, 0.f,
-                                          mine, i, pi, oi, ex, lane, sub, cnt);
+                        scan_range<false>(d, pos, items, sc, (int)d.cstart[col + u0], (int)d.cstart[col + u1 + 1], sx, sy, 0.f,
+                                          mine, i, qi, pi, oi, ex, lane, sub, cnt);
                     }
                 }
             }
@@ -660,17 +682,21 @@ void pair_variant(const PhysDev& d, int cur, int slot, cudaStream_t s) {
 
 }  // namespace
 
-void launch_keys(const PhysDev& d, int cur, cudaStream_t s) {
-    k_keys<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d, cur);
+void launch_keys(const PhysDev& d, const float4* pos, cudaStream_t s) {
+    k_keys<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d, pos);
+}
+
+void launch_cell_offsets(const PhysDev& d, const float4* pos, cudaStream_t s) {
+    k_cell_offsets<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d, pos);
 }
 
 void launch_permute(const PhysDev& d, int cur, bool mixed, cudaStream_t s) {
     k_permute<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d, cur, mixed ? 1 : 0);
 }
 
-void launch_build_list(const PhysDev& d, int cur, cudaStream_t s) {
+void launch_build_list(const PhysDev& d, const float4* pos, const uint32_t* items, cudaStream_t s) {
     const int warps = (d.n + 7) / 8;
-    k_build_list<<<(warps + kBuildWarps - 1) / kBuildWarps, kBuildWarps * 32, 0, s>>>(d, cur);
+    k_build_list<<<(warps + kBuildWarps - 1) / kBuildWarps, kBuildWarps * 32, 0, s>>>(d, pos, items);
 }
 
 void launch_copy_back(const PhysDev& d, int cur, bool mixed, cudaStream_t s) {

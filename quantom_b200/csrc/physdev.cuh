@@ -112,6 +112,8 @@ struct PhysHost {
 int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>& allocs, std::string& msg);
 void phys_upload_state(const PhysHost& h, PhysDev& d, int cur, cudaStream_t s);
 void phys_rebuild(const PhysDev& d, int cur, cudaStream_t s);
+// list of `pos` (particle order unchanged; reference positions reset)
+void phys_rebuild_inplace(const PhysDev& d, const float4* pos, cudaStream_t s);
 void phys_prime(PhysDev& d, int cur, cudaStream_t s);
 // dynamic lists: the step graph of parity `cur` ({check -> IF(rebuild)} || bonded -> pair);
 // returns the kernels of one replay without a rebuild, or -1 if the graph cannot be built

@@ -321,14 +321,27 @@ void phys_upload_state(const PhysHost& h, PhysDev& d, int cur, cudaStream_t s) {
 void phys_rebuild(const PhysDev& d, int cur, cudaStream_t s) {
     const size_t ncell = (size_t)d.n_cells;
     const bool mixed = d.precision == LIMA_PRECISION_MIXED;
-    launch_keys(d, cur, s);
+    launch_keys(d, d.pos[cur], s);
     size_t bytes = d.sort_tmp_bytes;
     int end_bit = 1;
     while ((1ull << end_bit) < (unsigned long long)ncell) end_bit++;
     cub::DeviceRadixSort::SortPairs(d.sort_tmp, bytes, d.keys[0], d.keys[1], d.vals[0], d.vals[1], d.n, 0, end_bit, s);
     launch_permute(d, cur, mixed, s);
     launch_copy_back(d, cur, mixed, s);
-    launch_build_list(d, cur, s);
+    launch_build_list(d, d.pos[cur], nullptr, s);
+}
+
+// The list of positions `pos` without moving any particle: keys, a sort of
+// the slots by cell (vals[1]), cell offsets, then the build through vals[1].
+void phys_rebuild_inplace(const PhysDev& d, const float4* pos, cudaStream_t s) {
+    const size_t ncell = (size_t)d.n_cells;
+    launch_keys(d, pos, s);
+    size_t bytes = d.sort_tmp_bytes;
+    int end_bit = 1;
+    while ((1ull << end_bit) < (unsigned long long)ncell) end_bit++;
+    cub::DeviceRadixSort::SortPairs(d.sort_tmp, bytes, d.keys[0], d.keys[1], d.vals[0], d.vals[1], d.n, 0, end_bit, s);
+    launch_cell_offsets(d, pos, s);
+    launch_build_list(d, pos, d.vals[1], s);
 }
 
 void phys_prime(PhysDev&, int, cudaStream_t) {}

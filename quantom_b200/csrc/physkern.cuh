@@ -12,9 +12,11 @@ constexpr int kGroup = 8;        // lanes per particle in the list and pair kern
 constexpr int kBuildWarps = 4;   // warps (8 particles each) per block of the list build
 constexpr int kMaxTypes = 32;    // LIMA_MAX_ATOM_TYPES
 
-void launch_keys(const PhysDev& d, int cur, cudaStream_t s);
+void launch_keys(const PhysDev& d, const float4* pos, cudaStream_t s);
+void launch_cell_offsets(const PhysDev& d, const float4* pos, cudaStream_t s);
 void launch_permute(const PhysDev& d, int cur, bool mixed, cudaStream_t s);
-void launch_build_list(const PhysDev& d, int cur, cudaStream_t s);
+// items (nullable): slots in cell order when the particles were not re-sorted
+void launch_build_list(const PhysDev& d, const float4* pos, const uint32_t* items, cudaStream_t s);
 void launch_copy_back(const PhysDev& d, int cur, bool mixed, cudaStream_t s);
 // slot: accumulator slot to add energies to; fold_src: slot to fold first (-1: none)
 void launch_bonded(const PhysDev& d, int cur, bool energy, int slot, int fold_src, cudaStream_t s);

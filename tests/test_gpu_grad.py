@@ -92,15 +92,16 @@ def test_grad_matches_fp64_finite_differences(gpu):
 
 
 def test_checkpoint_interval_does_not_change_the_gradient(gpu):
-    """C only moves the list rebuilds (and re-sorts) of the unroll, which
-    changes FP32 summation order: loss and gradient agree to rounding."""
+    """C only moves the re-sorts of the unroll (the list is also rebuilt in
+    place every 10 steps inside a segment), which changes FP32 summation
+    order: loss and gradient agree to rounding."""
     E = gpu
     s = _relaxed(E, "small_bridged", 6)
     tg = _target(po.PhysSystem(s, rc=s.spec.cutoff, r_on=1.0))
     out = []
     with E.Engine(s, _params(E, s)) as eng:
-        for c in (1, 7, 20):
-            out.append(eng.grad(20, c, NB, RMAX, 1.0, 1e3, tg))
+        for c in (1, 7, 40):
+            out.append(eng.grad(40, c, NB, RMAX, 1.0, 1e3, tg))
     for L, g in out[1:]:
         assert abs(L - out[0][0]) <= 1e-7 * abs(out[0][0])
         assert np.abs(g - out[0][1]).max() <= 1e-4 * np.abs(out[0][1]).max()
