@@ -48,9 +48,12 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-sample-steps", type=int, default=2)
-    ap.add_argument("--mode", default="full", choices=["full", "kernels", "precision", "grad"],
+    ap.add_argument("--mode", default="full", choices=["full", "kernels", "precision", "grad", "large"],
                     help="kernels: only warm-up + K plain-FP32 steps (the command profiled with ncu); "
-                         "precision: the NVE drift / force-error study of plain FP32 against mixed precision")
+                         "precision: the NVE drift / force-error study of plain FP32 against mixed precision; "
+                         "grad: the parameter-gradient study on the 8,192 LJ box; "
+                         "large: the 258k solvated-chain box, mixed forward and adjoint gradients")
+    ap.add_argument("--large-steps", type=int, default=10000, help="--mode large: mixed-precision forward steps")
     ap.add_argument("--nve-steps", type=int, default=50000, help="--mode precision: NVE steps per run")
     ap.add_argument("--eq-steps", type=int, default=5000, help="--mode precision: Berendsen equilibration steps")
     ap.add_argument("--fp64-fd", action="store_true",
@@ -286,6 +289,26 @@ def flat_forces(system, fc, fs):
     return np.concatenate(parts + [fs]) if parts else fs
 
 
+def drift_fit(t, e):
+    """Least-squares slope of e(t) and its standard error, the latter widened
+    for correlated residuals: SE = sigma_r * sqrt(tau / sum (t - mean t)^2),
+    tau = 1 + 2 * sum of the residual autocorrelation up to its first
+    negative lag (integrated autocorrelation time, in samples)."""
+    coef = np.polyfit(t, e, 1)
+    r = e - np.polyval(coef, t)
+    n = len(r)
+    var = float(r.var())
+    tau = 1.0
+    if var > 0:
+        for k in range(1, n // 2):
+            rho = float(np.dot(r[:-k], r[k:]) / ((n - k) * var))
+            if rho <= 0:
+                break
+            tau += 2 * rho
+    se = math.sqrt(var * tau / float(((t - t.mean()) ** 2).sum()))
+    return float(coef[0]), se, tau
+
+
 def run_precision(args):
     """Config-2 study on the 32k box: Berendsen equilibration, then NVE runs
     of plain FP32 and mixed precision at dt 2 fs and 1 fs.  Drift = slope of
@@ -338,11 +361,13 @@ def run_precision(args):
                     end = with_state(system, st2, prev2, eng.solvents())
             t = np.asarray(t_ns)
             et = np.asarray(etot)
-            slope = float(np.polyfit(t, et, 1)[0])            # J/mol per ns
+            slope, se, tau = drift_fit(t, et)
             resid = et - np.polyval(np.polyfit(t, et, 1), t)
             result["runs"].append({
                 "precision": name, "dt_fs": dt_fs, "simulated_ps": float(t[-1] * 1e3),
                 "drift_kT_per_particle_per_ns": slope / (n * kT),
+                "drift_stderr_kT_per_particle_per_ns": se / (n * kT),
+                "residual_autocorr_samples": tau,
                 "drift_J_per_mol_per_ns": slope,
                 "etot_fluct_rms_kT_per_particle": float(resid.std() / (n * kT)),
                 "temperature_mean_K": float(np.mean(temp)), "temperature_first_last_K": [temp[0], temp[-1]],
@@ -351,8 +376,13 @@ def run_precision(args):
     result["force_relrms_vs_fp64"]["after_nve_fp32_2fs"] = force_errors(end)
     for dt_fs in (2.0, 1.0):
         r = {x["precision"]: x for x in result["runs"] if x["dt_fs"] == dt_fs}
+        f32, mx = r["fp32"], r["mixed"]
         result[f"drift_ratio_fp32_over_mixed_{int(dt_fs)}fs"] = (
-            abs(r["fp32"]["drift_kT_per_particle_per_ns"]) / max(abs(r["mixed"]["drift_kT_per_particle_per_ns"]), 1e-30))
+            abs(f32["drift_kT_per_particle_per_ns"]) / max(abs(mx["drift_kT_per_particle_per_ns"]), 1e-30))
+        # lower bound: FP32 drift less 2 standard errors over mixed drift plus 2 standard errors
+        result[f"drift_ratio_lower_bound_2se_{int(dt_fs)}fs"] = (
+            max(abs(f32["drift_kT_per_particle_per_ns"]) - 2 * f32["drift_stderr_kT_per_particle_per_ns"], 0.0) /
+            (abs(mx["drift_kT_per_particle_per_ns"]) + 2 * mx["drift_stderr_kT_per_particle_per_ns"]))
     print(json.dumps(result), flush=True)
 
 
@@ -452,6 +482,130 @@ def run_grad(args):
     from quantom_b200 import engine as E
     from quantom_b200 import systems as S
     print(json.dumps({"mode": "grad", **grad_study(E, S, fp64_fd=args.fp64_fd)}), flush=True)
+
+
+# ------------------------------------------------- large solvated chains --
+LARGE_WORKLOAD = "solvated_chains_258k"
+
+
+def run_large(args):
+    """The 258k box: 64 chains x 128 particles (two compounds and one
+    bridge each) in 250,000 solvents, 20 nm box, rc 1.2 nm.  Mixed-precision
+    forward (Berendsen 300 K, tau 0.1 ps) for --large-steps steps: device time
+    of the whole run (one event pair; the pair list alone is larger than the
+    L2), ns/day, list rebuilds; forces of the first state against the FP64
+    oracle.  Then the adjoint gradient of <U>/N + 100 x RDF-bin loss over a
+    100-step NVE unroll with checkpoints every 10 with respect to sigma and
+    epsilon of every type (solvent and the 4 chain types) and the bond,
+    angle and dihedral scales; its cost against the forward loss; central
+    differences of the FP32 GPU loss (step 1e-3 relative) for every
+    component."""
+    import torch
+    from oracle import pyoracle as po
+    from quantom_b200 import engine as E
+    from quantom_b200 import systems as S
+    spec = S.CONFIGS[LARGE_WORKLOAD]
+    t0 = time.perf_counter()
+    system = S.make_system(LARGE_WORKLOAD, seed=args.seed)
+    t_gen = time.perf_counter() - t0
+    n = system.n_particles
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(device=dev)
+    out = {"mode": "large", "workload": f"{LARGE_WORKLOAD}: 64 chains x 128 (2 compounds + 1 bridge each) + "
+                                        f"250,000 solvents, {spec.box_len} nm box, rc 1.2 nm (C2 switch from 1.0), "
+                                        f"skin {SKIN} nm, dynamic lists, Berendsen 300 K tau 0.1 ps, dt 2 fs",
+           "particles": n, "compounds": system.n_compounds, "bridges": int(len(system.bridges)),
+           "generate_s": t_gen}
+
+    def params(prec, thermostat, skin=SKIN):
+        p = physics_params(E, spec, prec, stream.cuda_stream, 0)
+        p.thermostat = thermostat
+        p.skin = skin
+        return p
+
+    # forces of the generated state against the FP64 oracle
+    F64, en64 = po.PhysSystem(system, rc=spec.cutoff, r_on=1.0).forces()
+    for name, prec in (("fp32", E.PRECISION_FP32), ("mixed", E.PRECISION_MIXED)):
+        with E.Engine(system, params(prec, E.THERMOSTAT_NONE)) as eng:
+            tot = eng.compute_energies()
+            F = flat_forces(system, *eng.forces()).astype(np.float64)
+        out[f"force_relrms_vs_fp64_{name}"] = float(np.sqrt(((F - F64) ** 2).sum() / (F64 ** 2).sum()))
+        out[f"lj_energy_rel_err_{name}"] = abs(tot[E.E_LJ] - en64[0]) / abs(en64[0])
+
+    # mixed-precision forward
+    for name, prec in (("mixed", E.PRECISION_MIXED), ("fp32", E.PRECISION_FP32)):
+        steps = args.large_steps if name == "mixed" else max(1000, args.large_steps // 5)
+        with E.Engine(system, params(prec, E.THERMOSTAT_BERENDSEN)) as eng:
+            eng.step(max(3, args.warmup))
+            eng.synchronize()
+            r0 = eng.rebuild_count()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            eng.step(steps)
+            b.record(stream)
+            stream.synchronize()
+            eng.synchronize()
+            ms = a.elapsed_time(b) / steps
+            e = eng.compute_energies()
+            out[name] = {"steps": steps, "ms_per_step": ms, "ns_per_day": ns_per_day(spec.dt, ms),
+                         "steps_per_list_rebuild": steps / max(1, eng.rebuild_count() - r0),
+                         "temperature_end_K": e[E.E_TEMPERATURE], "kernels_ms": eng.profile_steps(100)}
+            if name == "mixed":
+                st, prev = eng.compound_states()
+                start = system.with_state(st, prev, eng.solvents())
+        print(json.dumps({name: out[name]}), flush=True)
+    out["mixed_over_fp32"] = out["mixed"]["ms_per_step"] / out["fp32"]["ms_per_step"]
+
+    # adjoint gradient over a 100-step NVE unroll
+    T, C, nb, rmax, w_e, w_r = 100, 10, 50, 1.2 * 50 / 51, 1.0, 100.0
+    with E.Engine(start, params(E.PRECISION_FP32, E.THERMOSTAT_BERENDSEN, skin=0.2)) as eq:
+        th = eq.get_params()
+        th2 = th.copy()
+        th2[0] *= 1.02
+        eq.set_params(th2)
+        eq.step(500)
+        target = np.zeros(nb)
+        for _ in range(5):
+            eq.step(20)
+            target += eq.rdf(nb, rmax) / 5
+    with E.Engine(start, params(E.PRECISION_FP32, E.THERMOSTAT_NONE, skin=0.2)) as eng:
+        theta = eng.get_params()
+
+        def wall(fn, reps=3):
+            fn()
+            torch.cuda.synchronize(dev)
+            ts = []
+            for _ in range(reps):
+                t1 = time.perf_counter()
+                r = fn()
+                torch.cuda.synchronize(dev)
+                ts.append(time.perf_counter() - t1)
+            return r, 1e3 * min(ts)
+        L, t_loss = wall(lambda: eng.loss(T, C, nb, rmax, w_e, w_r, target))
+        (_, g), t_grad = wall(lambda: eng.grad(T, C, nb, rmax, w_e, w_r, target))
+        fd, rel = [], []
+        for k in range(len(theta)):
+            h = 1e-3 * abs(theta[k])
+            tp = theta.copy()
+            tp[k] += h
+            eng.set_params(tp)
+            lp = eng.loss(T, C, nb, rmax, w_e, w_r, target)
+            tp[k] -= 2 * h
+            eng.set_params(tp)
+            lm = eng.loss(T, C, nb, rmax, w_e, w_r, target)
+            eng.set_params(theta)
+            fd.append((lp - lm) / (2 * h))
+            rel.append(abs(g[k] - fd[-1]) / max(abs(fd[-1]), 1e-300))
+        nt = (len(theta) - 3) // 2
+        names = [f"sigma[{t}]" for t in range(nt)] + [f"epsilon[{t}]" for t in range(nt)] + ["bond_k", "angle_k",
+                                                                                              "dihedral_k"]
+        out["grad"] = {"n_steps": T, "checkpoint_every": C, "n_bins": nb, "w_energy": w_e, "w_rdf": w_r,
+                       "target": "RDF-bin occupancy of the same box run with solvent sigma + 2 %",
+                       "loss": L, "ms_forward_loss": t_loss, "ms_grad": t_grad, "grad_over_forward": t_grad / t_loss,
+                       "params": names, "theta": theta.tolist(), "grad": g.tolist(), "fd_fp32_gpu_h1e-3": fd,
+                       "rel_err_vs_fd": rel}
+    print(json.dumps(out), flush=True)
 
 
 # --------------------------------------------------------------- CPU side --
@@ -644,6 +798,9 @@ def main():
         return
     if args.mode == "grad":
         run_grad(args)
+        return
+    if args.mode == "large":
+        run_large(args)
         return
     ws, rank, local, pg = dist_setup(args) if args.impl == "ours" else (int(os.environ.get("WORLD_SIZE", "1")),
                                                                         int(os.environ.get("RANK", "0")), 0, None)

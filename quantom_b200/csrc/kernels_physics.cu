@@ -329,21 +329,36 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_build_list(PhysDev d, cons
 }
 
 // ----------------------------------------------------------------- bonded ---
-template <bool ENERGY>
 // The bonded terms read the orig-ordered compound positions (pos_orig), none
 // of the arrays a list rebuild re-sorts, so a rebuild may run concurrently.
+// MIXED: every bond vector is (b_hi - a_hi) + (b_lo - a_lo), so the stiff
+// bonded forces see the (hi, lo) positions, not their FP32 rounding.
+template <bool ENERGY, bool MIXED>
 __global__ void __launch_bounds__(kTB) k_bonded(PhysDev d, int cur, int slot, int fold_src) {
     if (fold_src >= 0 && blockIdx.x == 0 && threadIdx.x == 0) fold(d, fold_src);
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double eb = 0.0, ea = 0.0, ed = 0.0, vir = 0.0;
     const float L = d.L, iL = d.invL;
     const float4* __restrict__ po = d.pos_orig[cur];
-    auto P = [&](int orig) { return po[orig]; };
+    const float4* __restrict__ pc = d.posc_orig[cur];
+    // minimum-image vector from particle a to particle b (orig ids)
+    auto V = [&](int a, int b, float& x, float& y, float& z) {
+        const float4 pa = po[a], pb = po[b];
+        x = mimg(pb.x - pa.x, L, iL);
+        y = mimg(pb.y - pa.y, L, iL);
+        z = mimg(pb.z - pa.z, L, iL);
+        if (MIXED) {
+            const float4 ca = pc[a], cb = pc[b];
+            x += cb.x - ca.x;
+            y += cb.y - ca.y;
+            z += cb.z - ca.z;
+        }
+    };
     if (t < d.n_bonds) {
         const int4 ix = d.bond_idx[t];
         const float2 par = d.bond_par[t];
-        const float4 a = P(ix.x), b = P(ix.y);
-        const float rx = mimg(b.x - a.x, L, iL), ry = mimg(b.y - a.y, L, iL), rz = mimg(b.z - a.z, L, iL);
+        float rx, ry, rz;
+        V(ix.x, ix.y, rx, ry, rz);
         const float rr = sqrtf(rx * rx + ry * ry + rz * rz);
         const float dr = rr - par.x;
         const float f = -par.y * dr / rr;   // F_j = f * r
@@ -357,9 +372,9 @@ __global__ void __launch_bounds__(kTB) k_bonded(PhysDev d, int cur, int slot, in
         const int a_ = t - d.n_bonds;
         const int4 ix = d.angle_idx[a_];
         const float2 par = d.angle_par[a_];
-        const float4 pi = P(ix.x), pj = P(ix.y), pk = P(ix.z);
-        const float ux = mimg(pi.x - pj.x, L, iL), uy = mimg(pi.y - pj.y, L, iL), uz = mimg(pi.z - pj.z, L, iL);
-        const float vx = mimg(pk.x - pj.x, L, iL), vy = mimg(pk.y - pj.y, L, iL), vz = mimg(pk.z - pj.z, L, iL);
+        float ux, uy, uz, vx, vy, vz;
+        V(ix.y, ix.x, ux, uy, uz);
+        V(ix.y, ix.z, vx, vy, vz);
         const float uu = ux * ux + uy * uy + uz * uz, vv = vx * vx + vy * vy + vz * vz;
         const float nu = sqrtf(uu), nv = sqrtf(vv);
         const float cx_ = uy * vz - uz * vy, cy_ = uz * vx - ux * vz, cz_ = ux * vy - uy * vx;
@@ -387,10 +402,10 @@ __global__ void __launch_bounds__(kTB) k_bonded(PhysDev d, int cur, int slot, in
         const int q = t - d.n_bonds - d.n_angles;
         const int4 ix = d.dih_idx[q];
         const float4 par = d.dih_par[q];
-        const float4 xi = P(ix.x), xj = P(ix.y), xk = P(ix.z), xl = P(ix.w);
-        const float b1x = mimg(xj.x - xi.x, L, iL), b1y = mimg(xj.y - xi.y, L, iL), b1z = mimg(xj.z - xi.z, L, iL);
-        const float b2x = mimg(xk.x - xj.x, L, iL), b2y = mimg(xk.y - xj.y, L, iL), b2z = mimg(xk.z - xj.z, L, iL);
-        const float b3x = mimg(xl.x - xk.x, L, iL), b3y = mimg(xl.y - xk.y, L, iL), b3z = mimg(xl.z - xk.z, L, iL);
+        float b1x, b1y, b1z, b2x, b2y, b2z, b3x, b3y, b3z;
+        V(ix.x, ix.y, b1x, b1y, b1z);
+        V(ix.y, ix.z, b2x, b2y, b2z);
+        V(ix.z, ix.w, b3x, b3y, b3z);
         const float m1x = b1y * b2z - b1z * b2y, m1y = b1z * b2x - b1x * b2z, m1z = b1x * b2y - b1y * b2x;
         const float m2x = b2y * b3z - b2z * b3y, m2y = b2z * b3x - b2x * b3z, m2z = b2x * b3y - b2y * b3x;
         const float m1m1 = m1x * m1x + m1y * m1y + m1z * m1z, m2m2 = m2x * m2x + m2y * m2y + m2z * m2z;
@@ -617,7 +632,10 @@ __global__ void __launch_bounds__(kTB) k_pair_integrate(PhysDev d, int cur, int 
                 if (y >= L) y -= L;
                 if (z >= L) z -= L;
                 d.pos[cur ^ 1][i] = make_float4(x, y, z, pi.w);
-                if (oi < (uint32_t)d.n_cp) d.pos_orig[cur ^ 1][oi] = make_float4(x, y, z, pi.w);
+                if (oi < (uint32_t)d.n_cp) {
+                    d.pos_orig[cur ^ 1][oi] = make_float4(x, y, z, pi.w);
+                    d.posc_orig[cur ^ 1][oi] = pc;
+                }
                 d.posc[i] = pc;
                 d.vel[i] = make_float4(vhx, vhy, vhz, im);
                 d.velc[i] = vc;
@@ -710,10 +728,15 @@ void launch_list_check(const PhysDev& d, cudaGraphConditionalHandle h, cudaStrea
 void launch_bonded(const PhysDev& d, int cur, bool energy, int slot, int fold_src, cudaStream_t s) {
     const int nterms = d.n_bonds + d.n_angles + d.n_dih;
     const int nb = std::max(1, (nterms + kTB - 1) / kTB);
-    if (energy)
-        k_bonded<true><<<nb, kTB, 0, s>>>(d, cur, slot, fold_src);
+    const bool mixed = d.precision == LIMA_PRECISION_MIXED;
+    if (energy && mixed)
+        k_bonded<true, true><<<nb, kTB, 0, s>>>(d, cur, slot, fold_src);
+    else if (energy)
+        k_bonded<true, false><<<nb, kTB, 0, s>>>(d, cur, slot, fold_src);
+    else if (mixed)
+        k_bonded<false, true><<<nb, kTB, 0, s>>>(d, cur, slot, fold_src);
     else
-        k_bonded<false><<<nb, kTB, 0, s>>>(d, cur, slot, fold_src);
+        k_bonded<false, false><<<nb, kTB, 0, s>>>(d, cur, slot, fold_src);
 }
 
 void launch_pair(const PhysDev& d, int cur, bool mixed, bool energy, bool integrate, int slot, cudaStream_t s) {

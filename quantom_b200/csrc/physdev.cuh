@@ -56,6 +56,7 @@ struct PhysDev {
     float4* xref;
     float4* force;
     float4* pos_orig[2];        // [n_cp] compound-particle positions in orig order (the bonded kernel's input)
+    float4* posc_orig[2];       // [n_cp] their low parts (mixed precision)
     uint32_t* orig_of_sorted;   // [n]
     uint32_t* sorted_of_orig;   // [n]
     float2* lj_table;           // [n_types^2] (sigma^2, 4 eps), Lorentz-Berthelot

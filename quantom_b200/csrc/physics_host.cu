@@ -202,6 +202,7 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
         d.xref = dalloc<float4>(allocs, d.n_pad);
         d.force = dalloc<float4>(allocs, d.n_pad);
         for (int b = 0; b < 2; b++) d.pos_orig[b] = dalloc<float4>(allocs, std::max(1, d.n_cp));
+        for (int b = 0; b < 2; b++) d.posc_orig[b] = dalloc<float4>(allocs, std::max(1, d.n_cp));
         d.orig_of_sorted = dalloc<uint32_t>(allocs, d.n_pad);
         d.sorted_of_orig = dalloc<uint32_t>(allocs, d.n);
         d.lj_table = dalloc<float2>(allocs, tab.size());
@@ -306,6 +307,7 @@ void phys_upload_state(const PhysHost& h, PhysDev& d, int cur, cudaStream_t s) {
     for (int i = 0; i < d.n_pad; i++) ident[i] = i < d.n ? i : 0xffffffffu;
     cudaMemcpyAsync(d.pos[cur], pos.data(), sizeof(float4) * d.n_pad, cudaMemcpyHostToDevice, s);
     if (d.n_cp) cudaMemcpyAsync(d.pos_orig[cur], pos.data(), sizeof(float4) * d.n_cp, cudaMemcpyHostToDevice, s);
+    if (d.n_cp) cudaMemcpyAsync(d.posc_orig[cur], zero.data(), sizeof(float4) * d.n_cp, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(d.vel, vel.data(), sizeof(float4) * d.n_pad, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(d.posc, zero.data(), sizeof(float4) * d.n_pad, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(d.velc, zero.data(), sizeof(float4) * d.n_pad, cudaMemcpyHostToDevice, s);

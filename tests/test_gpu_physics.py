@@ -8,6 +8,8 @@ compensated sums and FP64 reductions (mixed).  Stated errors: forces within
 at ~1e-6 nm), energies within 1e-5 relative, trajectories within 1e-5 nm
 over 20 steps.
 """
+import functools
+
 import numpy as np
 import pytest
 
@@ -38,13 +40,21 @@ def _positions(E, eng, s):
     return np.concatenate(parts + [sol["pos"]]) if parts else sol["pos"]
 
 
-@pytest.mark.parametrize("name", ["tiny_chains", "small_bridged", "lj_solvent_4096", "solvated_chains_32k"])
+@functools.lru_cache(maxsize=2)
+def _system_and_fp64_forces(name, seed):
+    s = S.make_system(name, seed=seed)
+    F64, en64 = po.PhysSystem(s, rc=s.spec.cutoff, r_on=1.0).forces()
+    return s, F64, en64
+
+
+# solvated_chains_258k: 64 chains of 128 particles (two compounds and a bridge
+# each) in 250,000 solvents, beyond the reference's 65,535-solvent layout
 @pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("name", ["tiny_chains", "small_bridged", "lj_solvent_4096", "solvated_chains_32k",
+                                  "solvated_chains_258k"])
 def test_forces_and_energies_match_fp64(gpu, name, precision):
     E = gpu
-    s = S.make_system(name, seed=7)
-    ps = po.PhysSystem(s, rc=s.spec.cutoff, r_on=1.0)
-    F64, en64 = ps.forces()
+    s, F64, en64 = _system_and_fp64_forces(name, 7)
     with E.Engine(s, _params(E, s, precision=precision)) as eng:
         tot = eng.compute_energies()
         fc, fs = eng.forces()
