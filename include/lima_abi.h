@@ -316,6 +316,84 @@ lima_status lima_grad(lima_ctx* ctx, const lima_loss_spec* spec, double* loss, d
 lima_status lima_rdf(lima_ctx* ctx, int n_bins, float r_max, double* h);
 
 /* ------------------------------------------------------------------ */
+/* Frame log (physics semantics).  Replaces the reference's logging      */
+/* buffers written by the force kernels every step (Box::potE_buffer,   */
+/* traj_buffer, outdata, data_GAN: Engine.cu:1007-1047, 1136-1145),      */
+/* their host offload every 40 / 100 steps (Engine::hostMaster,          */
+/* offloadLoggingData, offloadTrainData: Engine.cu:44-75, 290-310), the  */
+/* post-run Analyzer::analyzeEnergy (Analyzer.cu:33-207) and the output  */
+/* files of Environment::postRunEvents (Environment.cpp:124-166).        */
+/* ------------------------------------------------------------------ */
+#define LIMA_LOG_TRAJ 1     /* positions of every particle slot (traj_buffer) */
+#define LIMA_LOG_POTE 2     /* potential energy of every particle slot (potE_buffer): its LJ pair halves
+                               plus 1/2, 1/3, 1/4 of each bond, angle, dihedral it takes part in */
+#define LIMA_LOG_TRAIN 4    /* compound particles: position, LJ force from solvents, 0 (data_GAN,
+                               N_DATAGAN_VALUES = 3 float3; padding particles at (-1, -1, -1)) */
+#define LIMA_LOG_DATA_FLOATS 10   /* outdata floats per frame (Engine.cu:1022-1029) */
+
+typedef struct {
+    int every;          /* record the state of every `every`-th step (step % every == 0), >= 1;
+                           the reference records every step */
+    int ring_frames;    /* frames held in device memory between copies to the host, 1..65536 */
+    int flags;          /* LIMA_LOG_* (the FP64 energies and the outdata line are always recorded) */
+} lima_log_params;
+
+/* Starts recording (clears what an earlier start recorded).  A recorded step
+   runs the step's energy variant.  Frame f of step s holds the positions the
+   step's forces were evaluated at, that evaluation's energies, and the
+   velocity of the half step taken.  Layout per frame: traj[n_slots][3] float,
+   potE[n_slots] double, n_slots = n_compounds*64 + n_solvents (compound c
+   particle l at c*64 + l, solvent s at n_compounds*64 + s; empty compound
+   slots are zero); train[n_compounds*64][3][3] float; energies[LIMA_E_COUNT]
+   double; logdata[10] float (particle slot 0: speed, kinetic energy,
+   potential energy, |force|, then zeros). */
+lima_status lima_log_start(lima_ctx* ctx, const lima_log_params* params);
+/* Stops recording; what was recorded stays readable. */
+lima_status lima_log_stop(lima_ctx* ctx);
+/* Frames recorded so far (waits for the engine's stream). */
+lima_status lima_log_count(lima_ctx* ctx, uint64_t* n_frames);
+/* Frames [first, first+count) into caller arrays (any may be NULL; traj,
+   potE and train need the matching flag). */
+lima_status lima_log_read(lima_ctx* ctx, uint64_t first, uint64_t count, uint64_t* steps, double* energies,
+                          float* traj, double* potE, float* train, float* logdata);
+/* The recorded frames as the reference's output files in directory `dir`
+   (which must exist): logdata.bin (10 float per frame), energy.bin (float3
+   per frame: potential, kinetic and total energy per particle, J/mol),
+   temperature.bin (float per frame, K), sim_traindata.bin (with
+   LIMA_LOG_TRAIN: 3 float3 per compound particle slot per frame); with
+   LIMA_LOG_TRAJ / LIMA_LOG_POTE also traj.bin (float3 per slot per frame)
+   and potE.bin (double per slot per frame), the in-memory
+   Simulation::traj_buffer / potE_buffer of the reference. */
+lima_status lima_log_write(lima_ctx* ctx, const char* dir);
+
+/* ------------------------------------------------------------------ */
+/* Headless rasterizer.  Replaces Rasterizer::render (Rasterizer.cu:     */
+/* 12-294) and the picture DisplayV2::drawBalls draws from its output    */
+/* (DisplayV2.cpp:13-51); there is no window or OpenGL context.          */
+/* ------------------------------------------------------------------ */
+typedef struct {
+    lima_float3 pos;      /* normalised: (x / box_len - 0.5) * 1.8 per axis; drawn at (pos.x, pos.z) */
+    float radius;         /* 0.25 * r_type / (1 + 0.001 * y_nm) */
+    int32_t color[3];     /* RGB 0..255 of the atom type */
+    uint8_t disable;      /* 1 for an empty compound slot */
+    uint8_t pad[3];
+} lima_render_ball;       /* RenderBall (QuantomTypes.cuh:362-369), 32 bytes */
+
+/* One ball per particle slot (n_compounds*64 + n_solvents, compound c
+   particle l at c*64 + l, solvents after) of the current state, sorted by
+   pos.y ascending (ties in slot order).  Atom types: compound particles from
+   atom_color_types (0 SOL, 1 C, 2 O, 3 N, 4 H, 5 P, 6 SOL, else NONE),
+   solvents SOL, empty slots NONE at the box origin, disabled. */
+lima_status lima_render(lima_ctx* ctx, lima_render_ball* balls);
+/* The same balls drawn as the reference's display draws them, into a
+   width x height RGB image (row 0 at the top, device coordinates [-1, 1]
+   on both axes, black background): every pixel whose centre lies in a ball's
+   disc takes the colour of the front-most such ball (lowest pos.y), scaled by
+   the Gouraud light of the display's triangle fan, 0.5 + 0.5 * dy / radius
+   (floor per channel).  width, height 1..16384. */
+lima_status lima_render_image(lima_ctx* ctx, int width, int height, uint8_t* rgb);
+
+/* ------------------------------------------------------------------ */
 /* No counterpart in the reference.  The reference updates its lists on  */
 /* the host (Engine::updateNeighborLists, Engine.cu:208-287); this is a  */
 /* context-free, allocation-free form of the device build behind          */

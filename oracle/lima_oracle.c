@@ -844,3 +844,111 @@ long orc_sizeof(int which) {
         default: return -1;
     }
 }
+
+/* ======================================================================= */
+/* C. Headless rasterizer: restatement of Rasterizer.cu:150-251 (types,    */
+/*    colours, radii, normalisation), the depth sort (Rasterizer.cu:254-  */
+/*    293, here stable: equal depths keep slot order) and the display's    */
+/*    back-to-front triangle-fan discs (DisplayV2.cpp:13-51) as an image.  */
+/* ======================================================================= */
+
+enum { RAS_NONE = 0, RAS_O = 1, RAS_C = 2, RAS_P = 3, RAS_N = 4, RAS_H = 5, RAS_SOL = 6 };
+
+static void ras_color(int t, int* c) {                                  /* Rasterizer.cu:168-189 */
+    static const int tab[7][3] = {{0xF2, 0xE5, 0xD9}, {0xE0, 0x20, 0x20}, {0x30, 0x10, 0x90}, {0xFC, 0xF7, 0x5E},
+                                  {0x2E, 0x8B, 0x57}, {0xF1, 0xF1, 0xF1}, {0x03, 0xa9, 0xf4}};
+    for (int q = 0; q < 3; q++) c[q] = (t >= 0 && t < 7) ? tab[t][q] : 0;
+}
+
+static float ras_radius(int t) {                                        /* Rasterizer.cu:191-213 */
+    switch (t) {
+        case RAS_H: return 0.04f;
+        case RAS_C: return 0.1f;
+        case RAS_N: return 0.1f;
+        case RAS_O: return 0.12f;
+        case RAS_SOL: return 0.08f;
+        case RAS_P: return 0.15f;
+        default: return 1.f;
+    }
+}
+
+/* balls of n slots (positions n*3, kind = ATOM_TYPE per slot) sorted by pos.y */
+int orc_render_balls(int n, const float* pos, const unsigned char* kind, float L, lima_render_ball* out) {
+    lima_render_ball* tmp = (lima_render_ball*)malloc(sizeof(lima_render_ball) * (size_t)(n > 0 ? n : 1));
+    lima_render_ball* src = (lima_render_ball*)malloc(sizeof(lima_render_ball) * (size_t)(n > 0 ? n : 1));
+    if (!tmp || !src) return -1;
+    for (int i = 0; i < n; i++) {
+        const int t = kind[i];
+        const float x = t == RAS_NONE ? 0.f : pos[3 * i], y = t == RAS_NONE ? 0.f : pos[3 * i + 1],
+                    z = t == RAS_NONE ? 0.f : pos[3 * i + 2];
+        lima_render_ball b;
+        memset(&b, 0, sizeof b);
+        int c[3];
+        ras_color(t, c);
+        const float rad = ras_radius(t) / (1.f + y * 0.001f);
+        b.radius = 0.25f * rad;
+        const double dl = (double)L;
+        b.pos.x = (float)(((double)x / dl - 0.5) * 1.8);
+        b.pos.y = (float)(((double)y / dl - 0.5) * 1.8);
+        b.pos.z = (float)(((double)z / dl - 0.5) * 1.8);
+        for (int q = 0; q < 3; q++) b.color[q] = c[q];
+        b.disable = t == RAS_NONE;
+        src[i] = b;
+    }
+    /* stable bottom-up merge sort by pos.y */
+    for (int w = 1; w < n; w *= 2) {
+        for (int lo = 0; lo < n; lo += 2 * w) {
+            int mid = lo + w < n ? lo + w : n, hi = lo + 2 * w < n ? lo + 2 * w : n;
+            int a = lo, b = mid, k = lo;
+            while (a < mid && b < hi) tmp[k++] = (src[b].pos.y < src[a].pos.y) ? src[b++] : src[a++];
+            while (a < mid) tmp[k++] = src[a++];
+            while (b < hi) tmp[k++] = src[b++];
+        }
+        lima_render_ball* sw = src;
+        src = tmp;
+        tmp = sw;
+    }
+    memcpy(out, src, sizeof(lima_render_ball) * (size_t)n);
+    free(tmp);
+    free(src);
+    return 0;
+}
+
+static float ras_ndc_x(int px, int w) { return (float)(2 * px + 1) / (float)w + -1.f; }
+static float ras_ndc_y(int py, int h) { return 1.f + -((float)(2 * py + 1) / (float)h); }
+
+/* the sorted balls drawn back to front as shaded discs into w*h RGB */
+int orc_render_image(const lima_render_ball* balls, int n, int w, int h, unsigned char* rgb) {
+    int* win = (int*)malloc(sizeof(int) * (size_t)w * h);
+    if (!win) return -1;
+    for (size_t p = 0; p < (size_t)w * h; p++) win[p] = -1;
+    for (int k = n - 1; k >= 0; k--) {
+        const lima_render_ball b = balls[k];
+        if (b.disable) continue;
+        const float hw = 0.5f * (float)w, hh = 0.5f * (float)h;
+        int x0 = (int)floorf((b.pos.x - b.radius + 1.f) * hw) - 1, x1 = (int)ceilf((b.pos.x + b.radius + 1.f) * hw) + 1;
+        int y0 = (int)floorf((1.f - b.pos.z - b.radius) * hh) - 1, y1 = (int)ceilf((1.f - b.pos.z + b.radius) * hh) + 1;
+        if (x0 < 0) x0 = 0;
+        if (y0 < 0) y0 = 0;
+        if (x1 > w - 1) x1 = w - 1;
+        if (y1 > h - 1) y1 = h - 1;
+        for (int py = y0; py <= y1; py++)
+            for (int px = x0; px <= x1; px++) {
+                const float dx = ras_ndc_x(px, w) + -b.pos.x, dy = ras_ndc_y(py, h) + -b.pos.z;
+                if (dx * dx + dy * dy <= b.radius * b.radius) win[(size_t)py * w + px] = k;
+            }
+    }
+    for (size_t p = 0; p < (size_t)w * h; p++) {
+        unsigned char* o = rgb + 3 * p;
+        if (win[p] < 0) {
+            o[0] = o[1] = o[2] = 0;
+            continue;
+        }
+        const lima_render_ball b = balls[win[p]];
+        const float dy = ras_ndc_y((int)(p / (size_t)w), h) + -b.pos.z;
+        const float light = 0.5f + 0.5f * (dy / b.radius);
+        for (int q = 0; q < 3; q++) o[q] = (unsigned char)(int)floorf((float)b.color[q] * light);
+    }
+    free(win);
+    return 0;
+}

@@ -362,6 +362,34 @@ class PhysSystem:
         d -= self.box * np.round(d / self.box)
         return d / dt
 
+    def solvent_lj_on_compounds(self, x=None):
+        """FP64 LJ force (same switched Lorentz-Berthelot form as orc_phys_forces)
+        on every compound particle from the solvents alone: the reference's
+        force_LJ_sol of a compound particle (Engine.cu:1034).  numpy, O(n_cp * n_s)."""
+        x = np.asarray(self.x if x is None else x, np.float64)
+        ncp = self.n_compound_particles
+        F = np.zeros((ncp, 3))
+        xs, sig_s, eps_s = x[ncp:], self.sigma[ncp:], self.epsilon[ncp:]
+        rc2, ron2 = self.rc ** 2, self.r_on ** 2
+        for i in range(ncp):
+            r = xs - x[i]
+            r -= self.box * np.round(r / self.box)
+            r2 = (r * r).sum(1)
+            m = r2 < rc2
+            r, r2 = r[m], r2[m]
+            sig = 0.5 * (self.sigma[i] + sig_s[m])
+            eps = np.sqrt(self.epsilon[i] * eps_s[m])
+            sr6 = (sig * sig / r2) ** 3
+            v = 4 * eps * (sr6 * sr6 - sr6)
+            dvdr_r = -24 * eps * (2 * sr6 * sr6 - sr6) / r2
+            if self.r_on < self.rc:
+                t = np.where(r2 > ron2, (rc2 - r2) / (rc2 - ron2), 1.0)
+                sw = t ** 3 * (10 + t * (-15 + 6 * t))
+                dsw_r = np.where(r2 > ron2, -60 * t * t * (1 - t) ** 2 / (rc2 - ron2), 0.0)
+                dvdr_r = dvdr_r * sw + v * dsw_r
+            F[i] = (dvdr_r[:, None] * r).sum(0)   # force on i = -dV/dr * (x_i - x_j)/r = dvdr_r * (x_j - x_i)
+        return F
+
     def forces(self, x=None):
         x = np.ascontiguousarray(self.x if x is None else x, np.float64)
         F = np.zeros_like(x)
@@ -418,3 +446,48 @@ class PhysSystem:
         oracle_lib().orc_phys_run(ctypes.byref(st), _p(np.ascontiguousarray(self.mass)), dt, n_steps, thermostat,
                                   t0, tau, _p(x), _p(v), _p(F), ctypes.byref(tp), _p(en))
         return x, v, F, en
+
+
+# ------------------------------------------------------------ rasterizer ---
+def render_slots(system, comp_positions, sol_positions):
+    """(positions n_slots*3 float32, ATOM_TYPE per slot) of a state in the
+    reference's slot layout: compound c particle l at c*64 + l (empty slots
+    NONE), solvents SOL after them."""
+    from quantom_b200 import layout as L
+    nc, ns = system.n_compounds, system.n_solvents
+    pos = np.zeros((nc * 64 + ns, 3), np.float32)
+    kind = np.zeros(nc * 64 + ns, np.uint8)
+    for c in range(nc):
+        k = int(system.compounds[c]["n_particles"])
+        pos[c * 64: c * 64 + k] = comp_positions[c][:k]
+        for l in range(k):
+            t = int(system.compounds[c]["atom_color_types"][l])
+            kind[c * 64 + l] = L.RENDER_TYPE_OF_COLOR[t] if t < 7 else 0
+    pos[nc * 64:] = sol_positions
+    kind[nc * 64:] = 6
+    return pos, kind
+
+
+def render_balls(pos, kind, box_len):
+    """Oracle RenderBall list (lima_oracle.c part C), sorted by depth."""
+    from quantom_b200 import layout as L
+    lib = oracle_lib()
+    n = len(kind)
+    pos = np.ascontiguousarray(pos, np.float32)
+    kind = np.ascontiguousarray(kind, np.uint8)
+    out = np.zeros(n, L.RenderBall)
+    lib.orc_render_balls.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p]
+    if lib.orc_render_balls(n, _p(pos), _p(kind), float(box_len), _p(out)) != 0:
+        raise MemoryError("orc_render_balls")
+    return out
+
+
+def render_image(balls, width, height):
+    """Oracle image of sorted balls (lima_oracle.c part C), (h, w, 3) uint8."""
+    lib = oracle_lib()
+    balls = np.ascontiguousarray(balls)
+    img = np.zeros((height, width, 3), np.uint8)
+    lib.orc_render_image.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+    if lib.orc_render_image(_p(balls), len(balls), int(width), int(height), _p(img)) != 0:
+        raise MemoryError("orc_render_image")
+    return img

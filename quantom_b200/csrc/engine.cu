@@ -23,6 +23,8 @@
 #include <vector>
 
 #include "adjoint.cuh"
+#include "framelog.cuh"
+#include "render.cuh"
 #include "lima_abi.h"
 #include "physdev.cuh"
 #include "refdev.cuh"
@@ -76,6 +78,8 @@ struct lima_ctx {
     float ref_temperature = 0.f;
     uint64_t launches = 0;     // kernels of this library launched by this context
     int graph_kernels = 0;     // kernels in one replay of a step graph
+    lima::FrameLog log;        // physics: frames recorded every log.every steps
+    lima::RenderBuf render;    // headless rasterizer buffers (allocated by the first lima_render)
 
     template <typename T>
     T* dalloc(size_t n) {
@@ -85,6 +89,7 @@ struct lima_ctx {
         return static_cast<T*>(ptr);
     }
     ~lima_ctx() {
+        lima::framelog_free(log);
         for (auto& g : graph)
             if (g) cudaGraphExecDestroy(g);
         for (auto& row : dgraph)
@@ -401,7 +406,8 @@ void one_step(lima_ctx* c, cudaEvent_t* prof) {
             }
         }
     } else if (c->phys.dynamic_list) {
-        const bool energy = c->p.energy_period > 0 && (c->step % c->p.energy_period) == 0;
+        const bool logged = c->log.on && (c->step % static_cast<uint64_t>(c->log.every)) == 0;
+        const bool energy = logged || (c->p.energy_period > 0 && (c->step % c->p.energy_period) == 0);
         if (!prof) {
             cuda_ok(cudaGraphLaunch(c->dgraph[c->cur][energy ? 1 : 0], c->stream), "cudaGraphLaunch");
             c->launches += c->dgraph_kernels[energy ? 1 : 0];
@@ -415,6 +421,7 @@ void one_step(lima_ctx* c, cudaEvent_t* prof) {
             c->launches += lima::phys_step_kernels(c->phys, c->cur, c->stream, energy, prof + 2);
             cuda_ok(cudaEventRecord(prof[5], c->stream), "cudaEventRecord");
         }
+        if (logged) c->launches += lima::framelog_record(c->log, c->phys, c->cur, c->step, c->stream);
         c->cur ^= 1;
         c->step++;
     } else {
@@ -425,7 +432,8 @@ void one_step(lima_ctx* c, cudaEvent_t* prof) {
             c->last_nlist_step = c->step;
         }
         if (prof) cuda_ok(cudaEventRecord(prof[1], c->stream), "cudaEventRecord");
-        const bool energy = c->p.energy_period > 0 && (c->step % c->p.energy_period) == 0;
+        const bool logged = c->log.on && (c->step % static_cast<uint64_t>(c->log.every)) == 0;
+        const bool energy = logged || (c->p.energy_period > 0 && (c->step % c->p.energy_period) == 0);
         if (energy || !c->graph[c->cur] || prof) {
             c->launches += lima::phys_step_kernels(c->phys, c->cur, c->stream, energy, prof ? prof + 2 : nullptr);
             if (prof) cuda_ok(cudaEventRecord(prof[5], c->stream), "cudaEventRecord");
@@ -433,6 +441,7 @@ void one_step(lima_ctx* c, cudaEvent_t* prof) {
             cuda_ok(cudaGraphLaunch(c->graph[c->cur], c->stream), "cudaGraphLaunch");
             c->launches += c->graph_kernels;
         }
+        if (logged) c->launches += lima::framelog_record(c->log, c->phys, c->cur, c->step, c->stream);
         c->cur ^= 1;
         c->step++;
     }
@@ -821,6 +830,12 @@ lima_status lima_compute_energies(lima_ctx* c) {
         need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
         need(c->p.semantics == LIMA_SEMANTICS_PHYSICS, LIMA_ERR_UNSUPPORTED,
              "the reference computes no LJ energy; reference semantics report potE of the last step");
+        // fold the last step's accumulators first, so the readback that follows
+        // reports this evaluation's kinetic energy, not the previous step's
+        if (c->step > 0) {
+            lima::phys_finalize(c->phys, c->cur, c->stream);
+            c->launches++;
+        }
         if (c->phys.dynamic_list && lima::phys_rebuild_pending(c->phys, c->stream)) {
             lima::phys_rebuild(c->phys, c->cur, c->stream);
             c->launches += lima::kRebuildKernels;
@@ -961,6 +976,182 @@ lima_status lima_rdf(lima_ctx* c, int n_bins, float r_max, double* h) {
         std::string msg;
         const int st = lima::adj_rdf(c->phys, c->cur, c->adj, c->dallocs, n_bins, r_max, h, c->stream, msg);
         if (st != LIMA_OK) fail(static_cast<lima_status>(st), msg);
+    });
+}
+
+// ------------------------------------------------------------ frame log ---
+lima_status lima_log_start(lima_ctx* c, const lima_log_params* p) {
+    return guarded(c, [&] {
+        need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
+        need(c->p.semantics == LIMA_SEMANTICS_PHYSICS, LIMA_ERR_UNSUPPORTED,
+             "the frame log records the physics semantics (the reference path is the parity path)");
+        need(p != nullptr, LIMA_ERR_ARGUMENT, "null log params");
+        need(p->every >= 1, LIMA_ERR_ARGUMENT, "log every must be >= 1");
+        need(p->ring_frames >= 1 && p->ring_frames <= 65536, LIMA_ERR_ARGUMENT, "ring_frames outside 1..65536");
+        need((p->flags & ~(LIMA_LOG_TRAJ | LIMA_LOG_POTE | LIMA_LOG_TRAIN)) == 0, LIMA_ERR_ARGUMENT,
+             "unknown log flags");
+        sync_checked(c);
+        std::vector<int> np;
+        for (const auto& cp : c->comps) np.push_back(cp.n_particles);
+        std::string msg;
+        int st = LIMA_OK;
+        lima::framelog_start(c->log, c->phys, np, *p, msg, st);
+        if (st != LIMA_OK) fail(static_cast<lima_status>(st), msg);
+        sync_checked(c);
+    });
+}
+
+lima_status lima_log_stop(lima_ctx* c) {
+    return guarded(c, [&] {
+        if (!c->log.on) return;
+        lima::framelog_flush(c->log, c->stream);
+        c->log.on = false;
+        sync_checked(c);
+    });
+}
+
+lima_status lima_log_count(lima_ctx* c, uint64_t* n) {
+    return guarded(c, [&] {
+        need(n != nullptr, LIMA_ERR_ARGUMENT, "null count");
+        if (c->log.dev.ring) lima::framelog_flush(c->log, c->stream);
+        sync_checked(c);
+        *n = c->log.steps.size();
+    });
+}
+
+lima_status lima_log_read(lima_ctx* c, uint64_t first, uint64_t count, uint64_t* steps, double* energies, float* traj,
+                          double* potE, float* train, float* logdata) {
+    return guarded(c, [&] {
+        if (c->log.dev.ring) lima::framelog_flush(c->log, c->stream);
+        sync_checked(c);
+        const lima::FrameLog& g = c->log;
+        const uint64_t nf = g.steps.size();
+        need(first <= nf && count <= nf - first, LIMA_ERR_ARGUMENT, "frames outside what was recorded");
+        need(!traj || g.dev.traj, LIMA_ERR_ARGUMENT, "positions were not recorded (LIMA_LOG_TRAJ)");
+        need(!potE || g.dev.potE, LIMA_ERR_ARGUMENT, "potential energies were not recorded (LIMA_LOG_POTE)");
+        need(!train || g.dev.train, LIMA_ERR_ARGUMENT, "train data were not recorded (LIMA_LOG_TRAIN)");
+        const size_t ns = (size_t)g.dev.n_slots, nt = (size_t)g.dev.n_train * lima::kTrainValues * 3;
+        if (steps) std::copy(g.steps.begin() + first, g.steps.begin() + first + count, steps);
+        if (energies)
+            std::copy(g.energies.begin() + first * LIMA_E_COUNT, g.energies.begin() + (first + count) * LIMA_E_COUNT,
+                      energies);
+        if (traj) std::copy(g.traj.begin() + first * ns * 3, g.traj.begin() + (first + count) * ns * 3, traj);
+        if (potE) std::copy(g.potE.begin() + first * ns, g.potE.begin() + (first + count) * ns, potE);
+        if (train) std::copy(g.train.begin() + first * nt, g.train.begin() + (first + count) * nt, train);
+        if (logdata)
+            std::copy(g.logdata.begin() + first * lima::kLogDataFloats,
+                      g.logdata.begin() + (first + count) * lima::kLogDataFloats, logdata);
+    });
+}
+
+lima_status lima_log_write(lima_ctx* c, const char* dir) {
+    return guarded(c, [&] {
+        need(dir != nullptr, LIMA_ERR_ARGUMENT, "null directory");
+        if (c->log.dev.ring) lima::framelog_flush(c->log, c->stream);
+        sync_checked(c);
+        const lima::FrameLog& g = c->log;
+        const size_t nf = g.steps.size();
+        need(nf > 0, LIMA_ERR_STATE, "no frames recorded");
+        auto dump = [&](const char* name, const void* data, size_t bytes) {
+            const std::string path = std::string(dir) + "/" + name;
+            FILE* f = std::fopen(path.c_str(), "wb");
+            need(f != nullptr, LIMA_ERR_ARGUMENT, "cannot open " + path);
+            const size_t w = bytes ? std::fwrite(data, 1, bytes, f) : 0;
+            std::fclose(f);
+            need(w == bytes, LIMA_ERR_ARGUMENT, "short write to " + path);
+        };
+        // Environment.cpp:130: logging_data, 10 floats per step
+        dump("logdata.bin", g.logdata.data(), g.logdata.size() * sizeof(float));
+        // Analyzer::analyzeEnergy (Analyzer.cu:177-183): per step the mean per particle of
+        // (potential, kinetic, total) energy as a Float3; here from the step's FP64 sums
+        const double n = static_cast<double>(c->phys.n);
+        std::vector<float> energy(nf * 3), temperature(nf);
+        for (size_t f = 0; f < nf; f++) {
+            const double* e = &g.energies[f * LIMA_E_COUNT];
+            const double pot = e[LIMA_E_LJ] + e[LIMA_E_BOND] + e[LIMA_E_ANGLE] + e[LIMA_E_DIHEDRAL];
+            energy[3 * f + 0] = static_cast<float>(pot / n);
+            energy[3 * f + 1] = static_cast<float>(e[LIMA_E_KINETIC] / n);
+            energy[3 * f + 2] = static_cast<float>(e[LIMA_E_TOTAL] / n);
+            temperature[f] = static_cast<float>(e[LIMA_E_TEMPERATURE]);
+        }
+        dump("energy.bin", energy.data(), energy.size() * sizeof(float));
+        dump("temperature.bin", temperature.data(), temperature.size() * sizeof(float));
+        // Environment.cpp:137-141: data_GAN of every step
+        if (g.dev.train) dump("sim_traindata.bin", g.train.data(), g.train.size() * sizeof(float));
+        if (g.dev.traj) dump("traj.bin", g.traj.data(), g.traj.size() * sizeof(float));
+        if (g.dev.potE) dump("potE.bin", g.potE.data(), g.potE.size() * sizeof(double));
+    });
+}
+
+// ----------------------------------------------------------- rasterizer ---
+namespace {
+// balls of the current state into c->render.balls[1] (device), sorted by depth
+void render_now(lima_ctx* c) {
+    lima::RenderBuf& r = c->render;
+    const int nc = static_cast<int>(c->comps.size()), ns = static_cast<int>(c->sols.size());
+    const int n_slots = nc * lima::kMaxCP + ns;
+    if (!r.ready) {
+        // ATOM_TYPE per slot: compound particles by atom_color_types (RAS_getTypeFromIndex,
+        // Rasterizer.cu:126-146), solvents SOL, empty slots NONE (QuantomTypes.cuh:16)
+        static const uint8_t by_color[7] = {6, 2, 1, 4, 5, 3, 6};
+        std::vector<uint8_t> kind(n_slots, 0);
+        for (int cc = 0; cc < nc; cc++)
+            for (int l = 0; l < c->comps[cc].n_particles; l++) {
+                const int t = c->comps[cc].atom_color_types[l];
+                kind[cc * lima::kMaxCP + l] = t < 7 ? by_color[t] : 0;
+            }
+        for (int s = 0; s < ns; s++) kind[nc * lima::kMaxCP + s] = 6;
+        std::vector<uint32_t> ref_slot;
+        if (c->p.semantics == LIMA_SEMANTICS_PHYSICS) {
+            for (int cc = 0; cc < nc; cc++)
+                for (int l = 0; l < c->comps[cc].n_particles; l++) ref_slot.push_back(cc * lima::kMaxCP + l);
+            for (int s = 0; s < ns; s++) ref_slot.push_back(nc * lima::kMaxCP + s);
+        }
+        need(lima::render_setup(r, n_slots, kind, ref_slot, c->dallocs, c->stream), LIMA_ERR_CUDA,
+             "rasterizer: out of device memory");
+    }
+    if (c->p.semantics == LIMA_SEMANTICS_PHYSICS) {
+        lima::render_slot_positions_phys(r, c->phys, c->cur, c->stream);
+        c->launches++;
+    } else {
+        if (nc)
+            cuda_ok(cudaMemcpyAsync(r.slot_pos, c->ref.cpos[c->cur], sizeof(float4) * nc * lima::kMaxCP,
+                                    cudaMemcpyDeviceToDevice, c->stream),
+                    "cudaMemcpyAsync");
+        if (ns)
+            cuda_ok(cudaMemcpyAsync(r.slot_pos + nc * lima::kMaxCP, c->ref.spos[c->cur], sizeof(float4) * ns,
+                                    cudaMemcpyDeviceToDevice, c->stream),
+                    "cudaMemcpyAsync");
+    }
+    c->launches += lima::render_balls(r, c->p.box_len, c->stream);
+}
+}  // namespace
+
+lima_status lima_render(lima_ctx* c, lima_render_ball* balls) {
+    return guarded(c, [&] {
+        need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
+        need(balls != nullptr, LIMA_ERR_ARGUMENT, "null ball array");
+        sync_checked(c);
+        render_now(c);
+        cuda_ok(cudaMemcpyAsync(balls, c->render.balls[1], sizeof(lima_render_ball) * c->render.n_slots,
+                                cudaMemcpyDeviceToHost, c->stream),
+                "cudaMemcpyAsync");
+        sync_checked(c);
+    });
+}
+
+lima_status lima_render_image(lima_ctx* c, int width, int height, uint8_t* rgb) {
+    return guarded(c, [&] {
+        need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
+        need(rgb != nullptr, LIMA_ERR_ARGUMENT, "null image");
+        need(width >= 1 && width <= 16384 && height >= 1 && height <= 16384, LIMA_ERR_ARGUMENT,
+             "image size outside 1..16384");
+        sync_checked(c);
+        render_now(c);
+        need(lima::render_image(c->render, width, height, rgb, c->dallocs, c->stream), LIMA_ERR_CUDA,
+             "rasterizer: out of device memory for the image");
+        c->launches += 2;
+        sync_checked(c);
     });
 }
 

@@ -1,0 +1,315 @@
+// Frame log of the physics path (framelog.cuh).
+//
+//   k_log_frame  one thread per particle: position (traj_buffer) and
+//                potential energy (potE_buffer) into the reference slot of
+//                the particle; compound particles also their position into
+//                the train record (data_GAN value 0); thread 0 the frame's
+//                FP64 energies from the step's accumulator slot and the
+//                reference's 10-float log line of particle 0 (outdata)
+//   k_log_train  8 lanes per compound particle over its Verlet list: the LJ
+//                force from solvent neighbours only (data_GAN value 1,
+//                Engine.cu:1034 force_LJ_sol), reduced with warp shuffles
+#include <algorithm>
+#include <cstring>
+#include <type_traits>
+
+#include "framelog.cuh"
+#include "physkern.cuh"
+#include "physmath.cuh"
+
+namespace lima {
+namespace {
+
+constexpr double kRgas = 8.314462618;   // J/(mol K)
+
+__global__ void __launch_bounds__(kTB) k_log_frame(PhysDev d, FrameLogDev g, int cur, int r) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k == 0 && g.energies) {
+        const double* a = d.acc + cur * LIMA_E_COUNT;
+        double* e = g.energies + (size_t)r * LIMA_E_COUNT;
+        const double pot = a[LIMA_E_LJ] + a[LIMA_E_BOND] + a[LIMA_E_ANGLE] + a[LIMA_E_DIHEDRAL];
+        e[LIMA_E_LJ] = a[LIMA_E_LJ];
+        e[LIMA_E_BOND] = a[LIMA_E_BOND];
+        e[LIMA_E_ANGLE] = a[LIMA_E_ANGLE];
+        e[LIMA_E_DIHEDRAL] = a[LIMA_E_DIHEDRAL];
+        e[LIMA_E_KINETIC] = a[LIMA_E_KINETIC];
+        e[LIMA_E_VIRIAL] = a[LIMA_E_VIRIAL];
+        e[LIMA_E_TEMPERATURE] = 2.0 * a[LIMA_E_KINETIC] / (3.0 * (double)d.n * kRgas);
+        e[LIMA_E_TOTAL] = pot + a[LIMA_E_KINETIC];
+    }
+    if (k >= d.n) return;
+    const uint32_t o = d.orig_of_sorted[k];
+    const uint32_t slot = g.ref_slot[o];
+    float4 p = d.pos[cur][k];
+    const float4 f = d.force[k];
+    const uint32_t l = slot % LIMA_MAX_COMPOUND_PARTICLES;
+    if (o < (uint32_t)d.n_cp && l != 0) {
+        // a compound's particles in the periodic image of its particle 0, as the
+        // reference keeps them (applyHyperpos, Engine.cu:996) and lima_get_compound_states
+        // returns them: p0 + minimum image of (p - p0), in double
+        const float4 p0 = d.pos[cur][d.sorted_of_orig[o - l]];
+        const double L = (double)d.L;
+        double dd = (double)p.x - (double)p0.x;
+        dd -= L * rint(dd / L);
+        p.x = (float)((double)p0.x + dd);
+        dd = (double)p.y - (double)p0.y;
+        dd -= L * rint(dd / L);
+        p.y = (float)((double)p0.y + dd);
+        dd = (double)p.z - (double)p0.z;
+        dd -= L * rint(dd / L);
+        p.z = (float)((double)p0.z + dd);
+    }
+    if (g.traj) {
+        float* t = g.traj + ((size_t)r * g.n_slots + slot) * 3;
+        t[0] = p.x;
+        t[1] = p.y;
+        t[2] = p.z;
+    }
+    if (g.potE) g.potE[(size_t)r * g.n_slots + slot] = (double)f.w;
+    if (g.train && o < (uint32_t)d.n_cp) {
+        float* t = g.train + ((size_t)r * g.n_train + slot) * (kTrainValues * 3);
+        t[0] = p.x;
+        t[1] = p.y;
+        t[2] = p.z;
+    }
+    if (o == 0 && g.logdata) {
+        // the reference's outdata line of compound 0 particle 0 (Engine.cu:1022-1029):
+        // speed over the step, kinetic energy, potential energy, |force|
+        const float4 v = d.vel[k];   // velocity of the half step just taken, w = 1/m
+        const float v2 = v.x * v.x + v.y * v.y + v.z * v.z;
+        float* l = g.logdata + (size_t)r * kLogDataFloats;
+        l[0] = sqrtf(v2);
+        l[1] = 0.5f * v2 / v.w;
+        l[2] = f.w;
+        l[3] = sqrtf(f.x * f.x + f.y * f.y + f.z * f.z);
+        for (int q = 4; q < kLogDataFloats; q++) l[q] = 0.f;
+    }
+}
+
+template <bool SWITCH>
+__global__ void __launch_bounds__(kTB) k_log_train(PhysDev d, FrameLogDev g, int cur, int r) {
+    extern __shared__ float2 s_tab[];
+    const int nt2 = d.n_types * d.n_types;
+    for (int q = threadIdx.x; q < nt2; q += blockDim.x) s_tab[q] = d.lj_table[q];
+    __syncthreads();
+    const int o = (blockIdx.x * blockDim.x + threadIdx.x) / kGroup;
+    const int lane = threadIdx.x % kGroup;
+    const bool active = o < d.n_cp;
+    float fx = 0.f, fy = 0.f, fz = 0.f, e = 0.f, w = 0.f;
+    if (active) {
+        const int i = (int)d.sorted_of_orig[o];
+        const float4* __restrict__ pos = d.pos[cur];
+        const float4 pi = pos[i];
+        const float2* row = &s_tab[__float_as_int(pi.w) * d.n_types];
+        const int cnt = (int)d.nl_cnt[i];
+        for (int k = lane; k < cnt; k += kGroup) {
+            const uint32_t j = d.nl[((uint32_t)(k / kGroup) * (uint32_t)d.n_pad + (uint32_t)i) * kGroup + k % kGroup];
+            if (d.orig_of_sorted[j] < (uint32_t)d.n_cp) continue;   // solvent neighbours only
+            lj_pair<false, SWITCH>(d, row, pi, pos[j], fx, fy, fz, e, w);
+        }
+    }
+#pragma unroll
+    for (int q = kGroup / 2; q > 0; q >>= 1) {
+        fx += __shfl_xor_sync(0xffffffffu, fx, q);
+        fy += __shfl_xor_sync(0xffffffffu, fy, q);
+        fz += __shfl_xor_sync(0xffffffffu, fz, q);
+    }
+    if (active && lane == 0) {
+        float* t = g.train + ((size_t)r * g.n_train + g.ref_slot[o]) * (kTrainValues * 3) + 3;
+        t[0] = fx;
+        t[1] = fy;
+        t[2] = fz;
+    }
+}
+
+template <typename T>
+T* grow(std::vector<void*>& allocs, size_t n) {
+    void* ptr = nullptr;
+    if (cudaMalloc(&ptr, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) return nullptr;
+    allocs.push_back(ptr);
+    return static_cast<T*>(ptr);
+}
+
+// byte offsets of the arrays of one ring (device ring and pinned staging alike)
+struct Sections {
+    size_t traj, potE, train, energies, logdata, total;
+};
+
+Sections sections(const FrameLogDev& g, int frames) {
+    Sections s{};
+    const size_t f = (size_t)frames;
+    size_t o = 0;
+    s.traj = o;
+    if (g.traj) o += f * g.n_slots * 3 * sizeof(float);
+    o = (o + 15) & ~(size_t)15;
+    s.potE = o;
+    if (g.potE) o += f * g.n_slots * sizeof(double);
+    o = (o + 15) & ~(size_t)15;
+    s.train = o;
+    if (g.train) o += f * g.n_train * kTrainValues * 3 * sizeof(float);
+    o = (o + 15) & ~(size_t)15;
+    s.energies = o;
+    o += f * LIMA_E_COUNT * sizeof(double);
+    s.logdata = o;
+    o += f * kLogDataFloats * sizeof(float);
+    s.total = o;
+    return s;
+}
+
+// frames [0, count) of the device ring -> pinned buffer b, stream-ordered
+void copy_ring(FrameLog& g, int b, int count, cudaStream_t s) {
+    const FrameLogDev& v = g.dev;
+    const Sections R = sections(v, v.ring);   // device ring and staging share the full-ring layout
+    char* dst = static_cast<char*>(g.pinned[b]);
+    const size_t c = (size_t)count;
+    if (v.traj) cudaMemcpyAsync(dst + R.traj, v.traj, c * v.n_slots * 3 * sizeof(float), cudaMemcpyDeviceToHost, s);
+    if (v.potE) cudaMemcpyAsync(dst + R.potE, v.potE, c * v.n_slots * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (v.train)
+        cudaMemcpyAsync(dst + R.train, v.train, c * v.n_train * kTrainValues * 3 * sizeof(float),
+                        cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(dst + R.energies, v.energies, c * LIMA_E_COUNT * sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(dst + R.logdata, v.logdata, c * kLogDataFloats * sizeof(float), cudaMemcpyDeviceToHost, s);
+    cudaEventRecord(g.done[b], s);
+}
+
+// pinned buffer b (copy finished) -> the host store
+void absorb(FrameLog& g, int b) {
+    const int count = g.pending[b];
+    if (!count) return;
+    cudaEventSynchronize(g.done[b]);
+    const FrameLogDev& v = g.dev;
+    const Sections R = sections(v, v.ring);
+    const char* src = static_cast<const char*>(g.pinned[b]);
+    auto append = [&](auto& vec, size_t off, size_t n) {
+        using T = typename std::decay_t<decltype(vec)>::value_type;
+        const T* p = reinterpret_cast<const T*>(src + off);
+        vec.insert(vec.end(), p, p + n);
+    };
+    const size_t c = (size_t)count;
+    if (v.traj) append(g.traj, R.traj, c * v.n_slots * 3);
+    if (v.potE) append(g.potE, R.potE, c * v.n_slots);
+    if (v.train) append(g.train, R.train, c * v.n_train * kTrainValues * 3);
+    append(g.energies, R.energies, c * LIMA_E_COUNT);
+    append(g.logdata, R.logdata, c * kLogDataFloats);
+    g.steps.insert(g.steps.end(), g.buf_steps[b].begin(), g.buf_steps[b].end());
+    g.buf_steps[b].clear();
+    g.pending[b] = 0;
+}
+
+// the frames in the device ring -> the next pinned buffer (absorbing what it held first)
+void drain(FrameLog& g, cudaStream_t s) {
+    if (!g.in_ring) return;
+    const int b = g.next_buf;
+    absorb(g, b);
+    copy_ring(g, b, g.in_ring, s);
+    g.pending[b] = g.in_ring;
+    g.buf_steps[b].swap(g.ring_steps);
+    g.ring_steps.clear();
+    g.in_ring = 0;
+    g.next_buf ^= 1;
+}
+
+}  // namespace
+
+void framelog_free(FrameLog& g) {
+    for (int b = 0; b < 2; b++)
+        if (g.pending[b] && g.done[b]) cudaEventSynchronize(g.done[b]);   // copies still in flight
+    for (void* p : g.dallocs) cudaFree(p);
+    g.dallocs.clear();
+    for (auto& p : g.pinned)
+        if (p) {
+            cudaFreeHost(p);
+            p = nullptr;
+        }
+    for (auto& e : g.done)
+        if (e) {
+            cudaEventDestroy(e);
+            e = nullptr;
+        }
+    g = FrameLog{};
+}
+
+void framelog_start(FrameLog& g, const PhysDev& d, const std::vector<int>& n_compound_particles,
+                    const lima_log_params& p, std::string& msg, int& status) {
+    framelog_free(g);
+    status = LIMA_OK;
+    const int n_c = (int)n_compound_particles.size();
+    FrameLogDev& v = g.dev;
+    v.flags = p.flags;
+    v.ring = p.ring_frames;
+    v.n_train = n_c * LIMA_MAX_COMPOUND_PARTICLES;
+    v.n_slots = v.n_train + d.n_s;
+    std::vector<uint32_t> slot(d.n);
+    int o = 0;
+    for (int c = 0; c < n_c; c++)
+        for (int l = 0; l < n_compound_particles[c]; l++) slot[o++] = (uint32_t)(c * LIMA_MAX_COMPOUND_PARTICLES + l);
+    for (int s = 0; s < d.n_s; s++) slot[o++] = (uint32_t)(v.n_train + s);
+    const size_t f = (size_t)v.ring;
+    uint32_t* ref_slot = grow<uint32_t>(g.dallocs, d.n);
+    v.traj = (p.flags & LIMA_LOG_TRAJ) ? grow<float>(g.dallocs, f * v.n_slots * 3) : nullptr;
+    v.potE = (p.flags & LIMA_LOG_POTE) ? grow<double>(g.dallocs, f * v.n_slots) : nullptr;
+    v.train = (p.flags & LIMA_LOG_TRAIN) && n_c ? grow<float>(g.dallocs, f * v.n_train * kTrainValues * 3) : nullptr;
+    v.energies = grow<double>(g.dallocs, f * LIMA_E_COUNT);
+    v.logdata = grow<float>(g.dallocs, f * kLogDataFloats);
+    const Sections R = sections(v, v.ring);
+    g.ring_bytes = R.total;
+    bool ok = ref_slot && v.energies && v.logdata && (!(p.flags & LIMA_LOG_TRAJ) || v.traj) &&
+              (!(p.flags & LIMA_LOG_POTE) || v.potE) && (!(p.flags & LIMA_LOG_TRAIN) || !n_c || v.train);
+    for (int b = 0; ok && b < 2; b++) {
+        ok = cudaMallocHost(&g.pinned[b], g.ring_bytes) == cudaSuccess &&
+             cudaEventCreateWithFlags(&g.done[b], cudaEventDisableTiming) == cudaSuccess;
+    }
+    if (!ok) {
+        framelog_free(g);
+        cudaGetLastError();
+        msg = "frame log: out of device or pinned host memory for the ring";
+        status = LIMA_ERR_CUDA;
+        return;
+    }
+    v.ref_slot = ref_slot;
+    cudaMemcpy(ref_slot, slot.data(), sizeof(uint32_t) * d.n, cudaMemcpyHostToDevice);
+    if (v.traj) cudaMemset(v.traj, 0, f * v.n_slots * 3 * sizeof(float));
+    if (v.potE) cudaMemset(v.potE, 0, f * v.n_slots * sizeof(double));
+    if (v.train) {
+        // padding particles of a compound: position (-1, -1, -1) (Engine.cu:1036-1037), zero force
+        std::vector<float> pad((size_t)v.n_train * kTrainValues * 3, 0.f);
+        for (int c = 0; c < n_c; c++)
+            for (int l = n_compound_particles[c]; l < LIMA_MAX_COMPOUND_PARTICLES; l++)
+                for (int q = 0; q < 3; q++) pad[((size_t)c * LIMA_MAX_COMPOUND_PARTICLES + l) * kTrainValues * 3 + q] = -1.f;
+        for (size_t r = 0; r < f; r++)
+            cudaMemcpy(v.train + r * pad.size(), pad.data(), sizeof(float) * pad.size(), cudaMemcpyHostToDevice);
+    }
+    g.every = p.every;
+    g.on = true;
+}
+
+int framelog_record(FrameLog& g, const PhysDev& d, int cur, uint64_t step, cudaStream_t s) {
+    const FrameLogDev& v = g.dev;
+    const int r = g.in_ring;
+    k_log_frame<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d, v, cur, r);
+    int launched = 1;
+    if (v.train && d.n_cp > 0) {
+        const int nb = (int)(((size_t)d.n_cp * kGroup + kTB - 1) / kTB);
+        const size_t smem = sizeof(float2) * d.n_types * d.n_types;
+        if (d.use_switch)
+            k_log_train<true><<<nb, kTB, smem, s>>>(d, v, cur, r);
+        else
+            k_log_train<false><<<nb, kTB, smem, s>>>(d, v, cur, r);
+        launched++;
+    }
+    g.ring_steps.push_back(step);
+    g.in_ring++;
+    g.frames_logged++;
+    if (g.in_ring == v.ring) drain(g, s);
+    return launched;
+}
+
+void framelog_flush(FrameLog& g, cudaStream_t s) {
+    drain(g, s);
+    // the older pending buffer first
+    absorb(g, g.next_buf);
+    absorb(g, g.next_buf ^ 1);
+    cudaStreamSynchronize(s);
+}
+
+}  // namespace lima

@@ -23,14 +23,13 @@
 // 5x5x5 neighbourhood.
 #include "physdev.cuh"
 #include "physkern.cuh"
+#include "physmath.cuh"
 #include "refdev.cuh"
 
 namespace lima {
 namespace {
 
 constexpr double kR = 8.314462618;   // J/(mol K)
-
-__device__ __forceinline__ float mimg(float d, float L, float invL) { return d - L * rintf(d * invL); }
 
 // error-free sum: s + e == a + b exactly
 __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
@@ -362,12 +361,14 @@ __global__ void __launch_bounds__(kTB) k_bonded(PhysDev d, int cur, int slot, in
         const float rr = sqrtf(rx * rx + ry * ry + rz * rz);
         const float dr = rr - par.x;
         const float f = -par.y * dr / rr;   // F_j = f * r
-        d.term_force[2 * t + 0] = make_float4(-f * rx, -f * ry, -f * rz, 0.f);
-        d.term_force[2 * t + 1] = make_float4(f * rx, f * ry, f * rz, 0.f);
         if (ENERGY) {
             eb = 0.5 * (double)par.y * (double)dr * (double)dr;
             vir = (double)(f * rr * rr);
         }
+        // w: each atom's share of the term's energy (per-particle potential energy)
+        const float sh = ENERGY ? (float)(0.5 * eb) : 0.f;
+        d.term_force[2 * t + 0] = make_float4(-f * rx, -f * ry, -f * rz, sh);
+        d.term_force[2 * t + 1] = make_float4(f * rx, f * ry, f * rz, sh);
     } else if (t < d.n_bonds + d.n_angles) {
         const int a_ = t - d.n_bonds;
         const int4 ix = d.angle_idx[a_];
@@ -390,14 +391,15 @@ __global__ void __launch_bounds__(kTB) k_bonded(PhysDev d, int cur, int slot, in
                     fiz = gk * (vz * inuv - cosv * uz / uu);
         const float fkx = gk * (ux * inuv - cosv * vx / vv), fky = gk * (uy * inuv - cosv * vy / vv),
                     fkz = gk * (uz * inuv - cosv * vz / vv);
-        const int base = 2 * d.n_bonds + 3 * a_;
-        d.term_force[base + 0] = make_float4(fix, fiy, fiz, 0.f);
-        d.term_force[base + 1] = make_float4(-fix - fkx, -fiy - fky, -fiz - fkz, 0.f);
-        d.term_force[base + 2] = make_float4(fkx, fky, fkz, 0.f);
         if (ENERGY) {
             ea = 0.5 * (double)par.y * (double)dth * (double)dth;
             vir = (double)(ux * fix + uy * fiy + uz * fiz + vx * fkx + vy * fky + vz * fkz);
         }
+        const float sh = ENERGY ? (float)(ea / 3.0) : 0.f;
+        const int base = 2 * d.n_bonds + 3 * a_;
+        d.term_force[base + 0] = make_float4(fix, fiy, fiz, sh);
+        d.term_force[base + 1] = make_float4(-fix - fkx, -fiy - fky, -fiz - fkz, sh);
+        d.term_force[base + 2] = make_float4(fkx, fky, fkz, sh);
     } else if (t < d.n_bonds + d.n_angles + d.n_dih) {
         const int q = t - d.n_bonds - d.n_angles;
         const int4 ix = d.dih_idx[q];
@@ -425,13 +427,14 @@ __global__ void __launch_bounds__(kTB) k_bonded(PhysDev d, int cur, int slot, in
         const float r = (b3x * b2x + b3y * b2y + b3z * b2z) / b2b2;
         const float fjx = -fix - p * fix + r * flx, fjy = -fiy - p * fiy + r * fly, fjz = -fiz - p * fiz + r * flz;
         const float fkx = -flx + p * fix - r * flx, fky = -fly + p * fiy - r * fly, fkz = -flz + p * fiz - r * flz;
+        if (ENERGY) ed = (double)par.y * (1.0 + (double)cv);
+        const float sh = ENERGY ? (float)(0.25 * ed) : 0.f;
         const int base = 2 * d.n_bonds + 3 * d.n_angles + 4 * q;
-        d.term_force[base + 0] = make_float4(fix, fiy, fiz, 0.f);
-        d.term_force[base + 1] = make_float4(fjx, fjy, fjz, 0.f);
-        d.term_force[base + 2] = make_float4(fkx, fky, fkz, 0.f);
-        d.term_force[base + 3] = make_float4(flx, fly, flz, 0.f);
+        d.term_force[base + 0] = make_float4(fix, fiy, fiz, sh);
+        d.term_force[base + 1] = make_float4(fjx, fjy, fjz, sh);
+        d.term_force[base + 2] = make_float4(fkx, fky, fkz, sh);
+        d.term_force[base + 3] = make_float4(flx, fly, flz, sh);
         if (ENERGY) {
-            ed = (double)par.y * (1.0 + (double)cv);
             vir = (double)(b1x * fjx + b1y * fjy + b1z * fjz + (b1x + b2x) * fkx + (b1y + b2y) * fky +
                            (b1z + b2z) * fkz + (b1x + b2x + b3x) * flx + (b1y + b2y + b3y) * fly +
                            (b1z + b2z + b3z) * flz);
@@ -449,53 +452,7 @@ __global__ void __launch_bounds__(kTB) k_bonded(PhysDev d, int cur, int slot, in
 __global__ void k_finalize(PhysDev d, int src) { fold(d, src); }
 
 // ------------------------------------------------------- pair + integrate ---
-namespace {
-
-// One pair, branch-free: out-of-cutoff pairs contribute zero through a
-// select, the switch is evaluated for every pair (S = 1, S' = 0 below r_on).
-template <bool ENERGY, bool SWITCH>
-__device__ __forceinline__ void lj_pair(const PhysDev& d, const float2* __restrict__ row, float4 pi, float4 pj,
-                                        float& px, float& py, float& pz, float& e_i, float& w_i) {
-    const float dx = mimg(pj.x - pi.x, d.L, d.invL);
-    const float dy = mimg(pj.y - pi.y, d.L, d.invL);
-    const float dz = mimg(pj.z - pi.z, d.L, d.invL);
-    const float r2 = dx * dx + dy * dy + dz * dz;
-    const float2 tab = row[__float_as_int(pj.w)];
-    const float inv = __fdividef(1.f, r2);
-    const float sr2 = tab.x * inv;
-    const float sr6 = sr2 * sr2 * sr2;
-    float fr = 6.f * tab.y * inv * sr6 * (2.f * sr6 - 1.f);   // F_j / r_vec
-    float v = 0.f;
-    if (ENERGY || SWITCH) v = tab.y * (sr6 * sr6 - sr6);
-    if (SWITCH) {
-        // C2 switch in r^2: S = t^3 (10 - 15 t + 6 t^2), t = sat((rc^2 - r^2) / (rc^2 - r_on^2));
-        // S = 1 below r_on and S = S' = 0 beyond r_c, so no separate cutoff select
-        const float t = __saturatef((d.rc2 - r2) * d.inv_sw_d);
-        const float t2 = t * t, omt = 1.f - t;
-        const float sw = t2 * t * fmaf(t, fmaf(6.f, t, -15.f), 10.f);
-        const float dsw = -60.f * d.inv_sw_d * t2 * omt * omt;   // (dS/dr)/r
-        fr = fr * sw - v * dsw;
-        v *= sw;
-    } else {
-        if (ENERGY) {
-            const float src2 = tab.x / d.rc2, src6 = src2 * src2 * src2;
-            v -= tab.y * (src6 * src6 - src6);
-        }
-        const bool in = r2 < d.rc2;
-        fr = in ? fr : 0.f;
-        v = in ? v : 0.f;
-    }
-    px -= fr * dx;
-    py -= fr * dy;
-    pz -= fr * dz;
-    if (ENERGY) {
-        e_i += 0.5f * v;
-        w_i += 0.5f * fr * r2;
-    }
-}
-
-}  // namespace
-
+// (lj_pair: physmath.cuh)
 template <bool MIXED, bool ENERGY, bool INTEGRATE, bool SWITCH>
 __global__ void __launch_bounds__(kTB) k_pair_integrate(PhysDev d, int cur, int slot) {
     extern __shared__ float2 s_tab[];
@@ -564,17 +521,20 @@ __global__ void __launch_bounds__(kTB) k_pair_integrate(PhysDev d, int cur, int 
             w_i += __shfl_xor_sync(0xffffffffu, w_i, o);
         }
     }
+    float e_b = 0.f;
     if (active && g == 0) {
         // bonded contributions of this particle
         const uint32_t oi = d.orig_of_sorted[i];
         if (oi < (uint32_t)d.n_cp) {
-            float bx = 0.f, by = 0.f, bz = 0.f;
+            float bx = 0.f, by = 0.f, bz = 0.f, bw = 0.f;
             for (uint32_t q = d.bterm_off[oi]; q < d.bterm_off[oi + 1]; q++) {
                 const float4 tf = d.term_force[d.bterm_slot[q]];
                 bx += tf.x;
                 by += tf.y;
                 bz += tf.z;
+                bw += tf.w;
             }
+            e_b = bw;
             if (MIXED) {
                 ds_add(fx, cxx, bx);
                 ds_add(fy, cyy, by);
@@ -590,7 +550,8 @@ __global__ void __launch_bounds__(kTB) k_pair_integrate(PhysDev d, int cur, int 
             fy += cyy;
             fz += czz;
         }
-        d.force[i] = make_float4(fx, fy, fz, ENERGY ? e_i : 0.f);
+        // w: the particle's potential energy, its LJ pair halves plus its bonded-term shares
+        d.force[i] = make_float4(fx, fy, fz, ENERGY ? e_i + e_b : 0.f);
         if (ENERGY) {
             elj = (double)e_i;
             vir = (double)w_i;

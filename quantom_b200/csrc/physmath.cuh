@@ -1,0 +1,56 @@
+// Pair and periodic-boundary math of the physics path, shared by the step
+// kernels (kernels_physics.cu) and the frame log (framelog.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "physdev.cuh"
+
+namespace lima {
+
+// minimum image of one coordinate difference in a cubic box
+__device__ __forceinline__ float mimg(float d, float L, float invL) { return d - L * rintf(d * invL); }
+
+// One pair, branch-free: out-of-cutoff pairs contribute zero through a
+// select, the switch is evaluated for every pair (S = 1, S' = 0 below r_on).
+template <bool ENERGY, bool SWITCH>
+__device__ __forceinline__ void lj_pair(const PhysDev& d, const float2* __restrict__ row, float4 pi, float4 pj,
+                                        float& px, float& py, float& pz, float& e_i, float& w_i) {
+    const float dx = mimg(pj.x - pi.x, d.L, d.invL);
+    const float dy = mimg(pj.y - pi.y, d.L, d.invL);
+    const float dz = mimg(pj.z - pi.z, d.L, d.invL);
+    const float r2 = dx * dx + dy * dy + dz * dz;
+    const float2 tab = row[__float_as_int(pj.w)];
+    const float inv = __fdividef(1.f, r2);
+    const float sr2 = tab.x * inv;
+    const float sr6 = sr2 * sr2 * sr2;
+    float fr = 6.f * tab.y * inv * sr6 * (2.f * sr6 - 1.f);   // F_j / r_vec
+    float v = 0.f;
+    if (ENERGY || SWITCH) v = tab.y * (sr6 * sr6 - sr6);
+    if (SWITCH) {
+        // C2 switch in r^2: S = t^3 (10 - 15 t + 6 t^2), t = sat((rc^2 - r^2) / (rc^2 - r_on^2));
+        // S = 1 below r_on and S = S' = 0 beyond r_c, so no separate cutoff select
+        const float t = __saturatef((d.rc2 - r2) * d.inv_sw_d);
+        const float t2 = t * t, omt = 1.f - t;
+        const float sw = t2 * t * fmaf(t, fmaf(6.f, t, -15.f), 10.f);
+        const float dsw = -60.f * d.inv_sw_d * t2 * omt * omt;   // (dS/dr)/r
+        fr = fr * sw - v * dsw;
+        v *= sw;
+    } else {
+        if (ENERGY) {
+            const float src2 = tab.x / d.rc2, src6 = src2 * src2 * src2;
+            v -= tab.y * (src6 * src6 - src6);
+        }
+        const bool in = r2 < d.rc2;
+        fr = in ? fr : 0.f;
+        v = in ? v : 0.f;
+    }
+    px -= fr * dx;
+    py -= fr * dy;
+    pz -= fr * dz;
+    if (ENERGY) {
+        e_i += 0.5f * v;
+        w_i += 0.5f * fr * r2;
+    }
+}
+
+}  // namespace lima

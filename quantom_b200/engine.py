@@ -44,6 +44,15 @@ class LossSpec(ctypes.Structure):
                 ("rdf_target", ctypes.c_void_p)]
 
 
+LOG_TRAJ, LOG_POTE, LOG_TRAIN = 1, 2, 4
+LOG_DATA_FLOATS = 10
+
+
+class LogParams(ctypes.Structure):
+    """lima_log_params (include/lima_abi.h)."""
+    _fields_ = [("every", ctypes.c_int), ("ring_frames", ctypes.c_int), ("flags", ctypes.c_int)]
+
+
 class Params(ctypes.Structure):
     """lima_params (include/lima_abi.h)."""
     _fields_ = [("box_len", ctypes.c_float), ("cutoff", ctypes.c_float), ("ref_cutoff", ctypes.c_float),
@@ -97,6 +106,13 @@ def load_library():
         "lima_grad": (i, [vp, vp, ctypes.POINTER(d), vp]),
         "lima_rdf": (i, [vp, i, f, vp]),
         "lima_get_kernel_launches": (i, [vp, ctypes.POINTER(ctypes.c_uint64)]),
+        "lima_log_start": (i, [vp, vp]),
+        "lima_log_stop": (i, [vp]),
+        "lima_log_count": (i, [vp, ctypes.POINTER(ctypes.c_uint64)]),
+        "lima_log_read": (i, [vp, ctypes.c_uint64, ctypes.c_uint64, vp, vp, vp, vp, vp, vp]),
+        "lima_log_write": (i, [vp, ctypes.c_char_p]),
+        "lima_render": (i, [vp, vp]),
+        "lima_render_image": (i, [vp, i, i, vp]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name, None)
@@ -265,6 +281,65 @@ class Engine:
         self._check(self.lib.lima_get_rebuild_count(self.h, ctypes.byref(v)))
         return int(v.value)
 
+    # -- frame log (physics semantics) -------------------------------------
+    def log_start(self, every: int, ring_frames: int = 64, flags: int = LOG_TRAJ | LOG_POTE | LOG_TRAIN):
+        """Record the state of every `every`-th step: the reference's logging
+        buffers (traj, potE, data_GAN, outdata) and per-step energies."""
+        lp = LogParams(int(every), int(ring_frames), int(flags))
+        self._check(self.lib.lima_log_start(self.h, ctypes.byref(lp)))
+        self._log_flags = int(flags)
+
+    def log_stop(self):
+        self._check(self.lib.lima_log_stop(self.h))
+
+    def log_count(self) -> int:
+        v = ctypes.c_uint64()
+        self._check(self.lib.lima_log_count(self.h, ctypes.byref(v)))
+        return int(v.value)
+
+    def log_read(self, first: int = 0, count: int | None = None) -> dict:
+        """Frames [first, first+count) as arrays in the reference's indexing:
+        traj (F, n_c*64 + n_s, 3), potE (F, n_c*64 + n_s), train
+        (F, n_c, 64, 3, 3), energies (F, E_COUNT), logdata (F, 10), steps (F,)."""
+        total = self.log_count()
+        count = total - first if count is None else int(count)
+        nc, ns = self.system.n_compounds, self.system.n_solvents
+        slots = nc * L.MAX_COMPOUND_PARTICLES + ns
+        flags = getattr(self, "_log_flags", 0)
+        out = {"steps": np.zeros(count, np.uint64), "energies": np.zeros((count, E_COUNT), np.float64),
+               "logdata": np.zeros((count, LOG_DATA_FLOATS), np.float32)}
+        if flags & LOG_TRAJ:
+            out["traj"] = np.zeros((count, slots, 3), np.float32)
+        if flags & LOG_POTE:
+            out["potE"] = np.zeros((count, slots), np.float64)
+        if flags & LOG_TRAIN and nc:
+            out["train"] = np.zeros((count, nc, L.MAX_COMPOUND_PARTICLES, 3, 3), np.float32)
+        self._check(self.lib.lima_log_read(self.h, int(first), count, _ptr(out["steps"]), _ptr(out["energies"]),
+                                           _ptr(out.get("traj")), _ptr(out.get("potE")), _ptr(out.get("train")),
+                                           _ptr(out["logdata"])))
+        return out
+
+    def log_write(self, directory) -> None:
+        """The recorded frames as the reference's output files (logdata.bin,
+        energy.bin, temperature.bin, sim_traindata.bin, traj.bin, potE.bin)."""
+        self._check(self.lib.lima_log_write(self.h, str(directory).encode()))
+
+    # -- headless rasterizer -------------------------------------------------
+    def render(self) -> np.ndarray:
+        """RenderBall per particle slot of the current state, sorted by depth
+        (Rasterizer::render, Rasterizer.cu:12-27)."""
+        n = self.system.n_compounds * L.MAX_COMPOUND_PARTICLES + self.system.n_solvents
+        balls = np.zeros(n, L.RenderBall)
+        self._check(self.lib.lima_render(self.h, _ptr(balls)))
+        return balls
+
+    def render_image(self, width: int = 1080, height: int = 1080) -> np.ndarray:
+        """The picture the reference's display draws of render(): (height,
+        width, 3) uint8, row 0 at the top."""
+        img = np.zeros((int(height), int(width), 3), np.uint8)
+        self._check(self.lib.lima_render_image(self.h, int(width), int(height), _ptr(img)))
+        return img
+
     # -- state ---------------------------------------------------------------
     def compound_states(self):
         n = self.system.n_compounds
@@ -322,6 +397,14 @@ class Engine:
         offsets = np.ascontiguousarray(offsets, np.uint32)
         ids = np.ascontiguousarray(ids if len(ids) else np.zeros(1), np.uint32)
         self._check(self.lib.lima_set_nlist(self.h, which, _ptr(offsets), _ptr(ids)))
+
+
+def save_ppm(path, img: np.ndarray) -> None:
+    """Writes an (h, w, 3) uint8 image as binary PPM."""
+    h, w, _ = img.shape
+    with open(path, "wb") as f:
+        f.write(b"P6\n%d %d\n255\n" % (w, h))
+        f.write(np.ascontiguousarray(img, np.uint8).tobytes())
 
 
 def cuda_available() -> bool:

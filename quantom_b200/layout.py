@@ -83,6 +83,12 @@ CompoundBridgeCompact = np.dtype({
     "itemsize": 2352})
 
 ParticleParameters = np.dtype([("mass", np.float32), ("sigma", np.float32), ("epsilon", np.float32)])
+# RenderBall (QuantomTypes.cuh:362-369) = lima_render_ball, 32 bytes
+RenderBall = np.dtype([("pos", float3), ("radius", np.float32), ("color", np.int32, 3), ("disable", np.uint8),
+                       ("pad", np.uint8, 3)])
+# atom_color_types index -> ATOM_TYPE (Rasterizer.cu:126-146; QuantomTypes.cuh:16
+# NONE 0, O 1, C 2, P 3, N 4, H 5, SOL 6)
+RENDER_TYPE_OF_COLOR = (6, 2, 1, 4, 5, 3, 6)
 ForceField = np.dtype([("particle_parameters", (ParticleParameters, MAX_ATOM_TYPES))])
 
 # Offsets the tests compare with the reference build (ref_layout ids).

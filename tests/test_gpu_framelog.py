@@ -1,0 +1,163 @@
+"""Frame log of the physics path (lima_log_*): the reference's logging buffers
+(traj_buffer, potE_buffer, data_GAN, outdata: Engine.cu:1007-1047,
+1136-1145), their offload and the post-run energy analysis and output files
+(Environment.cpp:124-166, Analyzer.cu:33-207).
+
+Checked against a second engine stepped to the same steps (positions
+bit-identical, FP64 energies to 1e-9 relative), the FP64 oracle (LJ force
+from solvents on compound particles within 5e-5 relative RMS, the stated FP32
+force error), the per-particle energies summing to the FP64 totals, and the
+files read back in the reference's layouts.
+"""
+import numpy as np
+import pytest
+
+from conftest import relrms
+from oracle import pyoracle as po
+from quantom_b200 import systems as S
+
+pytestmark = pytest.mark.gpu
+
+EVERY, STEPS = 5, 40
+
+
+def _params(E, s, **kw):
+    p = E.default_params(box_len=s.spec.box_len, cutoff=s.spec.cutoff, dt=s.spec.dt, semantics=E.SEMANTICS_PHYSICS,
+                         skin=0.1, switch_on=1.0, nlist_period=0)
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def _slots(E, eng, s):
+    """Positions of the current state in the reference slot layout."""
+    st, _ = eng.compound_states()
+    out = np.zeros((s.n_compounds * 64 + s.n_solvents, 3), np.float32)
+    for c in range(s.n_compounds):
+        k = s.compounds[c]["n_particles"]
+        out[c * 64: c * 64 + k] = st[c]["positions"][:k]
+    out[s.n_compounds * 64:] = eng.solvents()["pos"]
+    return out
+
+
+@pytest.fixture(scope="module", params=["tiny_chains", "small_bridged"])
+def logged(request, gpu):
+    E = gpu
+    s = S.make_system(request.param, seed=5)
+    with E.Engine(s, _params(E, s)) as eng:
+        eng.log_start(EVERY, ring_frames=3)      # the ring wraps twice
+        eng.step(STEPS)
+        frames = eng.log_read()
+        # a second engine at the same steps, energy steps where the first one logged
+        ref_pos, ref_e = [], []
+        with E.Engine(s, _params(E, s, energy_period=EVERY)) as ref:
+            for k in range(STEPS // EVERY):
+                ref_pos.append(_slots(E, ref, s))
+                ref_e.append(ref.compute_energies())
+                ref.step(EVERY)
+        yield E, s, eng, frames, np.array(ref_pos), np.array(ref_e)
+
+
+def test_frames_are_the_logged_steps(logged):
+    E, s, eng, fr, ref_pos, _ = logged
+    assert fr["steps"].tolist() == list(range(0, STEPS, EVERY))
+    assert eng.log_count() == STEPS // EVERY
+    # positions the forces of each logged step were evaluated at
+    np.testing.assert_array_equal(fr["traj"], ref_pos)
+
+
+def test_frame_energies_match_the_step(logged):
+    E, s, eng, fr, _, ref_e = logged
+    e = fr["energies"]
+    for q in (E.E_LJ, E.E_BOND, E.E_ANGLE, E.E_DIHEDRAL, E.E_KINETIC, E.E_TOTAL, E.E_TEMPERATURE):
+        np.testing.assert_allclose(e[:, q], ref_e[:, q], rtol=1e-9, atol=1e-9 * np.abs(ref_e[:, E.E_TOTAL]).max())
+
+
+def test_per_particle_energies_sum_to_the_totals(logged):
+    E, s, eng, fr, _, _ = logged
+    e = fr["energies"]
+    pot = e[:, E.E_LJ] + e[:, E.E_BOND] + e[:, E.E_ANGLE] + e[:, E.E_DIHEDRAL]
+    scale = np.abs(e[:, E.E_LJ]) + np.abs(e[:, E.E_DIHEDRAL])
+    np.testing.assert_array_less(np.abs(fr["potE"].sum(1) - pot), 1e-5 * scale)
+    # empty compound slots stay zero
+    for c in range(s.n_compounds):
+        k = s.compounds[c]["n_particles"]
+        assert not fr["potE"][:, c * 64 + k: (c + 1) * 64].any()
+
+
+def test_train_record_matches_fp64_solvent_forces(logged):
+    E, s, eng, fr, _, _ = logged
+    ps = po.PhysSystem(s, rc=s.spec.cutoff, r_on=1.0)
+    tr = fr["train"]
+    assert tr.shape == (len(fr["steps"]), s.n_compounds, 64, 3, 3)
+    for f in (0, len(fr["steps"]) - 1):
+        x = np.concatenate([fr["traj"][f, c * 64: c * 64 + s.compounds[c]["n_particles"]]
+                            for c in range(s.n_compounds)] + [fr["traj"][f, s.n_compounds * 64:]])
+        F64 = ps.solvent_lj_on_compounds(x.astype(np.float64))
+        got = np.concatenate([tr[f, c, : s.compounds[c]["n_particles"], 1] for c in range(s.n_compounds)])
+        pos = np.concatenate([tr[f, c, : s.compounds[c]["n_particles"], 0] for c in range(s.n_compounds)])
+        assert relrms(got, F64) < 5e-5
+        np.testing.assert_array_equal(pos, x[: len(pos)])
+    for c in range(s.n_compounds):
+        k = s.compounds[c]["n_particles"]
+        assert (tr[:, c, k:, 0] == -1.0).all() and not tr[:, c, k:, 1:].any()
+        assert not tr[:, c, :k, 2].any()
+
+
+def test_logdata_line(logged):
+    E, s, eng, fr, _, _ = logged
+    ld = fr["logdata"]
+    np.testing.assert_allclose(ld[:, 2], fr["potE"][:, 0].astype(np.float32), rtol=1e-6)
+    assert np.isfinite(ld).all() and (ld[:, 0] > 0).all() and (ld[:, 3] > 0).all() and not ld[:, 4:].any()
+    m = s.forcefield["particle_parameters"][0]["mass"][s.compounds[0]["atom_types"][0]]
+    np.testing.assert_allclose(ld[:, 1], 0.5 * m * ld[:, 0] ** 2, rtol=1e-5)
+
+
+def test_files_in_reference_layout(logged, tmp_path):
+    E, s, eng, fr, _, _ = logged
+    eng.log_write(tmp_path)
+    nf, nc, ns = len(fr["steps"]), s.n_compounds, s.n_solvents
+    n = s.n_particles
+    ld = np.fromfile(tmp_path / "logdata.bin", np.float32).reshape(nf, 10)
+    np.testing.assert_array_equal(ld, fr["logdata"])
+    en = np.fromfile(tmp_path / "energy.bin", np.float32).reshape(nf, 3)
+    e = fr["energies"]
+    pot = e[:, E.E_LJ] + e[:, E.E_BOND] + e[:, E.E_ANGLE] + e[:, E.E_DIHEDRAL]
+    np.testing.assert_allclose(en[:, 0], pot / n, rtol=1e-6)
+    np.testing.assert_allclose(en[:, 1], e[:, E.E_KINETIC] / n, rtol=1e-6)
+    np.testing.assert_allclose(en[:, 2], e[:, E.E_TOTAL] / n, rtol=1e-6)
+    temp = np.fromfile(tmp_path / "temperature.bin", np.float32)
+    np.testing.assert_allclose(temp, e[:, E.E_TEMPERATURE], rtol=1e-6)
+    # sim_traindata.bin as LIMA_services reads it (main.cpp:269-300): per step, per
+    # particle slot, FLOAT3_PER_ATOM = 3 float3 (position, LJ force)
+    td = np.fromfile(tmp_path / "sim_traindata.bin", np.float32).reshape(nf, nc * 64, 3, 3)
+    np.testing.assert_array_equal(td, fr["train"].reshape(nf, nc * 64, 3, 3))
+    tj = np.fromfile(tmp_path / "traj.bin", np.float32).reshape(nf, nc * 64 + ns, 3)
+    np.testing.assert_array_equal(tj, fr["traj"])
+    pe = np.fromfile(tmp_path / "potE.bin", np.float64).reshape(nf, nc * 64 + ns)
+    np.testing.assert_array_equal(pe, fr["potE"])
+
+
+def test_stop_keeps_frames_and_stops_recording(gpu):
+    E = gpu
+    s = S.make_system("tiny_chains", seed=6)
+    with E.Engine(s, _params(E, s, precision=E.PRECISION_MIXED)) as eng:
+        eng.log_start(2, ring_frames=64, flags=E.LOG_TRAJ)
+        eng.step(10)
+        eng.log_stop()
+        eng.step(10)
+        fr = eng.log_read()
+        assert fr["steps"].tolist() == [0, 2, 4, 6, 8]
+        assert "potE" not in fr and "train" not in fr
+        buf = np.zeros(s.n_compounds * 64 + s.n_solvents)   # potentials were not recorded
+        assert eng.lib.lima_log_read(eng.h, 0, 1, None, None, None, buf.ctypes.data, None, None) == E.ERR_ARGUMENT
+
+
+def test_reference_semantics_refuses(gpu):
+    E = gpu
+    s = S.make_system("tiny_chains", seed=6)
+    p = E.default_params(box_len=s.spec.box_len, cutoff=s.spec.cutoff, dt=s.spec.dt)
+    with E.Engine(s, p) as eng:
+        with pytest.raises(E.LimaError) as ei:
+            eng.log_start(1)
+        assert ei.value.status == E.ERR_UNSUPPORTED

@@ -166,3 +166,17 @@ def test_dynamic_list_stays_valid_over_a_long_run(gpu):
         s2.compounds[c]["prev_positions"] = prev[c]
     F64, _ = po.PhysSystem(s2, rc=s.spec.cutoff, r_on=1.0).forces()
     assert relrms(F, F64) < 5e-5
+
+
+def test_compute_energies_reports_its_own_kinetic_energy(gpu):
+    """lima_compute_energies after steps: the kinetic energy and temperature
+    are those of the evaluated state, not of the step before it (the last
+    step's pending FP64 sums are folded first)."""
+    E = gpu
+    s = S.make_system("tiny_chains", seed=8)
+    with E.Engine(s, _params(E, s, nlist_period=0)) as eng:
+        eng.step(7)
+        a = eng.compute_energies()
+        b = eng.compute_energies()
+    for q in (E.E_KINETIC, E.E_TEMPERATURE, E.E_TOTAL, E.E_LJ):
+        assert abs(a[q] - b[q]) <= 1e-9 * abs(b[q]), q

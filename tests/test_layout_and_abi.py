@@ -75,3 +75,15 @@ def test_default_params():
     assert p.thermostat_period == 40      # Constants.cuh:82
     assert abs(p.dt - 1e-7) < 1e-20       # Simulation.cuh:152
     assert abs(p.box_len - 7.0) < 1e-6    # Constants.cuh:35
+
+
+def test_frame_log_entry_points_reject_a_null_context():
+    from quantom_b200 import engine
+    lib = engine.load_library()
+    lp = engine.LogParams(1, 1, engine.LOG_TRAJ)
+    n = ctypes.c_uint64()
+    assert lib.lima_log_start(None, ctypes.byref(lp)) == engine.ERR_ARGUMENT
+    assert lib.lima_log_stop(None) == engine.ERR_ARGUMENT
+    assert lib.lima_log_count(None, ctypes.byref(n)) == engine.ERR_ARGUMENT
+    assert lib.lima_log_read(None, 0, 0, None, None, None, None, None, None) == engine.ERR_ARGUMENT
+    assert lib.lima_log_write(None, b".") == engine.ERR_ARGUMENT
