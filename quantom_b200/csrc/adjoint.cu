@@ -100,18 +100,24 @@ struct AdjArgs {
 };
 
 // --------------------------------------------------------------- loss pass --
+// The block's occupancies accumulate in shared memory as 64-bit fixed point
+// in units of 2^-32 (each half weight, at most 0.375, converted from FP32;
+// integer sums do not depend on their order, so the block's sums are
+// deterministic), then go to FP64 once per bin and block.
+constexpr double kHistUnit = 1.0 / 4294967296.0;   // 2^-32
+
 __global__ void __launch_bounds__(kAdjTB) k_loss_pairs(PhysDev d, const float4* __restrict__ pos, int n_bins,
                                                        float inv_dr, float supp2, double inv_n,
                                                        double* __restrict__ U_out, double* __restrict__ h_out) {
-    extern __shared__ double s_red[];   // [kAdjTB / 32][n_bins + 1]
+    __shared__ unsigned long long s_hist[LIMA_LOSS_MAX_BINS];
+    __shared__ double s_e[kAdjTB / 32];
     __shared__ float2 s_tab[kMaxTypes * kMaxTypes];
     const int nt2 = d.n_types * d.n_types;
     for (int q = threadIdx.x; q < nt2; q += blockDim.x) s_tab[q] = d.lj_table[q];
+    for (int b = threadIdx.x; b < n_bins; b += blockDim.x) s_hist[b] = 0ull;
     __syncthreads();
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) / kGroup;
     const int g = threadIdx.x % kGroup;
-    float hl[LIMA_LOSS_MAX_BINS];
-    for (int b = 0; b < n_bins; b++) hl[b] = 0.f;
     float e = 0.f;
     if (i < d.n) {
         const float4 pi = pos[i];
@@ -133,22 +139,21 @@ __global__ void __launch_bounds__(kAdjTB) k_loss_pairs(PhysDev d, const float4* 
                 bspline3(sqrtf(r2), inv_dr, k0, w, dw);
 #pragma unroll
                 for (int q = 0; q < 3; q++)
-                    if (k0 + q >= 0 && k0 + q < n_bins) hl[k0 + q] += 0.5f * w[q];
+                    if (k0 + q >= 0 && k0 + q < n_bins)   // each pair is seen from both ends: half weight
+                        atomicAdd(&s_hist[k0 + q], (unsigned long long)__float2ull_rn(0.5f * w[q] * 4294967296.f));
             }
         }
     }
-    // block reduction in FP64, fixed order
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    double* red = s_red + w * (n_bins + 1);
-    for (int b = 0; b <= n_bins; b++) {
-        const double v = warp_sum_d((double)(b < n_bins ? hl[b] : e));
-        if (lane == 0) red[b] = v;
-    }
+    // energy: FP64 warp sums, then the block's warps in a fixed order
+    const double ew = warp_sum_d((double)e);
+    if ((threadIdx.x & 31) == 0) s_e[threadIdx.x >> 5] = ew;
     __syncthreads();
-    for (int b = threadIdx.x; b <= n_bins; b += blockDim.x) {
+    for (int b = threadIdx.x; b < n_bins; b += blockDim.x)
+        if (s_hist[b]) atomicAdd(&h_out[b], (double)s_hist[b] * kHistUnit * inv_n);
+    if (threadIdx.x == 0) {
         double v = 0.0;
-        for (int q = 0; q < (int)(blockDim.x >> 5); q++) v += s_red[q * (n_bins + 1) + b];
-        if (v != 0.0) atomicAdd(b < n_bins ? &h_out[b] : U_out, b < n_bins ? v * inv_n : v);
+        for (int q = 0; q < kAdjTB / 32; q++) v += s_e[q];
+        if (v != 0.0) atomicAdd(U_out, v);
     }
 }
 
@@ -626,9 +631,8 @@ struct Runner {
     }
     // energy and occupancies of the state in parity cur -> U[n], hist[n]
     void loss_pass(int cur, const float4* pos, const float4* po, int n) {
-        const size_t smem = sizeof(double) * (kAdjTB / 32) * (n_bins + 1);
-        k_loss_pairs<<<blocks_pair(), kAdjTB, smem, s>>>(d, pos, n_bins, inv_dr, supp2, 1.0 / d.n, A.U + n,
-                                                        A.hist + (size_t)n * n_bins);
+        k_loss_pairs<<<blocks_pair(), kAdjTB, 0, s>>>(d, pos, n_bins, inv_dr, supp2, 1.0 / d.n, A.U + n,
+                                                     A.hist + (size_t)n * n_bins);
         AdjArgs a{};
         k_adj_bonded<0><<<blocks_terms(), kAdjTB, 0, s>>>(d, po, a, 0, A.U + n);
         (void)cur;

@@ -454,7 +454,7 @@ __global__ void k_finalize(PhysDev d, int src) { fold(d, src); }
 // ------------------------------------------------------- pair + integrate ---
 // (lj_pair: physmath.cuh)
 template <bool MIXED, bool ENERGY, bool INTEGRATE, bool SWITCH>
-__global__ void __launch_bounds__(kTB) k_pair_integrate(PhysDev d, int cur, int slot) {
+__device__ __forceinline__ void pair_integrate(const PhysDev& d, int cur, int slot) {
     extern __shared__ float2 s_tab[];
     const int nt2 = d.n_types * d.n_types;
     for (int q = threadIdx.x; q < nt2; q += blockDim.x) s_tab[q] = d.lj_table[q];
@@ -646,6 +646,19 @@ __global__ void __launch_bounds__(kTB) k_pair_integrate(PhysDev d, int cur, int 
     }
 }
 
+// FP32: at most 48 registers, 5 blocks of 256 per SM (38.5 against 40.8 us
+// at 4 blocks on the 32k box).  Mixed keeps the compiler's own choice: a
+// bound of 5 blocks slowed it to 45 us, an explicit 4 or 1 changed its
+// allocation for the worse.
+template <bool ENERGY, bool INTEGRATE, bool SWITCH>
+__global__ void __launch_bounds__(kTB, 5) k_pair_integrate(PhysDev d, int cur, int slot) {
+    pair_integrate<false, ENERGY, INTEGRATE, SWITCH>(d, cur, slot);
+}
+template <bool ENERGY, bool INTEGRATE, bool SWITCH>
+__global__ void __launch_bounds__(kTB) k_pair_integrate_mixed(PhysDev d, int cur, int slot) {
+    pair_integrate<true, ENERGY, INTEGRATE, SWITCH>(d, cur, slot);
+}
+
 // ---------------------------------------------------------------- launchers --
 namespace {
 
@@ -653,10 +666,14 @@ template <bool MIXED, bool ENERGY, bool INTEGRATE>
 void pair_variant(const PhysDev& d, int cur, int slot, cudaStream_t s) {
     const int nb = (int)(((size_t)d.n_pad * kGroup + kTB - 1) / kTB);
     const size_t smem = sizeof(float2) * d.n_types * d.n_types;
-    if (d.use_switch)
-        k_pair_integrate<MIXED, ENERGY, INTEGRATE, true><<<nb, kTB, smem, s>>>(d, cur, slot);
+    if (MIXED && d.use_switch)
+        k_pair_integrate_mixed<ENERGY, INTEGRATE, true><<<nb, kTB, smem, s>>>(d, cur, slot);
+    else if (MIXED)
+        k_pair_integrate_mixed<ENERGY, INTEGRATE, false><<<nb, kTB, smem, s>>>(d, cur, slot);
+    else if (d.use_switch)
+        k_pair_integrate<ENERGY, INTEGRATE, true><<<nb, kTB, smem, s>>>(d, cur, slot);
     else
-        k_pair_integrate<MIXED, ENERGY, INTEGRATE, false><<<nb, kTB, smem, s>>>(d, cur, slot);
+        k_pair_integrate<ENERGY, INTEGRATE, false><<<nb, kTB, smem, s>>>(d, cur, slot);
 }
 
 }  // namespace
