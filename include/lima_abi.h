@@ -394,6 +394,48 @@ lima_status lima_render(lima_ctx* ctx, lima_render_ball* balls);
 lima_status lima_render_image(lima_ctx* ctx, int width, int height, uint8_t* rgb);
 
 /* ------------------------------------------------------------------ */
+/* Real-topology input.  Replaces the reference's input path:           */
+/* LIMA_ForcefieldMaker (CHARMM parameter files -> typed tables,         */
+/* LIMA_ForcefieldMaker.cpp:16-146), ForceFieldMaker::buildForcefield    */
+/* (Forcefield.cu:10-218), CompoundBuilder::buildMolecule                 */
+/* (CompoundBuilder.cpp:7-463) and BoxBuilder::addSingleMolecule /       */
+/* solvateBox (BoxBuilder.cu:42-218), as in Environment::Environment     */
+/* (Environment.cpp:15-40).  The result is the box arrays lima_load_*    */
+/* take.                                                                  */
+/* ------------------------------------------------------------------ */
+typedef struct {
+    float box_len;        /* nm; the molecule's centre goes to the box centre (BOX_LEN, Constants.cuh:35) */
+    int min_residue_id;   /* residues before min_residue_id are skipped, reading stops after max_residue_id */
+    int max_residue_id;
+    int ignore_hydrogens; /* 1: atoms whose name starts with 'H' and every term touching them are left out */
+    int solvate;          /* 1: the conf's SOL oxygens become solvents where no compound particle is within
+                             0.2 nm and no earlier solvent within 0.25 nm (BoxBuilder.cu:194-218, 440-461) */
+    double dt;            /* ns; a solvent's previous position is pos - v dt */
+    double temperature;   /* K; solvent speed sqrt(3 R T / M) (BoxBuilder.cuh:63-71) */
+    uint64_t seed;        /* solvent velocity directions (uniform on the sphere) */
+} lima_topology_options;
+
+typedef struct lima_topology lima_topology;
+
+/* Defaults of the reference's demo (Environment.cpp:21-24, Constants.cuh:35,
+   Simulation.cuh:152): 7 nm box, residues 0..200, hydrogens left out,
+   solvated, dt 1e-7 ns, 313 K. */
+void lima_topology_default_options(lima_topology_options* options);
+/* Builds the box from a GROMACS conf.gro, its topol.top and CHARMM parameter
+   files (read in the order given).  *out is set even on failure (then
+   lima_topology_error says why); free it with lima_topology_destroy. */
+lima_status lima_topology_build(const char* gro_path, const char* top_path, const char* const* prm_paths, int n_prm,
+                                const lima_topology_options* options, lima_topology** out);
+const char* lima_topology_error(const lima_topology* topology);
+lima_status lima_topology_sizes(const lima_topology* topology, int* n_compounds, int* n_bridges, uint32_t* n_solvents,
+                                int* n_atom_types);
+/* Copies the box into caller arrays sized by lima_topology_sizes (any may be NULL). */
+lima_status lima_topology_export(const lima_topology* topology, lima_forcefield* forcefield, lima_compound* compounds,
+                                 lima_compound_state* states, lima_compound_bridge_compact* bridges,
+                                 lima_solvent* solvents);
+void lima_topology_destroy(lima_topology* topology);
+
+/* ------------------------------------------------------------------ */
 /* No counterpart in the reference.  The reference updates its lists on  */
 /* the host (Engine::updateNeighborLists, Engine.cu:208-287); this is a  */
 /* context-free, allocation-free form of the device build behind          */

@@ -491,3 +491,56 @@ def render_image(balls, width, height):
     if lib.orc_render_image(_p(balls), len(balls), int(width), int(height), _p(img)) != 0:
         raise MemoryError("orc_render_image")
     return img
+
+
+# ------------------------------------------------------- reference input path --
+REF_FFMAKER = HERE / "_ref" / "lima_ref_ffmaker"
+REF_BOXDUMP = HERE / "_ref" / "lima_ref_boxdump"
+
+
+def ref_input_available() -> bool:
+    return REF_FFMAKER.exists() and REF_BOXDUMP.exists()
+
+
+def ref_input_box(gro, top, prms):
+    """The box the reference's own input path builds (LIMA_ForcefieldMaker,
+    then ForceFieldMaker + CompoundBuilder + BoxBuilder as Environment.cpp:15-40
+    does) from a conf.gro, topol.top and CHARMM parameter files, run in a
+    temporary copy of the directory layout those programs expect.  Returns
+    dict(forcefield, compounds, states, bridges, solvents) in the reference's
+    dtypes.  The parameter files are given to the force-field maker in the
+    order it reads them (par_all36_lipid, par_all36_na, par_all36m_prot)."""
+    import shutil
+    import subprocess
+    import tempfile
+    from quantom_b200 import layout as L
+    names = ["par_all36_lipid.prm", "par_all36_na.prm", "par_all36m_prot.prm"]
+    if [Path(p).name for p in prms] != names:
+        raise ValueError(f"the reference's force-field maker reads exactly {names}")
+    with tempfile.TemporaryDirectory() as tmp:
+        t = Path(tmp)
+        (t / "Simulation" / "Molecule").mkdir(parents=True)
+        (t / "Simulation" / "Forcefield").mkdir(parents=True)
+        (t / "a" / "b").mkdir(parents=True)
+        shutil.copy(gro, t / "Simulation" / "Molecule" / "conf.gro")
+        shutil.copy(top, t / "Simulation" / "Molecule" / "topol.top")
+        for p in prms:
+            shutil.copy(p, t / "Simulation" / "Forcefield" / Path(p).name)
+        run = dict(cwd=t / "a" / "b", stdout=subprocess.DEVNULL, stderr=subprocess.PIPE, check=True)
+        subprocess.run([str(REF_FFMAKER)], **run)
+        subprocess.run([str(REF_BOXDUMP), str(t / "box.bin")], **run)
+        raw = (t / "box.bin").read_bytes()
+    nc, nb, ns = np.frombuffer(raw[:12], np.int32)
+    o = 12
+    def take(dtype, n):
+        nonlocal o
+        a = np.frombuffer(raw[o:o + dtype.itemsize * n], dtype).copy()
+        o += dtype.itemsize * n
+        return a
+    ff = take(L.ForceField, 1)
+    comps = take(L.Compound, nc)
+    states = take(L.CompoundState, nc)
+    bridges = take(L.CompoundBridgeCompact, nb)
+    sols = take(L.Solvent, ns)
+    assert o == len(raw)
+    return dict(forcefield=ff, compounds=comps, states=states, bridges=bridges, solvents=sols)
