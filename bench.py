@@ -48,11 +48,12 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-sample-steps", type=int, default=2)
-    ap.add_argument("--mode", default="full", choices=["full", "kernels", "precision", "grad", "large"],
+    ap.add_argument("--mode", default="full", choices=["full", "kernels", "precision", "grad", "large", "6lzm"],
                     help="kernels: only warm-up + K plain-FP32 steps (the command profiled with ncu); "
                          "precision: the NVE drift / force-error study of plain FP32 against mixed precision; "
                          "grad: the parameter-gradient study on the 8,192 LJ box; "
-                         "large: the 258k solvated-chain box, mixed forward and adjoint gradients")
+                         "large: the 258k solvated-chain box, mixed forward and adjoint gradients; "
+                         "6lzm: the reference's own demo box and settings, next to its published ms/step")
     ap.add_argument("--large-steps", type=int, default=10000, help="--mode large: mixed-precision forward steps")
     ap.add_argument("--nve-steps", type=int, default=50000, help="--mode precision: NVE steps per run")
     ap.add_argument("--eq-steps", type=int, default=5000, help="--mode precision: Berendsen equilibration steps")
@@ -637,6 +638,60 @@ def run_large(args):
     print(json.dumps(out), flush=True)
 
 
+# ------------------------------------------------------- the reference's demo --
+PUBLISHED_6LZM_MS = 3.34   # README.md:19: LIMA_MD ms/step on this box, RTX 2080 Ti, all features on
+
+
+def run_6lzm(args):
+    """The reference's own benchmark system: T4 lysozyme (6LZM) heavy atoms in
+    36 compounds + 35 bridges and 5,000 single-site waters in a 7 nm box, as the
+    reference's input path builds it (the native builder reproduces it bit for
+    bit), with the settings of its published run: CUTOFF 0.7 nm, dt 0.1 fs,
+    lists every 200 steps, its thermostat every 40 steps.  Device time per step
+    with the L2 flushed before every step, next to the published 3.34 ms/step
+    (RTX 2080 Ti).  Also the physics semantics on the same box (cutoff 1.4 nm
+    with a C2 switch from 1.0, skin 0.1 nm, dynamic lists, NVE)."""
+    import torch
+    from oracle import pyoracle as po
+    from quantom_b200 import engine as E
+    from quantom_b200 import systems as S
+    system = S.load_6lzm()
+    spec = system.spec
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    steps = max(200, args.steps)
+    out = {"mode": "6lzm", "workload": "6lzm: T4 lysozyme heavy atoms (1,293 in 36 compounds, 35 bridges) + 5,000 "
+                                       "waters, 7 nm box, dt 0.1 fs", "particles": system.n_particles,
+           "steps": steps, "published_reference_ms_per_step": PUBLISHED_6LZM_MS,
+           "published_hardware": "RTX 2080 Ti (README.md:19)"}
+    p = E.default_params(box_len=spec.box_len, cutoff=spec.cutoff, dt=spec.dt, device=0)
+    p.thermostat = E.THERMOSTAT_REFERENCE
+    p.t_target = 310.0
+    p.stream = stream.cuda_stream
+    with E.Engine(system, p) as eng:
+        timed_steps(eng, stream, max(3, args.warmup), flush)
+        ms = timed_steps(eng, stream, steps, flush) / steps
+        out["reference_semantics"] = {"ms_per_step": ms, "speedup_vs_published": PUBLISHED_6LZM_MS / ms,
+                                      "kernels_ms": eng.profile_steps(50),
+                                      "settings": "CUTOFF 0.7 nm (lists within 2 CUTOFF), lists every 200 steps, "
+                                                  "reference thermostat every 40 steps, FP32"}
+    print(json.dumps({"reference_semantics": out["reference_semantics"]}), flush=True)
+    pp = E.default_params(box_len=spec.box_len, cutoff=spec.cutoff, dt=spec.dt, semantics=E.SEMANTICS_PHYSICS,
+                          skin=SKIN, switch_on=1.0, nlist_period=0, device=0)
+    pp.stream = stream.cuda_stream
+    F64, _ = po.PhysSystem(system, rc=spec.cutoff, r_on=1.0).forces()
+    with E.Engine(system, pp) as eng:
+        eng.compute_energies()
+        F = flat_forces(system, *eng.forces()).astype(np.float64)
+        timed_steps(eng, stream, max(3, args.warmup), flush)
+        ms = timed_steps(eng, stream, steps, flush) / steps
+        out["physics_semantics"] = {"ms_per_step": ms, "speedup_vs_published": PUBLISHED_6LZM_MS / ms,
+                                    "force_relrms_vs_fp64": float(np.sqrt(((F - F64) ** 2).sum() / (F64 ** 2).sum())),
+                                    "kernels_ms": eng.profile_steps(50)}
+    print(json.dumps(out), flush=True)
+
+
 # --------------------------------------------------------------- CPU side --
 def cpu_reference_rate(system, steps, threads):
     """Seconds per step of the reference's own step code on the host cores
@@ -830,6 +885,9 @@ def main():
         return
     if args.mode == "large":
         run_large(args)
+        return
+    if args.mode == "6lzm":
+        run_6lzm(args)
         return
     ws, rank, local, pg = dist_setup(args) if args.impl == "ours" else (int(os.environ.get("WORLD_SIZE", "1")),
                                                                         int(os.environ.get("RANK", "0")), 0, None)

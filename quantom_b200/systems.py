@@ -26,6 +26,7 @@ from __future__ import annotations
 
 import ctypes
 import math
+from pathlib import Path
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -476,3 +477,18 @@ def from_topology(gro, top, prms, options: TopologyOptions | None = None, name: 
                       temperature=float(opt.temperature))
     return System(spec, int(opt.seed), ff, comps, states, sols, bridges,
                   {"n_atom_types": nt.value, "n_compound_particles": int(comps["n_particles"].sum())})
+
+
+SIXLZM_FIXTURE = Path(__file__).resolve().parents[1] / "tests" / "golden" / "golden_6lzm.npz"
+
+
+def load_6lzm(path=None) -> System:
+    """The reference's 6LZM demo box (T4 lysozyme heavy atoms in 36 compounds
+    and 35 bridges, 5,000 single-site waters, 7 nm box), as its own input path
+    built it (tests/golden/make_6lzm.py); the native builder reproduces it from
+    the same files.  Settings of the reference's run: CUTOFF 0.7 nm (physics
+    cutoff 1.4), dt 0.1 fs (Constants.cuh:35,52; Simulation.cuh:152)."""
+    d = np.load(SIXLZM_FIXTURE if path is None else path)
+    spec = SystemSpec("6lzm", 7.0, int(len(d["solvents"])), cutoff=1.4, dt=1e-7, temperature=313.0)
+    return System(spec, 0, d["forcefield"].copy(), d["compounds"].copy(), d["states"].copy(), d["solvents"].copy(),
+                  d["bridges"].copy(), {"n_compound_particles": int(d["compounds"]["n_particles"].sum())})

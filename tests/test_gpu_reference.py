@@ -73,10 +73,12 @@ def test_matches_reference_fixtures(gpu, name):
         assert np.abs(sol["pos"] - z["step4_solvents"]["pos"]).max() < 1e-5
 
 
-@pytest.mark.parametrize("name", ["tiny_chains", "small_bridged", "lj_solvent_4096", "solvated_chains_32k"])
+# 6lzm: the reference's own demo box (T4 lysozyme, 36 compounds, 35 bridges,
+# 5,000 waters) as its input path built it (tests/golden/golden_6lzm.npz)
+@pytest.mark.parametrize("name", ["tiny_chains", "small_bridged", "lj_solvent_4096", "solvated_chains_32k", "6lzm"])
 def test_one_step_matches_oracle(gpu, name):
     E = gpu
-    s = S.make_system(name, seed=7)
+    s = S.load_6lzm() if name == "6lzm" else S.make_system(name, seed=7)
     lists = po.ref_nlist(s, ss_cap=1024, cells=True)
     new, fc_o, fs_o, pe_o = po.ref_step(s, lists)
     with _engine(E, s) as eng:
