@@ -263,6 +263,9 @@ int orc_ref_nlist(float L, float C, int n_c, const lima_compound* comps, const l
  * Same solvent-solvent list with a cell grid (O(N)), for large boxes.  The
  * pair test is the identical float expression; ids come out ascending.
  */
+/* periodic image in [0, L) of a coordinate, for cell assignment only */
+static float wrapf(float x, float L) { return x - L * floorf(x / L); }
+
 int orc_ref_nlist_ss_cells(float L, float C, int n_s, const lima_solvent* sols, int ss_cap, int* ss_ids,
                            int* ss_cnt) {
     const float Lh = L / 2.f;
@@ -274,7 +277,8 @@ int orc_ref_nlist_ss_cells(float L, float C, int n_s, const lima_solvent* sols, 
     int* next = (int*)malloc(sizeof(int) * (n_s > 0 ? n_s : 1));
     for (int k = 0; k < m * m * m; k++) head[k] = -1;
     for (int s = n_s - 1; s >= 0; s--) {
-        int ix = (int)(sols[s].pos.x / cell), iy = (int)(sols[s].pos.y / cell), iz = (int)(sols[s].pos.z / cell);
+        int ix = (int)(wrapf(sols[s].pos.x, L) / cell), iy = (int)(wrapf(sols[s].pos.y, L) / cell),
+            iz = (int)(wrapf(sols[s].pos.z, L) / cell);
         ix = ix < 0 ? 0 : (ix >= m ? m - 1 : ix);
         iy = iy < 0 ? 0 : (iy >= m ? m - 1 : iy);
         iz = iz < 0 ? 0 : (iz >= m ? m - 1 : iz);
@@ -286,7 +290,8 @@ int orc_ref_nlist_ss_cells(float L, float C, int n_s, const lima_solvent* sols, 
     int* tmp = (int*)malloc(sizeof(int) * (ss_cap + 1));
     for (int i = 0; i < n_s; i++) {
         int cnt = 0;
-        int ix = (int)(sols[i].pos.x / cell), iy = (int)(sols[i].pos.y / cell), iz = (int)(sols[i].pos.z / cell);
+        int ix = (int)(wrapf(sols[i].pos.x, L) / cell), iy = (int)(wrapf(sols[i].pos.y, L) / cell),
+            iz = (int)(wrapf(sols[i].pos.z, L) / cell);
         ix = ix < 0 ? 0 : (ix >= m ? m - 1 : ix);
         iy = iy < 0 ? 0 : (iy >= m ? m - 1 : iy);
         iz = iz < 0 ? 0 : (iz >= m ? m - 1 : iz);

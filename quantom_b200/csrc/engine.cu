@@ -171,8 +171,12 @@ void validate_box(lima_ctx* c) {
     }
     for (const auto& s : c->sols) {
         const float L = c->p.box_len;
-        need(s.pos.x >= 0.f && s.pos.x <= L && s.pos.y >= 0.f && s.pos.y <= L && s.pos.z >= 0.f && s.pos.z <= L,
-             LIMA_ERR_ARGUMENT, "solvent position outside [0, box_len]");
+        // the reference loads positions as given and wraps them after the first
+        // integration (applyPBC, Engine.cu:461-466); any image within one box
+        // length of [0, box_len] is accepted
+        need(s.pos.x >= -L && s.pos.x <= 2.f * L && s.pos.y >= -L && s.pos.y <= 2.f * L && s.pos.z >= -L &&
+                 s.pos.z <= 2.f * L,
+             LIMA_ERR_ARGUMENT, "solvent position more than one box length outside [0, box_len]");
     }
 }
 

@@ -25,7 +25,11 @@ using namespace refm;
 
 namespace {
 
-__device__ __forceinline__ int cell_of(float x, float cell, int m) {
+// cell of a coordinate's periodic image in [0, L): a position a little
+// outside the box (as loaded, before the first step wraps it) still lands in
+// the cell its neighbours search
+__device__ __forceinline__ int cell_of(float x, float L, float cell, int m) {
+    x -= L * floorf(x / L);
     int c = (int)(x / cell);
     return c < 0 ? 0 : (c >= m ? m - 1 : c);
 }
@@ -34,7 +38,7 @@ __global__ void k_cell_count(RefDev d, int cur) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= d.n_s) return;
     float4 p = d.spos[cur][s];
-    int k = (cell_of(p.x, d.cell, d.m) * d.m + cell_of(p.y, d.cell, d.m)) * d.m + cell_of(p.z, d.cell, d.m);
+    int k = (cell_of(p.x, d.L, d.cell, d.m) * d.m + cell_of(p.y, d.L, d.cell, d.m)) * d.m + cell_of(p.z, d.L, d.cell, d.m);
     d.sol_cell[s] = k;
     atomicAdd(&d.cell_count[k], 1u);
 }
@@ -95,7 +99,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_ss_list(RefDev d, int cur, int c
     const F3 pi = mk4(d.spos[cur][i]);
     const int m = d.m;
     const int span = m >= 3 ? 1 : 0;
-    const int cx = cell_of(pi.x, d.cell, m), cy = cell_of(pi.y, d.cell, m), cz = cell_of(pi.z, d.cell, m);
+    const int cx = cell_of(pi.x, d.L, d.cell, m), cy = cell_of(pi.y, d.L, d.cell, m), cz = cell_of(pi.z, d.L, d.cell, m);
     int cnt = 0;
     for (int dx = -span; dx <= span; dx++)
         for (int dy = -span; dy <= span; dy++)

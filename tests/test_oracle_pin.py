@@ -60,8 +60,11 @@ def test_oracle_multistep_matches_reference_fixtures(name):
     assert np.abs(s.solvents["pos"] - z["step4_solvents"]["pos"]).max() < 1e-5
 
 
-def test_cell_list_solvent_lists_equal_all_pairs():
-    s = S.make_system("tiny_solvent", seed=9)
+@pytest.mark.parametrize("name", ["tiny_solvent", "6lzm"])
+def test_cell_list_solvent_lists_equal_all_pairs(name):
+    # 6lzm: the reference's demo box, 18 of whose waters sit up to 0.01 nm
+    # outside [0, box_len] as loaded; cells are assigned from the wrapped image
+    s = S.load_6lzm() if name == "6lzm" else S.make_system(name, seed=9)
     a = po.ref_nlist(s, ss_cap=1024)
     b = po.ref_nlist(s, ss_cap=1024, cells=True)
     assert _lists_equal(a[3], b[3])
@@ -71,9 +74,9 @@ ref_needed = pytest.mark.skipif(not po.ref_available(), reason="reference build 
 
 
 @ref_needed
-@pytest.mark.parametrize("name", ["tiny_chains", "small_bridged", "tiny_solvent"])
+@pytest.mark.parametrize("name", ["tiny_chains", "small_bridged", "tiny_solvent", "6lzm"])
 def test_oracle_matches_reference_live(name):
-    s = S.make_system(name, seed=21)
+    s = S.load_6lzm() if name == "6lzm" else S.make_system(name, seed=21)
     ref = po.RefEngine(s, n_threads=4)
     ref.update_nlists()
     lists = po.ref_nlist(s, ss_cap=1024)
