@@ -595,6 +595,13 @@ lima_status lima_finish_box(lima_ctx* c) {
             const int rc = lima::phys_setup(h, c->phys, c->stream, c->dallocs, msg);
             if (rc != 0) fail(static_cast<lima_status>(rc), msg);
             lima::phys_rebuild(c->phys, c->cur, c->stream);
+            // a solute denser than the box average can overflow the first list:
+            // grow the capacity to the measured longest row once, and rebuild
+            if (lima::phys_fit_list(c->phys, c->stream, c->dallocs)) {
+                lima::phys_rebuild(c->phys, c->cur, c->stream);
+                c->launches += lima::kRebuildKernels;
+                c->host_rebuilds++;
+            }
             lima::phys_prime(c->phys, c->cur, c->stream);
             c->host_rebuilds++;
             sync_checked(c);

@@ -323,7 +323,10 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_build_list(PhysDev d, cons
     }
     if (have && sub == 0) {
         d.nl_cnt[i] = (uint32_t)min(cnt, d.nl_cap);
-        if (cnt > d.nl_cap) atomicOr(d.err, ERR_BIT_PHYS_LIST_OVERFLOW);
+        if (cnt > d.nl_cap) {
+            atomicOr(d.err, ERR_BIT_PHYS_LIST_OVERFLOW);
+            atomicMax(d.nl_need, cnt);
+        }
     }
 }
 

@@ -70,6 +70,7 @@ struct PhysDev {
     float4* pos_tmp; float4* vel_tmp; float4* posc_tmp; float4* velc_tmp; uint32_t* orig_tmp;
     // Verlet list (tile-local indices)
     uint32_t* nl; uint32_t* nl_cnt; int nl_cap;
+    int* nl_need;               // largest row length a build found beyond nl_cap (0: none)
     // dynamic lists (nlist_period <= 0): the pair kernel requests a rebuild
     // once a particle has moved more than skin/2 since the last one, and the
     // next step rebuilds before its forces (a conditional node of the step
@@ -116,6 +117,10 @@ void phys_rebuild(const PhysDev& d, int cur, cudaStream_t s);
 // list of `pos` (particle order unchanged; reference positions reset)
 void phys_rebuild_inplace(const PhysDev& d, const float4* pos, cudaStream_t s);
 void phys_prime(PhysDev& d, int cur, cudaStream_t s);
+// after a build: if a row overflowed the list capacity, grow the list to 1.25x
+// the longest row (the capacity starts from the box's mean density, which a
+// dense solute exceeds) and return true so the caller rebuilds; waits for s
+bool phys_fit_list(PhysDev& d, cudaStream_t s, std::vector<void*>& allocs);
 // dynamic lists: the step graph of parity `cur` ({check -> IF(rebuild)} || bonded -> pair);
 // returns the kernels of one replay without a rebuild, or -1 if the graph cannot be built
 int phys_capture_dynamic(const PhysDev& d, int cur, bool energy, cudaStream_t s, cudaGraphExec_t* out);

@@ -218,6 +218,7 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
         d.orig_tmp = dalloc<uint32_t>(allocs, d.n);
         d.nl = dalloc<uint32_t>(allocs, (size_t)d.nl_cap * d.n_pad);
         d.nl_cnt = dalloc<uint32_t>(allocs, d.n_pad);
+        d.nl_need = dalloc<int>(allocs, 1);
         d.excl_off = dalloc<uint32_t>(allocs, eoff.size());
         d.excl_ids = dalloc<uint32_t>(allocs, eids.size());
         d.bond_idx = dalloc<int4>(allocs, bidx.size());
@@ -264,6 +265,7 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
     cudaMemsetAsync(d.need_rebuild, 0, sizeof(int), s);
     cudaMemsetAsync(d.rebuild_count, 0, sizeof(unsigned long long), s);
     cudaMemsetAsync(d.nl_cnt, 0, sizeof(uint32_t) * d.n_pad, s);
+    cudaMemsetAsync(d.nl_need, 0, sizeof(int), s);
     cudaMemsetAsync(d.force, 0, sizeof(float4) * d.n_pad, s);
     phys_upload_state(h, d, 0, s);
     return cudaGetLastError() == cudaSuccess ? 0 : LIMA_ERR_CUDA;
@@ -347,6 +349,30 @@ void phys_rebuild_inplace(const PhysDev& d, const float4* pos, cudaStream_t s) {
 }
 
 void phys_prime(PhysDev&, int, cudaStream_t) {}
+
+bool phys_fit_list(PhysDev& d, cudaStream_t s, std::vector<void*>& allocs) {
+    int err = 0, need = 0;
+    cudaMemcpyAsync(&err, d.err, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&need, d.nl_need, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    if (!(err & ERR_BIT_PHYS_LIST_OVERFLOW) || need <= d.nl_cap) return false;
+    const int cap = std::min((d.n + kGroup - 1) / kGroup * kGroup, ((need * 5 / 4 + 32) / kGroup + 1) * kGroup);
+    uint32_t* nl = dalloc<uint32_t>(allocs, (size_t)cap * d.n_pad);   // throws like the other allocations
+    for (auto it = allocs.begin(); it != allocs.end(); ++it)
+        if (*it == d.nl) {
+            cudaFree(d.nl);
+            allocs.erase(it);
+            break;
+        }
+    d.nl = nl;
+    d.nl_cap = cap;
+    const int zero = 0;
+    const int keep = err & ~ERR_BIT_PHYS_LIST_OVERFLOW;
+    cudaMemcpyAsync(d.err, &keep, sizeof(int), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d.nl_need, &zero, sizeof(int), cudaMemcpyHostToDevice, s);
+    cudaStreamSynchronize(s);
+    return true;
+}
 
 bool phys_rebuild_pending(const PhysDev& d, cudaStream_t s) {
     int h = 0;
