@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -263,6 +264,20 @@ void ref_setup(lima_ctx* c) {
     d.sol_cell = c->dalloc<uint32_t>(ns);
     d.n_chunks = (d.cs_cap + lima::kCsChunk - 1) / lima::kCsChunk;
     d.cs_partial = c->dalloc<float4>(static_cast<size_t>(nc) * d.n_chunks * lima::kMaxCP);
+    d.cc_partial = c->dalloc<float4>(static_cast<size_t>(nc) * (1 + lima::kMaxCP) * lima::kMaxCP);
+    {   // enough lanes per solvent to fill the SMs, at most one wave of 1,024 threads per SM
+        int dev = 0, n_sm = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+        d.sol_lanes = 1;
+        while (d.sol_lanes < 16 && static_cast<size_t>(ns) * d.sol_lanes * 2 <= static_cast<size_t>(n_sm) * 1024)
+            d.sol_lanes *= 2;
+        // LIMA_SOLVENT_LANES=1|2|4|8|16 overrides the choice (results do not depend on it)
+        if (const char* e = std::getenv("LIMA_SOLVENT_LANES")) {
+            const int w = std::atoi(e);
+            if (w == 1 || w == 2 || w == 4 || w == 8 || w == 16) d.sol_lanes = w;
+        }
+    }
     d.force_c = c->dalloc<float4>(ncp);
     d.force_s = c->dalloc<float4>(ns);
     d.potE = c->dalloc<double>(ncp);

@@ -6,20 +6,25 @@
 // (:1168-1223), compoundKernel (:880-1057) and solventForceKernel
 // (:1070-1161).  Its compoundKernel uses one 64-thread block per compound for
 // everything — bonded terms accumulated one thread at a time behind 64
-// __syncthreads per term type, and ~3,000 compound<-solvent pairs per particle
-// — so a 16-compound box keeps 16 of 148 SMs busy.  Here:
+// __syncthreads per term type, intra- and inter-compound LJ and ~3,000
+// compound<-solvent pairs per particle — and its solventForceKernel one
+// thread per solvent, so a 36-compound, 5,000-water box keeps a few of 148
+// SMs busy.  Here every float sum keeps the reference's order, and:
 //   k_bridge        one 32-thread block per bridge, as the reference;
-//   k_cs_partial    compound<-solvent LJ split over (compound, 256-neighbour
-//                   chunk) blocks, solvent positions staged in shared memory;
+//   k_partials      the LJ sums of each compound particle split over
+//                   (source, compound) blocks: 256-neighbour chunks of the
+//                   compound's solvent list, its own particles, each
+//                   compound-list entry;
 //   k_compound      bonded terms computed one thread per term into shared
 //                   memory and summed per atom in term order (the order the
-//                   reference's serialised loop produces), intra- and
-//                   inter-compound LJ, the chunk partials, Stormer-Verlet,
-//                   PBC;
-//   k_solvent       one thread per solvent: all compound particles (staged
-//                   16 compounds at a time) + the solvent list, read
-//                   column-major so each warp's list reads coalesce.
-// k_solvent is independent of k_cs_partial/k_compound (both read the current
+//                   reference's serialised loop produces), the LJ partials
+//                   added in the reference's order, Stormer-Verlet, PBC;
+//   k_solvent<W>    W = 1..16 lanes per solvent over its two ordered loops
+//                   (all compound particles, staged 16 compounds at a time;
+//                   the solvent list, read column-major), image chain
+//                   replayed and partial terms added in order through warp
+//                   shuffles.
+// k_solvent is independent of k_partials/k_compound (both read the current
 // buffers and write the next ones).
 #include "refdev.cuh"
 #include "refmath.cuh"
@@ -102,37 +107,93 @@ __global__ void __launch_bounds__(32) k_bridge(RefDev d, int cur) {
     if (t < n) d.cbridge[br.particle_refs[t].compound_id * kMaxCP + br.particle_refs[t].local_id_compound] = to4(force);
 }
 
-// compound <- solvent LJ over one chunk of the compound's solvent list
-// (computeSolventToCompoundLJForces, Engine.cu:721-730, 965-973).
-__global__ void __launch_bounds__(64) k_cs_partial(RefDev d, int cur) {
+// The LJ sums each compound particle receives, one block per (partial sum,
+// compound), blockIdx.y the compound:
+//   blockIdx.x <  n_chunks      compound <- solvent over one 256-entry chunk
+//                               of the compound's solvent list
+//                               (computeSolventToCompoundLJForces,
+//                               Engine.cu:721-730, 965-973);
+//   blockIdx.x == n_chunks      intramolecular LJ
+//                               (computeIntramolecularLJForces, Engine.cu:678-700);
+//   blockIdx.x == n_chunks+1+k  compound <- compound-list entry k
+//                               (computerIntermolecularLJForces,
+//                               Engine.cu:653-676, 939-958).
+// Each is one of the reference's inner-loop sums for one particle, in its
+// order; k_compound adds them to the particle's force in the reference's
+// order, so the force is the reference's float sum.
+__global__ void __launch_bounds__(64) k_partials(RefDev d, int cur) {
     __shared__ F3 buf[kCsChunk];
-    const int c = blockIdx.y, k = blockIdx.x, t = threadIdx.x;
-    const int cnt = d.cs_cnt[c];
-    const int begin = k * kCsChunk;
-    if (begin >= cnt) return;
-    const int len_ = min(kCsChunk, cnt - begin);
+    __shared__ lima_particle_parameters opar[kMaxCP];
+    const int c = blockIdx.y, t = threadIdx.x;
+    const lima_compound& cp = d.comps[c];
+    const int n = cp.n_particles;
     const F3 p0 = mk4(d.cpos[cur][c * kMaxCP]);
-    for (int q = t; q < len_; q += 64) {
-        F3 v = mk4(d.spos[cur][d.cs_ids[(size_t)c * d.cs_cap + begin + q]]);
-        hyperpos(p0, v, d.L, d.Lh);
-        buf[q] = v;
+    if ((int)blockIdx.x < d.n_chunks) {
+        const int cnt = d.cs_cnt[c];
+        const int begin = blockIdx.x * kCsChunk;
+        if (begin >= cnt) return;
+        const int len_ = min(kCsChunk, cnt - begin);
+        for (int q = t; q < len_; q += 64) {
+            F3 v = mk4(d.spos[cur][d.cs_ids[(size_t)c * d.cs_cap + begin + q]]);
+            hyperpos(p0, v, d.L, d.Lh);
+            buf[q] = v;
+        }
+        __syncthreads();
+        if (t >= n) return;
+        F3 pt = mk4(d.cpos[cur][c * kMaxCP + t]);
+        if (t > 0) hyperpos(p0, pt, d.L, d.Lh);
+        const lima_particle_parameters a = d.pp[cp.atom_types[t]];
+        const lima_particle_parameters sol = d.pp[LIMA_ATOMTYPE_SOL];
+        const float sg = mix_sigma(a.sigma, sol.sigma), ep = eps_geo(a.epsilon, sol.epsilon);
+        F3 acc = mk(0.f, 0.f, 0.f);
+        for (int q = 0; q < len_; q++) acc = add(acc, lj_force(pt, buf[q], sg, ep));
+        d.cs_partial[((size_t)c * d.n_chunks + blockIdx.x) * kMaxCP + t] = to4(acc);
+        return;
+    }
+    const int k = (int)blockIdx.x - d.n_chunks;   // 0: intramolecular, 1 + e: list entry e
+    if (k > (int)d.cc_cnt[c]) return;
+    const int nb = k == 0 ? c : (int)d.cc_ids[c * kMaxCP + k - 1];
+    const lima_compound& ncp = d.comps[nb];
+    const int nn = ncp.n_particles;
+    if (t < nn) {
+        F3 v = mk4(d.cpos[cur][nb * kMaxCP + t]);
+        // own particles move to particle 0's image except particle 0 itself;
+        // every particle of another compound does
+        if (k != 0 || t > 0) hyperpos(p0, v, d.L, d.Lh);
+        buf[t] = v;
+        opar[t] = d.pp[ncp.atom_types[t]];
     }
     __syncthreads();
-    const lima_compound& cp = d.comps[c];
-    if (t >= cp.n_particles) return;
+    if (t >= n) return;
     F3 pt = mk4(d.cpos[cur][c * kMaxCP + t]);
     if (t > 0) hyperpos(p0, pt, d.L, d.Lh);
     const lima_particle_parameters a = d.pp[cp.atom_types[t]];
-    const lima_particle_parameters sol = d.pp[LIMA_ATOMTYPE_SOL];
-    const float sg = mix_sigma(a.sigma, sol.sigma), ep = eps_geo(a.epsilon, sol.epsilon);
+    // which particles of compound nb this particle ignores (LJ_Ignores::ignore, Bodies.cuh:191-197)
+    unsigned long long msk = 0ull;
+    {
+        const lima_lj_ignores& ig = cp.lj_ignore_list[t];
+        for (int q = 0; q < ig.n_ignores; q++)
+            if (ig.compound_ids[q] == (uint8_t)nb) msk |= 1ull << ig.local_ids[q];
+    }
     F3 acc = mk(0.f, 0.f, 0.f);
-    for (int q = 0; q < len_; q++) acc = add(acc, lj_force(pt, buf[q], sg, ep));
-    d.cs_partial[((size_t)c * d.n_chunks + k) * kMaxCP + t] = to4(acc);
+    if (k == 0) {
+        for (int i = 0; i < nn; i++) {
+            if (i == t || ((msk >> i) & 1ull)) continue;
+            const lima_particle_parameters o = opar[i];
+            acc = add(acc, lj_force(pt, buf[i], mix_sigma(a.sigma, o.sigma), eps_geo(a.epsilon, o.epsilon)));
+        }
+    } else {
+        for (int j = 0; j < nn; j++) {
+            if ((msk >> j) & 1ull) continue;
+            const lima_particle_parameters o = opar[j];
+            acc = add(acc, lj_force(pt, buf[j], mix_sigma(a.sigma, o.sigma), eps_arith(a.epsilon, o.epsilon)));
+        }
+    }
+    d.cc_partial[((size_t)c * (1 + kMaxCP) + k) * kMaxCP + t] = to4(acc);
 }
 
 __global__ void __launch_bounds__(64) k_compound(RefDev d, int cur) {
     __shared__ F3 pos[kMaxCP];
-    __shared__ F3 nbuf[kMaxCP];
     __shared__ BondedScratch<64, LIMA_MAX_PAIRBONDS, LIMA_MAX_ANGLEBONDS, LIMA_MAX_DIHEDRALS> sc;
     const int c = blockIdx.x, t = threadIdx.x;
     const lima_compound& cp = d.comps[c];
@@ -164,21 +225,6 @@ __global__ void __launch_bounds__(64) k_compound(RefDev d, int cur) {
         dihedral(pos[db.atom_indexes[0]], pos[db.atom_indexes[1]], pos[db.atom_indexes[2]], pos[db.atom_indexes[3]],
                  db.phi_0, db.k_phi, db.n, sc.rd[q], potE);
     }
-    // own particle parameters, and this particle's LJ_Ignores in shared memory
-    __shared__ lima_particle_parameters spar[kMaxCP];
-    __shared__ lima_particle_parameters npar[kMaxCP];
-    __shared__ uint8_t ig_local[kMaxCP][LIMA_LJ_IGNORES_MAX];
-    __shared__ uint8_t ig_comp[kMaxCP][LIMA_LJ_IGNORES_MAX];
-    int n_ig = 0;
-    if (t < n) {
-        spar[t] = d.pp[cp.atom_types[t]];
-        const lima_lj_ignores& ig = cp.lj_ignore_list[t];
-        n_ig = ig.n_ignores;
-        for (int q = 0; q < n_ig; q++) {
-            ig_local[t][q] = ig.local_ids[q];
-            ig_comp[t][q] = ig.compound_ids[q];
-        }
-    }
     __syncthreads();
     // per-atom sums in the reference's order: the bonds in index order, then
     // the angles, then the dihedrals (Engine.cu:765-771, 799-806, 834-842)
@@ -202,51 +248,13 @@ __global__ void __launch_bounds__(64) k_compound(RefDev d, int cur) {
             kind++;
         }
     }
-    const lima_particle_parameters a = t < n ? spar[t] : d.pp[0];
-    // which particles of compound `cid` this particle ignores (LJ_Ignores::ignore, Bodies.cuh:191-197)
-    auto ignore_mask = [&](int cid) {
-        unsigned long long msk = 0ull;
-        for (int q = 0; q < n_ig; q++)
-            if (ig_comp[t][q] == (uint8_t)cid) msk |= 1ull << ig_local[t][q];
-        return msk;
-    };
-    // computeIntramolecularLJForces (Engine.cu:678-700)
     if (t < n) {
-        const unsigned long long msk = ignore_mask(c);
-        F3 acc = mk(0.f, 0.f, 0.f);
-        for (int i = 0; i < n; i++) {
-            if (i == t || ((msk >> i) & 1ull)) continue;
-            const lima_particle_parameters o = spar[i];
-            acc = add(acc, lj_force(pos[t], pos[i], mix_sigma(a.sigma, o.sigma), eps_geo(a.epsilon, o.epsilon)));
-        }
-        force = add(force, acc);
-    }
-    // computerIntermolecularLJForces over the compound list (Engine.cu:653-676, 939-958)
-    const int ncc = d.cc_cnt[c];
-    for (int k = 0; k < ncc; k++) {
-        const int nb = d.cc_ids[c * kMaxCP + k];
-        const int nn = d.comps[nb].n_particles;
-        __syncthreads();
-        if (t < nn) {
-            F3 v = mk4(d.cpos[cur][nb * kMaxCP + t]);
-            hyperpos(p0, v, d.L, d.Lh);
-            nbuf[t] = v;
-            npar[t] = d.pp[d.comps[nb].atom_types[t]];
-        }
-        __syncthreads();
-        if (t < n) {
-            const unsigned long long msk = ignore_mask(nb);
-            F3 acc = mk(0.f, 0.f, 0.f);
-            for (int j = 0; j < nn; j++) {
-                if ((msk >> j) & 1ull) continue;
-                const lima_particle_parameters o = npar[j];
-                acc = add(acc, lj_force(pos[t], nbuf[j], mix_sigma(a.sigma, o.sigma), eps_arith(a.epsilon, o.epsilon)));
-            }
-            force = add(force, acc);
-        }
-    }
-    // compound <- solvent partial sums, in chunk order
-    if (t < n) {
+        // LJ in the reference's order: intramolecular, each compound-list
+        // entry, then the compound <- solvent chunks (k_partials)
+        const float4* part = d.cc_partial + (size_t)c * (1 + kMaxCP) * kMaxCP + t;
+        force = add(force, mk4(part[0]));
+        const int ncc = d.cc_cnt[c];
+        for (int k = 1; k <= ncc; k++) force = add(force, mk4(part[(size_t)k * kMaxCP]));
         const int nch = (d.cs_cnt[c] + kCsChunk - 1) / kCsChunk;
         F3 acc = mk(0.f, 0.f, 0.f);
         for (int k = 0; k < nch; k++) acc = add(acc, mk4(d.cs_partial[((size_t)c * d.n_chunks + k) * kMaxCP + t]));
@@ -256,7 +264,7 @@ __global__ void __launch_bounds__(64) k_compound(RefDev d, int cur) {
     // integratePosition (Engine.cu:981-984)
     if (t < n) {
         F3 prev = mk4(d.cprev[c * kMaxCP + t]);
-        integrate(pos[t], prev, force, (double)a.mass, d.dt, *d.lambda, d.L, d.Lh);
+        integrate(pos[t], prev, force, (double)d.pp[cp.atom_types[t]].mass, d.dt, *d.lambda, d.L, d.Lh);
         d.cprev[c * kMaxCP + t] = to4(prev);
         d.force_c[c * kMaxCP + t] = to4(force);
         if (len(force) > 2e12f) atomicOr(d.err, ERR_BIT_CRITICAL_FORCE);
@@ -275,12 +283,48 @@ __global__ void __launch_bounds__(64) k_compound(RefDev d, int cur) {
 
 constexpr int kSolBlock = 128;
 constexpr int kStageCompounds = 16;
+constexpr int kStageStride = kMaxCP + 1;   // lanes on different staged compounds read different banks
 
+__device__ __forceinline__ F3 shfl3(unsigned mask, F3 v, int src, int width) {
+    return mk(__shfl_sync(mask, v.x, src, width), __shfl_sync(mask, v.y, src, width), __shfl_sync(mask, v.z, src, width));
+}
+
+// applyHyperpos with the same arithmetic, telling whether any component
+// moved by a box length.
+__device__ __forceinline__ bool hyperpos_moved(const F3& s, F3& m, float L, float Lh) {
+    bool moved = false;
+    auto one = [&](float sv, float& mv) {
+        const bool a = (sv - mv) > Lh;
+        mv += L * (float)a;
+        const bool b = (sv - mv) < -Lh;
+        mv -= L * (float)b;
+        moved |= a | b;
+    };
+    one(s.x, m.x);
+    one(s.y, m.y);
+    one(s.z, m.z);
+    return moved;
+}
+
+// solventForceKernel (Engine.cu:1070-1161) with W lanes per solvent.  The
+// reference's solvent loops are two ordered chains: over every compound
+// (computeLJForces, Engine.cu:1099-1117; no list) the solvent moves to the
+// image nearest the compound's particle 0 and adds that compound's LJ sum;
+// over the solvent list (computeSolventToSolventLJForces, Engine.cu:706-720)
+// it moves to each neighbour's image and adds the pair force.  Lane j takes
+// compounds / neighbours j, j+W, ...; every lane replays the image chain
+// (one hyperpos per compound; per neighbour block only when some neighbour
+// of the block moves the image, the others leave it unchanged) and the
+// lanes' terms are added in the reference's order through shuffles, so the
+// result is the reference's float sum whatever W is.
+template <int W>
 __global__ void __launch_bounds__(kSolBlock) k_solvent(RefDev d, int cur) {
-    __shared__ F3 cbuf[kStageCompounds * kMaxCP];
-    __shared__ lima_particle_parameters cpar[kStageCompounds * kMaxCP];
+    __shared__ float4 cbuf[kStageCompounds * kStageStride];   // x, y, z, sigma mixed with the solvent's
+    __shared__ float cep[kStageCompounds * kStageStride];     // epsilon mixed with the solvent's
     __shared__ int cn[kStageCompounds];
-    const int s = blockIdx.x * kSolBlock + threadIdx.x;
+    const int j = threadIdx.x % W;
+    const int s = blockIdx.x * (kSolBlock / W) + threadIdx.x / W;
+    const unsigned gmask = W == 32 ? 0xffffffffu : (((1u << W) - 1u) << ((threadIdx.x % 32) & ~(W - 1)));
     const bool active = s < d.n_s;
     F3 pos = mk(0.f, 0.f, 0.f), prev = pos;
     if (active) {
@@ -289,54 +333,93 @@ __global__ void __launch_bounds__(kSolBlock) k_solvent(RefDev d, int cur) {
     }
     const lima_particle_parameters sol = d.pp[LIMA_ATOMTYPE_SOL];
     F3 force = mk(0.f, 0.f, 0.f);
-    // solvent <- every compound particle, no list (computeLJForces, Engine.cu:1099-1117)
+    // solvent <- every compound particle, staged 16 compounds at a time
     for (int c0 = 0; c0 < d.n_c; c0 += kStageCompounds) {
         const int nst = min(kStageCompounds, d.n_c - c0);
         __syncthreads();
         for (int q = threadIdx.x; q < nst * kMaxCP; q += kSolBlock) {
-            const int c = c0 + q / kMaxCP, l = q % kMaxCP;
-            const lima_compound& cp = d.comps[c];
+            const int cc = q / kMaxCP, l = q % kMaxCP;
+            const lima_compound& cp = d.comps[c0 + cc];
             if (l < cp.n_particles) {
-                cbuf[q] = mk4(d.cpos[cur][c * kMaxCP + l]);
-                cpar[q] = d.pp[cp.atom_types[l]];
+                const float4 v = d.cpos[cur][(c0 + cc) * kMaxCP + l];
+                const lima_particle_parameters o = d.pp[cp.atom_types[l]];
+                cbuf[cc * kStageStride + l] = make_float4(v.x, v.y, v.z, mix_sigma(sol.sigma, o.sigma));
+                cep[cc * kStageStride + l] = eps_arith(sol.epsilon, o.epsilon);
             }
-            if (l == 0) cn[q / kMaxCP] = cp.n_particles;
+            if (l == 0) cn[cc] = cp.n_particles;
         }
         __syncthreads();
-        if (active) {
-            for (int cc = 0; cc < nst; cc++) {
-                const F3* P = &cbuf[cc * kMaxCP];
-                hyperpos(P[0], pos, d.L, d.Lh);
-                F3 acc = mk(0.f, 0.f, 0.f);
-                const int nn = cn[cc];
+        for (int b = 0; b < nst; b += W) {   // compounds b .. b+nv-1, compound b+j on lane j
+            const int nv = min(W, nst - b);
+            F3 mine = pos;
+            for (int q = 0; q < nv; q++) {
+                const float4 k0 = cbuf[(b + q) * kStageStride];
+                hyperpos(mk(k0.x, k0.y, k0.z), pos, d.L, d.Lh);
+                if (q == j) mine = pos;
+            }
+            F3 acc = mk(0.f, 0.f, 0.f);
+            if (active && j < nv) {
+                const float4* P = &cbuf[(b + j) * kStageStride];
+                const float* EP = &cep[(b + j) * kStageStride];
+                const int nn = cn[b + j];
                 for (int i = 0; i < nn; i++) {
-                    const lima_particle_parameters o = cpar[cc * kMaxCP + i];
-                    acc = add(acc, lj_force(pos, P[i], mix_sigma(sol.sigma, o.sigma), eps_arith(sol.epsilon, o.epsilon)));
+                    const float4 pi = P[i];
+                    acc = add(acc, lj_force(mine, mk(pi.x, pi.y, pi.z), pi.w, EP[i]));
                 }
+            }
+            if (W == 1) {
                 force = add(force, acc);
+            } else {
+                for (int q = 0; q < nv; q++) force = add(force, shfl3(gmask, acc, q, W));
             }
         }
     }
-    if (!active) return;
-    // computeSolventToSolventLJForces (Engine.cu:706-720): self moves to each neighbour's image
+    if (!active) return;   // a solvent's W lanes leave together
+    // solvent <- solvent list, read column-major
     {
         F3 acc = mk(0.f, 0.f, 0.f);
         const int cnt = d.ss_cnt[s];
         const float sg = sol.sigma, ep = sol.epsilon;
-        for (int k = 0; k < cnt; k++) {
-            const uint32_t j = d.ss_ids[(size_t)k * d.n_s + s];
-            const F3 nb = mk4(__ldg(&d.spos[cur][j]));
-            hyperpos(nb, pos, d.L, d.Lh);
-            acc = add(acc, lj_force(pos, nb, sg, ep));
+        for (int k0 = 0; k0 < cnt; k0 += W) {
+            const int nv = min(W, cnt - k0);
+            F3 nb = pos;
+            if (j < nv) nb = mk4(__ldg(&d.spos[cur][d.ss_ids[(size_t)(k0 + j) * d.n_s + s]]));
+            F3 mine = pos;
+            const bool moved = hyperpos_moved(nb, mine, d.L, d.Lh);
+            if (W == 1) {
+                pos = mine;
+            } else if (__any_sync(gmask, moved)) {   // replay the block's chain in order
+                for (int q = 0; q < nv; q++) {
+                    hyperpos(shfl3(gmask, nb, q, W), pos, d.L, d.Lh);
+                    if (q == j) mine = pos;
+                }
+            } else {   // no neighbour moves the image: every step of the chain gives this value
+                pos = mine;
+            }
+            F3 f = mk(0.f, 0.f, 0.f);
+            if (j < nv) f = lj_force(mine, nb, sg, ep);
+            if (W == 1) {
+                acc = add(acc, f);
+            } else {
+                for (int q = 0; q < nv; q++) acc = add(acc, shfl3(gmask, f, q, W));
+            }
         }
         force = add(force, acc);
     }
+    // every lane holds the same state; lane 0 stores it
     integrate(pos, prev, force, (double)sol.mass, d.dt, *d.lambda, d.L, d.Lh);
     apply_pbc(pos, d.L);
+    if (j != 0) return;
     flag_nan(d, pos);
     d.spos[cur ^ 1][s] = to4(pos);
     d.sprev[cur ^ 1][s] = to4(prev);
     d.force_s[s] = to4(force);
+}
+
+template <int W>
+void launch_solvent(const RefDev& d, int cur, cudaStream_t s) {
+    constexpr int per_block = kSolBlock / W;
+    k_solvent<W><<<(d.n_s + per_block - 1) / per_block, kSolBlock, 0, s>>>(d, cur);
 }
 
 // Engine::getBoxTemperature's KE term (LIMAENG::calcKineticEnergy,
@@ -396,16 +479,19 @@ int ref_step_kernels(const RefDev& d, int cur, cudaStream_t s, cudaEvent_t* ev) 
     }
     if (ev) cudaEventRecord(ev[1], s);
     if (d.n_c > 0) {
-        if (d.n_s > 0) {
-            k_cs_partial<<<dim3(d.n_chunks, d.n_c), 64, 0, s>>>(d, cur);
-            launched++;
-        }
+        k_partials<<<dim3(d.n_chunks + 1 + kMaxCP, d.n_c), 64, 0, s>>>(d, cur);
         k_compound<<<d.n_c, 64, 0, s>>>(d, cur);
-        launched++;
+        launched += 2;
     }
     if (ev) cudaEventRecord(ev[2], s);
     if (d.n_s > 0) {
-        k_solvent<<<(d.n_s + kSolBlock - 1) / kSolBlock, kSolBlock, 0, s>>>(d, cur);
+        switch (d.sol_lanes) {
+            case 16: launch_solvent<16>(d, cur, s); break;
+            case 8: launch_solvent<8>(d, cur, s); break;
+            case 4: launch_solvent<4>(d, cur, s); break;
+            case 2: launch_solvent<2>(d, cur, s); break;
+            default: launch_solvent<1>(d, cur, s); break;
+        }
         launched++;
     }
     if (ev) cudaEventRecord(ev[3], s);

@@ -50,6 +50,11 @@ struct RefDev {
     uint32_t* cell_count; uint32_t* cell_start; uint32_t* cell_fill; uint32_t* cell_items; uint32_t* sol_cell;
     // compound <- solvent partial sums [n_c][n_chunks][64]
     float4* cs_partial; int n_chunks;
+    // compound LJ partial sums [n_c][1 + 64][64]: slot 0 the intramolecular
+    // sum, slot 1 + k the sum over compound-list entry k
+    float4* cc_partial;
+    // lanes per solvent in the solvent kernel (1, 2, 4, 8 or 16)
+    int sol_lanes;
     // outputs of the last step
     float4* force_c;         // [n_c*64]
     float4* force_s;         // [n_s]

@@ -88,6 +88,40 @@ def test_one_step_matches_oracle(gpu, name):
         _check_step(s, eng, fc_o, fs_o, pe_o, new.states, new.compounds["prev_positions"], new.solvents)
 
 
+_ORACLE_STEP = {}
+
+
+def _oracle_step(name):
+    if name not in _ORACLE_STEP:
+        s = S.load_6lzm() if name == "6lzm" else S.make_system(name, seed=7)
+        lists = po.ref_nlist(s, ss_cap=1024, cells=True)
+        _ORACLE_STEP[name] = (s, po.ref_step(s, lists))
+    return _ORACLE_STEP[name]
+
+
+# The solvent kernel splits each solvent's ordered loops over 1-16 lanes;
+# the image chain is replayed and the lanes' terms added in order, so the
+# solvent path stays the oracle's (and the reference's) float arithmetic.
+@pytest.mark.parametrize("lanes", [1, 2, 4, 8, 16])
+@pytest.mark.parametrize("name", ["small_bridged", "lj_solvent_4096", "6lzm"])
+def test_solvent_path_bit_identical_at_every_lane_count(gpu, name, lanes, monkeypatch):
+    E = gpu
+    monkeypatch.setenv("LIMA_SOLVENT_LANES", str(lanes))
+    s, (new, fc_o, fs_o, pe_o) = _oracle_step(name)
+    with _engine(E, s) as eng:
+        eng.step(1)
+        fc, fs = eng.forces()
+        sol = eng.solvents()
+        st, _ = eng.compound_states()
+    np.testing.assert_array_equal(fs, fs_o)
+    np.testing.assert_array_equal(sol["pos"], new.solvents["pos"])
+    np.testing.assert_array_equal(sol["pos_tsub1"], new.solvents["pos_tsub1"])
+    if s.n_compounds:
+        m = compound_mask(s)
+        assert relrms(fc[m], fc_o[m]) < FORCE_TOL
+        assert np.abs(st["positions"][m] - new.states["positions"][m]).max() < 1e-5
+
+
 def test_multistep_with_list_rebuilds_matches_oracle(gpu):
     E = gpu
     s = S.make_system("small_bridged", seed=3)
