@@ -74,8 +74,12 @@ def run_kernels_only(args):
     import torch
     from quantom_b200 import engine as E
     from quantom_b200 import systems as S
-    spec = S.CONFIGS[args.workload]
-    system = S.make_system(args.workload, seed=args.seed)
+    if args.workload == "6lzm":   # the reference's demo box, as its input path builds it
+        system = S.load_6lzm()
+        spec = system.spec
+    else:
+        spec = S.CONFIGS[args.workload]
+        system = S.make_system(args.workload, seed=args.seed)
     if args.semantics == "adjoint":
         # one loss + adjoint gradient pass: args.steps unrolled NVE steps, checkpoints every 10
         p = physics_params(E, spec, E.PRECISION_FP32, None, 0)

@@ -74,6 +74,7 @@ struct lima_ctx {
     lima::PhysParams params;
     lima::AdjBuffers adj;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    lima::StepFork fork;       // reference semantics: solvent kernel beside the compound kernels
     bool timed = false;
     bool lambda_pending_reset = false;
     float ref_temperature = 0.f;
@@ -99,6 +100,9 @@ struct lima_ctx {
         for (void* ptr : dallocs) cudaFree(ptr);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        if (fork.fork) cudaEventDestroy(fork.fork);
+        if (fork.join) cudaEventDestroy(fork.join);
+        if (fork.side) cudaStreamDestroy(fork.side);
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
 };
@@ -341,7 +345,9 @@ void capture_graphs(lima_ctx* c, void (*launch)(lima_ctx*, int)) {
     }
 }
 
-void ref_launch_step(lima_ctx* c, int parity) { c->graph_kernels = lima::ref_step_kernels(c->ref, parity, c->stream); }
+void ref_launch_step(lima_ctx* c, int parity) {
+    c->graph_kernels = lima::ref_step_kernels(c->ref, parity, c->stream, nullptr, &c->fork);
+}
 void phys_launch_step(lima_ctx* c, int parity) {
     c->graph_kernels = lima::phys_step_kernels(c->phys, parity, c->stream);
 }
@@ -401,7 +407,7 @@ void one_step(lima_ctx* c, cudaEvent_t* prof) {
             cuda_ok(cudaGraphLaunch(c->graph[c->cur], c->stream), "cudaGraphLaunch");
             c->launches += c->graph_kernels;
         } else {
-            c->launches += lima::ref_step_kernels(d, c->cur, c->stream, prof ? prof + 2 : nullptr);
+            c->launches += lima::ref_step_kernels(d, c->cur, c->stream, prof ? prof + 2 : nullptr, &c->fork);
         }
         c->cur ^= 1;
         c->step++;
@@ -529,6 +535,9 @@ lima_status lima_create(const lima_params* params, lima_ctx** out) {
         }
         cuda_ok(cudaEventCreate(&c->ev0), "cudaEventCreate");
         cuda_ok(cudaEventCreate(&c->ev1), "cudaEventCreate");
+        cuda_ok(cudaStreamCreateWithFlags(&c->fork.side, cudaStreamNonBlocking), "cudaStreamCreate");
+        cuda_ok(cudaEventCreateWithFlags(&c->fork.fork, cudaEventDisableTiming), "cudaEventCreate");
+        cuda_ok(cudaEventCreateWithFlags(&c->fork.join, cudaEventDisableTiming), "cudaEventCreate");
     });
     if (st != LIMA_OK) {
         fprintf(stderr, "lima_create: %s\n", c->err.c_str());

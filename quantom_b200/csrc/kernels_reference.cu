@@ -422,6 +422,17 @@ void launch_solvent(const RefDev& d, int cur, cudaStream_t s) {
     k_solvent<W><<<(d.n_s + per_block - 1) / per_block, kSolBlock, 0, s>>>(d, cur);
 }
 
+int launch_solvent_kernel(const RefDev& d, int cur, cudaStream_t s) {
+    switch (d.sol_lanes) {
+        case 16: launch_solvent<16>(d, cur, s); break;
+        case 8: launch_solvent<8>(d, cur, s); break;
+        case 4: launch_solvent<4>(d, cur, s); break;
+        case 2: launch_solvent<2>(d, cur, s); break;
+        default: launch_solvent<1>(d, cur, s); break;
+    }
+    return 1;
+}
+
 // Engine::getBoxTemperature's KE term (LIMAENG::calcKineticEnergy,
 // Engine.cuh:32-45): positions two steps apart, central-difference speed.
 __global__ void k_ref_ke(RefDev d, int cur) {
@@ -469,9 +480,19 @@ __global__ void k_snapshot(RefDev d, int cur) {
 }  // namespace
 
 // ev (nullable): events recorded before the bridges, after them, after the
-// compound kernels and after the solvent kernel.  Returns kernels launched.
-int ref_step_kernels(const RefDev& d, int cur, cudaStream_t s, cudaEvent_t* ev) {
+// compound kernels and after the solvent kernel (the kernels then run one
+// after another).  Without ev and with fk the solvent kernel runs on
+// fk->side beside the bridge and compound kernels, joined before return.
+// Returns kernels launched.
+int ref_step_kernels(const RefDev& d, int cur, cudaStream_t s, cudaEvent_t* ev, const StepFork* fk) {
     int launched = 0;
+    const bool forked = !ev && fk && fk->side && d.n_s > 0 && (d.n_c > 0 || d.n_b > 0);
+    if (forked) {
+        cudaEventRecord(fk->fork, s);
+        cudaStreamWaitEvent(fk->side, fk->fork, 0);
+        launched += launch_solvent_kernel(d, cur, fk->side);
+        cudaEventRecord(fk->join, fk->side);
+    }
     if (ev) cudaEventRecord(ev[0], s);
     if (d.n_b > 0) {
         k_bridge<<<d.n_b, 32, 0, s>>>(d, cur);
@@ -484,16 +505,10 @@ int ref_step_kernels(const RefDev& d, int cur, cudaStream_t s, cudaEvent_t* ev) 
         launched += 2;
     }
     if (ev) cudaEventRecord(ev[2], s);
-    if (d.n_s > 0) {
-        switch (d.sol_lanes) {
-            case 16: launch_solvent<16>(d, cur, s); break;
-            case 8: launch_solvent<8>(d, cur, s); break;
-            case 4: launch_solvent<4>(d, cur, s); break;
-            case 2: launch_solvent<2>(d, cur, s); break;
-            default: launch_solvent<1>(d, cur, s); break;
-        }
-        launched++;
-    }
+    if (forked)
+        cudaStreamWaitEvent(s, fk->join, 0);
+    else if (d.n_s > 0)
+        launched += launch_solvent_kernel(d, cur, s);
     if (ev) cudaEventRecord(ev[3], s);
     return launched;
 }

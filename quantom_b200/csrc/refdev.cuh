@@ -74,7 +74,14 @@ struct RefDev {
 // nlist_reference.cu
 void ref_build_nlists(const RefDev& d, int cur, cudaStream_t s);
 // kernels_reference.cu
-int ref_step_kernels(const RefDev& d, int cur, cudaStream_t s, cudaEvent_t* ev = nullptr);
+// A second stream and two events: the solvent kernel runs beside the
+// compound kernels (they read the same current buffers and write disjoint
+// next ones).
+struct StepFork {
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+};
+int ref_step_kernels(const RefDev& d, int cur, cudaStream_t s, cudaEvent_t* ev = nullptr, const StepFork* fk = nullptr);
 void ref_thermostat_snapshot(const RefDev& d, int cur, cudaStream_t s);
 void ref_thermostat_update(const RefDev& d, int cur, int n_particles, float t_target, bool apply, cudaStream_t s);
 void set_device_float(float* p, float v, cudaStream_t s);
