@@ -273,15 +273,31 @@ void ref_setup(lima_ctx* c) {
         int dev = 0, n_sm = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+        // the loop over the compounds: up to two waves of 1,024 threads per SM
         d.sol_lanes = 1;
-        while (d.sol_lanes < 16 && static_cast<size_t>(ns) * d.sol_lanes * 2 <= static_cast<size_t>(n_sm) * 1024)
+        while (d.sol_lanes < 16 && static_cast<size_t>(ns) * d.sol_lanes * 2 <= static_cast<size_t>(n_sm) * 2048)
             d.sol_lanes *= 2;
-        // LIMA_SOLVENT_LANES=1|2|4|8|16 overrides the choice (results do not depend on it)
-        if (const char* e = std::getenv("LIMA_SOLVENT_LANES")) {
-            const int w = std::atoi(e);
-            if (w == 1 || w == 2 || w == 4 || w == 8 || w == 16) d.sol_lanes = w;
-        }
+        // the list loop: one lane per solvent (gathers pipelined) once the
+        // solvents give every SM 64 threads, else 16 lanes
+        d.sol_list_lanes = static_cast<size_t>(ns) >= static_cast<size_t>(n_sm) * 64 ? 1 : 16;
+        // LIMA_SOLVENT_LANES / LIMA_SOLVENT_LIST_LANES = 1|2|4|8|16 override the
+        // choices (results do not depend on them)
+        auto lanes_env = [](const char* name, int& out) {
+            if (const char* e = std::getenv(name)) {
+                const int w = std::atoi(e);
+                if (w == 1 || w == 2 || w == 4 || w == 8 || w == 16) out = w;
+            }
+        };
+        lanes_env("LIMA_SOLVENT_LANES", d.sol_lanes);
+        lanes_env("LIMA_SOLVENT_LIST_LANES", d.sol_list_lanes);
+        // blocks of 32-128 threads, at least two blocks per SM where the solvents allow
+        d.sol_list_block = 128;
+        while (d.sol_list_block > 32 &&
+               static_cast<size_t>(ns) * d.sol_list_lanes < static_cast<size_t>(d.sol_list_block) * n_sm * 2)
+            d.sol_list_block /= 2;
     }
+    d.sol_force = c->dalloc<float4>(ns);
+    d.sol_image = c->dalloc<float4>(ns);
     d.force_c = c->dalloc<float4>(ncp);
     d.force_s = c->dalloc<float4>(ns);
     d.potE = c->dalloc<double>(ncp);

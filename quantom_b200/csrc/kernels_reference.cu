@@ -19,13 +19,14 @@
 //                   memory and summed per atom in term order (the order the
 //                   reference's serialised loop produces), the LJ partials
 //                   added in the reference's order, Stormer-Verlet, PBC;
-//   k_solvent<W>    W = 1..16 lanes per solvent over its two ordered loops
-//                   (all compound particles, staged 16 compounds at a time;
-//                   the solvent list, read column-major), image chain
-//                   replayed and partial terms added in order through warp
-//                   shuffles.
-// k_solvent is independent of k_partials/k_compound (both read the current
-// buffers and write the next ones).
+//   k_solvent_compounds<W>, k_solvent_list<W>
+//                   the solvent's two ordered loops (all compound particles,
+//                   staged 16 compounds at a time; the solvent list, read
+//                   column-major) with W = 1..16 lanes per solvent each, the
+//                   image chain replayed and partial terms added in order
+//                   through warp shuffles; the second integrates.
+// The solvent kernels are independent of k_partials/k_compound (both read
+// the current buffers and write the next ones).
 #include "refdev.cuh"
 #include "refmath.cuh"
 
@@ -289,36 +290,54 @@ __device__ __forceinline__ F3 shfl3(unsigned mask, F3 v, int src, int width) {
     return mk(__shfl_sync(mask, v.x, src, width), __shfl_sync(mask, v.y, src, width), __shfl_sync(mask, v.z, src, width));
 }
 
-// applyHyperpos with the same arithmetic, telling whether any component
-// moved by a box length.
-__device__ __forceinline__ bool hyperpos_moved(const F3& s, F3& m, float L, float Lh) {
-    bool moved = false;
-    auto one = [&](float sv, float& mv) {
-        const bool a = (sv - mv) > Lh;
-        mv += L * (float)a;
-        const bool b = (sv - mv) < -Lh;
-        mv -= L * (float)b;
-        moved |= a | b;
-    };
-    one(s.x, m.x);
-    one(s.y, m.y);
-    one(s.z, m.z);
-    return moved;
+// applyHyperpos on one component, telling whether it moved
+__device__ __forceinline__ bool hyperpos1_moved(float s, float& m, float L, float Lh) {
+    const bool a = (s - m) > Lh;
+    m += L * (float)a;
+    const bool b = (s - m) < -Lh;
+    m -= L * (float)b;
+    return a || b;
 }
 
-// solventForceKernel (Engine.cu:1070-1161) with W lanes per solvent.  The
-// reference's solvent loops are two ordered chains: over every compound
-// (computeLJForces, Engine.cu:1099-1117; no list) the solvent moves to the
-// image nearest the compound's particle 0 and adds that compound's LJ sum;
-// over the solvent list (computeSolventToSolventLJForces, Engine.cu:706-720)
-// it moves to each neighbour's image and adds the pair force.  Lane j takes
-// compounds / neighbours j, j+W, ...; every lane replays the image chain
-// (one hyperpos per compound; per neighbour block only when some neighbour
-// of the block moves the image, the others leave it unchanged) and the
-// lanes' terms are added in the reference's order through shuffles, so the
-// result is the reference's float sum whatever W is.
+// One component of the image chain over a block of nv neighbours, one per
+// lane: m_q = hyperpos(s_q, m_{q-1}) from m_{-1} = m.  If no lane's
+// neighbour moves the component, every m_q equals the value a lane got from
+// its own neighbour (mine); else the block is replayed in order.  On return
+// m is the block's last value and mine this lane's.
 template <int W>
-__global__ void __launch_bounds__(kSolBlock) k_solvent(RefDev d, int cur) {
+__device__ __forceinline__ void replay_component(unsigned gmask, bool moved, float s, int nv, int j, float& m,
+                                                 float& mine, float L, float Lh) {
+    if (!__any_sync(gmask, moved)) {
+        m = mine;
+        return;
+    }
+    for (int q = 0; q < nv; q++) {
+        const float sq = __shfl_sync(gmask, s, q, W);
+        const bool a = (sq - m) > Lh;
+        m += L * (float)a;
+        const bool b = (sq - m) < -Lh;
+        m -= L * (float)b;
+        if (q == j) mine = m;
+    }
+}
+
+// solventForceKernel (Engine.cu:1070-1161) as two kernels with W lanes per
+// solvent each.  The reference's solvent loops are two ordered chains: over
+// every compound (computeLJForces, Engine.cu:1099-1117; no list) the solvent
+// moves to the image nearest the compound's particle 0 and adds that
+// compound's LJ sum; over the solvent list (computeSolventToSolventLJForces,
+// Engine.cu:706-720) it moves to each neighbour's image and adds the pair
+// force.  Lane j takes compounds / neighbours j, j+W, ...; every lane replays
+// the image chain (one hyperpos per compound; per block of W neighbours only
+// when some neighbour of the block moves the image, the others leave it
+// unchanged) and the lanes' terms are added in the reference's order through
+// shuffles, so the result is the reference's float sum whatever W is.  The
+// list loop's replay is frequent in small boxes (most solvents then have
+// neighbours across a face), so its lane count is chosen separately.
+
+// the loop over the compounds: force and image after it -> sol_force, sol_image
+template <int W>
+__global__ void __launch_bounds__(kSolBlock) k_solvent_compounds(RefDev d, int cur) {
     __shared__ float4 cbuf[kStageCompounds * kStageStride];   // x, y, z, sigma mixed with the solvent's
     __shared__ float cep[kStageCompounds * kStageStride];     // epsilon mixed with the solvent's
     __shared__ int cn[kStageCompounds];
@@ -326,14 +345,10 @@ __global__ void __launch_bounds__(kSolBlock) k_solvent(RefDev d, int cur) {
     const int s = blockIdx.x * (kSolBlock / W) + threadIdx.x / W;
     const unsigned gmask = W == 32 ? 0xffffffffu : (((1u << W) - 1u) << ((threadIdx.x % 32) & ~(W - 1)));
     const bool active = s < d.n_s;
-    F3 pos = mk(0.f, 0.f, 0.f), prev = pos;
-    if (active) {
-        pos = mk4(d.spos[cur][s]);
-        prev = mk4(d.sprev[cur][s]);
-    }
+    F3 pos = active ? mk4(d.spos[cur][s]) : mk(0.f, 0.f, 0.f);
     const lima_particle_parameters sol = d.pp[LIMA_ATOMTYPE_SOL];
     F3 force = mk(0.f, 0.f, 0.f);
-    // solvent <- every compound particle, staged 16 compounds at a time
+    // every compound particle, staged 16 compounds at a time
     for (int c0 = 0; c0 < d.n_c; c0 += kStageCompounds) {
         const int nst = min(kStageCompounds, d.n_c - c0);
         __syncthreads();
@@ -374,33 +389,66 @@ __global__ void __launch_bounds__(kSolBlock) k_solvent(RefDev d, int cur) {
             }
         }
     }
-    if (!active) return;   // a solvent's W lanes leave together
-    // solvent <- solvent list, read column-major
+    if (active && j == 0) {
+        d.sol_force[s] = to4(force);
+        d.sol_image[s] = to4(pos);
+    }
+}
+
+// the loop over the solvent list (read column-major), then integratePosition
+// and applyPBC; starts from sol_force / sol_image when there are compounds.
+// U blocks of W neighbours are gathered before the chain walks them, so U
+// gathers per lane are in flight at once.
+template <int W, int U>
+__global__ void __launch_bounds__(kSolBlock) k_solvent_list(RefDev d, int cur) {
+    const int j = threadIdx.x % W;
+    const int s = blockIdx.x * (blockDim.x / W) + threadIdx.x / W;
+    const unsigned gmask = W == 32 ? 0xffffffffu : (((1u << W) - 1u) << ((threadIdx.x % 32) & ~(W - 1)));
+    if (s >= d.n_s) return;   // a solvent's W lanes leave together
+    const lima_particle_parameters sol = d.pp[LIMA_ATOMTYPE_SOL];
+    F3 pos, force;
+    if (d.n_c > 0) {
+        pos = mk4(d.sol_image[s]);
+        force = mk4(d.sol_force[s]);
+    } else {
+        pos = mk4(d.spos[cur][s]);
+        force = mk(0.f, 0.f, 0.f);
+    }
+    F3 prev = mk4(d.sprev[cur][s]);
     {
         F3 acc = mk(0.f, 0.f, 0.f);
         const int cnt = d.ss_cnt[s];
         const float sg = sol.sigma, ep = sol.epsilon;
-        for (int k0 = 0; k0 < cnt; k0 += W) {
-            const int nv = min(W, cnt - k0);
-            F3 nb = pos;
-            if (j < nv) nb = mk4(__ldg(&d.spos[cur][d.ss_ids[(size_t)(k0 + j) * d.n_s + s]]));
-            F3 mine = pos;
-            const bool moved = hyperpos_moved(nb, mine, d.L, d.Lh);
-            if (W == 1) {
-                pos = mine;
-            } else if (__any_sync(gmask, moved)) {   // replay the block's chain in order
-                for (int q = 0; q < nv; q++) {
-                    hyperpos(shfl3(gmask, nb, q, W), pos, d.L, d.Lh);
-                    if (q == j) mine = pos;
-                }
-            } else {   // no neighbour moves the image: every step of the chain gives this value
-                pos = mine;
+        for (int k0 = 0; k0 < cnt; k0 += W * U) {
+            F3 nbs[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int k = k0 + u * W + j;
+                nbs[u] = k < cnt ? mk4(__ldg(&d.spos[cur][__ldg(&d.ss_ids[(size_t)k * d.n_s + s])])) : pos;
             }
-            F3 f = mk(0.f, 0.f, 0.f);
-            if (j < nv) f = lj_force(mine, nb, sg, ep);
-            if (W == 1) {
-                acc = add(acc, f);
-            } else {
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int base = k0 + u * W;
+                if (base >= cnt) break;   // uniform over the solvent's lanes
+                // a lane past the list's end stands at the current image, which no step moves
+                const F3 nb = base + j < cnt ? nbs[u] : pos;
+                if (W == 1) {
+                    hyperpos(nb, pos, d.L, d.Lh);
+                    acc = add(acc, lj_force(pos, nb, sg, ep));
+                    continue;
+                }
+                const int nv = min(W, cnt - base);
+                // each component's image chain is independent: replay only a
+                // component that some neighbour of this block moves
+                F3 mine = pos;
+                const bool mx = hyperpos1_moved(nb.x, mine.x, d.L, d.Lh);
+                const bool my = hyperpos1_moved(nb.y, mine.y, d.L, d.Lh);
+                const bool mz = hyperpos1_moved(nb.z, mine.z, d.L, d.Lh);
+                replay_component<W>(gmask, mx, nb.x, nv, j, pos.x, mine.x, d.L, d.Lh);
+                replay_component<W>(gmask, my, nb.y, nv, j, pos.y, mine.y, d.L, d.Lh);
+                replay_component<W>(gmask, mz, nb.z, nv, j, pos.z, mine.z, d.L, d.Lh);
+                F3 f = mk(0.f, 0.f, 0.f);
+                if (j < nv) f = lj_force(mine, nb, sg, ep);
                 for (int q = 0; q < nv; q++) acc = add(acc, shfl3(gmask, f, q, W));
             }
         }
@@ -417,20 +465,39 @@ __global__ void __launch_bounds__(kSolBlock) k_solvent(RefDev d, int cur) {
 }
 
 template <int W>
-void launch_solvent(const RefDev& d, int cur, cudaStream_t s) {
+void launch_solvent_compounds(const RefDev& d, int cur, cudaStream_t s) {
     constexpr int per_block = kSolBlock / W;
-    k_solvent<W><<<(d.n_s + per_block - 1) / per_block, kSolBlock, 0, s>>>(d, cur);
+    k_solvent_compounds<W><<<(d.n_s + per_block - 1) / per_block, kSolBlock, 0, s>>>(d, cur);
 }
 
+template <int W>
+void launch_solvent_list(const RefDev& d, int cur, cudaStream_t s) {
+    constexpr int U = W == 1 ? 8 : (W <= 4 ? 4 : 2);
+    const int per_block = d.sol_list_block / W;
+    k_solvent_list<W, U><<<(d.n_s + per_block - 1) / per_block, d.sol_list_block, 0, s>>>(d, cur);
+}
+
+// the solvent kernels of one step; returns kernels launched
 int launch_solvent_kernel(const RefDev& d, int cur, cudaStream_t s) {
-    switch (d.sol_lanes) {
-        case 16: launch_solvent<16>(d, cur, s); break;
-        case 8: launch_solvent<8>(d, cur, s); break;
-        case 4: launch_solvent<4>(d, cur, s); break;
-        case 2: launch_solvent<2>(d, cur, s); break;
-        default: launch_solvent<1>(d, cur, s); break;
+    int n = 0;
+    if (d.n_c > 0) {
+        switch (d.sol_lanes) {
+            case 16: launch_solvent_compounds<16>(d, cur, s); break;
+            case 8: launch_solvent_compounds<8>(d, cur, s); break;
+            case 4: launch_solvent_compounds<4>(d, cur, s); break;
+            case 2: launch_solvent_compounds<2>(d, cur, s); break;
+            default: launch_solvent_compounds<1>(d, cur, s); break;
+        }
+        n++;
     }
-    return 1;
+    switch (d.sol_list_lanes) {
+        case 16: launch_solvent_list<16>(d, cur, s); break;
+        case 8: launch_solvent_list<8>(d, cur, s); break;
+        case 4: launch_solvent_list<4>(d, cur, s); break;
+        case 2: launch_solvent_list<2>(d, cur, s); break;
+        default: launch_solvent_list<1>(d, cur, s); break;
+    }
+    return n + 1;
 }
 
 // Engine::getBoxTemperature's KE term (LIMAENG::calcKineticEnergy,

@@ -53,8 +53,12 @@ struct RefDev {
     // compound LJ partial sums [n_c][1 + 64][64]: slot 0 the intramolecular
     // sum, slot 1 + k the sum over compound-list entry k
     float4* cc_partial;
-    // lanes per solvent in the solvent kernel (1, 2, 4, 8 or 16)
-    int sol_lanes;
+    // lanes per solvent (1, 2, 4, 8 or 16) in the solvent kernels' loop over
+    // the compounds and over the solvent list
+    int sol_lanes, sol_list_lanes;
+    int sol_list_block;      // threads per block of the list loop's kernel (32, 64 or 128)
+    // solvent force and image after the loop over the compounds [n_s]
+    float4* sol_force; float4* sol_image;
     // outputs of the last step
     float4* force_c;         // [n_c*64]
     float4* force_s;         // [n_s]

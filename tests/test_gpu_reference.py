@@ -99,14 +99,16 @@ def _oracle_step(name):
     return _ORACLE_STEP[name]
 
 
-# The solvent kernel splits each solvent's ordered loops over 1-16 lanes;
-# the image chain is replayed and the lanes' terms added in order, so the
-# solvent path stays the oracle's (and the reference's) float arithmetic.
-@pytest.mark.parametrize("lanes", [1, 2, 4, 8, 16])
+# The solvent kernels split each solvent's two ordered loops (compounds,
+# solvent list) over 1-16 lanes each; the image chain is replayed and the
+# lanes' terms added in order, so the solvent path stays the oracle's (and
+# the reference's) float arithmetic.
+@pytest.mark.parametrize("lanes", [(1, 1), (1, 16), (2, 8), (4, 4), (8, 2), (16, 1), (16, 16)])
 @pytest.mark.parametrize("name", ["small_bridged", "lj_solvent_4096", "6lzm"])
 def test_solvent_path_bit_identical_at_every_lane_count(gpu, name, lanes, monkeypatch):
     E = gpu
-    monkeypatch.setenv("LIMA_SOLVENT_LANES", str(lanes))
+    monkeypatch.setenv("LIMA_SOLVENT_LANES", str(lanes[0]))
+    monkeypatch.setenv("LIMA_SOLVENT_LIST_LANES", str(lanes[1]))
     s, (new, fc_o, fs_o, pe_o) = _oracle_step(name)
     with _engine(E, s) as eng:
         eng.step(1)
