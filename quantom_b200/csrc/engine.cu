@@ -102,7 +102,9 @@ struct lima_ctx {
         if (ev1) cudaEventDestroy(ev1);
         if (fork.fork) cudaEventDestroy(fork.fork);
         if (fork.join) cudaEventDestroy(fork.join);
+        if (fork.join2) cudaEventDestroy(fork.join2);
         if (fork.side) cudaStreamDestroy(fork.side);
+        if (fork.side2) cudaStreamDestroy(fork.side2);
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
 };
@@ -277,9 +279,9 @@ void ref_setup(lima_ctx* c) {
         d.sol_lanes = 1;
         while (d.sol_lanes < 16 && static_cast<size_t>(ns) * d.sol_lanes * 2 <= static_cast<size_t>(n_sm) * 2048)
             d.sol_lanes *= 2;
-        // the list loop: one lane per solvent (gathers pipelined) once the
-        // solvents give every SM 64 threads, else 16 lanes
-        d.sol_list_lanes = static_cast<size_t>(ns) >= static_cast<size_t>(n_sm) * 64 ? 1 : 16;
+        // the list loop: one lane per solvent, gathers pipelined (it runs
+        // beside the loop over the compounds, which fills the SMs' issue slots)
+        d.sol_list_lanes = 1;
         // LIMA_SOLVENT_LANES / LIMA_SOLVENT_LIST_LANES = 1|2|4|8|16 override the
         // choices (results do not depend on them)
         auto lanes_env = [](const char* name, int& out) {
@@ -297,6 +299,7 @@ void ref_setup(lima_ctx* c) {
             d.sol_list_block /= 2;
     }
     d.sol_force = c->dalloc<float4>(ns);
+    d.sol_acc = c->dalloc<float4>(ns);
     d.sol_image = c->dalloc<float4>(ns);
     d.force_c = c->dalloc<float4>(ncp);
     d.force_s = c->dalloc<float4>(ns);
@@ -554,6 +557,8 @@ lima_status lima_create(const lima_params* params, lima_ctx** out) {
         cuda_ok(cudaStreamCreateWithFlags(&c->fork.side, cudaStreamNonBlocking), "cudaStreamCreate");
         cuda_ok(cudaEventCreateWithFlags(&c->fork.fork, cudaEventDisableTiming), "cudaEventCreate");
         cuda_ok(cudaEventCreateWithFlags(&c->fork.join, cudaEventDisableTiming), "cudaEventCreate");
+        cuda_ok(cudaStreamCreateWithFlags(&c->fork.side2, cudaStreamNonBlocking), "cudaStreamCreate");
+        cuda_ok(cudaEventCreateWithFlags(&c->fork.join2, cudaEventDisableTiming), "cudaEventCreate");
     });
     if (st != LIMA_OK) {
         fprintf(stderr, "lima_create: %s\n", c->err.c_str());

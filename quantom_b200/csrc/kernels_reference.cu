@@ -22,11 +22,13 @@
 //   k_solvent_compounds<W>, k_solvent_list<W>
 //                   the solvent's two ordered loops (all compound particles,
 //                   staged 16 compounds at a time; the solvent list, read
-//                   column-major) with W = 1..16 lanes per solvent each, the
-//                   image chain replayed and partial terms added in order
-//                   through warp shuffles; the second integrates.
+//                   column-major), run at the same time, with W = 1..16
+//                   lanes per solvent each, the image chain replayed and
+//                   partial terms added in order through warp shuffles;
+//   k_solvent_integrate  the two sums added in the reference's order,
+//                   Stormer-Verlet, PBC.
 // The solvent kernels are independent of k_partials/k_compound (both read
-// the current buffers and write the next ones).
+// the current buffers and write the next ones); all run at once.
 #include "refdev.cuh"
 #include "refmath.cuh"
 
@@ -335,7 +337,7 @@ __device__ __forceinline__ void replay_component(unsigned gmask, bool moved, flo
 // list loop's replay is frequent in small boxes (most solvents then have
 // neighbours across a face), so its lane count is chosen separately.
 
-// the loop over the compounds: force and image after it -> sol_force, sol_image
+// the loop over the compounds: the force summed over them -> sol_force
 template <int W>
 __global__ void __launch_bounds__(kSolBlock) k_solvent_compounds(RefDev d, int cur) {
     __shared__ float4 cbuf[kStageCompounds * kStageStride];   // x, y, z, sigma mixed with the solvent's
@@ -389,16 +391,15 @@ __global__ void __launch_bounds__(kSolBlock) k_solvent_compounds(RefDev d, int c
             }
         }
     }
-    if (active && j == 0) {
-        d.sol_force[s] = to4(force);
-        d.sol_image[s] = to4(pos);
-    }
+    if (active && j == 0) d.sol_force[s] = to4(force);
 }
 
-// the loop over the solvent list (read column-major), then integratePosition
-// and applyPBC; starts from sol_force / sol_image when there are compounds.
-// U blocks of W neighbours are gathered before the chain walks them, so U
-// gathers per lane are in flight at once.
+// the loop over the solvent list (read column-major) -> sol_acc, sol_image.
+// Its image chain starts where the loop over the compounds leaves it: the
+// solvent moved to each compound's particle-0 image in compound order,
+// recomputed here so that the two loops run at the same time.  U blocks of
+// W neighbours are gathered before the chain walks them, so U gathers per
+// lane are in flight at once.
 template <int W, int U>
 __global__ void __launch_bounds__(kSolBlock) k_solvent_list(RefDev d, int cur) {
     const int j = threadIdx.x % W;
@@ -406,15 +407,8 @@ __global__ void __launch_bounds__(kSolBlock) k_solvent_list(RefDev d, int cur) {
     const unsigned gmask = W == 32 ? 0xffffffffu : (((1u << W) - 1u) << ((threadIdx.x % 32) & ~(W - 1)));
     if (s >= d.n_s) return;   // a solvent's W lanes leave together
     const lima_particle_parameters sol = d.pp[LIMA_ATOMTYPE_SOL];
-    F3 pos, force;
-    if (d.n_c > 0) {
-        pos = mk4(d.sol_image[s]);
-        force = mk4(d.sol_force[s]);
-    } else {
-        pos = mk4(d.spos[cur][s]);
-        force = mk(0.f, 0.f, 0.f);
-    }
-    F3 prev = mk4(d.sprev[cur][s]);
+    F3 pos = mk4(d.spos[cur][s]);
+    for (int c = 0; c < d.n_c; c++) hyperpos(mk4(__ldg(&d.cpos[cur][c * kMaxCP])), pos, d.L, d.Lh);
     {
         F3 acc = mk(0.f, 0.f, 0.f);
         const int cnt = d.ss_cnt[s];
@@ -452,12 +446,25 @@ __global__ void __launch_bounds__(kSolBlock) k_solvent_list(RefDev d, int cur) {
                 for (int q = 0; q < nv; q++) acc = add(acc, shfl3(gmask, f, q, W));
             }
         }
-        force = add(force, acc);
+        if (j == 0) {   // every lane holds the same state
+            d.sol_acc[s] = to4(acc);
+            d.sol_image[s] = to4(pos);
+        }
     }
-    // every lane holds the same state; lane 0 stores it
+}
+
+// the solvent's force (the sum over the compounds, then the list loop's
+// sum, as the reference adds them), integratePosition and applyPBC
+__global__ void k_solvent_integrate(RefDev d, int cur) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= d.n_s) return;
+    const lima_particle_parameters sol = d.pp[LIMA_ATOMTYPE_SOL];
+    F3 force = d.n_c > 0 ? mk4(d.sol_force[s]) : mk(0.f, 0.f, 0.f);
+    force = add(force, mk4(d.sol_acc[s]));
+    F3 pos = mk4(d.sol_image[s]);
+    F3 prev = mk4(d.sprev[cur][s]);
     integrate(pos, prev, force, (double)sol.mass, d.dt, *d.lambda, d.L, d.Lh);
     apply_pbc(pos, d.L);
-    if (j != 0) return;
     flag_nan(d, pos);
     d.spos[cur ^ 1][s] = to4(pos);
     d.sprev[cur ^ 1][s] = to4(prev);
@@ -477,19 +484,19 @@ void launch_solvent_list(const RefDev& d, int cur, cudaStream_t s) {
     k_solvent_list<W, U><<<(d.n_s + per_block - 1) / per_block, d.sol_list_block, 0, s>>>(d, cur);
 }
 
-// the solvent kernels of one step; returns kernels launched
-int launch_solvent_kernel(const RefDev& d, int cur, cudaStream_t s) {
-    int n = 0;
-    if (d.n_c > 0) {
-        switch (d.sol_lanes) {
-            case 16: launch_solvent_compounds<16>(d, cur, s); break;
-            case 8: launch_solvent_compounds<8>(d, cur, s); break;
-            case 4: launch_solvent_compounds<4>(d, cur, s); break;
-            case 2: launch_solvent_compounds<2>(d, cur, s); break;
-            default: launch_solvent_compounds<1>(d, cur, s); break;
-        }
-        n++;
+int launch_solvent_compounds_kernel(const RefDev& d, int cur, cudaStream_t s) {
+    if (d.n_c == 0) return 0;
+    switch (d.sol_lanes) {
+        case 16: launch_solvent_compounds<16>(d, cur, s); break;
+        case 8: launch_solvent_compounds<8>(d, cur, s); break;
+        case 4: launch_solvent_compounds<4>(d, cur, s); break;
+        case 2: launch_solvent_compounds<2>(d, cur, s); break;
+        default: launch_solvent_compounds<1>(d, cur, s); break;
     }
+    return 1;
+}
+
+int launch_solvent_list_kernel(const RefDev& d, int cur, cudaStream_t s) {
     switch (d.sol_list_lanes) {
         case 16: launch_solvent_list<16>(d, cur, s); break;
         case 8: launch_solvent_list<8>(d, cur, s); break;
@@ -497,7 +504,12 @@ int launch_solvent_kernel(const RefDev& d, int cur, cudaStream_t s) {
         case 2: launch_solvent_list<2>(d, cur, s); break;
         default: launch_solvent_list<1>(d, cur, s); break;
     }
-    return n + 1;
+    return 1;
+}
+
+int launch_solvent_integrate(const RefDev& d, int cur, cudaStream_t s) {
+    k_solvent_integrate<<<(d.n_s + 255) / 256, 256, 0, s>>>(d, cur);
+    return 1;
 }
 
 // Engine::getBoxTemperature's KE term (LIMAENG::calcKineticEnergy,
@@ -553,11 +565,18 @@ __global__ void k_snapshot(RefDev d, int cur) {
 // Returns kernels launched.
 int ref_step_kernels(const RefDev& d, int cur, cudaStream_t s, cudaEvent_t* ev, const StepFork* fk) {
     int launched = 0;
-    const bool forked = !ev && fk && fk->side && d.n_s > 0 && (d.n_c > 0 || d.n_b > 0);
+    const bool forked = !ev && fk && fk->side && fk->side2 && d.n_s > 0;
     if (forked) {
+        // side2: the loop over the compounds; side: the list loop, then the
+        // sum of the two and the integration
         cudaEventRecord(fk->fork, s);
         cudaStreamWaitEvent(fk->side, fk->fork, 0);
-        launched += launch_solvent_kernel(d, cur, fk->side);
+        cudaStreamWaitEvent(fk->side2, fk->fork, 0);
+        launched += launch_solvent_compounds_kernel(d, cur, fk->side2);
+        cudaEventRecord(fk->join2, fk->side2);
+        launched += launch_solvent_list_kernel(d, cur, fk->side);
+        cudaStreamWaitEvent(fk->side, fk->join2, 0);
+        launched += launch_solvent_integrate(d, cur, fk->side);
         cudaEventRecord(fk->join, fk->side);
     }
     if (ev) cudaEventRecord(ev[0], s);
@@ -572,10 +591,13 @@ int ref_step_kernels(const RefDev& d, int cur, cudaStream_t s, cudaEvent_t* ev, 
         launched += 2;
     }
     if (ev) cudaEventRecord(ev[2], s);
-    if (forked)
+    if (forked) {
         cudaStreamWaitEvent(s, fk->join, 0);
-    else if (d.n_s > 0)
-        launched += launch_solvent_kernel(d, cur, s);
+    } else if (d.n_s > 0) {
+        launched += launch_solvent_compounds_kernel(d, cur, s);
+        launched += launch_solvent_list_kernel(d, cur, s);
+        launched += launch_solvent_integrate(d, cur, s);
+    }
     if (ev) cudaEventRecord(ev[3], s);
     return launched;
 }

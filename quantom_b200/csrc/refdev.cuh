@@ -57,8 +57,9 @@ struct RefDev {
     // the compounds and over the solvent list
     int sol_lanes, sol_list_lanes;
     int sol_list_block;      // threads per block of the list loop's kernel (32, 64 or 128)
-    // solvent force and image after the loop over the compounds [n_s]
-    float4* sol_force; float4* sol_image;
+    // per solvent [n_s]: the force summed over the compounds, the list
+    // loop's sum, and the image the list loop ends on
+    float4* sol_force; float4* sol_acc; float4* sol_image;
     // outputs of the last step
     float4* force_c;         // [n_c*64]
     float4* force_s;         // [n_s]
@@ -78,12 +79,12 @@ struct RefDev {
 // nlist_reference.cu
 void ref_build_nlists(const RefDev& d, int cur, cudaStream_t s);
 // kernels_reference.cu
-// A second stream and two events: the solvent kernel runs beside the
+// Two more streams and three events: the solvent kernels run beside the
 // compound kernels (they read the same current buffers and write disjoint
-// next ones).
+// next ones), the solvents' loop over the compounds beside their list loop.
 struct StepFork {
-    cudaStream_t side = nullptr;
-    cudaEvent_t fork = nullptr, join = nullptr;
+    cudaStream_t side = nullptr, side2 = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr, join2 = nullptr;
 };
 int ref_step_kernels(const RefDev& d, int cur, cudaStream_t s, cudaEvent_t* ev = nullptr, const StepFork* fk = nullptr);
 void ref_thermostat_snapshot(const RefDev& d, int cur, cudaStream_t s);
