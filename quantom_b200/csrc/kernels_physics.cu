@@ -456,6 +456,55 @@ __global__ void k_finalize(PhysDev d, int src) { fold(d, src); }
 
 // ------------------------------------------------------- pair + integrate ---
 // (lj_pair: physmath.cuh)
+// position loads in flight per lane in the mixed-precision pair kernel: two
+// keep it at 48 registers (four: 56, one block fewer per SM)
+constexpr int kMixedGathers = 2;
+
+// One lane's rows of its particle's Verlet list, GATHERS (4 or 2) position
+// loads in flight; MIXED: compensated sums every 8 pairs.
+template <bool MIXED, bool ENERGY, bool SWITCH, bool WRAP, int GATHERS = 4>
+__device__ __forceinline__ void pair_rows(const PhysDev& d, const float2* row, float4 pi, const float4* __restrict__ pos,
+                                          const uint32_t* __restrict__ nl, uint32_t stride, int rows, float& fx,
+                                          float& fy, float& fz, float& cxx, float& cyy, float& czz, float& e_i,
+                                          float& w_i) {
+    int r = 0;
+    while (r < rows) {
+        const int rend = MIXED ? min(rows, r + 8) : rows;
+        float px = 0.f, py = 0.f, pz = 0.f;
+        if (GATHERS == 4) {
+            for (; r + 3 < rend; r += 4) {
+                const uint32_t j0 = __ldg(nl + r * stride), j1 = __ldg(nl + (r + 1) * stride);
+                const uint32_t j2 = __ldg(nl + (r + 2) * stride), j3 = __ldg(nl + (r + 3) * stride);
+                const float4 p0 = __ldg(pos + j0), p1 = __ldg(pos + j1), p2 = __ldg(pos + j2), p3 = __ldg(pos + j3);
+                lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p0, px, py, pz, e_i, w_i);
+                lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p1, px, py, pz, e_i, w_i);
+                lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p2, px, py, pz, e_i, w_i);
+                lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p3, px, py, pz, e_i, w_i);
+            }
+        } else {
+            for (; r + 1 < rend; r += 2) {
+                const uint32_t j0 = __ldg(nl + r * stride), j1 = __ldg(nl + (r + 1) * stride);
+                const float4 p0 = __ldg(pos + j0), p1 = __ldg(pos + j1);
+                lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p0, px, py, pz, e_i, w_i);
+                lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p1, px, py, pz, e_i, w_i);
+            }
+        }
+        for (; r < rend; r++) {
+            const uint32_t j0 = __ldg(nl + r * stride);
+            lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, __ldg(pos + j0), px, py, pz, e_i, w_i);
+        }
+        if (MIXED) {
+            ds_add(fx, cxx, px);
+            ds_add(fy, cyy, py);
+            ds_add(fz, czz, pz);
+        } else {
+            fx += px;
+            fy += py;
+            fz += pz;
+        }
+    }
+}
+
 template <bool MIXED, bool ENERGY, bool INTEGRATE, bool SWITCH>
 __device__ __forceinline__ void pair_integrate(const PhysDev& d, int cur, int slot) {
     extern __shared__ float2 s_tab[];
@@ -475,33 +524,13 @@ __device__ __forceinline__ void pair_integrate(const PhysDev& d, int cur, int sl
     const uint32_t stride = (uint32_t)d.n_pad * kGroup;
     const uint32_t* __restrict__ nl = d.nl + (uint32_t)i * kGroup + g;
     const int rows = cnt > g ? (cnt - g + kGroup - 1) / kGroup : 0;
-    int r = 0;
-    while (r < rows) {
-        const int rend = MIXED ? min(rows, r + 8) : rows;
-        float px = 0.f, py = 0.f, pz = 0.f;
-        for (; r + 3 < rend; r += 4) {   // four gathers in flight
-            const uint32_t j0 = __ldg(nl + r * stride), j1 = __ldg(nl + (r + 1) * stride);
-            const uint32_t j2 = __ldg(nl + (r + 2) * stride), j3 = __ldg(nl + (r + 3) * stride);
-            const float4 p0 = __ldg(pos + j0), p1 = __ldg(pos + j1), p2 = __ldg(pos + j2), p3 = __ldg(pos + j3);
-            lj_pair<ENERGY, SWITCH>(d, row, pi, p0, px, py, pz, e_i, w_i);
-            lj_pair<ENERGY, SWITCH>(d, row, pi, p1, px, py, pz, e_i, w_i);
-            lj_pair<ENERGY, SWITCH>(d, row, pi, p2, px, py, pz, e_i, w_i);
-            lj_pair<ENERGY, SWITCH>(d, row, pi, p3, px, py, pz, e_i, w_i);
-        }
-        for (; r < rend; r++) {
-            const uint32_t j0 = __ldg(nl + r * stride);
-            lj_pair<ENERGY, SWITCH>(d, row, pi, __ldg(pos + j0), px, py, pz, e_i, w_i);
-        }
-        if (MIXED) {
-            ds_add(fx, cxx, px);
-            ds_add(fy, cyy, py);
-            ds_add(fz, czz, pz);
-        } else {
-            fx += px;
-            fy += py;
-            fz += pz;
-        }
-    }
+    // warps whose particles are all away from the box faces skip the minimum image
+    if (__all_sync(0xffffffffu, !active || away_from_faces(d, pi)))
+        pair_rows<MIXED, ENERGY, SWITCH, false, MIXED ? kMixedGathers : 4>(d, row, pi, pos, nl, stride, rows, fx, fy, fz,
+                                                                           cxx, cyy, czz, e_i, w_i);
+    else
+        pair_rows<MIXED, ENERGY, SWITCH, true, MIXED ? kMixedGathers : 4>(d, row, pi, pos, nl, stride, rows, fx, fy, fz,
+                                                                          cxx, cyy, czz, e_i, w_i);
     // reduce the kGroup lanes of this particle (warp shuffles)
 #pragma unroll
     for (int o = kGroup / 2; o > 0; o >>= 1) {

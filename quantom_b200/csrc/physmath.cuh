@@ -10,14 +10,23 @@ namespace lima {
 // minimum image of one coordinate difference in a cubic box
 __device__ __forceinline__ float mimg(float d, float L, float invL) { return d - L * rintf(d * invL); }
 
+// A particle at least r_c from every face of the box: every particle within
+// r_c of it (minimum image) is so in plain coordinates too, and a pair beyond
+// r_c contributes zero either way, so its pairs need no minimum image.
+__device__ __forceinline__ bool away_from_faces(const PhysDev& d, float4 p) {
+    const float m = d.rc * 1.0001f + 1e-5f, hi = d.L - m;
+    return p.x >= m && p.x <= hi && p.y >= m && p.y <= hi && p.z >= m && p.z <= hi;
+}
+
 // One pair, branch-free: out-of-cutoff pairs contribute zero through a
 // select, the switch is evaluated for every pair (S = 1, S' = 0 below r_on).
-template <bool ENERGY, bool SWITCH>
+// WRAP false: i is away_from_faces, the plain difference is the minimum image.
+template <bool ENERGY, bool SWITCH, bool WRAP = true>
 __device__ __forceinline__ void lj_pair(const PhysDev& d, const float2* __restrict__ row, float4 pi, float4 pj,
                                         float& px, float& py, float& pz, float& e_i, float& w_i) {
-    const float dx = mimg(pj.x - pi.x, d.L, d.invL);
-    const float dy = mimg(pj.y - pi.y, d.L, d.invL);
-    const float dz = mimg(pj.z - pi.z, d.L, d.invL);
+    const float dx = WRAP ? mimg(pj.x - pi.x, d.L, d.invL) : pj.x - pi.x;
+    const float dy = WRAP ? mimg(pj.y - pi.y, d.L, d.invL) : pj.y - pi.y;
+    const float dz = WRAP ? mimg(pj.z - pi.z, d.L, d.invL) : pj.z - pi.z;
     const float r2 = dx * dx + dy * dy + dz * dz;
     const float2 tab = row[__float_as_int(pj.w)];
     const float inv = __fdividef(1.f, r2);
