@@ -1225,7 +1225,7 @@ lima_status lima_get_nlist(lima_ctx* c, int which, uint32_t* offsets, uint32_t* 
     return guarded(c, [&] {
         need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
         need(c->p.semantics == LIMA_SEMANTICS_REFERENCE, LIMA_ERR_UNSUPPORTED,
-             "entity neighbour lists exist in reference semantics; physics uses a cluster-pair list");
+             "entity neighbour lists exist in reference semantics; physics keeps one cell-sorted Verlet list");
         need(which >= 0 && which <= 3, LIMA_ERR_ARGUMENT, "unknown list selector");
         need(offsets != nullptr, LIMA_ERR_ARGUMENT, "null offsets");
         sync_checked(c);
