@@ -217,6 +217,13 @@ lima_status lima_synchronize(lima_ctx* ctx);
    Compound::prev_positions, Box::solvents). */
 lima_status lima_get_compound_states(lima_ctx* ctx, lima_compound_state* states, lima_float3* prev_positions);
 lima_status lima_get_solvents(lima_ctx* ctx, lima_solvent* solvents);
+/* The same positions as flat float arrays, for callers that do not use the
+   reference's structs: compound particle (c, l) at compound_xyz[3 * (c * 64 + l)]
+   (slots past a compound's n_particles are zero), solvent s at
+   solvent_xyz[3 * s].  Either pointer may be NULL.  The reference's caller reads
+   the same values from Box::compound_state_array and Box::solvents
+   (Simulation.cuh:35-92). */
+lima_status lima_get_positions(lima_ctx* ctx, float* compound_xyz, float* solvent_xyz);
 /* Replace the positions of a loaded box in place (same layout as loading). */
 lima_status lima_set_state(lima_ctx* ctx, const lima_compound_state* states, const lima_float3* prev_positions,
                            const lima_solvent* solvents);

@@ -810,6 +810,41 @@ lima_status lima_get_solvents(lima_ctx* c, lima_solvent* sols) {
     });
 }
 
+lima_status lima_get_positions(lima_ctx* c, float* cxyz, float* sxyz) {
+    return guarded(c, [&] {
+        need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
+        sync_checked(c);
+        const int nc = static_cast<int>(c->comps.size()), ns = static_cast<int>(c->sols.size());
+        const size_t ncp = static_cast<size_t>(nc) * lima::kMaxCP;
+        std::vector<float4> hp(ncp), hq(ncp), a(ns), b(ns);
+        if (cxyz) {
+            if (c->p.semantics == LIMA_SEMANTICS_REFERENCE)
+                cuda_ok(cudaMemcpy(hp.data(), c->ref.cpos[c->cur], sizeof(float4) * ncp, cudaMemcpyDeviceToHost), "D2H");
+            else
+                lima::phys_read_compounds(c->phys, c->cur, c->comps.data(), hp.data(), hq.data());
+            for (int i = 0; i < nc; i++)
+                for (int t = 0; t < lima::kMaxCP; t++) {
+                    const size_t k = static_cast<size_t>(i) * lima::kMaxCP + t;
+                    const bool live = t < c->comps[i].n_particles;
+                    cxyz[3 * k] = live ? hp[k].x : 0.f;
+                    cxyz[3 * k + 1] = live ? hp[k].y : 0.f;
+                    cxyz[3 * k + 2] = live ? hp[k].z : 0.f;
+                }
+        }
+        if (sxyz && ns > 0) {
+            if (c->p.semantics == LIMA_SEMANTICS_REFERENCE)
+                cuda_ok(cudaMemcpy(a.data(), c->ref.spos[c->cur], sizeof(float4) * ns, cudaMemcpyDeviceToHost), "D2H");
+            else
+                lima::phys_read_solvents(c->phys, c->cur, a.data(), b.data());
+            for (int i = 0; i < ns; i++) {
+                sxyz[3 * i] = a[i].x;
+                sxyz[3 * i + 1] = a[i].y;
+                sxyz[3 * i + 2] = a[i].z;
+            }
+        }
+    });
+}
+
 lima_status lima_set_state(lima_ctx* c, const lima_compound_state* states, const lima_float3* prev,
                            const lima_solvent* sols) {
     return guarded(c, [&] {

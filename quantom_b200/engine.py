@@ -87,6 +87,7 @@ def load_library():
         "lima_synchronize": (i, [vp]),
         "lima_get_compound_states": (i, [vp, vp, vp]),
         "lima_get_solvents": (i, [vp, vp]),
+        "lima_get_positions": (i, [vp, vp, vp]),
         "lima_set_state": (i, [vp, vp, vp, vp]),
         "lima_get_forces": (i, [vp, vp, vp]),
         "lima_get_energies": (i, [vp, vp, vp]),
@@ -354,6 +355,14 @@ class Engine:
         if len(s):
             self._check(self.lib.lima_get_solvents(self.h, _ptr(s)))
         return s
+
+    def positions(self):
+        """Flat float32 positions: compound slots (n_compounds, 64, 3), empty
+        slots zero, and solvents (n_solvents, 3) (lima_get_positions)."""
+        c = np.zeros((self.system.n_compounds, 64, 3), np.float32)
+        s = np.zeros((self.system.n_solvents, 3), np.float32)
+        self._check(self.lib.lima_get_positions(self.h, _ptr(c) if c.size else None, _ptr(s) if s.size else None))
+        return c, s
 
     def set_state(self, states, prev_positions, solvents):
         self._check(self.lib.lima_set_state(self.h, _ptr(states), _ptr(prev_positions), _ptr(solvents)))

@@ -124,6 +124,25 @@ def test_solvent_path_bit_identical_at_every_lane_count(gpu, name, lanes, monkey
         assert np.abs(st["positions"][m] - new.states["positions"][m]).max() < 1e-5
 
 
+@pytest.mark.parametrize("semantics", ["reference", "physics"])
+def test_flat_positions_are_the_struct_positions(gpu, semantics):
+    """lima_get_positions returns the positions lima_get_compound_states and
+    lima_get_solvents return, flattened, with empty compound slots zero."""
+    E = gpu
+    s = S.make_system("small_bridged", seed=5)
+    kw = {} if semantics == "reference" else dict(semantics=E.SEMANTICS_PHYSICS, skin=0.1, switch_on=1.0)
+    with _engine(E, s, **kw) as eng:
+        eng.step(3)
+        cxyz, sxyz = eng.positions()
+        st, _ = eng.compound_states()
+        sol = eng.solvents()
+    for c in range(s.n_compounds):
+        k = s.compounds[c]["n_particles"]
+        np.testing.assert_array_equal(cxyz[c, :k], st[c]["positions"][:k])
+        assert not cxyz[c, k:].any()
+    np.testing.assert_array_equal(sxyz, sol["pos"])
+
+
 def test_multistep_with_list_rebuilds_matches_oracle(gpu):
     E = gpu
     s = S.make_system("small_bridged", seed=3)

@@ -87,3 +87,9 @@ def test_frame_log_entry_points_reject_a_null_context():
     assert lib.lima_log_count(None, ctypes.byref(n)) == engine.ERR_ARGUMENT
     assert lib.lima_log_read(None, 0, 0, None, None, None, None, None, None) == engine.ERR_ARGUMENT
     assert lib.lima_log_write(None, b".") == engine.ERR_ARGUMENT
+
+
+def test_positions_entry_point_rejects_a_null_context():
+    from quantom_b200 import engine
+    lib = engine.load_library()
+    assert lib.lima_get_positions(None, None, None) == engine.ERR_ARGUMENT
