@@ -110,7 +110,10 @@ def run_kernels_only(args):
                           "ms_per_step_unflushed": eng.last_step_ms() / max(1, args.steps)}), flush=True)
 
 
-def dist_setup(args):
+def dist_setup(args, backend="nccl", timeout_s=120):
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE): the
+    replicas share only a barrier and the max of their step times.  backend
+    "gloo" runs the same plumbing on host processes."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -119,9 +122,10 @@ def dist_setup(args):
         import datetime
         import torch.distributed as dist
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        import torch
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
         pg = dist
     return ws, rank, local, pg
 
