@@ -177,16 +177,16 @@ __global__ void k_list_check(const int* need, unsigned long long* count, cudaGra
     if (v) *count += 1ull;
 }
 
-// Verlet-list build: one warp per 8 consecutive sorted particles, four lanes
-// per particle (lane = 4 * particle + slice).  The warp's particles are split
+// Verlet-list build: one warp per 32 / kSlices consecutive sorted particles,
+// kSlices lanes per particle (lane = kSlices * particle + slice).  The warp's particles are split
 // into groups that share a home column (cells (x, y, *)) and a z-window of at
 // most m-4 cells; particles outside the current group idle.  For a group with
 // home cells z0..z1, the candidates are the cells z0-2..z1+2 of the 25
 // columns around it (cells of side >= r_list/2, so they cover r_list), each
 // one or two contiguous slot ranges of the cell-sorted order.  Candidates
 // come through shared memory 32 at a time, shifted into the home frame by
-// whole box lengths; each lane tests every fourth candidate against its
-// particle, the four lanes' hit masks are merged with two xor-shuffles, and
+// whole box lengths; each lane tests every kSlices-th candidate against its
+// particle, the slices' hit masks are merged with xor-shuffles, and
 // every lane writes its own hits at their rank in the merged mask, so each
 // row lists its neighbours in candidate order (deterministic).  Collectives
 // (ballots, shuffles, __syncwarp) only occur in warp-uniform code.  Boxes
@@ -217,13 +217,13 @@ __device__ __forceinline__ void scan_range(const PhysDev& d, const float4* __res
             sc[lane].j = (uint32_t)j | (oj < (uint32_t)d.n_cp ? 0x80000000u : 0u);
         }
         __syncwarp();
-        // slice `sub` tests candidates sub, sub+4, ..., sub+28 (consecutive lanes of a
-        // particle read consecutive 32-byte records: no shared-memory bank conflicts)
+        // slice `sub` tests candidates sub, sub + kSlices, ... (consecutive lanes of a
+        // particle read consecutive 32-byte records)
         uint32_t mine_bits = 0;
         if (mine) {
 #pragma unroll
-            for (int t = 0; t < 8; t++) {
-                const int c = 4 * t + sub;
+            for (int t = 0; t < 32 / kSlices; t++) {
+                const int c = kSlices * t + sub;
                 if (c < nv) {
                     const float4 q = sc[c].p;
                     float dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
@@ -245,8 +245,8 @@ __device__ __forceinline__ void scan_range(const PhysDev& d, const float4* __res
                 }
         }
         uint32_t m32 = mine_bits;
-        m32 |= __shfl_xor_sync(0xffffffffu, m32, 1);
-        m32 |= __shfl_xor_sync(0xffffffffu, m32, 2);
+#pragma unroll
+        for (int o = 1; o < kSlices; o <<= 1) m32 |= __shfl_xor_sync(0xffffffffu, m32, o);
         for (uint32_t b = mine_bits; b; b &= b - 1u) {
             const int c = __ffs(b) - 1;
             const int k = cnt + __popc(m32 & ((1u << c) - 1u));
@@ -262,8 +262,8 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_build_list(PhysDev d, cons
                                                                  const uint32_t* __restrict__ items) {
     __shared__ Cand s_cand[kBuildWarps][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int pl = lane >> 2, sub = lane & 3;
-    const int base = (blockIdx.x * kBuildWarps + w) * 8;
+    const int pl = lane / kSlices, sub = lane % kSlices;
+    const int base = (blockIdx.x * kBuildWarps + w) * (32 / kSlices);
     if (base >= d.n) return;   // the whole warp
     Cand* sc = s_cand[w];
     const int qi = base + pl;   // position in the cell order
@@ -287,7 +287,7 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_build_list(PhysDev d, cons
             const int hx = __shfl_sync(0xffffffffu, cx, lead);
             const int hy = __shfl_sync(0xffffffffu, cy, lead);
             const int hz0 = __shfl_sync(0xffffffffu, cz, lead);
-            const bool mine = ((todo >> (pl * 4)) & 1u) && cx == hx && cy == hy && cz <= hz0 + (m - 5);
+            const bool mine = ((todo >> (pl * kSlices)) & 1u) && cx == hx && cy == hy && cz <= hz0 + (m - 5);
             const unsigned grp = __ballot_sync(0xffffffffu, mine && sub == 0);
             todo &= ~grp;
             // sorted by cell: the group's last particle has its top cell
@@ -723,7 +723,7 @@ void launch_permute(const PhysDev& d, int cur, bool mixed, cudaStream_t s) {
 }
 
 void launch_build_list(const PhysDev& d, const float4* pos, const uint32_t* items, cudaStream_t s) {
-    const int warps = (d.n + 7) / 8;
+    const int warps = (d.n + 32 / kSlices - 1) / (32 / kSlices);
     k_build_list<<<(warps + kBuildWarps - 1) / kBuildWarps, kBuildWarps * 32, 0, s>>>(d, pos, items);
 }
 

@@ -9,7 +9,8 @@ namespace lima {
 
 constexpr int kTB = 256;         // threads per block of the per-particle / per-term kernels
 constexpr int kGroup = 8;        // lanes per particle in the list and pair kernels
-constexpr int kBuildWarps = 4;   // warps (8 particles each) per block of the list build
+constexpr int kBuildWarps = 4;   // warps per block of the list build
+constexpr int kSlices = 8;       // lanes per particle in the list build (32 / kSlices particles per warp)
 constexpr int kMaxTypes = 32;    // LIMA_MAX_ATOM_TYPES
 
 void launch_keys(const PhysDev& d, const float4* pos, cudaStream_t s);
