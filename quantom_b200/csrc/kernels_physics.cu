@@ -196,9 +196,11 @@ __global__ void k_list_check(const int* need, unsigned long long* count, cudaGra
 // slots index the particle data and the list rows.
 namespace {
 
+// A warp's staged candidates, as two arrays so that the slices of one
+// particle read consecutive 16-byte positions.
 struct Cand {
-    float4 p;       // shifted position
-    uint32_t j;     // slot | bit 31 when the particle is a compound particle
+    float4 p[32];     // shifted positions
+    uint32_t j[32];   // slot | bit 31 when the particle is a compound particle
 };
 
 template <bool MIN_IMAGE>
@@ -213,19 +215,19 @@ __device__ __forceinline__ void scan_range(const PhysDev& d, const float4* __res
             const int j = items ? (int)items[jc + lane] : jc + lane;
             const float4 p = pos[j];
             const uint32_t oj = d.orig_of_sorted[j];
-            sc[lane].p = make_float4(p.x + sx, p.y + sy, p.z + sz, 0.f);
-            sc[lane].j = (uint32_t)j | (oj < (uint32_t)d.n_cp ? 0x80000000u : 0u);
+            sc->p[lane] = make_float4(p.x + sx, p.y + sy, p.z + sz, 0.f);
+            sc->j[lane] = (uint32_t)j | (oj < (uint32_t)d.n_cp ? 0x80000000u : 0u);
         }
         __syncwarp();
-        // slice `sub` tests candidates sub, sub + kSlices, ... (consecutive lanes of a
-        // particle read consecutive 32-byte records)
+        // slice `sub` tests candidates sub, sub + kSlices, ... (the slices of a
+        // particle read consecutive 16-byte positions: one wavefront per 8 lanes)
         uint32_t mine_bits = 0;
         if (mine) {
 #pragma unroll
             for (int t = 0; t < 32 / kSlices; t++) {
                 const int c = kSlices * t + sub;
                 if (c < nv) {
-                    const float4 q = sc[c].p;
+                    const float4 q = sc->p[c];
                     float dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
                     if (MIN_IMAGE) {
                         dx = mimg(dx, d.L, d.invL);
@@ -240,7 +242,7 @@ __device__ __forceinline__ void scan_range(const PhysDev& d, const float4* __res
             if (ex)
                 for (uint32_t b = mine_bits; b; b &= b - 1u) {
                     const int c = __ffs(b) - 1;
-                    const uint32_t jw = sc[c].j;
+                    const uint32_t jw = sc->j[c];
                     if ((jw >> 31) && excluded(d, oi, d.orig_of_sorted[jw & 0x7fffffffu])) mine_bits &= ~(1u << c);
                 }
         }
@@ -250,7 +252,7 @@ __device__ __forceinline__ void scan_range(const PhysDev& d, const float4* __res
         for (uint32_t b = mine_bits; b; b &= b - 1u) {
             const int c = __ffs(b) - 1;
             const int k = cnt + __popc(m32 & ((1u << c) - 1u));
-            if (k < d.nl_cap) d.nl[nl_index(d, i, k)] = sc[c].j & 0x7fffffffu;
+            if (k < d.nl_cap) d.nl[nl_index(d, i, k)] = sc->j[c] & 0x7fffffffu;
         }
         cnt += __popc(m32);
     }
@@ -260,12 +262,12 @@ __device__ __forceinline__ void scan_range(const PhysDev& d, const float4* __res
 
 __global__ void __launch_bounds__(kBuildWarps * 32) k_build_list(PhysDev d, const float4* __restrict__ pos,
                                                                  const uint32_t* __restrict__ items) {
-    __shared__ Cand s_cand[kBuildWarps][32];
+    __shared__ Cand s_cand[kBuildWarps];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int pl = lane / kSlices, sub = lane % kSlices;
     const int base = (blockIdx.x * kBuildWarps + w) * (32 / kSlices);
     if (base >= d.n) return;   // the whole warp
-    Cand* sc = s_cand[w];
+    Cand* sc = &s_cand[w];
     const int qi = base + pl;   // position in the cell order
     const bool have = qi < d.n;
     const int i = have ? (items ? (int)items[qi] : qi) : qi;   // slot
