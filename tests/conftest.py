@@ -70,3 +70,17 @@ def sorted_csr(off, ids):
     ids = np.asarray(ids, np.int64)
     return off, np.concatenate([np.sort(ids[off[i]:off[i + 1]]) for i in range(len(off) - 1)]) if len(off) > 1 \
         else np.zeros(0, np.int64)
+
+
+def make_named(name, seed):
+    """A workload by name: "6lzm" (the reference's demo box), "<config>_dry"
+    (that config with its solvents removed: compounds and bridges only), or a
+    config of quantom_b200.systems."""
+    import dataclasses
+    from quantom_b200 import systems as S
+    if name == "6lzm":
+        return S.load_6lzm()
+    if name.endswith("_dry"):
+        spec = dataclasses.replace(S.CONFIGS[name[:-4]], name=name, n_solvents=0)
+        return S.make_system(spec, seed=seed)
+    return S.make_system(name, seed=seed)

@@ -13,7 +13,7 @@ import functools
 import numpy as np
 import pytest
 
-from conftest import relrms
+from conftest import make_named, relrms
 from oracle import pyoracle as po
 from quantom_b200 import systems as S
 
@@ -42,7 +42,7 @@ def _positions(E, eng, s):
 
 @functools.lru_cache(maxsize=2)
 def _system_and_fp64_forces(name, seed):
-    s = S.load_6lzm() if name == "6lzm" else S.make_system(name, seed=seed)
+    s = make_named(name, seed)
     F64, en64 = po.PhysSystem(s, rc=s.spec.cutoff, r_on=1.0).forces()
     return s, F64, en64
 
@@ -51,7 +51,7 @@ def _system_and_fp64_forces(name, seed):
 # each) in 250,000 solvents, beyond the reference's 65,535-solvent layout
 @pytest.mark.parametrize("precision", [0, 1])
 @pytest.mark.parametrize("name", ["tiny_chains", "small_bridged", "lj_solvent_4096", "solvated_chains_32k",
-                                  "solvated_chains_258k", "6lzm"])
+                                  "solvated_chains_258k", "6lzm", "small_bridged_dry"])
 def test_forces_and_energies_match_fp64(gpu, name, precision):
     E = gpu
     s, F64, en64 = _system_and_fp64_forces(name, 7)

@@ -11,7 +11,7 @@ per-particle potE within 1e-6 relative.
 import numpy as np
 import pytest
 
-from conftest import compound_mask, golden_lists, load_golden, relrms, sorted_csr
+from conftest import compound_mask, golden_lists, load_golden, make_named, relrms, sorted_csr
 from oracle import pyoracle as po
 from quantom_b200 import systems as S
 
@@ -74,11 +74,13 @@ def test_matches_reference_fixtures(gpu, name):
 
 
 # 6lzm: the reference's own demo box (T4 lysozyme, 36 compounds, 35 bridges,
-# 5,000 waters) as its input path built it (tests/golden/golden_6lzm.npz)
-@pytest.mark.parametrize("name", ["tiny_chains", "small_bridged", "lj_solvent_4096", "solvated_chains_32k", "6lzm"])
+# 5,000 waters) as its input path built it (tests/golden/golden_6lzm.npz);
+# *_dry: compounds (and bridges) with no solvent
+@pytest.mark.parametrize("name", ["tiny_chains", "small_bridged", "lj_solvent_4096", "solvated_chains_32k", "6lzm",
+                                  "tiny_chains_dry", "small_bridged_dry"])
 def test_one_step_matches_oracle(gpu, name):
     E = gpu
-    s = S.load_6lzm() if name == "6lzm" else S.make_system(name, seed=7)
+    s = make_named(name, 7)
     lists = po.ref_nlist(s, ss_cap=1024, cells=True)
     new, fc_o, fs_o, pe_o = po.ref_step(s, lists)
     with _engine(E, s) as eng:

@@ -13,7 +13,7 @@ the bonded sums, see oracle/ref_emu.cpp).
 import numpy as np
 import pytest
 
-from conftest import compound_mask, golden_lists, load_golden, relrms, sorted_csr
+from conftest import compound_mask, golden_lists, load_golden, make_named, relrms, sorted_csr
 from oracle import pyoracle as po
 from quantom_b200 import systems as S
 
@@ -74,9 +74,9 @@ ref_needed = pytest.mark.skipif(not po.ref_available(), reason="reference build 
 
 
 @ref_needed
-@pytest.mark.parametrize("name", ["tiny_chains", "small_bridged", "tiny_solvent", "6lzm"])
+@pytest.mark.parametrize("name", ["tiny_chains", "small_bridged", "tiny_solvent", "6lzm", "small_bridged_dry"])
 def test_oracle_matches_reference_live(name):
-    s = S.load_6lzm() if name == "6lzm" else S.make_system(name, seed=21)
+    s = make_named(name, 21)
     ref = po.RefEngine(s, n_threads=4)
     ref.update_nlists()
     lists = po.ref_nlist(s, ss_cap=1024)
