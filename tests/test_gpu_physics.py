@@ -59,12 +59,9 @@ def test_forces_and_energies_match_fp64(gpu, name, precision):
         tot = eng.compute_energies()
         fc, fs = eng.forces()
     F = _flat(s, fc, fs)
-    # No solvent: each particle is wrapped into [0, L) on its own, so a bond across a
-    # box face (4 of the 188 in small_bridged_dry) starts from an FP32 difference of
-    # ~L: ~2.4e-7 nm at 5 nm, times k_bond 2.5e8 J/(mol nm^2), ~60 J/(mol nm) on
-    # forces of ~1e4.  Solvent forces dilute that in the other boxes' RMS.  The mixed
-    # path starts from the same FP32 positions (low words zero) and the same hi
-    # difference, so it shares the bar here.
+    # small_bridged_dry (no solvent) differs from the FP64 oracle by 3.8e-4 relative
+    # RMS in both precisions, a difference whose cause is still open (bonds across a
+    # box face were ruled out); it is held to 1e-3 meanwhile
     tol = 1e-3 if name.endswith("_dry") else 5e-5
     assert relrms(F, F64) < tol
     scale = abs(en64[0]) + abs(en64[3])
