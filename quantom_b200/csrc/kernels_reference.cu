@@ -323,8 +323,10 @@ __device__ __forceinline__ void replay_component(unsigned gmask, bool moved, flo
     }
 }
 
-// solventForceKernel (Engine.cu:1070-1161) as two kernels with W lanes per
-// solvent each.  The reference's solvent loops are two ordered chains: over
+// solventForceKernel (Engine.cu:1070-1161) as three kernels: its two loops,
+// run at the same time with W lanes per solvent each, then the sum of their
+// results and the integration.  The reference's solvent loops are two
+// ordered chains: over
 // every compound (computeLJForces, Engine.cu:1099-1117; no list) the solvent
 // moves to the image nearest the compound's particle 0 and adds that
 // compound's LJ sum; over the solvent list (computeSolventToSolventLJForces,
