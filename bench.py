@@ -145,14 +145,17 @@ def barrier(pg):
 
 
 class ClockSampler:
-    """SM clock and clock-event reasons sampled every 50 ms through NVML
-    (read-only queries) by a background thread; `window()` brackets the timed
-    region and `summary()` keeps the samples taken inside it."""
+    """SM clock and clock-event reasons sampled every 10 ms through NVML
+    (read-only queries) by a background thread, plus one sample at the entry
+    and one at the exit of the timed window, so a window shorter than the
+    period still has samples; `window()` brackets the timed region and
+    `summary()` keeps the samples taken inside it."""
     REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
                ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
 
-    def __init__(self, device, period_s=0.05):
+    def __init__(self, device, period_s=0.01):
         self.device = device
+        self._sample = None
         self.period = period_s
         self.samples = []          # (t, sm_mhz, reasons bitmask, power W)
         self.win = [None, None]
@@ -180,16 +183,20 @@ class ClockSampler:
             return self
         self._stop = threading.Event()
 
+        def sample():
+            try:
+                t = time.perf_counter()
+                sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+                pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                self.samples.append((t, sm, rs, pw))
+            except Exception:
+                pass
+        self._sample = sample
+
         def loop():
             while not self._stop.is_set():
-                try:
-                    t = time.perf_counter()
-                    sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
-                    rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
-                    pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
-                    self.samples.append((t, sm, rs, pw))
-                except Exception:
-                    pass
+                sample()
                 self._stop.wait(self.period)
 
         self._thr = threading.Thread(target=loop, daemon=True)
@@ -202,8 +209,12 @@ class ClockSampler:
         class _W:
             def __enter__(self_):
                 s.win[0] = time.perf_counter()
+                if s._sample:
+                    s._sample()   # one sample at the window's entry, whatever the period
 
             def __exit__(self_, *a):
+                if s._sample:
+                    s._sample()   # and one at its exit, before the window closes
                 s.win[1] = time.perf_counter()
         return _W()
 
@@ -224,7 +235,7 @@ class ClockSampler:
         return {"sm_mhz": statistics.median([x[1] for x in inside]) if inside else None,
                 "sm_max_mhz": self.sm_max, "reasons": reasons, "samples": len(inside),
                 "power_w_median": statistics.median([x[3] for x in inside]) if inside else None,
-                "source": "NVML, every 50 ms during the timed steps"}
+                "source": "NVML, every 10 ms during the timed steps and at the window's entry and exit"}
 
 
 def measured_peaks():
@@ -728,17 +739,19 @@ def c0_study(E, S, stream, flush, device):
 
 
 # --------------------------------------------------------------- CPU side --
-def cpu_reference_rate(system, steps, threads):
+def cpu_reference_rate(system, steps, threads, warmup=1):
     """Seconds per step of the reference's own step code on the host cores
     (oracle/_ref: Engine.cu kernels + host neighbour list), with its list
-    update (every 200 steps, Constants.cuh:71) amortised."""
+    update (every 200 steps, Constants.cuh:71) amortised: `warmup` untimed
+    steps, then `steps` timed ones, and one timed list update."""
     from oracle import pyoracle as po
     if po.ref_available():
         ref = po.RefEngine(system, n_threads=threads)
         t0 = time.perf_counter()
         ref.update_nlists()
         t_nl = time.perf_counter() - t0
-        ref.step(1)   # warm
+        if warmup > 0:
+            ref.step(warmup)
         t0 = time.perf_counter()
         ref.step(steps)
         t_step = (time.perf_counter() - t0) / steps
@@ -749,6 +762,8 @@ def cpu_reference_rate(system, steps, threads):
         lists = po.ref_nlist(system, cells=False, ss_cap=1024)
         t_nl = time.perf_counter() - t0
         s = system
+        for _ in range(warmup):
+            s, _, _, _ = po.ref_step(s, lists)
         t0 = time.perf_counter()
         for _ in range(steps):
             s, _, _, _ = po.ref_step(s, lists)
@@ -757,24 +772,47 @@ def cpu_reference_rate(system, steps, threads):
     return t_step + t_nl / 200.0, t_step, t_nl, kind, used
 
 
+def metric_name(workload):
+    """The headline metric string, identical in both arms."""
+    return f"ns/day, {workload}"
+
+
+def workload_text(workload, spec, n, ws):
+    """What the workload is, in BASELINE's terms and where it departs from them."""
+    if workload != WORKLOAD:
+        return workload
+    return (f"{workload}: 16 chains x 64 (4 LJ types, harmonic bonds/angles, periodic dihedrals, one compound per "
+            f"chain) + 31,000 single-site solvents = {n} particles, 10 nm cubic PBC box, dt 2 fs, Berendsen 300 K "
+            f"tau 0.1 ps; solvent positions uniform conditioned on a 0.28 nm minimum separation (0.95 sigma_ij where "
+            f"larger), sampled by hard-sphere Monte Carlo from a lattice instead of sequential rejection; LJ cut at "
+            f"1.2 nm with a C2 potential switch from 1.0 nm (plain truncation drifts); Verlet list skin 0.1 nm, "
+            f"rebuilt when a particle moved > skin/2")
+
+
 def run_reference_arm(args, ws, rank):
+    """The reference's own step code (Engine.cu built for the host, oracle/_ref)
+    on all host threads, on the same seeded box as the GPU arm.  The box is
+    packed by oracle/liblima_inputs.so (builder.cpp built for the host), so
+    this arm loads no library of the product."""
     if rank != 0:
         return
     from quantom_b200 import systems as S
     spec = S.CONFIGS[args.workload]
-    system = S.make_system(args.workload, seed=args.seed)
+    system = S.make_system(args.workload, seed=args.seed, packer_lib=ROOT / "oracle" / "liblima_inputs.so")
     threads = os.cpu_count() or 1
-    budget_steps = max(1, min(args.steps, 6))
-    per_step, t_step, t_nl, kind, used = cpu_reference_rate(system, budget_steps, threads)
+    steps, warmup = max(1, args.steps), max(0, args.warmup)
+    per_step, t_step, t_nl, kind, used = cpu_reference_rate(system, steps, threads, warmup)
     v = ns_per_day(spec.dt, per_step * 1e3)
-    sample = (f"{budget_steps} reference steps of the {system.n_particles}-particle box on {used} host threads "
-              f"(+ one neighbour-list update, {t_nl:.2f} s, amortised over its 200-step period)")
+    sample = (f"{steps} timed steps (after {warmup} untimed) of the reference's step code on the same "
+              f"{system.n_particles}-particle box, reference semantics, {used} host threads, plus one "
+              f"neighbour-list update ({t_nl:.2f} s) amortised over its 200-step period")
     print(json.dumps({
-        "impl": "reference", "metric": f"ns/day, {args.workload}", "value": v, "unit": "ns/day", "n_gpus": ws,
-        "steps": budget_steps, "warmup": 1, "ms_per_step": per_step * 1e3, "higher_is_better": True,
+        "impl": "reference", "metric": metric_name(args.workload), "value": v, "unit": "ns/day", "n_gpus": ws,
+        "steps": steps, "warmup": warmup, "ms_per_step": per_step * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-        "config": {"workload": args.workload, "particles": system.n_particles, "semantics": "reference",
-                   "dt_fs": spec.dt * 1e6},
+        "config": {"workload": workload_text(args.workload, spec, system.n_particles, ws),
+                   "particles": system.n_particles, "semantics": "reference", "dt_fs": spec.dt * 1e6,
+                   "force_integrate_ms_per_step": t_step * 1e3, "nlist_update_ms": t_nl * 1e3},
         "cpu_baseline": {"value": v, "unit": "ns/day", "cores": used, "kind": kind, "sample": sample},
         "e2e": {"value": v, "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
@@ -867,21 +905,43 @@ def run_ours(args, ws, rank, local, pg):
                        "oracle's central differences (bench.py --mode grad --fp64-fd) the gradient agrees to "
                        "8.5e-8 (sigma) and 5.8e-7 (epsilon) relative")
     # ---- roofline of the dominant kernel (pair + integrate) -----------------
+    # The pair terms are bound by the FP32 pipe: 32 FLOP per unique pair within
+    # r_c (minimum image 9, r^2 5, rcp 1, s^6 3, scalar force 5, vector force 3,
+    # accumulation on both sides 6), pairs = N (4/3) pi r_c^3 rho / 2.  The peak
+    # is clock-derived (148 SMs x 128 FP32 lanes x 2 FLOP x 1.965 GHz): the
+    # measured-peaks file holds HBM and bf16 figures only.  HBM is reported
+    # beside it on the compulsory 80 B per particle (read position + velocity,
+    # write position, velocity, force), and the ncu-measured DRAM traffic of one
+    # launch against those compulsory bytes.
     peaks = measured_peaks()
     hbm = peaks.get("hbm_gbs")
-    peak_src = "measured (MEASURED_PEAKS.json)"
+    hbm_src = "measured (MEASURED_PEAKS.json hbm_gbs)"
     if not hbm:
-        hbm, peak_src = 6650.0, "fallback"
+        hbm, hbm_src = 6650.0, "fallback"
     rho = n / spec.box_len ** 3
     pairs = n * (4.0 / 3.0) * math.pi * spec.cutoff ** 3 * rho / 2.0
     t_pair = prof["pair"] * 1e-3
-
-    list_len = (4.0 / 3.0) * math.pi * (spec.cutoff + SKIN) ** 3 * rho    # expected Verlet-list entries
-    # read pos, vel, 4-byte list entries; write pos, vel, force (16 B each)
-    bytes_pair = n * (80.0 + 4.0 * list_len)
     flops_pair = pairs * FLOP_PER_PAIR
-    achieved = bytes_pair / t_pair / 1e9
+    tflops = flops_pair / t_pair / 1e12
+    compulsory = 80.0 * n
+    list_len = (4.0 / 3.0) * math.pi * (spec.cutoff + SKIN) ** 3 * rho    # expected Verlet-list entries
+    bytes_list = n * (80.0 + 4.0 * list_len)
     traffic = ncu_traffic("k_pair_integrate", args.workload)
+    roofline = {
+        "kernel": "k_pair_integrate", "bound": "fp32", "achieved": tflops, "peak": FP32_NOMINAL_TFLOPS,
+        "unit": "TFLOP/s", "frac": tflops / FP32_NOMINAL_TFLOPS, "traffic": traffic,
+        "peak_source": "nominal, clock-derived (148 SMs x 128 lanes x 2 FLOP x 1.965 GHz); no measured FP32 figure",
+        "kernel_ms": prof["pair"], "flops_per_launch": flops_pair, "unique_pairs_within_rc": pairs,
+        "flop_per_pair": FLOP_PER_PAIR,
+        "hbm": {"compulsory_bytes_per_launch": compulsory, "achieved_gbs": compulsory / t_pair / 1e9,
+                "peak_gbs": hbm, "frac": compulsory / t_pair / 1e9 / hbm, "peak_source": hbm_src,
+                "traffic_over_compulsory": (traffic / compulsory) if traffic else None,
+                "list_inclusive": {"bytes_per_launch": bytes_list, "achieved_gbs": bytes_list / t_pair / 1e9,
+                                   "frac": bytes_list / t_pair / 1e9 / hbm,
+                                   "note": "counts the 4-byte Verlet-list entries (an implementation choice, "
+                                           "not algorithmic bytes)"}},
+        "step": {"ms": ms_step, "frac_fp32": flops_pair / (ms_step * 1e-3) / 1e12 / FP32_NOMINAL_TFLOPS},
+    }
     cpu = None
     c0 = None
     if ws == 1:
@@ -894,28 +954,17 @@ def run_ours(args, ws, rank, local, pg):
         c0 = c0_study(E, S, stream, flush, local)
     value = ws * ns_per_day(spec.dt, ms_step)
     out = {
-        "metric": f"ns/day, {args.workload} (32k particles)", "value": value, "unit": "ns/day", "n_gpus": ws,
+        "metric": metric_name(args.workload), "value": value, "unit": "ns/day", "n_gpus": ws,
         "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-        "config": {"workload": f"{args.workload}: 16 chains x 64 + 31,000 solvents, 10 nm box, rc 1.2 nm "
-                               f"(C2 switch from 1.0), skin 0.1 nm, list rebuilt when a particle moved > skin/2, Berendsen 300 K tau 0.1 ps, "
-                               f"dt 2 fs, plain FP32", "particles": n,
+        "mixed_ratio_to_fp32": ms_mixed / ms_step, "mixed_ms_per_step": ms_mixed,
+        "gpu_launches": launches,
+        "config": {"workload": workload_text(args.workload, spec, n, ws), "particles": n,
+                   "semantics": "physics (conservative LJ + bonded forms, velocity Verlet), plain FP32",
                    "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
                    "l2": "flushed before every timed step (256 MiB memset on the engine stream, outside the timed "
                          "events)"},
-        "mixed": {"ms_per_step": ms_mixed, "ratio_to_fp32": ms_mixed / ms_step,
-                  "l2_warm": {"fp32_ms_per_step": ms_warm, "mixed_ms_per_step": ms_mixed_warm,
-                              "ratio_to_fp32": ms_mixed_warm / ms_warm,
-                              "note": "the same steps without the L2 flush in between"},
-                  "ns_per_day": ns_per_day(spec.dt, ms_mixed), "kernels_ms": prof_m},
-        "reference_semantics_gpu": {"ms_per_step": ms_ref_sem, "ns_per_day": ns_per_day(spec.dt, ms_ref_sem)},
-        "kernels_ms": prof,
-        "roofline": {"kernel": "k_pair_integrate", "bound": "hbm", "achieved": achieved, "peak": hbm,
-                     "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic, "peak_source": peak_src,
-                     "algorithmic_bytes_per_launch": bytes_pair, "algorithmic_flops_per_launch": flops_pair,
-                     "fp32": {"achieved_tflops": flops_pair / t_pair / 1e12, "peak_tflops": FP32_NOMINAL_TFLOPS,
-                              "frac": flops_pair / t_pair / 1e12 / FP32_NOMINAL_TFLOPS,
-                              "peak_source": "nominal 148 SMs x 128 lanes x 2 x 1.965 GHz"}},
+        "roofline": roofline,
         "e2e": {"value": ws * ns_per_day(spec.dt, t_e2e * 1e3 / args.steps), "unit": "ns/day",
                 "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                 "split": e2e_split,
@@ -923,11 +972,19 @@ def run_ours(args, ws, rank, local, pg):
                         "N-step call; every step's FP64 energies read back through the frame log "
                         "(stream-ordered copies to pinned memory, no per-step sync), final state read back; the "
                         "engine's teardown comes after the clock stops"},
+        "clocks": clocks,
+        "mixed": {"ms_per_step": ms_mixed, "ratio_to_fp32": ms_mixed / ms_step,
+                  "l2_warm": {"fp32_ms_per_step": ms_warm, "mixed_ms_per_step": ms_mixed_warm,
+                              "ratio_to_fp32": ms_mixed_warm / ms_warm,
+                              "note": "the same steps without the L2 flush in between"},
+                  "ns_per_day": ns_per_day(spec.dt, ms_mixed), "kernels_ms": prof_m},
+        "reference_semantics_gpu": {"ms_per_step": ms_ref_sem, "ns_per_day": ns_per_day(spec.dt, ms_ref_sem),
+                                    "note": "the reference's own functional forms on the GPU, same box: the "
+                                            "same-semantics counterpart of the CPU reference arm"},
+        "kernels_ms": prof,
+        "steps_per_list_rebuild": steps_per_rebuild,
         "grad": grad,
         "c0": c0,
-        "gpu_launches": launches,
-        "steps_per_list_rebuild": steps_per_rebuild,
-        "clocks": clocks,
     }
     if cpu:
         out["cpu_baseline"] = cpu

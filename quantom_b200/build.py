@@ -5,6 +5,8 @@ One shared library holds the C-ABI (include/lima_abi.h), the host engine
 """
 from __future__ import annotations
 
+import hashlib
+from concurrent.futures import ThreadPoolExecutor
 import os
 import subprocess
 import sys
@@ -34,24 +36,47 @@ def sources():
     return sorted(list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cpp")))
 
 
+def _stamp(cmd, src, headers) -> str:
+    """Content hash of one object's inputs: the compile command, the source and
+    every header (an object is reused only when none of them changed)."""
+    h = hashlib.sha256(" ".join(cmd).encode())
+    for f in [src, *sorted(headers)]:
+        h.update(f.name.encode())
+        h.update(f.read_bytes())
+    return h.hexdigest()
+
+
 def build(verbose: bool = False, force: bool = False) -> Path:
+    """Compile every source to _build/*.o and link the library.  An object is
+    recompiled when the content hash of its command, source and the headers
+    differs from the one recorded beside it, or always with force=True."""
     BUILD.mkdir(exist_ok=True)
     srcs = sources()
-    headers = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [ROOT / "include" / "lima_abi.h"]
-    newest_hdr = max((h.stat().st_mtime for h in headers if h.exists()), default=0)
+    headers = [h for h in list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [ROOT / "include" / "lima_abi.h"]
+               if h.exists()]
     objs = []
+    jobs = []
     nvcc = _nvcc()
     for s in srcs:
         o = BUILD / (s.name + ".o")
         objs.append(o)
-        if not force and o.exists() and o.stat().st_mtime >= max(s.stat().st_mtime, newest_hdr):
-            continue
         cmd = [nvcc, *ARCH, *NVCC_FLAGS, *PER_FILE.get(s.name, []), "-c", str(s), "-o", str(o)]
         if s.suffix == ".cpp":
             cmd = [nvcc, *NVCC_FLAGS, "-x", "cu", *ARCH, "-c", str(s), "-o", str(o)]
+        stamp_file = o.with_suffix(".o.sha256")
+        stamp = _stamp(cmd, s, headers)
+        if not force and o.exists() and stamp_file.exists() and stamp_file.read_text() == stamp:
+            continue
+        jobs.append((cmd, stamp_file, stamp))
+
+    def compile_one(job):
+        cmd, stamp_file, stamp = job
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
+        stamp_file.write_text(stamp)
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+        list(pool.map(compile_one, jobs))
     tmp = OUT.with_suffix(".so.tmp")
     cmd = [nvcc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart", "-Xcompiler", "-fPIC"]
     if verbose:

@@ -131,9 +131,16 @@ CONFIGS = {
 }
 
 
-def _lib_builder():
-    from .engine import load_library
-    lib = load_library()
+def _lib_builder(lib_path=None):
+    """`lima_builder_pack_spheres` from the product library, or from the
+    library at `lib_path` (the same builder.cpp compiled on its own for the
+    host, so that a caller timing a CPU implementation builds identical inputs
+    without loading any CUDA code)."""
+    if lib_path is not None:
+        lib = ctypes.CDLL(str(lib_path))
+    else:
+        from .engine import load_library
+        lib = load_library()
     fn = lib.lima_builder_pack_spheres
     fn.restype = ctypes.c_long
     fn.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
@@ -217,7 +224,10 @@ def _mb_velocities(rng, masses, temperature):
     return v
 
 
-def make_system(name_or_spec, seed: int = 2024) -> System:
+def make_system(name_or_spec, seed: int = 2024, packer_lib=None) -> System:
+    """The seeded system `name_or_spec`.  packer_lib (optional): path of a
+    host build of builder.cpp to pack the solvents with instead of the
+    product library (bit-identical output)."""
     spec = CONFIGS[name_or_spec] if isinstance(name_or_spec, str) else name_or_spec
     rng = np.random.default_rng(seed)
     box = spec.box_len
@@ -269,7 +279,7 @@ def make_system(name_or_spec, seed: int = 2024) -> System:
 
     # ---- solvents --------------------------------------------------------
     out = np.zeros((spec.n_solvents, 3))
-    pack = _lib_builder()
+    pack = _lib_builder(packer_lib)
     fixed_c = np.ascontiguousarray(fixed, dtype=np.float64)
     fixed_r = np.ascontiguousarray(fixed_rmin if len(fixed_rmin) else np.zeros(1), dtype=np.float64)
     acc = pack(box, spec.min_sep, fixed_c.ctypes.data, fixed_r.ctypes.data, len(fixed_c), spec.n_solvents,

@@ -8,6 +8,7 @@ the native builder (lima_topology_build) in tests/test_topology.py.
 
     python tests/golden/make_6lzm.py [reference root]
 """
+import os
 import sys
 from pathlib import Path
 
@@ -26,7 +27,7 @@ def demo_paths(ref_root):
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("LIMA_REF_ROOT", "/root/reference")
     gro, top, prms = demo_paths(ref_root)
     box = po.ref_input_box(gro, top, prms)
     # entries past each count are left uninitialised by the reference: zero them

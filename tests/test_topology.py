@@ -4,6 +4,7 @@ CompoundBuilder, BoxBuilder; tests/golden/golden_6lzm.npz and, where the
 reference tree is present, a live run of it), and its rules on a small system
 written here."""
 import ctypes
+import os
 from pathlib import Path
 
 import numpy as np
@@ -12,7 +13,8 @@ import pytest
 from oracle import pyoracle as po
 from quantom_b200 import systems as S
 
-REF = Path("/root/reference")
+# the reference tree: $LIMA_REF_ROOT, as the oracle build scripts read it
+REF = Path(os.environ.get("LIMA_REF_ROOT", "/root/reference"))
 DEMO = REF / "Demo"
 PRMS = [DEMO / "CHARMM_FF" / n for n in ("par_all36_lipid.prm", "par_all36_na.prm", "par_all36m_prot.prm")]
 GRO, TOP = DEMO / "6lzm" / "conf.gro", DEMO / "6lzm" / "topol.top"
