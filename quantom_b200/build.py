@@ -23,7 +23,10 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
               "--expt-relaxed-constexpr", f"-I{ROOT / 'include'}", f"-I{CSRC}"]
 # Reference-semantics kernels reproduce the reference's host-compiled float
 # operation order: no a*b+c contraction into FMA in that translation unit.
-PER_FILE = {"kernels_reference.cu": ["-fmad=false"], "nlist_reference.cu": ["-fmad=false"]}
+# The physics step kernel launches the list rebuild graph from the device
+# (device graph launch): relocatable device code, linked with cudadevrt.
+PER_FILE = {"kernels_reference.cu": ["-fmad=false"], "nlist_reference.cu": ["-fmad=false"],
+            "kernels_physics.cu": ["-rdc=true"]}
 
 
 def _nvcc() -> str:
@@ -78,7 +81,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
         list(pool.map(compile_one, jobs))
     tmp = OUT.with_suffix(".so.tmp")
-    cmd = [nvcc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart", "-Xcompiler", "-fPIC"]
+    cmd = [nvcc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudadevrt", "-lcudart", "-Xcompiler", "-fPIC"]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)

@@ -723,19 +723,36 @@ int adj_run(const PhysDev& d0, int cur, const PhysParams& pp, AdjBuffers& A, std
     cudaMemsetAsync(d.err, 0, sizeof(int), s);
 
     const int start_cur = cur;
+    // the first launch or copy that failed, for the error message
+    const char* fail_at = nullptr;
+    cudaError_t fail_err = cudaSuccess;
+    auto note = [&](const char* where) {
+        if (fail_at) return;
+        const cudaError_t e = cudaPeekAtLastError();
+        if (e != cudaSuccess) {
+            fail_at = where;
+            fail_err = e;
+        }
+    };
+    note("set-up copies");
     // forward: checkpoints at the start of every segment (re-sorted from orig
     // order there, so a recomputation reproduces the trajectory bit for bit)
     R.save(cur, 0);
+    note("checkpoint save");
     for (int k = 0; k < K; k++) {
         const bool last = k == K - 1;
         if (grad && last) break;   // the backward pass recomputes the last segment anyway
         R.restore(cur, k);
+        note("checkpoint restore and list rebuild");
         const int n0 = k * C, len = std::min(C, T - n0);
         for (int q = 0; q < len; q++) {
             if (q > 0 && q % kListEpoch == 0) phys_rebuild_inplace(d, d.pos[cur], s);
+            note("in-place list rebuild");
             phys_step_kernels(d, cur, s, false);
+            note("forward step kernels");
             cur ^= 1;
             if (!grad) R.loss_pass(cur, d.pos[cur], d.pos_orig[cur], n0 + q + 1);
+            note("loss pass");
         }
         if (!last) R.save(cur, k + 1);
     }
@@ -820,11 +837,12 @@ int adj_run(const PhysDev& d0, int cur, const PhysParams& pp, AdjBuffers& A, std
     // leave the state as found: restore the first checkpoint into the starting parity
     if (cur != start_cur) cur = start_cur;
     R.restore(cur, 0);
-    cudaMemsetAsync(d.acc, 0, sizeof(double) * kAccSlots * LIMA_E_COUNT, s);
-    cudaMemsetAsync(d.acc_energy, 0, sizeof(int) * kAccSlots, s);
     cudaStreamSynchronize(s);
-    if (cudaGetLastError() != cudaSuccess) {
-        msg = "CUDA error in the loss / adjoint passes";
+    note("the passes");
+    const cudaError_t last_err = cudaGetLastError();
+    if (fail_at || last_err != cudaSuccess) {
+        msg = std::string("CUDA error in the loss / adjoint passes (") + (fail_at ? fail_at : "the passes") + "): " +
+              cudaGetErrorString(fail_at ? fail_err : last_err);
         return LIMA_ERR_CUDA;
     }
     if (err) {

@@ -92,6 +92,7 @@ struct lima_ctx {
     }
     ~lima_ctx() {
         lima::framelog_free(log);
+        lima::phys_free_rebuild(phys);
         for (auto& g : graph)
             if (g) cudaGraphExecDestroy(g);
         for (auto& row : dgraph)
@@ -388,6 +389,7 @@ void check_device_errors(lima_ctx* c) {
             m += "pair list went stale: a particle moved more than skin/2 between rebuilds (raise skin or lower "
                  "nlist_period); ";
         if (h & lima::ERR_BIT_TILE_TIMEOUT) m += "shared-memory staging wait timed out; ";
+        if (h & lima::ERR_BIT_REBUILD_LAUNCH) m += "the device could not launch a due pair-list rebuild; ";
         if (h & lima::ERR_BIT_NAN) m += "NaN position; ";
         if (h & lima::ERR_BIT_CRITICAL_FORCE) m += "critical force (|F| > 2e12); ";
         const bool cap = h & (lima::ERR_BIT_SS_OVERFLOW | lima::ERR_BIT_CS_OVERFLOW | lima::ERR_BIT_CC_OVERFLOW |
@@ -652,12 +654,14 @@ lima_status lima_finish_box(lima_ctx* c) {
             sync_checked(c);
             lima::phys_params_init(c->phys, c->ff, c->params, c->stream);
             if (c->phys.dynamic_list) {
+                std::string rmsg;
+                const int rrc = lima::phys_capture_rebuild(c->phys, c->stream, rmsg);
+                if (rrc != 0) fail(static_cast<lima_status>(rrc), rmsg);
                 for (int parity = 0; parity < 2; parity++)
                     for (int energy = 0; energy < 2; energy++) {
                         const int k = lima::phys_capture_dynamic(c->phys, parity, energy != 0, c->stream,
                                                                  &c->dgraph[parity][energy]);
-                        need(k > 0, LIMA_ERR_CUDA,
-                             "dynamic pair lists need CUDA graphs with conditional nodes (CUDA 12.4+ driver)");
+                        need(k > 0, LIMA_ERR_CUDA, "cannot build the step graph of a dynamic pair list");
                         c->dgraph_kernels[energy] = k;
                     }
             } else {
@@ -718,6 +722,14 @@ lima_status lima_profile_steps(lima_ctx* c, int n_steps, float* ms) {
         }
         for (auto& e : ev) cudaEventDestroy(e);
         if (st != LIMA_OK) fail(st, msg);
+        // the profiled steps ran outside the step graphs, so a rebuild the last
+        // one asked for is still due: run it before the next step
+        if (c->p.semantics == LIMA_SEMANTICS_PHYSICS && c->phys.dynamic_list &&
+            lima::phys_rebuild_pending(c->phys, c->stream)) {
+            lima::phys_rebuild(c->phys, c->cur, c->stream);
+            c->launches += lima::kRebuildKernels;
+            c->host_rebuilds++;
+        }
         for (int k = 0; k < LIMA_PROF_COUNT; k++) ms[k] = static_cast<float>(acc[k] / n_steps);
         sync_checked(c);
     });
@@ -921,19 +933,13 @@ lima_status lima_compute_energies(lima_ctx* c) {
         need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
         need(c->p.semantics == LIMA_SEMANTICS_PHYSICS, LIMA_ERR_UNSUPPORTED,
              "the reference computes no LJ energy; reference semantics report potE of the last step");
-        // fold the last step's accumulators first, so the readback that follows
-        // reports this evaluation's kinetic energy, not the previous step's
-        if (c->step > 0) {
-            lima::phys_finalize(c->phys, c->cur, c->stream);
-            c->launches++;
-        }
         if (c->phys.dynamic_list && lima::phys_rebuild_pending(c->phys, c->stream)) {
             lima::phys_rebuild(c->phys, c->cur, c->stream);
             c->launches += lima::kRebuildKernels;
             c->host_rebuilds++;
         }
         lima::phys_energy_now(c->phys, c->cur, c->stream);
-        c->launches += 3;
+        c->launches += 2;
         sync_checked(c);
     });
 }
@@ -963,10 +969,6 @@ lima_status lima_get_energies(lima_ctx* c, double* totals, double* per_particle)
                 totals[LIMA_E_TEMPERATURE] = temp;
             }
         } else {
-            if (c->step > 0) {   // fold the last step's FP64 accumulators
-                lima::phys_finalize(c->phys, c->cur, c->stream);
-                sync_checked(c);
-            }
             lima::phys_read_energies(c->phys, totals, per_particle, c->comps.data(), nc, ns);
         }
     });

@@ -20,22 +20,11 @@
 namespace lima {
 namespace {
 
-constexpr double kRgas = 8.314462618;   // J/(mol K)
-
 __global__ void __launch_bounds__(kTB) k_log_frame(PhysDev d, FrameLogDev g, int cur, int r) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k == 0 && g.energies) {
-        const double* a = d.acc + cur * LIMA_E_COUNT;
+    if (k == 0 && g.energies) {   // the step kernel's FP64 totals of the logged step
         double* e = g.energies + (size_t)r * LIMA_E_COUNT;
-        const double pot = a[LIMA_E_LJ] + a[LIMA_E_BOND] + a[LIMA_E_ANGLE] + a[LIMA_E_DIHEDRAL];
-        e[LIMA_E_LJ] = a[LIMA_E_LJ];
-        e[LIMA_E_BOND] = a[LIMA_E_BOND];
-        e[LIMA_E_ANGLE] = a[LIMA_E_ANGLE];
-        e[LIMA_E_DIHEDRAL] = a[LIMA_E_DIHEDRAL];
-        e[LIMA_E_KINETIC] = a[LIMA_E_KINETIC];
-        e[LIMA_E_VIRIAL] = a[LIMA_E_VIRIAL];
-        e[LIMA_E_TEMPERATURE] = 2.0 * a[LIMA_E_KINETIC] / (3.0 * (double)d.n * kRgas);
-        e[LIMA_E_TOTAL] = pot + a[LIMA_E_KINETIC];
+        for (int q = 0; q < LIMA_E_COUNT; q++) e[q] = d.e_last[q];
     }
     if (k >= d.n) return;
     const uint32_t o = d.orig_of_sorted[k];

@@ -3,24 +3,29 @@
 // Verlet with an optional Berendsen thermostat.  FP32 forces; in MIXED
 // precision the force sums are compensated (every 8 pairs per lane and across
 // lanes) and positions/velocities carry FP32 low parts; energy, virial and
-// kinetic-energy reductions and the thermostat scalar are FP64.
+// kinetic-energy reductions and the thermostat scalar are FP64, summed in a
+// fixed order (run-to-run identical).
 //
 // Layout: particles sorted by cell (side >= r_list/2, x-major), so the
 // kGroup = 8 lanes of the 4 particles a warp handles share a cell and read
 // largely the same neighbours — the position gathers of a warp hit L1.
 //
-// Per step (two launches, captured in a CUDA graph):
-//   k_bonded          one thread per bonded term -> term_force slots; block 0
-//                     also folds the previous step's FP64 accumulators into
-//                     e_last and the Berendsen lambda for this step
-//   k_pair_integrate  8 lanes per particle walk its Verlet list (blocked so
-//                     the lanes of consecutive particles read one line),
-//                     branch-free LJ + switch, partial forces reduced with
-//                     warp shuffles; lane 0 gathers the bonded term forces,
-//                     kicks, drifts and adds 1/2 m v^2 to the FP64 accumulator
-// Every nlist_period steps (physics_host.cu): k_keys, a radix sort by cell,
-// k_permute, and k_build_list — one warp per cell over the 25 columns of its
-// 5x5x5 neighbourhood.
+// Per step, one launch (captured in a CUDA graph):
+//   k_step   8 lanes per particle walk its Verlet list (blocked so the
+//            lanes of consecutive particles read one line), branch-free LJ +
+//            switch; a compound particle's lanes also evaluate the bonded
+//            terms it takes part in and keep its role's force; partial forces
+//            reduced with warp shuffles; lane 0 kicks, drifts and gives the
+//            kinetic energy.  Each block sums its FP64 values in a fixed
+//            order into a partial; the block that finishes last adds the
+//            partials in block order, sets the next step's Berendsen scalar
+//            and, when a particle moved more than skin/2, tail-launches the
+//            rebuild graph, which runs before the next step.
+// Rebuild (a device-launchable graph, or host launches): k_sort_count,
+// k_sort_scan, k_sort_fill, k_sort_order (a stable counting sort by cell),
+// k_permute + k_copy_back (every per-slot array into the new order) and
+// k_build_list — one warp per 4 particles over the 25 columns of their
+// 5x5x5 cell neighbourhood.
 #include "physdev.cuh"
 #include "physkern.cuh"
 #include "physmath.cuh"
@@ -45,14 +50,10 @@ __device__ __forceinline__ void ds_add(float& hi, float& lo, float x) {
     lo = e;
 }
 
+// lane 0 receives the warp's sum; the order of the additions is fixed
 __device__ __forceinline__ double warp_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     return v;
-}
-
-__device__ __forceinline__ void block_add(double* acc, int idx, double v) {
-    v = warp_sum(v);
-    if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(&acc[idx], v);
 }
 
 __device__ __forceinline__ void cell_xyz(const PhysDev& d, float4 p, int& cx, int& cy, int& cz) {
@@ -72,52 +73,92 @@ __device__ __forceinline__ bool excluded(const PhysDev& d, uint32_t oi, uint32_t
     return false;
 }
 
-// Fold an accumulator slot into e_last; parity slots also set the next
-// step's Berendsen lambda.  Idempotent: a folded slot reads zero.
-__device__ void fold(const PhysDev& d, int src) {
-    volatile double* a = d.acc + src * LIMA_E_COUNT;
-    const double kin = a[LIMA_E_KINETIC];
-    if (kin == 0.0) return;
-    const double temp = 2.0 * kin / (3.0 * (double)d.n * kR);
-    d.e_last[LIMA_E_KINETIC] = kin;
-    d.e_last[LIMA_E_TEMPERATURE] = temp;
-    if (d.acc_energy[src]) {
-        d.e_last[LIMA_E_LJ] = a[LIMA_E_LJ];
-        d.e_last[LIMA_E_BOND] = a[LIMA_E_BOND];
-        d.e_last[LIMA_E_ANGLE] = a[LIMA_E_ANGLE];
-        d.e_last[LIMA_E_DIHEDRAL] = a[LIMA_E_DIHEDRAL];
-        d.e_last[LIMA_E_VIRIAL] = a[LIMA_E_VIRIAL];
-        d.e_last[LIMA_E_TOTAL] = a[LIMA_E_LJ] + a[LIMA_E_BOND] + a[LIMA_E_ANGLE] + a[LIMA_E_DIHEDRAL] + kin;
-        d.acc_energy[src] = 0;
-    }
-    if (src < 2) {
-        float lam = 1.f;
-        if (d.thermostat == LIMA_THERMOSTAT_BERENDSEN && temp > 0.0)
-            lam = (float)sqrt(1.0 + d.dt / d.tau_t * (d.t_target / temp - 1.0));
-        d.lambda[src ^ 1] = lam;
-    }
-    for (int q = 0; q < LIMA_E_COUNT; q++) a[q] = 0.0;
-}
-
 }  // namespace
 
-// ---------------------------------------------------------------- rebuild ---
-__global__ void k_keys(PhysDev d, const float4* __restrict__ pos) {
+// ----------------------------------------------------- counting sort by cell ---
+// Cell of every slot and its arrival rank in the cell (atomic, so the ranks
+// are put in slot order by k_sort_order).
+__global__ void k_sort_count(PhysDev d, const float4* __restrict__ pos) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= d.n) return;
     int cx, cy, cz;
     cell_xyz(d, pos[i], cx, cy, cz);
-    d.keys[0][i] = (uint32_t)((cx * d.m + cy) * d.m + cz);
-    d.vals[0][i] = i;
+    const uint32_t c = (uint32_t)((cx * d.m + cy) * d.m + cz);
+    d.cell_key[i] = c;
+    d.cell_rank[i] = atomicAdd(&d.ccount[c], 1u);
 }
 
+// One block: exclusive scan of the cell occupancies into cstart (cstart[n_cells]
+// = n); the occupancies are reset to zero for the next sort.  Thread t owns a
+// contiguous run of cells.
+__global__ void __launch_bounds__(kScanThreads) k_sort_scan(PhysDev d) {
+    __shared__ uint32_t s_warp[kScanThreads / 32];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int per = (d.n_cells + kScanThreads - 1) / kScanThreads;
+    const int b = t * per, e = min(d.n_cells, b + per);
+    uint32_t sum = 0u;
+    for (int c = b; c < e; c++) sum += d.ccount[c];
+    uint32_t x = sum;   // inclusive scan over the warp
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[w] = x;
+    __syncthreads();
+    if (w == 0) {   // kScanThreads / 32 == 32 warp totals
+        uint32_t v = s_warp[lane];
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += y;
+        }
+        s_warp[lane] = v;
+    }
+    __syncthreads();
+    uint32_t run = (w ? s_warp[w - 1] : 0u) + x - sum;
+    for (int c = b; c < e; c++) {
+        const uint32_t k = d.ccount[c];
+        d.cstart[c] = run;
+        d.ccount[c] = 0u;
+        run += k;
+    }
+    if (t == 0) d.cstart[d.n_cells] = (uint32_t)d.n;
+}
+
+__global__ void k_sort_fill(PhysDev d) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    d.order[d.cstart[d.cell_key[i]] + d.cell_rank[i]] = (uint32_t)i;
+}
+
+// One thread per cell: the cell's slots in ascending order (insertion sort;
+// cells hold ~10 particles), which makes the sort stable and the new order a
+// function of the positions and the old order only.
+__global__ void k_sort_order(PhysDev d) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= d.n_cells) return;
+    const uint32_t b = d.cstart[c], e = d.cstart[c + 1];
+    for (uint32_t k = b + 1; k < e; k++) {
+        const uint32_t v = d.order[k];
+        uint32_t j = k;
+        while (j > b && d.order[j - 1] > v) {
+            d.order[j] = d.order[j - 1];
+            j--;
+        }
+        d.order[j] = v;
+    }
+}
+
+// Every per-slot array gathered into cell order (tmp arrays); reference
+// positions of the list; the orig <-> slot maps.
 __global__ void k_permute(PhysDev d, int cur, int mixed) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= d.n) return;
-    const uint32_t src = d.vals[1][k];
+    const uint32_t src = d.order[k];
     const float4 p = d.pos[cur][src];
-    d.pos_tmp[k] = p;
+    d.pos_tmp[0][k] = p;
+    d.pos_tmp[1][k] = d.pos[cur ^ 1][src];
     d.vel_tmp[k] = d.vel[src];
+    d.force_tmp[k] = d.force[src];
     if (mixed) {
         d.posc_tmp[k] = d.posc[src];
         d.velc_tmp[k] = d.velc[src];
@@ -126,33 +167,11 @@ __global__ void k_permute(PhysDev d, int cur, int mixed) {
     d.orig_tmp[k] = o;
     d.sorted_of_orig[o] = k;
     d.xref[k] = p;
-    // cstart[c] = first sorted slot of cell c for every c in 0..n_cells (empty cells included)
-    const uint32_t c = d.keys[1][k];
-    if (k == 0) {
-        for (uint32_t q = 0; q <= c; q++) d.cstart[q] = 0;
-    } else {
-        const uint32_t cp = d.keys[1][k - 1];
-        for (uint32_t q = cp + 1; q <= c; q++) d.cstart[q] = k;
-    }
-    if (k == d.n - 1)
-        for (uint32_t q = c + 1; q <= (uint32_t)d.n_cells; q++) d.cstart[q] = d.n;
 }
 
-// In-place rebuild: cell offsets of the sorted keys (the particles stay where
-// they are; vals[1] lists them in cell order) and the list's reference positions.
-__global__ void k_cell_offsets(PhysDev d, const float4* __restrict__ pos) {
+__global__ void k_set_xref(PhysDev d, const float4* __restrict__ pos) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= d.n) return;
-    d.xref[k] = pos[k];
-    const uint32_t c = d.keys[1][k];
-    if (k == 0) {
-        for (uint32_t q = 0; q <= c; q++) d.cstart[q] = 0;
-    } else {
-        const uint32_t cp = d.keys[1][k - 1];
-        for (uint32_t q = cp + 1; q <= c; q++) d.cstart[q] = k;
-    }
-    if (k == d.n - 1)
-        for (uint32_t q = c + 1; q <= (uint32_t)d.n_cells; q++) d.cstart[q] = d.n;
+    if (k < d.n) d.xref[k] = pos[k];
 }
 
 // Sorted copies back into the step arrays; clears the rebuild request.
@@ -160,21 +179,15 @@ __global__ void k_copy_back(PhysDev d, int cur, int mixed) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k == 0) *d.need_rebuild = 0;
     if (k >= d.n) return;
-    d.pos[cur][k] = d.pos_tmp[k];
+    d.pos[cur][k] = d.pos_tmp[0][k];
+    d.pos[cur ^ 1][k] = d.pos_tmp[1][k];
     d.vel[k] = d.vel_tmp[k];
+    d.force[k] = d.force_tmp[k];
     if (mixed) {
         d.posc[k] = d.posc_tmp[k];
         d.velc[k] = d.velc_tmp[k];
     }
     d.orig_of_sorted[k] = d.orig_tmp[k];
-}
-
-// First node of a dynamic-list step graph: requests the conditional rebuild
-// when the previous step's pair kernel asked for one.
-__global__ void k_list_check(const int* need, unsigned long long* count, cudaGraphConditionalHandle h) {
-    const int v = *need;
-    cudaGraphSetConditional(h, v ? 1u : 0u);
-    if (v) *count += 1ull;
 }
 
 // Verlet-list build: one warp per 32 / kSlices consecutive sorted particles,
@@ -332,14 +345,50 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_build_list(PhysDev d, cons
     }
 }
 
-// ----------------------------------------------------------------- bonded ---
+// ------------------------------------------------------------- bonded terms ---
 // The bonded terms read the orig-ordered compound positions (pos_orig), none
-// of the arrays a list rebuild re-sorts, so a rebuild may run concurrently.
-// MIXED: every bond vector is (b_hi - a_hi) + (b_lo - a_lo), so the stiff
-// bonded forces see the (hi, lo) positions, not their FP32 rounding.
+// of the arrays a list rebuild re-sorts.  MIXED: every bond vector is
+// (b_hi - a_hi) + (b_lo - a_lo), so the stiff bonded forces see the (hi, lo)
+// positions, not their FP32 rounding.
+namespace {
+
+// programmatic dependent launch: let the next kernel of the stream start /
+// wait until the kernels this one depends on have finished and their writes
+// are visible (a no-op without a programmatic dependency)
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// lane 0 receives the warp's sum of v[0..K); then thread 0 adds the warps in
+// order into out[0..K) (fixed order)
+template <int K>
+__device__ __forceinline__ void block_sums_fixed(double (&v)[K], double* out) {
+    __shared__ double s_b[kTB / 32][K];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < K; q++) {
+        const double x = warp_sum(v[q]);
+        if (lane == 0) s_b[w][q] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int q = 0; q < K; q++) {
+            double t = 0.0;
+            for (int k = 0; k < (int)(blockDim.x / 32); k++) t += s_b[k][q];
+            out[q] = t;
+        }
+}
+
+}  // namespace
+
+// One thread per bonded term: the forces on its atoms into its term_force
+// slots (w: each atom's share of the term's energy).  The step kernel that
+// follows is launched programmatically and starts right away; only the lanes
+// that gather these slots wait for this kernel.  ENERGY: per-block FP64 sums
+// of the bond, angle and dihedral energies and the virial into bpart.
 template <bool ENERGY, bool MIXED>
-__global__ void __launch_bounds__(kTB) k_bonded(PhysDev d, int cur, int slot, int fold_src) {
-    if (fold_src >= 0 && blockIdx.x == 0 && threadIdx.x == 0) fold(d, fold_src);
+__global__ void __launch_bounds__(kTB) k_bonded(PhysDev d, int cur) {
+    pdl_launch_dependents();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double eb = 0.0, ea = 0.0, ed = 0.0, vir = 0.0;
     const float L = d.L, iL = d.invL;
@@ -446,19 +495,102 @@ __global__ void __launch_bounds__(kTB) k_bonded(PhysDev d, int cur, int slot, in
         }
     }
     if (ENERGY) {
-        double* acc = d.acc + slot * LIMA_E_COUNT;
-        block_add(acc, LIMA_E_BOND, eb);
-        block_add(acc, LIMA_E_ANGLE, ea);
-        block_add(acc, LIMA_E_DIHEDRAL, ed);
-        block_add(acc, LIMA_E_VIRIAL, vir);
+        double v[4] = {eb, ea, ed, vir};
+        block_sums_fixed<4>(v, d.bpart + (size_t)blockIdx.x * 4);
     }
 }
 
-__global__ void k_finalize(PhysDev d, int src) { fold(d, src); }
+namespace {
 
-// ------------------------------------------------------- pair + integrate ---
+// The FP64 sums of a step kernel (kinetic energy; with ENERGY also the LJ
+// energy and virial), per block in a fixed order, then over the blocks by the
+// block that finishes last (in block order).  That block adds the bonded
+// kernel's block partials (ENERGY), folds the totals into e_last and the next
+// Berendsen scalar and, when a rebuild is due and `tail` is set, launches it.
+// TAIL: this kernel may launch the rebuild graph; a kernel that holds a
+// device-side graph launch must itself run inside a graph, so the direct
+// launches use the variant without it.
+template <bool ENERGY, bool INTEGRATE, bool TAIL>
+__device__ __forceinline__ void finish_sums(const PhysDev& d, int slot, cudaGraphExec_t tail, double (&v)[kRed]) {
+    __shared__ double s_red[kTB / 32][kRed];
+    __shared__ int s_last;
+    constexpr int nq = ENERGY ? kRed : 1;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < nq; q++) {
+        const double x = warp_sum(v[q]);
+        if (lane == 0) s_red[w][q] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < nq; q++) {
+            double t = 0.0;
+            for (int k = 0; k < kTB / 32; k++) t += s_red[k][q];
+            d.part[(size_t)blockIdx.x * kRedStride + q] = t;
+        }
+        __threadfence();
+        s_last = atomicAdd(d.done, 1u) == gridDim.x - 1u;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    double a[kRed];
+#pragma unroll
+    for (int q = 0; q < nq; q++) a[q] = 0.0;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+#pragma unroll
+        for (int q = 0; q < nq; q++) a[q] += __ldcg(&d.part[(size_t)b * kRedStride + q]);
+#pragma unroll
+    for (int q = 0; q < nq; q++) {
+        const double x = warp_sum(a[q]);
+        if (lane == 0) s_red[w][q] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    double tot[kRed] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int q = 0; q < nq; q++)
+        for (int k = 0; k < kTB / 32; k++) tot[q] += s_red[k][q];
+    const double kin = tot[0];
+    const double temp = 2.0 * kin / (3.0 * (double)d.n * kR);
+    d.e_last[LIMA_E_KINETIC] = kin;
+    d.e_last[LIMA_E_TEMPERATURE] = temp;
+    if (ENERGY) {
+        // the bonded kernel's block partials (bond, angle, dihedral, virial), in block order
+        pdl_wait();
+        double bs[4] = {0.0, 0.0, 0.0, 0.0};
+        const int nbb = bonded_blocks(d);
+        for (int b = 0; b < nbb; b++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) bs[q] += __ldcg(&d.bpart[(size_t)b * 4 + q]);
+        d.e_last[LIMA_E_LJ] = tot[1];
+        d.e_last[LIMA_E_BOND] = bs[0];
+        d.e_last[LIMA_E_ANGLE] = bs[1];
+        d.e_last[LIMA_E_DIHEDRAL] = bs[2];
+        d.e_last[LIMA_E_VIRIAL] = tot[2] + bs[3];
+        d.e_last[LIMA_E_TOTAL] = tot[1] + bs[0] + bs[1] + bs[2] + kin;
+    }
+    if (slot < 2) {
+        float lam = 1.f;
+        if (d.thermostat == LIMA_THERMOSTAT_BERENDSEN && temp > 0.0)
+            lam = (float)sqrt(1.0 + d.dt / d.tau_t * (d.t_target / temp - 1.0));
+        d.lambda[slot ^ 1] = lam;
+    }
+    *d.done = 0u;   // for the next launch
+    if (TAIL && INTEGRATE && tail != nullptr && *(volatile int*)d.need_rebuild) {
+        if (cudaGraphLaunch(tail, cudaStreamGraphTailLaunch) == cudaSuccess)
+            *d.rebuild_count += 1ull;
+        else
+            atomicOr(d.err, ERR_BIT_REBUILD_LAUNCH);
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ the step ---
 // (lj_pair: physmath.cuh)
-// position loads in flight per lane in the mixed-precision pair kernel: two
+// position loads in flight per lane in the mixed-precision pair loop: two
 // keep it at 48 registers (four: 56, one block fewer per SM)
 constexpr int kMixedGathers = 2;
 
@@ -507,8 +639,8 @@ __device__ __forceinline__ void pair_rows(const PhysDev& d, const float2* row, f
     }
 }
 
-template <bool MIXED, bool ENERGY, bool INTEGRATE, bool SWITCH>
-__device__ __forceinline__ void pair_integrate(const PhysDev& d, int cur, int slot) {
+template <bool MIXED, bool ENERGY, bool INTEGRATE, bool SWITCH, bool TAIL>
+__device__ __forceinline__ void step_body(const PhysDev& d, int cur, int slot, cudaGraphExec_t tail) {
     extern __shared__ float2 s_tab[];
     const int nt2 = d.n_types * d.n_types;
     for (int q = threadIdx.x; q < nt2; q += blockDim.x) s_tab[q] = d.lj_table[q];
@@ -516,7 +648,8 @@ __device__ __forceinline__ void pair_integrate(const PhysDev& d, int cur, int sl
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) / kGroup;
     const int g = threadIdx.x % kGroup;
     const bool active = i < d.n;
-    double ke = 0.0, elj = 0.0, vir = 0.0;
+    // FP64 sums of this thread: kinetic energy, LJ energy, LJ virial
+    double red[kRed] = {0.0, 0.0, 0.0};
     const float4* __restrict__ pos = d.pos[cur];
     const float4 pi = active ? pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
     const float2* row = &s_tab[__float_as_int(pi.w) * d.n_types];
@@ -555,14 +688,16 @@ __device__ __forceinline__ void pair_integrate(const PhysDev& d, int cur, int sl
             w_i += __shfl_xor_sync(0xffffffffu, w_i, o);
         }
     }
-    float e_b = 0.f;
+    const uint32_t oi = active ? d.orig_of_sorted[i] : 0xffffffffu;
     if (active && g == 0) {
-        // bonded contributions of this particle
-        const uint32_t oi = d.orig_of_sorted[i];
+        float e_b = 0.f;
         if (oi < (uint32_t)d.n_cp) {
+            // the bonded kernel's forces on this particle (it runs beside this
+            // kernel's list walk; wait for it only here)
+            pdl_wait();
             float bx = 0.f, by = 0.f, bz = 0.f, bw = 0.f;
             for (uint32_t q = d.bterm_off[oi]; q < d.bterm_off[oi + 1]; q++) {
-                const float4 tf = d.term_force[d.bterm_slot[q]];
+                const float4 tf = __ldcg(&d.term_force[d.bterm_slot[q]]);
                 bx += tf.x;
                 by += tf.y;
                 bz += tf.z;
@@ -587,8 +722,8 @@ __device__ __forceinline__ void pair_integrate(const PhysDev& d, int cur, int sl
         // w: the particle's potential energy, its LJ pair halves plus its bonded-term shares
         d.force[i] = make_float4(fx, fy, fz, ENERGY ? e_i + e_b : 0.f);
         if (ENERGY) {
-            elj = (double)e_i;
-            vir = (double)w_i;
+            red[1] = (double)e_i;
+            red[2] = (double)w_i;
         }
         // velocity Verlet as kick-drift over half-step velocities
         const float4 v = d.vel[i];
@@ -603,7 +738,7 @@ __device__ __forceinline__ void pair_integrate(const PhysDev& d, int cur, int sl
             ds_add(vhy, vc.y, ay * h);
             ds_add(vhz, vc.z, az * h);
             const double vx = (double)vhx + vc.x, vy = (double)vhy + vc.y, vz = (double)vhz + vc.z;
-            ke = 0.5 / (double)im * (vx * vx + vy * vy + vz * vz);
+            red[0] = 0.5 / (double)im * (vx * vx + vy * vy + vz * vz);
             if (INTEGRATE) {
                 const float lam = d.lambda[slot];
                 if (lam != 1.f) {   // scale (hi, lo): keep the product's rounding error in lo
@@ -637,14 +772,14 @@ __device__ __forceinline__ void pair_integrate(const PhysDev& d, int cur, int sl
                 const float4 xr = d.xref[i];
                 const float ddx = mimg(x - xr.x, L, iL), ddy = mimg(y - xr.y, L, iL), ddz = mimg(z - xr.z, L, iL);
                 if (ddx * ddx + ddy * ddy + ddz * ddz > d.half_skin2) {
-                    if (d.dynamic_list) *d.need_rebuild = 1;
+                    if (d.dynamic_list) atomicExch(d.need_rebuild, 1);
                     else atomicOr(d.err, ERR_BIT_LIST_STALE);
                 }
                 if (!(x == x) || !(y == y) || !(z == z)) atomicOr(d.err, ERR_BIT_NAN);
             }
         } else {
             float vx = v.x + ax * h, vy = v.y + ay * h, vz = v.z + az * h;
-            ke = 0.5 / (double)im * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
+            red[0] = 0.5 / (double)im * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
             if (INTEGRATE) {
                 const float lam = d.lambda[slot];
                 vx = lam * vx + ax * h;
@@ -664,64 +799,85 @@ __device__ __forceinline__ void pair_integrate(const PhysDev& d, int cur, int sl
                 const float4 xr = d.xref[i];
                 const float ddx = mimg(x - xr.x, L, iL), ddy = mimg(y - xr.y, L, iL), ddz = mimg(z - xr.z, L, iL);
                 if (ddx * ddx + ddy * ddy + ddz * ddz > d.half_skin2) {
-                    if (d.dynamic_list) *d.need_rebuild = 1;
+                    if (d.dynamic_list) atomicExch(d.need_rebuild, 1);
                     else atomicOr(d.err, ERR_BIT_LIST_STALE);
                 }
                 if (!(x == x) || !(y == y) || !(z == z)) atomicOr(d.err, ERR_BIT_NAN);
             }
         }
     }
-    double* acc = d.acc + slot * LIMA_E_COUNT;
-    block_add(acc, LIMA_E_KINETIC, ke);
-    if (ENERGY) {
-        block_add(acc, LIMA_E_LJ, elj);
-        block_add(acc, LIMA_E_VIRIAL, vir);
-        if (blockIdx.x == 0 && threadIdx.x == 0) d.acc_energy[slot] = 1;
-    }
+    finish_sums<ENERGY, INTEGRATE, TAIL>(d, slot, tail, red);
 }
 
-// FP32: at most 48 registers, 5 blocks of 256 per SM (38.5 against 40.8 us
-// at 4 blocks on the 32k box).  Mixed keeps the compiler's own choice: a
-// bound of 5 blocks slowed it to 45 us, an explicit 4 or 1 changed its
-// allocation for the worse.
-template <bool ENERGY, bool INTEGRATE, bool SWITCH>
-__global__ void __launch_bounds__(kTB, 5) k_pair_integrate(PhysDev d, int cur, int slot) {
-    pair_integrate<false, ENERGY, INTEGRATE, SWITCH>(d, cur, slot);
+// FP32: at most 48 registers, 5 blocks of 256 per SM.  Mixed keeps the
+// compiler's own choice (a 5-block bound slowed it).
+template <bool ENERGY, bool INTEGRATE, bool SWITCH, bool TAIL>
+__global__ void __launch_bounds__(kTB, 5) k_step(PhysDev d, int cur, int slot, cudaGraphExec_t tail) {
+    step_body<false, ENERGY, INTEGRATE, SWITCH, TAIL>(d, cur, slot, tail);
 }
-template <bool ENERGY, bool INTEGRATE, bool SWITCH>
-__global__ void __launch_bounds__(kTB) k_pair_integrate_mixed(PhysDev d, int cur, int slot) {
-    pair_integrate<true, ENERGY, INTEGRATE, SWITCH>(d, cur, slot);
+template <bool ENERGY, bool INTEGRATE, bool SWITCH, bool TAIL>
+__global__ void __launch_bounds__(kTB) k_step_mixed(PhysDev d, int cur, int slot, cudaGraphExec_t tail) {
+    step_body<true, ENERGY, INTEGRATE, SWITCH, TAIL>(d, cur, slot, tail);
 }
 
 // ---------------------------------------------------------------- launchers --
 namespace {
 
-template <bool MIXED, bool ENERGY, bool INTEGRATE>
-void pair_variant(const PhysDev& d, int cur, int slot, cudaStream_t s) {
-    const int nb = (int)(((size_t)d.n_pad * kGroup + kTB - 1) / kTB);
+// The step kernel with a programmatic dependency on the kernel before it in
+// the stream (the bonded kernel): it may start before that one has finished
+// and waits for it only where it reads its results.
+template <typename K>
+void launch_programmatic(K kernel, const PhysDev& d, int cur, int slot, cudaGraphExec_t tail, size_t smem,
+                         cudaStream_t s) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)step_blocks(d));
+    cfg.blockDim = dim3(kTB);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, d, cur, slot, tail);
+}
+
+template <bool MIXED, bool ENERGY, bool INTEGRATE, bool TAIL>
+void step_variant(const PhysDev& d, int cur, int slot, cudaGraphExec_t tail, cudaStream_t s) {
     const size_t smem = sizeof(float2) * d.n_types * d.n_types;
     if (MIXED && d.use_switch)
-        k_pair_integrate_mixed<ENERGY, INTEGRATE, true><<<nb, kTB, smem, s>>>(d, cur, slot);
+        launch_programmatic(k_step_mixed<ENERGY, INTEGRATE, true, TAIL>, d, cur, slot, tail, smem, s);
     else if (MIXED)
-        k_pair_integrate_mixed<ENERGY, INTEGRATE, false><<<nb, kTB, smem, s>>>(d, cur, slot);
+        launch_programmatic(k_step_mixed<ENERGY, INTEGRATE, false, TAIL>, d, cur, slot, tail, smem, s);
     else if (d.use_switch)
-        k_pair_integrate<ENERGY, INTEGRATE, true><<<nb, kTB, smem, s>>>(d, cur, slot);
+        launch_programmatic(k_step<ENERGY, INTEGRATE, true, TAIL>, d, cur, slot, tail, smem, s);
     else
-        k_pair_integrate<ENERGY, INTEGRATE, false><<<nb, kTB, smem, s>>>(d, cur, slot);
+        launch_programmatic(k_step<ENERGY, INTEGRATE, false, TAIL>, d, cur, slot, tail, smem, s);
+}
+
+template <bool MIXED, bool ENERGY, bool INTEGRATE>
+void step_tail(const PhysDev& d, int cur, int slot, cudaGraphExec_t tail, cudaStream_t s) {
+    if (tail)
+        step_variant<MIXED, ENERGY, INTEGRATE, true>(d, cur, slot, tail, s);
+    else
+        step_variant<MIXED, ENERGY, INTEGRATE, false>(d, cur, slot, nullptr, s);
 }
 
 }  // namespace
 
-void launch_keys(const PhysDev& d, const float4* pos, cudaStream_t s) {
-    k_keys<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d, pos);
-}
-
-void launch_cell_offsets(const PhysDev& d, const float4* pos, cudaStream_t s) {
-    k_cell_offsets<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d, pos);
+void launch_sort(const PhysDev& d, const float4* pos, cudaStream_t s) {
+    k_sort_count<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d, pos);
+    k_sort_scan<<<1, kScanThreads, 0, s>>>(d);
+    k_sort_fill<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d);
+    k_sort_order<<<(d.n_cells + kTB - 1) / kTB, kTB, 0, s>>>(d);
 }
 
 void launch_permute(const PhysDev& d, int cur, bool mixed, cudaStream_t s) {
     k_permute<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d, cur, mixed ? 1 : 0);
+}
+
+void launch_set_xref(const PhysDev& d, const float4* pos, cudaStream_t s) {
+    k_set_xref<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d, pos);
 }
 
 void launch_build_list(const PhysDev& d, const float4* pos, const uint32_t* items, cudaStream_t s) {
@@ -733,36 +889,30 @@ void launch_copy_back(const PhysDev& d, int cur, bool mixed, cudaStream_t s) {
     k_copy_back<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d, cur, mixed ? 1 : 0);
 }
 
-void launch_list_check(const PhysDev& d, cudaGraphConditionalHandle h, cudaStream_t s) {
-    k_list_check<<<1, 1, 0, s>>>(d.need_rebuild, d.rebuild_count, h);
-}
-
-void launch_bonded(const PhysDev& d, int cur, bool energy, int slot, int fold_src, cudaStream_t s) {
-    const int nterms = d.n_bonds + d.n_angles + d.n_dih;
-    const int nb = std::max(1, (nterms + kTB - 1) / kTB);
+void launch_bonded(const PhysDev& d, int cur, bool energy, cudaStream_t s) {
+    const int nb = bonded_blocks(d);
     const bool mixed = d.precision == LIMA_PRECISION_MIXED;
     if (energy && mixed)
-        k_bonded<true, true><<<nb, kTB, 0, s>>>(d, cur, slot, fold_src);
+        k_bonded<true, true><<<nb, kTB, 0, s>>>(d, cur);
     else if (energy)
-        k_bonded<true, false><<<nb, kTB, 0, s>>>(d, cur, slot, fold_src);
+        k_bonded<true, false><<<nb, kTB, 0, s>>>(d, cur);
     else if (mixed)
-        k_bonded<false, true><<<nb, kTB, 0, s>>>(d, cur, slot, fold_src);
+        k_bonded<false, true><<<nb, kTB, 0, s>>>(d, cur);
     else
-        k_bonded<false, false><<<nb, kTB, 0, s>>>(d, cur, slot, fold_src);
+        k_bonded<false, false><<<nb, kTB, 0, s>>>(d, cur);
 }
 
-void launch_pair(const PhysDev& d, int cur, bool mixed, bool energy, bool integrate, int slot, cudaStream_t s) {
+void launch_step(const PhysDev& d, int cur, bool mixed, bool energy, bool integrate, int slot, cudaGraphExec_t tail,
+                 cudaStream_t s) {
     if (mixed) {
-        if (!integrate) pair_variant<true, true, false>(d, cur, slot, s);
-        else if (energy) pair_variant<true, true, true>(d, cur, slot, s);
-        else pair_variant<true, false, true>(d, cur, slot, s);
+        if (!integrate) step_variant<true, true, false, false>(d, cur, slot, nullptr, s);
+        else if (energy) step_tail<true, true, true>(d, cur, slot, tail, s);
+        else step_tail<true, false, true>(d, cur, slot, tail, s);
     } else {
-        if (!integrate) pair_variant<false, true, false>(d, cur, slot, s);
-        else if (energy) pair_variant<false, true, true>(d, cur, slot, s);
-        else pair_variant<false, false, true>(d, cur, slot, s);
+        if (!integrate) step_variant<false, true, false, false>(d, cur, slot, nullptr, s);
+        else if (energy) step_tail<false, true, true>(d, cur, slot, tail, s);
+        else step_tail<false, false, true>(d, cur, slot, tail, s);
     }
 }
-
-void launch_finalize(const PhysDev& d, int src, cudaStream_t s) { k_finalize<<<1, 1, 0, s>>>(d, src); }
 
 }  // namespace lima

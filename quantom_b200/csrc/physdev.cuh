@@ -16,13 +16,18 @@
 //   vel[n_pad]      half-step velocity, w = 1/m
 //   posc/velc       low parts of pos/vel (mixed precision)
 //   xref[n_pad]     positions at the last rebuild (list validity check)
-//   force[n_pad]    total force of the last evaluation, w = per-particle LJ energy
+//   force[n_pad]    total force of the last evaluation, w = per-particle potential energy
 //   nl[cap][n_pad]  Verlet list of sorted slots, entry k of particle i at
 //                   ((k / kGroup) * n_pad + i) * kGroup + k % kGroup: the
 //                   kGroup lanes of one particle read kGroup consecutive
 //                   entries and consecutive particles follow each other
 //   term_force      one float4 per (term, atom) of every bonded term; gathered
 //                   per particle through bterm_off/bterm_slot (CSR over orig)
+//   part[blocks][4] per-block FP64 partial sums of the last step kernel; the
+//                   block that finishes last adds them in block order
+// A list rebuild permutes every per-slot array (both position buffers,
+// velocities, forces, low parts, orig ids), so readbacks after it stay
+// consistent with the forces of the step before it.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -34,8 +39,13 @@
 
 namespace lima {
 
-// accumulator slots: 0/1 = step parity, 2 = on-demand energy evaluation
-constexpr int kAccSlots = 3;
+// FP64 sums of a step kernel: kinetic energy, LJ energy, LJ virial (the
+// bonded kernel sums bond, angle, dihedral energy and bonded virial)
+constexpr int kRed = 3;
+constexpr int kRedStride = 4;   // doubles per block partial
+// step-kernel slots: 0/1 = the step of that parity (sets lambda[parity ^ 1]),
+// 2 = an energy evaluation without integration
+constexpr int kSlotEval = 2;
 
 struct PhysDev {
     int n;              // particles
@@ -55,44 +65,49 @@ struct PhysDev {
     float4* velc;
     float4* xref;
     float4* force;
-    float4* pos_orig[2];        // [n_cp] compound-particle positions in orig order (the bonded kernel's input)
+    float4* pos_orig[2];        // [n_cp] compound-particle positions in orig order (the bonded terms' input)
     float4* posc_orig[2];       // [n_cp] their low parts (mixed precision)
     uint32_t* orig_of_sorted;   // [n]
     uint32_t* sorted_of_orig;   // [n]
     float2* lj_table;           // [n_types^2] (sigma^2, 4 eps), Lorentz-Berthelot
-    // cell grid
+    // cell grid and the counting sort by cell (stable: ascending slot inside a cell)
     int m;                      // cells per dimension
     int n_cells;                // m^3
-    uint32_t* keys[2];
-    uint32_t* vals[2];
-    void* sort_tmp; size_t sort_tmp_bytes;
+    uint32_t* cell_key;         // [n] cell of each slot
+    uint32_t* cell_rank;        // [n] arrival order of the slot in its cell
+    uint32_t* ccount;           // [n_cells] occupancy during a sort; zero between sorts
+    uint32_t* order;            // [n] slots in cell order
     uint32_t* cstart;           // [n_cells + 1]: cell c holds sorted slots [cstart[c], cstart[c+1])
-    float4* pos_tmp; float4* vel_tmp; float4* posc_tmp; float4* velc_tmp; uint32_t* orig_tmp;
+    float4* pos_tmp[2]; float4* vel_tmp; float4* posc_tmp; float4* velc_tmp; float4* force_tmp; uint32_t* orig_tmp;
     // Verlet list (tile-local indices)
     uint32_t* nl; uint32_t* nl_cnt; int nl_cap;
     int* nl_need;               // largest row length a build found beyond nl_cap (0: none)
-    // dynamic lists (nlist_period <= 0): the pair kernel requests a rebuild
-    // once a particle has moved more than skin/2 since the last one, and the
-    // next step rebuilds before its forces (a conditional node of the step
-    // graph); fixed period: the same test is an error (ERR_BIT_LIST_STALE)
+    // dynamic lists (nlist_period <= 0): the step kernel's last block sees
+    // that a particle moved more than skin/2 since the last build and
+    // tail-launches the device-launchable rebuild graph of the next parity,
+    // which runs before anything that follows the step in its stream; fixed
+    // period: the same test is an error (ERR_BIT_LIST_STALE)
     int dynamic_list;
     int* need_rebuild;
-    unsigned long long* rebuild_count;   // rebuilds decided on the device
+    unsigned long long* rebuild_count;   // rebuilds launched from the device
+    cudaGraphExec_t rebuild_exec[2];     // device-launchable rebuild of pos[parity] (null: host decides)
     // exclusions (CSR over orig ids)
     uint32_t* excl_off; uint32_t* excl_ids;
-    // bonded terms (orig ids)
+    // bonded terms (orig ids); a term slot numbers (term, role): bond b role r
+    // -> 2b + r, angle a -> 2 n_bonds + 3a + r, dihedral q -> 2 n_bonds +
+    // 3 n_angles + 4q + r
     int n_bonds, n_angles, n_dih;
     int4* bond_idx; float2* bond_par;          // (r0, k)
     int4* angle_idx; float2* angle_par;        // (theta0, k)
     int4* dih_idx; float4* dih_par;            // (phi0, k, n)
     uint32_t* bterm_off; uint32_t* bterm_slot;
-    float4* term_force;
+    float4* term_force;         // [n_term_slots] the bonded kernel's force per (term, role), w = energy share
     int n_term_slots;
-    // FP64 reductions: acc[slot*8 + LIMA_E_*]; slot 0/1 are folded into e_last
-    // (and the next Berendsen lambda[1-slot]) by the first kernel of the next
-    // step or by k_finalize before a readback
-    double* acc;
-    int* acc_energy;    // [kAccSlots] energies were accumulated into this slot
+    // FP64 reductions: block partials, the count of blocks that wrote theirs,
+    // the latest totals (LIMA_E_*) and the Berendsen scalar per parity
+    double* part;
+    double* bpart;      // [bonded blocks][4] the bonded kernel's block partials
+    unsigned int* done;
     double* e_last;
     float* lambda;      // [2]
     int* err;
@@ -121,17 +136,24 @@ void phys_prime(PhysDev& d, int cur, cudaStream_t s);
 // the longest row (the capacity starts from the box's mean density, which a
 // dense solute exceeds) and return true so the caller rebuilds; waits for s
 bool phys_fit_list(PhysDev& d, cudaStream_t s, std::vector<void*>& allocs);
-// dynamic lists: the step graph of parity `cur` ({check -> IF(rebuild)} || bonded -> pair);
-// returns the kernels of one replay without a rebuild, or -1 if the graph cannot be built
+// dynamic lists: the step graph of parity `cur` (the step kernel, which tail-launches
+// the rebuild when one is due); returns its kernel count, or -1 if the graph cannot be built
 int phys_capture_dynamic(const PhysDev& d, int cur, bool energy, cudaStream_t s, cudaGraphExec_t* out);
 bool phys_rebuild_pending(const PhysDev& d, cudaStream_t s);
 unsigned long long phys_device_rebuilds(const PhysDev& d, cudaStream_t s);
-constexpr int kRebuildKernels = 4;   // k_keys, k_permute, k_copy_back, k_build_list (plus the library sort)
-// ev (nullable): events before the bonded kernel, after it, after the pair
-// kernel.  Returns kernels launched.
-int phys_step_kernels(const PhysDev& d, int cur, cudaStream_t s, bool energy = false, cudaEvent_t* ev = nullptr);
+// the device-launchable rebuild graphs of both parities (after the list capacity is final)
+int phys_capture_rebuild(PhysDev& d, cudaStream_t s, std::string& msg);
+void phys_free_rebuild(PhysDev& d);
+// k_sort_count, k_sort_scan, k_sort_fill, k_sort_order, k_permute, k_copy_back, k_build_list
+constexpr int kRebuildKernels = 7;
+// One step: the bonded kernel, then the step kernel (pair terms,
+// integration, FP64 sums) launched programmatically so that it overlaps the
+// bonded kernel.  tail: launch the due rebuild from the device (the launch
+// must be captured in a graph).  ev (nullable): events before the bonded
+// kernel, after it, after the step kernel.  Returns kernels launched.
+int phys_step_kernels(const PhysDev& d, int cur, cudaStream_t s, bool energy = false, cudaEvent_t* ev = nullptr,
+                      bool tail = false);
 void phys_energy_now(PhysDev& d, int cur, cudaStream_t s);
-void phys_finalize(const PhysDev& d, int cur, cudaStream_t s);
 void phys_read_compounds(const PhysDev& d, int cur, const lima_compound* comps, float4* pos_out, float4* prev_out);
 void phys_read_solvents(const PhysDev& d, int cur, float4* pos_out, float4* prev_out);
 void phys_read_forces(const PhysDev& d, const lima_compound* comps, float4* fc, float4* fs);

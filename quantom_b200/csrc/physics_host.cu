@@ -1,7 +1,5 @@
 // Host side of the physics-semantics path: set-up from the reference layout,
 // list rebuilds, step launches and readback (kernels in kernels_physics.cu).
-#include <cub/device/device_radix_sort.cuh>
-
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -206,15 +204,16 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
         d.orig_of_sorted = dalloc<uint32_t>(allocs, d.n_pad);
         d.sorted_of_orig = dalloc<uint32_t>(allocs, d.n);
         d.lj_table = dalloc<float2>(allocs, tab.size());
-        for (int b = 0; b < 2; b++) {
-            d.keys[b] = dalloc<uint32_t>(allocs, d.n);
-            d.vals[b] = dalloc<uint32_t>(allocs, d.n);
-        }
+        d.cell_key = dalloc<uint32_t>(allocs, d.n);
+        d.cell_rank = dalloc<uint32_t>(allocs, d.n);
+        d.ccount = dalloc<uint32_t>(allocs, d.n_cells);
+        d.order = dalloc<uint32_t>(allocs, d.n);
         d.cstart = dalloc<uint32_t>(allocs, (size_t)d.n_cells + 1);
-        d.pos_tmp = dalloc<float4>(allocs, d.n);
+        for (int b = 0; b < 2; b++) d.pos_tmp[b] = dalloc<float4>(allocs, d.n);
         d.vel_tmp = dalloc<float4>(allocs, d.n);
         d.posc_tmp = dalloc<float4>(allocs, d.n);
         d.velc_tmp = dalloc<float4>(allocs, d.n);
+        d.force_tmp = dalloc<float4>(allocs, d.n);
         d.orig_tmp = dalloc<uint32_t>(allocs, d.n);
         d.nl = dalloc<uint32_t>(allocs, (size_t)d.nl_cap * d.n_pad);
         d.nl_cnt = dalloc<uint32_t>(allocs, d.n_pad);
@@ -230,16 +229,14 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
         d.bterm_off = dalloc<uint32_t>(allocs, boff.size());
         d.bterm_slot = dalloc<uint32_t>(allocs, bslot.size());
         d.term_force = dalloc<float4>(allocs, d.n_term_slots);
-        d.acc = dalloc<double>(allocs, kAccSlots * LIMA_E_COUNT);
-        d.acc_energy = dalloc<int>(allocs, kAccSlots);
+        d.part = dalloc<double>(allocs, (size_t)step_blocks(d) * kRedStride);
+        d.bpart = dalloc<double>(allocs, (size_t)bonded_blocks(d) * 4);
+        d.done = dalloc<unsigned int>(allocs, 1);
         d.e_last = dalloc<double>(allocs, LIMA_E_COUNT);
         d.lambda = dalloc<float>(allocs, 2);
         d.err = dalloc<int>(allocs, 1);
         d.need_rebuild = dalloc<int>(allocs, 1);
         d.rebuild_count = dalloc<unsigned long long>(allocs, 1);
-        cub::DeviceRadixSort::SortPairs(nullptr, d.sort_tmp_bytes, d.keys[0], d.keys[1], d.vals[0], d.vals[1], d.n, 0,
-                                        32, s);
-        d.sort_tmp = dalloc<uint8_t>(allocs, d.sort_tmp_bytes);
     } catch (const std::exception& e) {
         msg = std::string("device allocation failed: ") + e.what();
         return LIMA_ERR_CUDA;
@@ -258,8 +255,8 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
     up(d.dih_par, dpar.data(), sizeof(float4) * dpar.size());
     up(d.bterm_off, boff.data(), sizeof(uint32_t) * boff.size());
     up(d.bterm_slot, bslot.data(), sizeof(uint32_t) * bslot.size());
-    cudaMemsetAsync(d.acc, 0, sizeof(double) * kAccSlots * LIMA_E_COUNT, s);
-    cudaMemsetAsync(d.acc_energy, 0, sizeof(int) * kAccSlots, s);
+    cudaMemsetAsync(d.ccount, 0, sizeof(uint32_t) * d.n_cells, s);
+    cudaMemsetAsync(d.done, 0, sizeof(unsigned int), s);
     cudaMemsetAsync(d.e_last, 0, sizeof(double) * LIMA_E_COUNT, s);
     cudaMemsetAsync(d.err, 0, sizeof(int), s);
     cudaMemsetAsync(d.need_rebuild, 0, sizeof(int), s);
@@ -317,35 +314,24 @@ void phys_upload_state(const PhysHost& h, PhysDev& d, int cur, cudaStream_t s) {
     cudaMemcpyAsync(d.sorted_of_orig, ident.data(), sizeof(uint32_t) * d.n, cudaMemcpyHostToDevice, s);
     set_device_float(d.lambda, 1.f, s);
     set_device_float(d.lambda + 1, 1.f, s);
-    cudaMemsetAsync(d.acc, 0, sizeof(double) * kAccSlots * LIMA_E_COUNT, s);
-    cudaMemsetAsync(d.acc_energy, 0, sizeof(int) * kAccSlots, s);
+    cudaMemsetAsync(d.force, 0, sizeof(float4) * d.n_pad, s);
     cudaStreamSynchronize(s);
 }
 
 void phys_rebuild(const PhysDev& d, int cur, cudaStream_t s) {
-    const size_t ncell = (size_t)d.n_cells;
     const bool mixed = d.precision == LIMA_PRECISION_MIXED;
-    launch_keys(d, d.pos[cur], s);
-    size_t bytes = d.sort_tmp_bytes;
-    int end_bit = 1;
-    while ((1ull << end_bit) < (unsigned long long)ncell) end_bit++;
-    cub::DeviceRadixSort::SortPairs(d.sort_tmp, bytes, d.keys[0], d.keys[1], d.vals[0], d.vals[1], d.n, 0, end_bit, s);
+    launch_sort(d, d.pos[cur], s);
     launch_permute(d, cur, mixed, s);
     launch_copy_back(d, cur, mixed, s);
     launch_build_list(d, d.pos[cur], nullptr, s);
 }
 
-// The list of positions `pos` without moving any particle: keys, a sort of
-// the slots by cell (vals[1]), cell offsets, then the build through vals[1].
+// The list of positions `pos` without moving any particle: the sort of the
+// slots by cell (order), reference positions, then the build through order.
 void phys_rebuild_inplace(const PhysDev& d, const float4* pos, cudaStream_t s) {
-    const size_t ncell = (size_t)d.n_cells;
-    launch_keys(d, pos, s);
-    size_t bytes = d.sort_tmp_bytes;
-    int end_bit = 1;
-    while ((1ull << end_bit) < (unsigned long long)ncell) end_bit++;
-    cub::DeviceRadixSort::SortPairs(d.sort_tmp, bytes, d.keys[0], d.keys[1], d.vals[0], d.vals[1], d.n, 0, end_bit, s);
-    launch_cell_offsets(d, pos, s);
-    launch_build_list(d, pos, d.vals[1], s);
+    launch_sort(d, pos, s);
+    launch_set_xref(d, pos, s);
+    launch_build_list(d, pos, d.order, s);
 }
 
 void phys_prime(PhysDev&, int, cudaStream_t) {}
@@ -401,82 +387,82 @@ void end_open_capture(cudaStream_t s) {
 }
 }  // namespace
 
-// {k_list_check -> IF(rebuild requested){ sort, permute, copy back, list }}
-// in parallel with the bonded terms, then the pair kernel after both: the
-// conditional's own latency hides behind the bonded kernel.  The conditional
-// body is captured from the same launch sequence as a host-driven rebuild, so
-// both paths run identical kernels.
+// The rebuild of pos[parity] as a graph the step kernel launches from the
+// device (instantiated for device launch and uploaded), one per parity.
+int phys_capture_rebuild(PhysDev& d, cudaStream_t s, std::string& msg) {
+    for (int parity = 0; parity < 2; parity++) {
+        cudaGraph_t g = nullptr;
+        if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            msg = "cannot capture the list rebuild";
+            cudaGetLastError();
+            return LIMA_ERR_CUDA;
+        }
+        phys_rebuild(d, parity, s);
+        if (cudaStreamEndCapture(s, &g) != cudaSuccess || !g) {
+            end_open_capture(s);
+            msg = "cannot capture the list rebuild";
+            return LIMA_ERR_CUDA;
+        }
+        const cudaError_t ie = cudaGraphInstantiate(&d.rebuild_exec[parity], g, cudaGraphInstantiateFlagDeviceLaunch);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess || cudaGraphUpload(d.rebuild_exec[parity], s) != cudaSuccess) {
+            cudaGetLastError();
+            msg = std::string("dynamic pair lists need device-launchable CUDA graphs: ") + cudaGetErrorString(ie);
+            phys_free_rebuild(d);
+            return LIMA_ERR_CUDA;
+        }
+    }
+    return cudaStreamSynchronize(s) == cudaSuccess ? 0 : LIMA_ERR_CUDA;
+}
+
+void phys_free_rebuild(PhysDev& d) {
+    for (auto& g : d.rebuild_exec) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
+}
+
+// The step graph of a dynamic list: the step kernel alone, with the rebuild
+// of the next parity as its tail launch.
 int phys_capture_dynamic(const PhysDev& d, int cur, bool energy, cudaStream_t s, cudaGraphExec_t* out) {
     *out = nullptr;
+    if (!d.rebuild_exec[cur ^ 1]) return -1;
     cudaGraph_t g = nullptr;
-    if (cudaGraphCreate(&g, 0) != cudaSuccess) {
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
         cudaGetLastError();
         return -1;
     }
-    const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
-    int kernels = -1;
-    do {
-        cudaGraphConditionalHandle h;
-        if (cudaGraphConditionalHandleCreate(&h, g, 0, 0) != cudaSuccess) break;
-        cudaGraph_t tmp = nullptr;
-        // two roots: the check (then the conditional rebuild) and the bonded terms
-        if (cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, mode) != cudaSuccess) break;
-        launch_list_check(d, h, s);
-        if (cudaStreamEndCapture(s, &tmp) != cudaSuccess) break;
-        cudaGraphNode_t check = nullptr;
-        size_t nn = 1;
-        if (cudaGraphGetNodes(g, &check, &nn) != cudaSuccess || nn != 1) break;
-        if (cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, mode) != cudaSuccess) break;
-        launch_bonded(d, cur, energy, cur, cur ^ 1, s);
-        if (cudaStreamEndCapture(s, &tmp) != cudaSuccess) break;
-        cudaGraphNode_t roots[2] = {nullptr, nullptr};
-        nn = 2;
-        if (cudaGraphGetNodes(g, roots, &nn) != cudaSuccess || nn != 2) break;
-        const cudaGraphNode_t bonded = roots[0] == check ? roots[1] : roots[0];
-        cudaGraphNodeParams cp = {};
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = h;
-        cp.conditional.type = cudaGraphCondTypeIf;
-        cp.conditional.size = 1;
-        cudaGraphNode_t cond = nullptr;
-        if (cudaGraphAddNode(&cond, g, &check, 1, &cp) != cudaSuccess) break;
-        cudaGraph_t body = cp.conditional.phGraph_out[0];
-        if (cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, mode) != cudaSuccess) break;
-        phys_rebuild(d, cur, s);
-        if (cudaStreamEndCapture(s, &tmp) != cudaSuccess) break;
-        const cudaGraphNode_t before_pair[2] = {cond, bonded};
-        if (cudaStreamBeginCaptureToGraph(s, g, before_pair, nullptr, 2, mode) != cudaSuccess) break;
-        launch_pair(d, cur, d.precision == LIMA_PRECISION_MIXED, energy, true, cur, s);
-        if (cudaStreamEndCapture(s, &tmp) != cudaSuccess) break;
-        if (cudaGraphInstantiate(out, g, 0) != cudaSuccess) {
-            *out = nullptr;
-            break;
-        }
-        kernels = 3;
-    } while (false);
-    end_open_capture(s);
+    const int k = phys_step_kernels(d, cur, s, energy, nullptr, true);
+    if (cudaStreamEndCapture(s, &g) != cudaSuccess || !g) {
+        end_open_capture(s);
+        return -1;
+    }
+    const cudaError_t ie = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
-    return kernels;
+    if (ie != cudaSuccess) {
+        cudaGetLastError();
+        *out = nullptr;
+        return -1;
+    }
+    return k;
 }
 
-// The step of parity `cur` accumulates into slot cur; its bonded kernel first
-// folds slot cur^1 (the previous step) into e_last and lambda[cur].
-int phys_step_kernels(const PhysDev& d, int cur, cudaStream_t s, bool energy, cudaEvent_t* ev) {
+// The step of parity `cur` runs the step kernel in slot cur: it integrates
+// with lambda[cur] and sets lambda[cur ^ 1] from its kinetic energy.
+int phys_step_kernels(const PhysDev& d, int cur, cudaStream_t s, bool energy, cudaEvent_t* ev, bool tail) {
     if (ev) cudaEventRecord(ev[0], s);
-    launch_bonded(d, cur, energy, cur, cur ^ 1, s);
+    launch_bonded(d, cur, energy, s);
     if (ev) cudaEventRecord(ev[1], s);
-    launch_pair(d, cur, d.precision == LIMA_PRECISION_MIXED, energy, true, cur, s);
+    launch_step(d, cur, d.precision == LIMA_PRECISION_MIXED, energy, true, cur, tail ? d.rebuild_exec[cur ^ 1] : nullptr,
+                s);
     if (ev) cudaEventRecord(ev[2], s);
     return 2;
 }
 
 void phys_energy_now(PhysDev& d, int cur, cudaStream_t s) {
-    launch_bonded(d, cur, true, 2, -1, s);
-    launch_pair(d, cur, d.precision == LIMA_PRECISION_MIXED, true, false, 2, s);
-    launch_finalize(d, 2, s);
+    launch_bonded(d, cur, true, s);
+    launch_step(d, cur, d.precision == LIMA_PRECISION_MIXED, true, false, kSlotEval, nullptr, s);
 }
-
-void phys_finalize(const PhysDev& d, int cur, cudaStream_t s) { launch_finalize(d, cur ^ 1, s); }
 
 namespace {
 struct Snapshot {

@@ -7,22 +7,37 @@
 
 namespace lima {
 
-constexpr int kTB = 256;         // threads per block of the per-particle / per-term kernels
-constexpr int kGroup = 8;        // lanes per particle in the list and pair kernels
+constexpr int kTB = 256;         // threads per block of the per-particle kernels and the step kernel
+constexpr int kGroup = 8;        // lanes per particle in the list and step kernels
 constexpr int kBuildWarps = 4;   // warps per block of the list build
 constexpr int kSlices = 8;       // lanes per particle in the list build (32 / kSlices particles per warp)
 constexpr int kMaxTypes = 32;    // LIMA_MAX_ATOM_TYPES
+constexpr int kScanThreads = 1024;
 
-void launch_keys(const PhysDev& d, const float4* pos, cudaStream_t s);
-void launch_cell_offsets(const PhysDev& d, const float4* pos, cudaStream_t s);
+// blocks of the step kernel (kGroup lanes per particle slot, n_pad a multiple of 32)
+__host__ __device__ inline int step_blocks(const PhysDev& d) { return (int)(((size_t)d.n_pad * kGroup + kTB - 1) / kTB); }
+// blocks of the bonded kernel (one thread per term)
+__host__ __device__ inline int bonded_blocks(const PhysDev& d) {
+    const int nt = d.n_bonds + d.n_angles + d.n_dih;
+    return nt > 0 ? (nt + kTB - 1) / kTB : 1;
+}
+
+// the counting sort of the slots by the cell of `pos`: cell_key, cstart, order
+void launch_sort(const PhysDev& d, const float4* pos, cudaStream_t s);
+// every per-slot array into cell order (through the tmp arrays), reference positions
 void launch_permute(const PhysDev& d, int cur, bool mixed, cudaStream_t s);
+void launch_copy_back(const PhysDev& d, int cur, bool mixed, cudaStream_t s);
+// reference positions of an in-place build (particles not moved)
+void launch_set_xref(const PhysDev& d, const float4* pos, cudaStream_t s);
 // items (nullable): slots in cell order when the particles were not re-sorted
 void launch_build_list(const PhysDev& d, const float4* pos, const uint32_t* items, cudaStream_t s);
-void launch_copy_back(const PhysDev& d, int cur, bool mixed, cudaStream_t s);
-// slot: accumulator slot to add energies to; fold_src: slot to fold first (-1: none)
-void launch_bonded(const PhysDev& d, int cur, bool energy, int slot, int fold_src, cudaStream_t s);
-void launch_list_check(const PhysDev& d, cudaGraphConditionalHandle h, cudaStream_t s);
-void launch_pair(const PhysDev& d, int cur, bool mixed, bool energy, bool integrate, int slot, cudaStream_t s);
-void launch_finalize(const PhysDev& d, int src, cudaStream_t s);
+// The bonded kernel of parity `cur` (term forces; ENERGY: block partials)
+void launch_bonded(const PhysDev& d, int cur, bool energy, cudaStream_t s);
+// The step kernel of parity `cur` (slot cur) or an energy evaluation (slot
+// kSlotEval, integrate false), launched with a programmatic dependency on the
+// bonded kernel before it.  tail: device-launchable rebuild graph the last
+// block launches when a rebuild is due (nullptr: none).
+void launch_step(const PhysDev& d, int cur, bool mixed, bool energy, bool integrate, int slot, cudaGraphExec_t tail,
+                 cudaStream_t s);
 
 }  // namespace lima

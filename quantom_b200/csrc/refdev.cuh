@@ -25,6 +25,7 @@ enum : int {
     ERR_BIT_PHYS_LIST_OVERFLOW = 32,
     ERR_BIT_LIST_STALE = 64,      // a particle moved more than skin/2 since the last list build
     ERR_BIT_TILE_TIMEOUT = 128,   // a shared-memory staging wait ran out (bounded mbarrier wait)
+    ERR_BIT_REBUILD_LAUNCH = 256, // the device could not launch a due list rebuild
 };
 
 struct RefDev {
