@@ -177,7 +177,8 @@ enum {
     LIMA_NL_COMPOUND_COMPOUND = 0,  /* NeighborList::neighborcompound_ids of compounds */
     LIMA_NL_COMPOUND_SOLVENT = 1,   /* NeighborList::neighborsolvent_ids of compounds */
     LIMA_NL_SOLVENT_COMPOUND = 2,   /* NeighborList::neighborcompound_ids of solvents */
-    LIMA_NL_SOLVENT_SOLVENT = 3     /* NeighborList::neighborsolvent_ids of solvents */
+    LIMA_NL_SOLVENT_SOLVENT = 3,    /* NeighborList::neighborsolvent_ids of solvents */
+    LIMA_NL_PAIR = 4                /* physics semantics: the Verlet list of every particle */
 };
 
 /* Defaults: reference semantics, FP32, box 7 nm, cutoff 1.4 nm (reference
@@ -243,7 +244,10 @@ lima_status lima_compute_energies(lima_ctx* ctx);
    lima_build_nlist runs one update now.  lima_get_nlist writes CSR offsets
    (n_entities+1) and ids (sorted ascending within each list); with ids NULL
    only offsets and *total are written.  lima_set_nlist installs a previous
-   compound-compound list state, which the reference's update depends on. */
+   compound-compound list state, which the reference's update depends on.
+   Physics semantics: LIMA_NL_PAIR gives the Verlet list of the last build,
+   rows and ids in particle order (compound particles compound by compound,
+   then solvents); the other selectors belong to reference semantics. */
 lima_status lima_build_nlist(lima_ctx* ctx);
 lima_status lima_get_nlist(lima_ctx* ctx, int which, uint32_t* offsets, uint32_t* ids, uint32_t* total);
 lima_status lima_set_nlist(lima_ctx* ctx, int which, const uint32_t* offsets, const uint32_t* ids);

@@ -1261,10 +1261,16 @@ lima_status lima_get_rebuild_count(lima_ctx* c, uint64_t* count) {
 lima_status lima_get_nlist(lima_ctx* c, int which, uint32_t* offsets, uint32_t* ids, uint32_t* total) {
     return guarded(c, [&] {
         need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
-        need(c->p.semantics == LIMA_SEMANTICS_REFERENCE, LIMA_ERR_UNSUPPORTED,
-             "entity neighbour lists exist in reference semantics; physics keeps one cell-sorted Verlet list");
-        need(which >= 0 && which <= 3, LIMA_ERR_ARGUMENT, "unknown list selector");
         need(offsets != nullptr, LIMA_ERR_ARGUMENT, "null offsets");
+        if (c->p.semantics == LIMA_SEMANTICS_PHYSICS) {
+            need(which == LIMA_NL_PAIR, LIMA_ERR_UNSUPPORTED,
+                 "physics semantics keeps one Verlet list (LIMA_NL_PAIR); entity lists belong to reference semantics");
+            sync_checked(c);
+            const uint32_t tot = lima::phys_read_list(c->phys, offsets, ids);
+            if (total) *total = tot;
+            return;
+        }
+        need(which >= 0 && which <= 3, LIMA_ERR_ARGUMENT, "unknown list selector");
         sync_checked(c);
         const lima::RefDev& d = c->ref;
         const int nc = d.n_c, ns = d.n_s;

@@ -23,9 +23,10 @@
 //            rebuild graph, which runs before the next step.
 // Rebuild (a device-launchable graph, or host launches): k_sort_count,
 // k_sort_scan, k_sort_fill, k_sort_order (a stable counting sort by cell),
-// k_permute + k_copy_back (every per-slot array into the new order) and
-// k_build_list — one warp per 4 particles over the 25 columns of their
-// 5x5x5 cell neighbourhood.
+// k_permute (every per-slot array into the new order, through tmp arrays)
+// and k_build_list — one warp per 8 particles over the columns of their
+// 5x5x5 cell neighbourhood that their bounding box can reach, which also
+// copies the permuted arrays back.
 #include "physdev.cuh"
 #include "physkern.cuh"
 #include "physmath.cuh"
@@ -61,10 +62,6 @@ __device__ __forceinline__ void cell_xyz(const PhysDev& d, float4 p, int& cx, in
     cx = min(max((int)(p.x * inv), 0), d.m - 1);
     cy = min(max((int)(p.y * inv), 0), d.m - 1);
     cz = min(max((int)(p.z * inv), 0), d.m - 1);
-}
-
-__device__ __forceinline__ uint32_t nl_index(const PhysDev& d, int i, int k) {
-    return ((uint32_t)(k / kGroup) * (uint32_t)d.n_pad + (uint32_t)i) * kGroup + (uint32_t)(k % kGroup);
 }
 
 __device__ __forceinline__ bool excluded(const PhysDev& d, uint32_t oi, uint32_t oj) {
@@ -130,14 +127,27 @@ __global__ void k_sort_fill(PhysDev d) {
     d.order[d.cstart[d.cell_key[i]] + d.cell_rank[i]] = (uint32_t)i;
 }
 
-// One thread per cell: the cell's slots in ascending order (insertion sort;
-// cells hold ~10 particles), which makes the sort stable and the new order a
-// function of the positions and the old order only.
+// One warp per cell: the cell's slots (in arrival order from k_sort_fill) put
+// in ascending order, which makes the sort stable and the new order a
+// function of the positions and the old order only.  Each lane ranks its slot
+// by counting the smaller ones; cells of more than 32 particles are sorted by
+// lane 0 (insertion sort).
 __global__ void k_sort_order(PhysDev d) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int c = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (c >= d.n_cells) return;
-    const uint32_t b = d.cstart[c], e = d.cstart[c + 1];
-    for (uint32_t k = b + 1; k < e; k++) {
+    const uint32_t b = d.cstart[c], n = d.cstart[c + 1] - b;
+    if (n <= 1u) return;
+    if (n <= 32u) {
+        const uint32_t v = (uint32_t)lane < n ? d.order[b + lane] : 0xffffffffu;
+        uint32_t rank = 0u;
+        for (uint32_t k = 0; k < n; k++) rank += __shfl_sync(0xffffffffu, v, (int)k) < v ? 1u : 0u;
+        __syncwarp();
+        if ((uint32_t)lane < n) d.order[b + rank] = v;
+        return;
+    }
+    if (lane != 0) return;
+    for (uint32_t k = b + 1; k < b + n; k++) {
         const uint32_t v = d.order[k];
         uint32_t j = k;
         while (j > b && d.order[j - 1] > v) {
@@ -174,125 +184,160 @@ __global__ void k_set_xref(PhysDev d, const float4* __restrict__ pos) {
     if (k < d.n) d.xref[k] = pos[k];
 }
 
-// Sorted copies back into the step arrays; clears the rebuild request.
-__global__ void k_copy_back(PhysDev d, int cur, int mixed) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k == 0) *d.need_rebuild = 0;
-    if (k >= d.n) return;
-    d.pos[cur][k] = d.pos_tmp[0][k];
-    d.pos[cur ^ 1][k] = d.pos_tmp[1][k];
-    d.vel[k] = d.vel_tmp[k];
-    d.force[k] = d.force_tmp[k];
-    if (mixed) {
-        d.posc[k] = d.posc_tmp[k];
-        d.velc[k] = d.velc_tmp[k];
-    }
-    d.orig_of_sorted[k] = d.orig_tmp[k];
-}
 
-// Verlet-list build: one warp per 32 / kSlices consecutive sorted particles,
-// kSlices lanes per particle (lane = kSlices * particle + slice).  The warp's particles are split
-// into groups that share a home column (cells (x, y, *)) and a z-window of at
-// most m-4 cells; particles outside the current group idle.  For a group with
-// home cells z0..z1, the candidates are the cells z0-2..z1+2 of the 25
-// columns around it (cells of side >= r_list/2, so they cover r_list), each
-// one or two contiguous slot ranges of the cell-sorted order.  Candidates
-// come through shared memory 32 at a time, shifted into the home frame by
-// whole box lengths; each lane tests every kSlices-th candidate against its
-// particle, the slices' hit masks are merged with xor-shuffles, and
-// every lane writes its own hits at their rank in the merged mask, so each
-// row lists its neighbours in candidate order (deterministic).  Collectives
-// (ballots, shuffles, __syncwarp) only occur in warp-uniform code.  Boxes
-// with fewer than 5 cells per side test all particles with the minimum image.
-// items (nullable): the cell order as a list of slots when the particles were
-// not moved into it (in-place rebuild); positions q of that order index cells,
-// slots index the particle data and the list rows.
+// Verlet-list build: one warp per 8 consecutive particles of the cell order,
+// 4 lanes per particle (lane = 4 p + s).  The warp's particles are taken in
+// groups that share a home column (cells (x, y, *)) and a z-window of at most
+// m-4 cells; lanes outside the current group idle.  For a group, each of the
+// 25 columns around it is culled when the xy gap between the group's bounding
+// box and the column exceeds r_list, and otherwise contributes the cells that
+// the group's z-range, widened by the reach sqrt(r_list^2 - gap^2), overlaps:
+// one or two contiguous slot ranges of the cell order (at most m cells).  The
+// ranges are walked as one stream of candidates, 32 at a time: each lane
+// fetches one (the next batch while the current one is tested), shifts it
+// into the home frame by whole box lengths and stages it in shared memory.
+// Slice s of a particle tests candidates s, s+4, ..., drops itself and
+// bonded exclusions, and the slices' hit masks are merged with xor-shuffles;
+// each lane then writes its hits at their rank in the merged mask, so rows
+// list their neighbours in candidate order (deterministic).  Boxes with fewer
+// than 5 cells per side stream all particles with the minimum image.
+// pos/orig: positions and orig ids by slot.  items (nullable): the cell order
+// as a list of slots when the particles were not moved into it (in-place
+// rebuild).  copy_cur >= 0: the particles were permuted into the tmp arrays
+// (pos = pos_tmp[0], orig = orig_tmp); the build also copies every slot back
+// into the step arrays of parity copy_cur (the rebuild's last copy).
 namespace {
 
-// A warp's staged candidates, as two arrays so that the slices of one
-// particle read consecutive 16-byte positions.
-struct Cand {
-    float4 p[32];     // shifted positions
-    uint32_t j[32];   // slot | bit 31 when the particle is a compound particle
+constexpr int kBuildSlices = 4;                  // lanes per particle
+constexpr int kBuildPerWarp = 32 / kBuildSlices; // particles per warp
+constexpr int kMaxRanges = 50;                   // 25 columns, one or two slot ranges each
+
+struct BuildSmem {
+    float4 cand[32];                 // staged candidates: shifted position, w = slot | compound bit
+    int rstart[kMaxRanges + 1];      // first stream index of range r; rstart[kMaxRanges] = stream length
+    int rbase[kMaxRanges];           // first cell-order position of range r
+    float rsx[kMaxRanges], rsy[kMaxRanges], rsz[kMaxRanges];   // shift of range r
 };
 
+// candidate f of the stream (shifted position, w = slot | compound bit), or a
+// NaN sentinel past its end (fails the distance test)
+__device__ __forceinline__ float4 fetch_cand(const PhysDev& d, const BuildSmem* sm, const float4* __restrict__ pos,
+                                             const uint32_t* __restrict__ orig, const uint32_t* __restrict__ items,
+                                             int f, int total, bool any_ex) {
+    if (f >= total) {
+        const float nan = __int_as_float(0x7fc00000);
+        return make_float4(nan, nan, nan, __uint_as_float(0u));
+    }
+    int lo = 0, hi = kMaxRanges - 1;   // the last range starting at or before f (skips empty ranges)
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (sm->rstart[mid] <= f) lo = mid;
+        else hi = mid - 1;
+    }
+    const int q = sm->rbase[lo] + (f - sm->rstart[lo]);
+    const int j = items ? (int)items[q] : q;
+    const float4 p = pos[j];
+    uint32_t tag = (uint32_t)j;
+    if (any_ex && orig[j] < (uint32_t)d.n_cp) tag |= 0x80000000u;
+    return make_float4(p.x + sm->rsx[lo], p.y + sm->rsy[lo], p.z + sm->rsz[lo], __uint_as_float(tag));
+}
+
+// The group's candidate stream (ranges set up in sm) against every member's particle.
 template <bool MIN_IMAGE>
-__device__ __forceinline__ void scan_range(const PhysDev& d, const float4* __restrict__ pos,
-                                           const uint32_t* __restrict__ items, Cand* sc, int jb, int je, float sx,
-                                           float sy, float sz, bool mine, int i, int qi, float4 pi, uint32_t oi,
-                                           bool ex, int lane, int sub, int& cnt) {
-    for (int jc = jb; jc < je; jc += 32) {
-        const int nv = min(32, je - jc);
+__device__ __forceinline__ void scan_stream(const PhysDev& d, const float4* __restrict__ pos,
+                                            const uint32_t* __restrict__ orig, const uint32_t* __restrict__ items,
+                                            BuildSmem* sm, int total, bool mine, bool any_ex, int i, float4 pi,
+                                            uint32_t oi, bool ex, int lane, int sub, int& cnt) {
+    float4 nxt = fetch_cand(d, sm, pos, orig, items, lane, total, any_ex);
+    for (int t0 = 0; t0 < total; t0 += 32) {
         __syncwarp();
-        if (lane < nv) {
-            const int j = items ? (int)items[jc + lane] : jc + lane;
-            const float4 p = pos[j];
-            const uint32_t oj = d.orig_of_sorted[j];
-            sc->p[lane] = make_float4(p.x + sx, p.y + sy, p.z + sz, 0.f);
-            sc->j[lane] = (uint32_t)j | (oj < (uint32_t)d.n_cp ? 0x80000000u : 0u);
-        }
+        sm->cand[lane] = nxt;
         __syncwarp();
-        // slice `sub` tests candidates sub, sub + kSlices, ... (the slices of a
-        // particle read consecutive 16-byte positions: one wavefront per 8 lanes)
-        uint32_t mine_bits = 0;
+        nxt = fetch_cand(d, sm, pos, orig, items, t0 + 32 + lane, total, any_ex);   // in flight during the tests
+        uint32_t hm = 0u;
         if (mine) {
 #pragma unroll
-            for (int t = 0; t < 32 / kSlices; t++) {
-                const int c = kSlices * t + sub;
-                if (c < nv) {
-                    const float4 q = sc->p[c];
-                    float dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
-                    if (MIN_IMAGE) {
-                        dx = mimg(dx, d.L, d.invL);
-                        dy = mimg(dy, d.L, d.invL);
-                        dz = mimg(dz, d.L, d.invL);
-                    }
-                    mine_bits |= (dx * dx + dy * dy + dz * dz < d.rlist2 ? 1u : 0u) << c;
+            for (int t = 0; t < 32 / kBuildSlices; t++) {
+                const int c = kBuildSlices * t + sub;
+                const float4 q = sm->cand[c];
+                float dx = q.x - pi.x, dy = q.y - pi.y, dz = q.z - pi.z;
+                if (MIN_IMAGE) {
+                    dx = mimg(dx, d.L, d.invL);
+                    dy = mimg(dy, d.L, d.invL);
+                    dz = mimg(dz, d.L, d.invL);
                 }
+                hm |= (dx * dx + dy * dy + dz * dz < d.rlist2 ? 1u : 0u) << c;
             }
-            const int self = qi - jc;
-            if (self >= 0 && self < 32) mine_bits &= ~(1u << self);
-            if (ex)
-                for (uint32_t b = mine_bits; b; b &= b - 1u) {
-                    const int c = __ffs(b) - 1;
-                    const uint32_t jw = sc->j[c];
-                    if ((jw >> 31) && excluded(d, oi, d.orig_of_sorted[jw & 0x7fffffffu])) mine_bits &= ~(1u << c);
-                }
+            // drop the particle itself and its bonded exclusions
+            for (uint32_t b = hm; b; b &= b - 1u) {
+                const int c = __ffs(b) - 1;
+                const uint32_t tag = __float_as_uint(sm->cand[c].w);
+                const uint32_t j = tag & 0x7fffffffu;
+                if (j == (uint32_t)i || (ex && (tag >> 31) && excluded(d, oi, orig[j]))) hm &= ~(1u << c);
+            }
         }
-        uint32_t m32 = mine_bits;
-#pragma unroll
-        for (int o = 1; o < kSlices; o <<= 1) m32 |= __shfl_xor_sync(0xffffffffu, m32, o);
-        for (uint32_t b = mine_bits; b; b &= b - 1u) {
+        uint32_t all = hm;   // the particle's hits (the 4 slices are lanes 4p .. 4p+3)
+        all |= __shfl_xor_sync(0xffffffffu, all, 1);
+        all |= __shfl_xor_sync(0xffffffffu, all, 2);
+        for (uint32_t b = hm; b; b &= b - 1u) {
             const int c = __ffs(b) - 1;
-            const int k = cnt + __popc(m32 & ((1u << c) - 1u));
-            if (k < d.nl_cap) d.nl[nl_index(d, i, k)] = sc->j[c] & 0x7fffffffu;
+            const int k = cnt + __popc(all & ((1u << c) - 1u));
+            if (k < d.nl_cap)
+                d.nl[((size_t)(k / kGroup) * d.n_pad + (size_t)i) * kGroup + (k % kGroup)] =
+                    __float_as_uint(sm->cand[c].w) & 0x7fffffffu;
         }
-        cnt += __popc(m32);
+        cnt += __popc(all);
     }
 }
 
 }  // namespace
 
 __global__ void __launch_bounds__(kBuildWarps * 32) k_build_list(PhysDev d, const float4* __restrict__ pos,
-                                                                 const uint32_t* __restrict__ items) {
-    __shared__ Cand s_cand[kBuildWarps];
+                                                                 const uint32_t* __restrict__ orig,
+                                                                 const uint32_t* __restrict__ items, int copy_cur,
+                                                                 int mixed) {
+    __shared__ BuildSmem s_build[kBuildWarps];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int pl = lane / kSlices, sub = lane % kSlices;
-    const int base = (blockIdx.x * kBuildWarps + w) * (32 / kSlices);
+    const int pl = lane / kBuildSlices, sub = lane % kBuildSlices;
+    const int gw = blockIdx.x * kBuildWarps + w;
+    if (copy_cur >= 0) {   // the rebuild's copy of the permuted tmp arrays into the step arrays
+        if (gw == 0 && lane == 0) *d.need_rebuild = 0;
+        for (int k = gw * 32 + lane; k < d.n; k += gridDim.x * kBuildWarps * 32) {
+            d.pos[copy_cur][k] = d.pos_tmp[0][k];
+            d.pos[copy_cur ^ 1][k] = d.pos_tmp[1][k];
+            d.vel[k] = d.vel_tmp[k];
+            d.force[k] = d.force_tmp[k];
+            if (mixed) {
+                d.posc[k] = d.posc_tmp[k];
+                d.velc[k] = d.velc_tmp[k];
+            }
+            d.orig_of_sorted[k] = d.orig_tmp[k];
+        }
+    }
+    const int base = gw * kBuildPerWarp;
     if (base >= d.n) return;   // the whole warp
-    Cand* sc = &s_cand[w];
+    BuildSmem* sm = &s_build[w];
     const int qi = base + pl;   // position in the cell order
     const bool have = qi < d.n;
-    const int i = have ? (items ? (int)items[qi] : qi) : qi;   // slot
+    const int i = have ? (items ? (int)items[qi] : qi) : 0;   // slot
     const float4 pi = have ? pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const uint32_t oi = have ? d.orig_of_sorted[i] : 0u;
+    const uint32_t oi = have ? orig[i] : 0u;
     const bool ex = have && oi < (uint32_t)d.n_cp && d.excl_off[oi + 1] > d.excl_off[oi];
+    const bool any_ex = __any_sync(0xffffffffu, ex);
     int cnt = 0;
     const int m = d.m;
 
-    if (m < 5) {
-        scan_range<true>(d, pos, items, sc, 0, d.n, 0.f, 0.f, 0.f, have, i, qi, pi, oi, ex, lane, sub, cnt);
+    if (m < 5) {   // one range: every particle, minimum image
+        if (lane == 0) {
+            sm->rstart[0] = 0;
+            sm->rbase[0] = 0;
+            sm->rsx[0] = sm->rsy[0] = sm->rsz[0] = 0.f;
+            for (int r = 1; r <= kMaxRanges; r++) sm->rstart[r] = d.n;
+        }
+        __syncwarp();
+        scan_stream<true>(d, pos, orig, items, sm, d.n, have, any_ex, i, pi, oi, ex, lane, sub, cnt);
     } else {
+        const float cs = d.L / (float)m;   // cell side
         int cx = -1, cy = -1, cz = 0;
         if (have) cell_xyz(d, pi, cx, cy, cz);
         // one bit per particle, at its slice-0 lane
@@ -302,38 +347,84 @@ __global__ void __launch_bounds__(kBuildWarps * 32) k_build_list(PhysDev d, cons
             const int hx = __shfl_sync(0xffffffffu, cx, lead);
             const int hy = __shfl_sync(0xffffffffu, cy, lead);
             const int hz0 = __shfl_sync(0xffffffffu, cz, lead);
-            const bool mine = ((todo >> (pl * kSlices)) & 1u) && cx == hx && cy == hy && cz <= hz0 + (m - 5);
-            const unsigned grp = __ballot_sync(0xffffffffu, mine && sub == 0);
-            todo &= ~grp;
-            // sorted by cell: the group's last particle has its top cell
-            const int hz1 = __shfl_sync(0xffffffffu, cz, 31 - __clz(grp));
-            for (int ox = -2; ox <= 2; ox++) {
-                int x = hx + ox;
-                float sx = 0.f;
-                if (x < 0) { x += m; sx = -d.L; } else if (x >= m) { x -= m; sx = d.L; }
-                for (int oy = -2; oy <= 2; oy++) {
-                    int y = hy + oy;
-                    float sy = 0.f;
+            const bool mine = ((todo >> (pl * kBuildSlices)) & 1u) && cx == hx && cy == hy && cz <= hz0 + (m - 5);
+            todo &= ~__ballot_sync(0xffffffffu, mine && sub == 0);
+            int hz1 = mine ? cz : -1;   // the group's top cell
+            float bxl = mine ? pi.x : 3.4e38f, bxh = mine ? pi.x : -3.4e38f;
+            float byl = mine ? pi.y : 3.4e38f, byh = mine ? pi.y : -3.4e38f;
+            float bzl = mine ? pi.z : 3.4e38f, bzh = mine ? pi.z : -3.4e38f;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                hz1 = max(hz1, __shfl_xor_sync(0xffffffffu, hz1, o));
+                bxl = fminf(bxl, __shfl_xor_sync(0xffffffffu, bxl, o));
+                bxh = fmaxf(bxh, __shfl_xor_sync(0xffffffffu, bxh, o));
+                byl = fminf(byl, __shfl_xor_sync(0xffffffffu, byl, o));
+                byh = fmaxf(byh, __shfl_xor_sync(0xffffffffu, byh, o));
+                bzl = fminf(bzl, __shfl_xor_sync(0xffffffffu, bzl, o));
+                bzh = fmaxf(bzh, __shfl_xor_sync(0xffffffffu, bzh, o));
+            }
+            // lane c < 25: column (hx + c / 5 - 2, hy + c % 5 - 2), ranges 2c and 2c + 1
+            int b0 = 0, l0 = 0, b1 = 0, l1 = 0;
+            float sx = 0.f, sy = 0.f, sz0 = 0.f, sz1 = 0.f;
+            if (lane < 25) {
+                const int ox = lane / 5 - 2, oy = lane % 5 - 2;
+                const float cxl = (float)(hx + ox) * cs, cxh = cxl + cs;   // unwrapped, home frame
+                const float cyl = (float)(hy + oy) * cs, cyh = cyl + cs;
+                const float gx = fmaxf(0.f, fmaxf(cxl - bxh, bxl - cxh));
+                const float gy = fmaxf(0.f, fmaxf(cyl - byh, byl - cyh));
+                const float g2 = gx * gx + gy * gy;
+                if (g2 < d.rlist2 * 1.0001f) {   // the margin covers cell rounding
+                    int x = hx + ox, y = hy + oy;
+                    if (x < 0) { x += m; sx = -d.L; } else if (x >= m) { x -= m; sx = d.L; }
                     if (y < 0) { y += m; sy = -d.L; } else if (y >= m) { y -= m; sy = d.L; }
                     const int col = (x * m + y) * m;
-                    // unwrapped cells u0..u1 (at most m of them) -> one or two real ranges
-                    const int u0 = hz0 - 2, u1 = hz1 + 2;
+                    // cells within the reach of the group's z-range (unwrapped; at
+                    // most m of them: the group spans <= m - 4 cells)
+                    const float reach = sqrtf(fmaxf(d.rlist2 - g2, 0.f)) + 1e-4f * cs;
+                    const int u0 = max((int)floorf((bzl - reach) / cs), hz0 - 2);
+                    const int u1 = min((int)floorf((bzh + reach) / cs), hz1 + 2);
                     if (u0 < 0) {
-                        scan_range<false>(d, pos, items, sc, (int)d.cstart[col + u0 + m], (int)d.cstart[col + m], sx, sy, -d.L,
-                                          mine, i, qi, pi, oi, ex, lane, sub, cnt);
-                        scan_range<false>(d, pos, items, sc, (int)d.cstart[col], (int)d.cstart[col + u1 + 1], sx, sy, 0.f, mine,
-                                          i, qi, pi, oi, ex, lane, sub, cnt);
+                        b0 = (int)d.cstart[col + u0 + m];
+                        l0 = (int)d.cstart[col + m] - b0;
+                        sz0 = -d.L;
+                        b1 = (int)d.cstart[col];
+                        l1 = (int)d.cstart[col + u1 + 1] - b1;
                     } else if (u1 >= m) {
-                        scan_range<false>(d, pos, items, sc, (int)d.cstart[col + u0], (int)d.cstart[col + m], sx, sy, 0.f, mine,
-                                          i, qi, pi, oi, ex, lane, sub, cnt);
-                        scan_range<false>(d, pos, items, sc, (int)d.cstart[col], (int)d.cstart[col + u1 - m + 1], sx, sy, d.L,
-                                          mine, i, qi, pi, oi, ex, lane, sub, cnt);
-                    } else {
-                        scan_range<false>(d, pos, items, sc, (int)d.cstart[col + u0], (int)d.cstart[col + u1 + 1], sx, sy, 0.f,
-                                          mine, i, qi, pi, oi, ex, lane, sub, cnt);
+                        b0 = (int)d.cstart[col + u0];
+                        l0 = (int)d.cstart[col + m] - b0;
+                        b1 = (int)d.cstart[col];
+                        l1 = (int)d.cstart[col + u1 - m + 1] - b1;
+                        sz1 = d.L;
+                    } else if (u1 >= u0) {
+                        b0 = (int)d.cstart[col + u0];
+                        l0 = (int)d.cstart[col + u1 + 1] - b0;
                     }
                 }
             }
+            // stream offsets: inclusive scan of the per-column lengths
+            const int len = l0 + l1;
+            int incl = len;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            __syncwarp();   // the previous group's readers of sm are done
+            if (lane < 25) {
+                const int st = incl - len;
+                sm->rstart[2 * lane] = st;
+                sm->rstart[2 * lane + 1] = st + l0;
+                sm->rbase[2 * lane] = b0;
+                sm->rbase[2 * lane + 1] = b1;
+                sm->rsx[2 * lane] = sm->rsx[2 * lane + 1] = sx;
+                sm->rsy[2 * lane] = sm->rsy[2 * lane + 1] = sy;
+                sm->rsz[2 * lane] = sz0;
+                sm->rsz[2 * lane + 1] = sz1;
+            }
+            if (lane == 0) sm->rstart[kMaxRanges] = total;
+            __syncwarp();
+            scan_stream<false>(d, pos, orig, items, sm, total, mine, any_ex, i, pi, oi, ex, lane, sub, cnt);
         }
     }
     if (have && sub == 0) {
@@ -869,7 +960,7 @@ void launch_sort(const PhysDev& d, const float4* pos, cudaStream_t s) {
     k_sort_count<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d, pos);
     k_sort_scan<<<1, kScanThreads, 0, s>>>(d);
     k_sort_fill<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d);
-    k_sort_order<<<(d.n_cells + kTB - 1) / kTB, kTB, 0, s>>>(d);
+    k_sort_order<<<(int)(((size_t)d.n_cells * 32 + kTB - 1) / kTB), kTB, 0, s>>>(d);
 }
 
 void launch_permute(const PhysDev& d, int cur, bool mixed, cudaStream_t s) {
@@ -880,13 +971,11 @@ void launch_set_xref(const PhysDev& d, const float4* pos, cudaStream_t s) {
     k_set_xref<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d, pos);
 }
 
-void launch_build_list(const PhysDev& d, const float4* pos, const uint32_t* items, cudaStream_t s) {
-    const int warps = (d.n + 32 / kSlices - 1) / (32 / kSlices);
-    k_build_list<<<(warps + kBuildWarps - 1) / kBuildWarps, kBuildWarps * 32, 0, s>>>(d, pos, items);
-}
-
-void launch_copy_back(const PhysDev& d, int cur, bool mixed, cudaStream_t s) {
-    k_copy_back<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d, cur, mixed ? 1 : 0);
+void launch_build_list(const PhysDev& d, const float4* pos, const uint32_t* orig, const uint32_t* items, int copy_cur,
+                       bool mixed, cudaStream_t s) {
+    const int warps = (d.n + 7) / 8;   // 8 particles per warp
+    k_build_list<<<(warps + kBuildWarps - 1) / kBuildWarps, kBuildWarps * 32, 0, s>>>(d, pos, orig, items, copy_cur,
+                                                                                    mixed ? 1 : 0);
 }
 
 void launch_bonded(const PhysDev& d, int cur, bool energy, cudaStream_t s) {

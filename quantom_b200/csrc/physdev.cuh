@@ -144,8 +144,8 @@ unsigned long long phys_device_rebuilds(const PhysDev& d, cudaStream_t s);
 // the device-launchable rebuild graphs of both parities (after the list capacity is final)
 int phys_capture_rebuild(PhysDev& d, cudaStream_t s, std::string& msg);
 void phys_free_rebuild(PhysDev& d);
-// k_sort_count, k_sort_scan, k_sort_fill, k_sort_order, k_permute, k_copy_back, k_build_list
-constexpr int kRebuildKernels = 7;
+// k_sort_count, k_sort_scan, k_sort_fill, k_sort_order, k_permute, k_build_list
+constexpr int kRebuildKernels = 6;
 // One step: the bonded kernel, then the step kernel (pair terms,
 // integration, FP64 sums) launched programmatically so that it overlaps the
 // bonded kernel.  tail: launch the due rebuild from the device (the launch
@@ -157,6 +157,9 @@ void phys_energy_now(PhysDev& d, int cur, cudaStream_t s);
 void phys_read_compounds(const PhysDev& d, int cur, const lima_compound* comps, float4* pos_out, float4* prev_out);
 void phys_read_solvents(const PhysDev& d, int cur, float4* pos_out, float4* prev_out);
 void phys_read_forces(const PhysDev& d, const lima_compound* comps, float4* fc, float4* fs);
+// the Verlet list as CSR over orig ids (offsets[n + 1]; ids, nullable, sorted
+// ascending in each row); returns the total entry count
+uint32_t phys_read_list(const PhysDev& d, uint32_t* offsets, uint32_t* ids);
 void phys_read_energies(const PhysDev& d, double* totals, double* per_particle, const lima_compound* comps, int n_c,
                         int n_s);
 

@@ -322,8 +322,7 @@ void phys_rebuild(const PhysDev& d, int cur, cudaStream_t s) {
     const bool mixed = d.precision == LIMA_PRECISION_MIXED;
     launch_sort(d, d.pos[cur], s);
     launch_permute(d, cur, mixed, s);
-    launch_copy_back(d, cur, mixed, s);
-    launch_build_list(d, d.pos[cur], nullptr, s);
+    launch_build_list(d, d.pos_tmp[0], d.orig_tmp, nullptr, cur, mixed, s);
 }
 
 // The list of positions `pos` without moving any particle: the sort of the
@@ -331,7 +330,7 @@ void phys_rebuild(const PhysDev& d, int cur, cudaStream_t s) {
 void phys_rebuild_inplace(const PhysDev& d, const float4* pos, cudaStream_t s) {
     launch_sort(d, pos, s);
     launch_set_xref(d, pos, s);
-    launch_build_list(d, pos, d.order, s);
+    launch_build_list(d, pos, d.orig_of_sorted, d.order, -1, false, s);
 }
 
 void phys_prime(PhysDev&, int, cudaStream_t) {}
@@ -558,6 +557,30 @@ void phys_read_forces(const PhysDev& d, const lima_compound* comps, float4* fc, 
         o += comps[c].n_particles;
     }
     for (int si = 0; si < d.n_s; si++) fs[si] = by_orig[d.n_cp + si];
+}
+
+uint32_t phys_read_list(const PhysDev& d, uint32_t* offsets, uint32_t* ids) {
+    std::vector<uint32_t> cnt(d.n), orig(d.n), nl((size_t)d.nl_cap * d.n_pad);
+    cudaMemcpy(cnt.data(), d.nl_cnt, sizeof(uint32_t) * d.n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(orig.data(), d.orig_of_sorted, sizeof(uint32_t) * d.n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(nl.data(), d.nl, sizeof(uint32_t) * nl.size(), cudaMemcpyDeviceToHost);
+    std::vector<uint32_t> by_orig(d.n);
+    for (int k = 0; k < d.n; k++) by_orig[orig[k]] = (uint32_t)k;
+    uint32_t pos = 0;
+    for (int o = 0; o < d.n; o++) {
+        const uint32_t k = by_orig[o];
+        offsets[o] = pos;
+        if (ids) {
+            std::vector<uint32_t> row(cnt[k]);
+            for (uint32_t e = 0; e < cnt[k]; e++)
+                row[e] = orig[nl[((size_t)(e / kGroup) * d.n_pad + k) * kGroup + e % kGroup]];
+            std::sort(row.begin(), row.end());
+            std::copy(row.begin(), row.end(), ids + pos);
+        }
+        pos += cnt[k];
+    }
+    offsets[d.n] = pos;
+    return pos;
 }
 
 void phys_read_energies(const PhysDev& d, double* totals, double* per_particle, const lima_compound* comps, int n_c,

@@ -9,8 +9,7 @@ namespace lima {
 
 constexpr int kTB = 256;         // threads per block of the per-particle kernels and the step kernel
 constexpr int kGroup = 8;        // lanes per particle in the list and step kernels
-constexpr int kBuildWarps = 4;   // warps per block of the list build
-constexpr int kSlices = 8;       // lanes per particle in the list build (32 / kSlices particles per warp)
+constexpr int kBuildWarps = 4;   // warps per block of the list build (8 particles per warp)
 constexpr int kMaxTypes = 32;    // LIMA_MAX_ATOM_TYPES
 constexpr int kScanThreads = 1024;
 
@@ -24,13 +23,16 @@ __host__ __device__ inline int bonded_blocks(const PhysDev& d) {
 
 // the counting sort of the slots by the cell of `pos`: cell_key, cstart, order
 void launch_sort(const PhysDev& d, const float4* pos, cudaStream_t s);
-// every per-slot array into cell order (through the tmp arrays), reference positions
+// every per-slot array into cell order in the tmp arrays, reference positions
 void launch_permute(const PhysDev& d, int cur, bool mixed, cudaStream_t s);
-void launch_copy_back(const PhysDev& d, int cur, bool mixed, cudaStream_t s);
 // reference positions of an in-place build (particles not moved)
 void launch_set_xref(const PhysDev& d, const float4* pos, cudaStream_t s);
-// items (nullable): slots in cell order when the particles were not re-sorted
-void launch_build_list(const PhysDev& d, const float4* pos, const uint32_t* items, cudaStream_t s);
+// The Verlet list of positions pos (orig: orig ids by slot).  items
+// (nullable): slots in cell order when the particles were not re-sorted.
+// copy_cur >= 0: pos/orig are the permuted tmp arrays, and the build copies
+// every tmp array back into the step arrays of that parity.
+void launch_build_list(const PhysDev& d, const float4* pos, const uint32_t* orig, const uint32_t* items, int copy_cur,
+                       bool mixed, cudaStream_t s);
 // The bonded kernel of parity `cur` (term forces; ENERGY: block partials)
 void launch_bonded(const PhysDev& d, int cur, bool energy, cudaStream_t s);
 // The step kernel of parity `cur` (slot cur) or an energy evaluation (slot

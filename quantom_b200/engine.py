@@ -24,7 +24,7 @@ OK, ERR_ARGUMENT, ERR_CUDA, ERR_CAPACITY, ERR_STATE, ERR_NUMERIC, ERR_UNSUPPORTE
 SEMANTICS_REFERENCE, SEMANTICS_PHYSICS = 0, 1
 PRECISION_FP32, PRECISION_MIXED = 0, 1
 THERMOSTAT_NONE, THERMOSTAT_REFERENCE, THERMOSTAT_BERENDSEN = 0, 1, 2
-NL_COMPOUND_COMPOUND, NL_COMPOUND_SOLVENT, NL_SOLVENT_COMPOUND, NL_SOLVENT_SOLVENT = 0, 1, 2, 3
+NL_COMPOUND_COMPOUND, NL_COMPOUND_SOLVENT, NL_SOLVENT_COMPOUND, NL_SOLVENT_SOLVENT, NL_PAIR = 0, 1, 2, 3, 4
 E_LJ, E_BOND, E_ANGLE, E_DIHEDRAL, E_KINETIC, E_VIRIAL, E_TEMPERATURE, E_TOTAL = range(8)
 E_COUNT = 8
 PROF_NAMES = ("total", "nlist", "bonded", "pair", "compound")
@@ -394,7 +394,12 @@ class Engine:
         self._check(self.lib.lima_build_nlist(self.h))
 
     def nlist(self, which: int):
-        n = self.system.n_compounds if which in (NL_COMPOUND_COMPOUND, NL_COMPOUND_SOLVENT) else self.system.n_solvents
+        """CSR (offsets, ids) of a neighbour list; NL_PAIR (physics): the Verlet
+        list of every particle, compound particles first, then solvents."""
+        if which == NL_PAIR:
+            n = self.system.n_particles
+        else:
+            n = self.system.n_compounds if which in (NL_COMPOUND_COMPOUND, NL_COMPOUND_SOLVENT) else self.system.n_solvents
         off = np.zeros(n + 1, np.uint32)
         tot = ctypes.c_uint32()
         self._check(self.lib.lima_get_nlist(self.h, which, _ptr(off), None, ctypes.byref(tot)))

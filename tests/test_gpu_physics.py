@@ -207,3 +207,48 @@ def test_compute_energies_reports_its_own_kinetic_energy(gpu):
         b = eng.compute_energies()
     for q in (E.E_KINETIC, E.E_TEMPERATURE, E.E_TOTAL, E.E_LJ):
         assert abs(a[q] - b[q]) <= 1e-9 * abs(b[q]), q
+
+
+def _wrapped_f32(s):
+    """Positions as the physics loader stores them: wrapped into [0, L) in
+    double, then rounded to FP32, compound particles first, then solvents."""
+    parts = [s.states[c]["positions"][: s.compounds[c]["n_particles"]] for c in range(s.n_compounds)]
+    x = np.concatenate(parts + [s.solvents["pos"]]).astype(np.float64) if parts else s.solvents["pos"].astype(np.float64)
+    L = s.spec.box_len
+    w = np.mod(x, L).astype(np.float32)
+    w[w >= np.float32(L)] = 0.0
+    return w
+
+
+@pytest.mark.parametrize("name", ["tiny_chains", "small_bridged", "lj_solvent_4096"])
+def test_verlet_list_matches_brute_force(gpu, name):
+    """The Verlet list of a fresh engine against every pair of the loaded
+    positions: all pairs closer than r_list (outside a 1e-5 rounding band)
+    are listed, none farther, no particle twice or itself, and no bonded
+    exclusion (LJ_Ignores)."""
+    E = gpu
+    s = make_named(name, 2)
+    skin = 0.1
+    with E.Engine(s, _params(E, s, skin=skin)) as eng:
+        off, ids = eng.nlist(E.NL_PAIR)
+    off = off.astype(np.int64)
+    ids = ids.astype(np.int64)
+    x = _wrapped_f32(s).astype(np.float64)
+    n = len(x)
+    L = s.spec.box_len
+    rl2 = (s.spec.cutoff + skin) ** 2
+    ps = po.PhysSystem(s, rc=s.spec.cutoff, r_on=1.0)
+    excl = {(i, int(j)) for i in range(n) for j in ps.excl_ids[ps.excl_off[i]:ps.excl_off[i + 1]]}
+    for i in range(n):
+        row = ids[off[i]:off[i + 1]]
+        assert len(np.unique(row)) == len(row) and i not in row
+        d = x - x[i]
+        d -= L * np.round(d / L)
+        r2 = (d * d).sum(1)
+        must = set(np.nonzero(r2 < rl2 * (1 - 1e-5))[0].tolist()) - {i}
+        may = set(np.nonzero(r2 < rl2 * (1 + 1e-5))[0].tolist()) - {i}
+        must -= {j for j in must if (i, j) in excl}
+        got = set(row.tolist())
+        assert must <= got, (i, sorted(must - got)[:5])
+        assert got <= may, (i, sorted(got - may)[:5])
+        assert not any((i, j) in excl for j in got)
