@@ -63,6 +63,7 @@ struct lima_ctx {
     int cur = 0;
     int n_particles_total = 0;
     std::vector<void*> dallocs;
+    std::vector<void*> pool_allocs;   // physics buffers from the process-wide pool (freed on the stream)
     lima::RefDev ref{};
     lima::PhysDev phys{};
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -81,6 +82,11 @@ struct lima_ctx {
     uint64_t launches = 0;     // kernels of this library launched by this context
     int graph_kernels = 0;     // kernels in one replay of a step graph
     lima::FrameLog log;        // physics: frames recorded every log.every steps
+    // physics readbacks: the orig-ordered state of the last read, kept until the
+    // state changes (state_version names the state; every call that may change
+    // it moves it on)
+    lima::PhysReadCache read_cache;
+    uint64_t state_version = 0;
     lima::RenderBuf render;    // headless rasterizer buffers (allocated by the first lima_render)
 
     template <typename T>
@@ -99,6 +105,8 @@ struct lima_ctx {
             for (auto& g : row)
                 if (g) cudaGraphExecDestroy(g);
         for (void* ptr : dallocs) cudaFree(ptr);
+        for (void* ptr : pool_allocs) lima::pool_free(ptr, stream);
+        if (!pool_allocs.empty()) cudaStreamSynchronize(stream);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (fork.fork) cudaEventDestroy(fork.fork);
@@ -127,6 +135,10 @@ lima_status guarded(lima_ctx* c, F&& f) {
     }
 }
 
+// the message is built only when the check fails (the box checks run per particle)
+void need(bool cond, lima_status st, const char* msg) {
+    if (!cond) fail(st, msg);
+}
 void need(bool cond, lima_status st, const std::string& msg) {
     if (!cond) fail(st, msg);
 }
@@ -414,6 +426,7 @@ void ref_nlist_now(lima_ctx* c) {
 // the four per-kernel-group events of ref_step_kernels / phys_step_kernels;
 // with prof the step is launched directly instead of through the graph.
 void one_step(lima_ctx* c, cudaEvent_t* prof) {
+    c->state_version++;
     const int period = std::max(1, c->p.nlist_period);
     const bool rebuild = c->step > 0 && c->step - c->last_nlist_step >= static_cast<uint64_t>(period);
     // profiling a dynamic list: the host reads the rebuild request before the first event
@@ -455,7 +468,13 @@ void one_step(lima_ctx* c, cudaEvent_t* prof) {
         const bool logged = c->log.on && (c->step % static_cast<uint64_t>(c->log.every)) == 0;
         const bool energy = logged || (c->p.energy_period > 0 && (c->step % c->p.energy_period) == 0);
         if (!prof) {
-            cuda_ok(cudaGraphLaunch(c->dgraph[c->cur][energy ? 1 : 0], c->stream), "cudaGraphLaunch");
+            cudaGraphExec_t& g = c->dgraph[c->cur][energy ? 1 : 0];
+            if (!g) {   // instantiated on first use: a short run pays only for the variants it steps
+                const int k = lima::phys_capture_dynamic(c->phys, c->cur, energy, c->stream, &g);
+                need(k > 0, LIMA_ERR_CUDA, "cannot build the step graph of a dynamic pair list");
+                c->dgraph_kernels[energy ? 1 : 0] = k;
+            }
+            cuda_ok(cudaGraphLaunch(g, c->stream), "cudaGraphLaunch");
             c->launches += c->dgraph_kernels[energy ? 1 : 0];
         } else {   // profiling: the same kernels launched directly, the rebuild decided on the host
             if (dyn_rebuild) {
@@ -556,11 +575,13 @@ lima_status lima_create(const lima_params* params, lima_ctx** out) {
         }
         cuda_ok(cudaEventCreate(&c->ev0), "cudaEventCreate");
         cuda_ok(cudaEventCreate(&c->ev1), "cudaEventCreate");
-        cuda_ok(cudaStreamCreateWithFlags(&c->fork.side, cudaStreamNonBlocking), "cudaStreamCreate");
-        cuda_ok(cudaEventCreateWithFlags(&c->fork.fork, cudaEventDisableTiming), "cudaEventCreate");
-        cuda_ok(cudaEventCreateWithFlags(&c->fork.join, cudaEventDisableTiming), "cudaEventCreate");
-        cuda_ok(cudaStreamCreateWithFlags(&c->fork.side2, cudaStreamNonBlocking), "cudaStreamCreate");
-        cuda_ok(cudaEventCreateWithFlags(&c->fork.join2, cudaEventDisableTiming), "cudaEventCreate");
+        if (p.semantics == LIMA_SEMANTICS_REFERENCE) {   // the solvent kernels' side streams
+            cuda_ok(cudaStreamCreateWithFlags(&c->fork.side, cudaStreamNonBlocking), "cudaStreamCreate");
+            cuda_ok(cudaEventCreateWithFlags(&c->fork.fork, cudaEventDisableTiming), "cudaEventCreate");
+            cuda_ok(cudaEventCreateWithFlags(&c->fork.join, cudaEventDisableTiming), "cudaEventCreate");
+            cuda_ok(cudaStreamCreateWithFlags(&c->fork.side2, cudaStreamNonBlocking), "cudaStreamCreate");
+            cuda_ok(cudaEventCreateWithFlags(&c->fork.join2, cudaEventDisableTiming), "cudaEventCreate");
+        }
     });
     if (st != LIMA_OK) {
         fprintf(stderr, "lima_create: %s\n", c->err.c_str());
@@ -639,12 +660,12 @@ lima_status lima_finish_box(lima_ctx* c) {
             h.sols = c->sols.data();
             h.n_s = static_cast<int>(c->sols.size());
             std::string msg;
-            const int rc = lima::phys_setup(h, c->phys, c->stream, c->dallocs, msg);
+            const int rc = lima::phys_setup(h, c->phys, c->stream, c->pool_allocs, msg);
             if (rc != 0) fail(static_cast<lima_status>(rc), msg);
             lima::phys_rebuild(c->phys, c->cur, c->stream);
             // a solute denser than the box average can overflow the first list:
             // grow the capacity to the measured longest row once, and rebuild
-            if (lima::phys_fit_list(c->phys, c->stream, c->dallocs)) {
+            if (lima::phys_fit_list(c->phys, c->stream, c->pool_allocs)) {
                 lima::phys_rebuild(c->phys, c->cur, c->stream);
                 c->launches += lima::kRebuildKernels;
                 c->host_rebuilds++;
@@ -657,13 +678,7 @@ lima_status lima_finish_box(lima_ctx* c) {
                 std::string rmsg;
                 const int rrc = lima::phys_capture_rebuild(c->phys, c->stream, rmsg);
                 if (rrc != 0) fail(static_cast<lima_status>(rrc), rmsg);
-                for (int parity = 0; parity < 2; parity++)
-                    for (int energy = 0; energy < 2; energy++) {
-                        const int k = lima::phys_capture_dynamic(c->phys, parity, energy != 0, c->stream,
-                                                                 &c->dgraph[parity][energy]);
-                        need(k > 0, LIMA_ERR_CUDA, "cannot build the step graph of a dynamic pair list");
-                        c->dgraph_kernels[energy] = k;
-                    }
+                // the step graphs themselves are instantiated on first use (one_step)
             } else {
                 capture_graphs(c, phys_launch_step);
             }
@@ -786,7 +801,7 @@ lima_status lima_get_compound_states(lima_ctx* c, lima_compound_state* states, l
             cuda_ok(cudaMemcpy(hp.data(), c->ref.cpos[c->cur], sizeof(float4) * ncp, cudaMemcpyDeviceToHost), "D2H");
             cuda_ok(cudaMemcpy(hq.data(), c->ref.cprev, sizeof(float4) * ncp, cudaMemcpyDeviceToHost), "D2H");
         } else {
-            lima::phys_read_compounds(c->phys, c->cur, c->comps.data(), hp.data(), hq.data());
+            lima::phys_read_compounds(c->phys, c->cur, c->comps.data(), hp.data(), hq.data(), c->read_cache, c->state_version);
         }
         for (int i = 0; i < nc; i++) {
             if (states) {
@@ -813,7 +828,7 @@ lima_status lima_get_solvents(lima_ctx* c, lima_solvent* sols) {
             cuda_ok(cudaMemcpy(a.data(), c->ref.spos[c->cur], sizeof(float4) * ns, cudaMemcpyDeviceToHost), "D2H");
             cuda_ok(cudaMemcpy(b.data(), c->ref.sprev[c->cur], sizeof(float4) * ns, cudaMemcpyDeviceToHost), "D2H");
         } else {
-            lima::phys_read_solvents(c->phys, c->cur, a.data(), b.data());
+            lima::phys_read_solvents(c->phys, c->cur, a.data(), b.data(), c->read_cache, c->state_version);
         }
         for (int i = 0; i < ns; i++) {
             sols[i].pos = lima_float3{a[i].x, a[i].y, a[i].z};
@@ -833,7 +848,7 @@ lima_status lima_get_positions(lima_ctx* c, float* cxyz, float* sxyz) {
             if (c->p.semantics == LIMA_SEMANTICS_REFERENCE)
                 cuda_ok(cudaMemcpy(hp.data(), c->ref.cpos[c->cur], sizeof(float4) * ncp, cudaMemcpyDeviceToHost), "D2H");
             else
-                lima::phys_read_compounds(c->phys, c->cur, c->comps.data(), hp.data(), hq.data());
+                lima::phys_read_compounds(c->phys, c->cur, c->comps.data(), hp.data(), hq.data(), c->read_cache, c->state_version);
             for (int i = 0; i < nc; i++)
                 for (int t = 0; t < lima::kMaxCP; t++) {
                     const size_t k = static_cast<size_t>(i) * lima::kMaxCP + t;
@@ -847,7 +862,7 @@ lima_status lima_get_positions(lima_ctx* c, float* cxyz, float* sxyz) {
             if (c->p.semantics == LIMA_SEMANTICS_REFERENCE)
                 cuda_ok(cudaMemcpy(a.data(), c->ref.spos[c->cur], sizeof(float4) * ns, cudaMemcpyDeviceToHost), "D2H");
             else
-                lima::phys_read_solvents(c->phys, c->cur, a.data(), b.data());
+                lima::phys_read_solvents(c->phys, c->cur, a.data(), b.data(), c->read_cache, c->state_version);
             for (int i = 0; i < ns; i++) {
                 sxyz[3 * i] = a[i].x;
                 sxyz[3 * i + 1] = a[i].y;
@@ -860,6 +875,7 @@ lima_status lima_get_positions(lima_ctx* c, float* cxyz, float* sxyz) {
 lima_status lima_set_state(lima_ctx* c, const lima_compound_state* states, const lima_float3* prev,
                            const lima_solvent* sols) {
     return guarded(c, [&] {
+        c->state_version++;
         need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
         sync_checked(c);
         const int nc = static_cast<int>(c->comps.size()), ns = static_cast<int>(c->sols.size());
@@ -976,6 +992,7 @@ lima_status lima_get_energies(lima_ctx* c, double* totals, double* per_particle)
 
 lima_status lima_build_nlist(lima_ctx* c) {
     return guarded(c, [&] {
+        c->state_version++;
         need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
         if (c->p.semantics == LIMA_SEMANTICS_REFERENCE) {
             ref_nlist_now(c);
@@ -1022,6 +1039,7 @@ lima_status lima_get_params(lima_ctx* c, double* theta) {
 
 lima_status lima_set_params(lima_ctx* c, const double* theta) {
     return guarded(c, [&] {
+        c->state_version++;
         need(theta != nullptr, LIMA_ERR_ARGUMENT, "null parameter vector");
         need_physics(c);
         sync_checked(c);
@@ -1037,6 +1055,7 @@ lima_status lima_set_params(lima_ctx* c, const double* theta) {
 
 lima_status lima_loss(lima_ctx* c, const lima_loss_spec* spec, double* loss) {
     return guarded(c, [&] {
+        c->state_version++;
         need(spec != nullptr && loss != nullptr, LIMA_ERR_ARGUMENT, "null spec or output");
         need_gradable(c);
         sync_checked(c);
@@ -1050,6 +1069,7 @@ lima_status lima_loss(lima_ctx* c, const lima_loss_spec* spec, double* loss) {
 
 lima_status lima_grad(lima_ctx* c, const lima_loss_spec* spec, double* loss, double* grad) {
     return guarded(c, [&] {
+        c->state_version++;
         need(spec != nullptr && loss != nullptr && grad != nullptr, LIMA_ERR_ARGUMENT, "null spec or output");
         need_gradable(c);
         sync_checked(c);

@@ -161,14 +161,10 @@ void copy_ring(FrameLog& g, int b, int count, cudaStream_t s) {
     cudaEventRecord(g.done[b], s);
 }
 
-// pinned buffer b (copy finished) -> the host store
-void absorb(FrameLog& g, int b) {
-    const int count = g.pending[b];
-    if (!count) return;
-    cudaEventSynchronize(g.done[b]);
+// `count` frames laid out as a full ring at src (host memory) -> the host store
+void append_frames(FrameLog& g, const char* src, int count) {
     const FrameLogDev& v = g.dev;
     const Sections R = sections(v, v.ring);
-    const char* src = static_cast<const char*>(g.pinned[b]);
     auto append = [&](auto& vec, size_t off, size_t n) {
         using T = typename std::decay_t<decltype(vec)>::value_type;
         const T* p = reinterpret_cast<const T*>(src + off);
@@ -180,14 +176,69 @@ void absorb(FrameLog& g, int b) {
     if (v.train) append(g.train, R.train, c * v.n_train * kTrainValues * 3);
     append(g.energies, R.energies, c * LIMA_E_COUNT);
     append(g.logdata, R.logdata, c * kLogDataFloats);
+}
+
+// pinned buffer b (copy finished) -> the host store
+void absorb(FrameLog& g, int b) {
+    const int count = g.pending[b];
+    if (!count) return;
+    cudaEventSynchronize(g.done[b]);
+    append_frames(g, static_cast<const char*>(g.pinned[b]), count);
     g.steps.insert(g.steps.end(), g.buf_steps[b].begin(), g.buf_steps[b].end());
     g.buf_steps[b].clear();
     g.pending[b] = 0;
 }
 
+// The two pinned staging rings, allocated when a ring first fills (a short
+// run whose frames fit in the device ring never needs them).  Both rings are
+// one allocation: a pinned allocation costs far more than its size.
+bool ensure_pinned(FrameLog& g) {
+    if (g.pinned[0]) return true;
+    const size_t stride = (g.ring_bytes + 255) & ~static_cast<size_t>(255);
+    if (cudaMallocHost(&g.pinned[0], 2 * stride) != cudaSuccess) {
+        cudaGetLastError();
+        g.pinned[0] = nullptr;
+        return false;
+    }
+    g.pinned[1] = static_cast<char*>(g.pinned[0]) + stride;
+    for (int b = 0; b < 2; b++)
+        if (cudaEventCreateWithFlags(&g.done[b], cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+    return true;
+}
+
+// the frames in the device ring -> the host store, waiting for the stream
+// (no staging rings: a readback, or pinned memory ran out)
+void drain_sync(FrameLog& g, cudaStream_t s) {
+    if (!g.in_ring) return;
+    std::vector<char> buf(g.ring_bytes);
+    const FrameLogDev& v = g.dev;
+    const Sections R = sections(v, v.ring);
+    const size_t c = (size_t)g.in_ring;
+    char* dst = buf.data();
+    if (v.traj) cudaMemcpyAsync(dst + R.traj, v.traj, c * v.n_slots * 3 * sizeof(float), cudaMemcpyDeviceToHost, s);
+    if (v.potE) cudaMemcpyAsync(dst + R.potE, v.potE, c * v.n_slots * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (v.train)
+        cudaMemcpyAsync(dst + R.train, v.train, c * v.n_train * kTrainValues * 3 * sizeof(float),
+                        cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(dst + R.energies, v.energies, c * LIMA_E_COUNT * sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(dst + R.logdata, v.logdata, c * kLogDataFloats * sizeof(float), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    append_frames(g, dst, g.in_ring);
+    g.steps.insert(g.steps.end(), g.ring_steps.begin(), g.ring_steps.end());
+    g.ring_steps.clear();
+    g.in_ring = 0;
+}
+
 // the frames in the device ring -> the next pinned buffer (absorbing what it held first)
 void drain(FrameLog& g, cudaStream_t s) {
     if (!g.in_ring) return;
+    if (!ensure_pinned(g)) {
+        drain_sync(g, s);
+        return;
+    }
     const int b = g.next_buf;
     absorb(g, b);
     copy_ring(g, b, g.in_ring, s);
@@ -205,11 +256,8 @@ void framelog_free(FrameLog& g) {
         if (g.pending[b] && g.done[b]) cudaEventSynchronize(g.done[b]);   // copies still in flight
     for (void* p : g.dallocs) cudaFree(p);
     g.dallocs.clear();
-    for (auto& p : g.pinned)
-        if (p) {
-            cudaFreeHost(p);
-            p = nullptr;
-        }
+    if (g.pinned[0]) cudaFreeHost(g.pinned[0]);   // one allocation holds both staging rings
+    g.pinned[0] = g.pinned[1] = nullptr;
     for (auto& e : g.done)
         if (e) {
             cudaEventDestroy(e);
@@ -244,14 +292,10 @@ void framelog_start(FrameLog& g, const PhysDev& d, const std::vector<int>& n_com
     g.ring_bytes = R.total;
     bool ok = ref_slot && v.energies && v.logdata && (!(p.flags & LIMA_LOG_TRAJ) || v.traj) &&
               (!(p.flags & LIMA_LOG_POTE) || v.potE) && (!(p.flags & LIMA_LOG_TRAIN) || !n_c || v.train);
-    for (int b = 0; ok && b < 2; b++) {
-        ok = cudaMallocHost(&g.pinned[b], g.ring_bytes) == cudaSuccess &&
-             cudaEventCreateWithFlags(&g.done[b], cudaEventDisableTiming) == cudaSuccess;
-    }
     if (!ok) {
         framelog_free(g);
         cudaGetLastError();
-        msg = "frame log: out of device or pinned host memory for the ring";
+        msg = "frame log: out of device memory for the ring";
         status = LIMA_ERR_CUDA;
         return;
     }
@@ -294,11 +338,12 @@ int framelog_record(FrameLog& g, const PhysDev& d, int cur, uint64_t step, cudaS
 }
 
 void framelog_flush(FrameLog& g, cudaStream_t s) {
-    drain(g, s);
-    // the older pending buffer first
-    absorb(g, g.next_buf);
-    absorb(g, g.next_buf ^ 1);
-    cudaStreamSynchronize(s);
+    // the older pending buffer first, then the frames still in the device ring
+    if (g.pinned[0]) {
+        absorb(g, g.next_buf);
+        absorb(g, g.next_buf ^ 1);
+    }
+    drain_sync(g, s);
 }
 
 }  // namespace lima

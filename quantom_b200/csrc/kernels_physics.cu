@@ -219,27 +219,25 @@ struct BuildSmem {
     float rsx[kMaxRanges], rsy[kMaxRanges], rsz[kMaxRanges];   // shift of range r
 };
 
+static_assert(kGroup == 8, "the list build writes blocks of 8 entries");
+
 // candidate f of the stream (shifted position, w = slot | compound bit), or a
-// NaN sentinel past its end (fails the distance test)
+// NaN sentinel past its end (fails the distance test).  r: the lane's current
+// range, advanced past the ranges that end at or before f (f only grows).
 __device__ __forceinline__ float4 fetch_cand(const PhysDev& d, const BuildSmem* sm, const float4* __restrict__ pos,
                                              const uint32_t* __restrict__ orig, const uint32_t* __restrict__ items,
-                                             int f, int total, bool any_ex) {
+                                             int f, int total, bool any_ex, int& r) {
     if (f >= total) {
         const float nan = __int_as_float(0x7fc00000);
         return make_float4(nan, nan, nan, __uint_as_float(0u));
     }
-    int lo = 0, hi = kMaxRanges - 1;   // the last range starting at or before f (skips empty ranges)
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (sm->rstart[mid] <= f) lo = mid;
-        else hi = mid - 1;
-    }
-    const int q = sm->rbase[lo] + (f - sm->rstart[lo]);
+    while (sm->rstart[r + 1] <= f) r++;   // rstart[kMaxRanges] = total > f
+    const int q = sm->rbase[r] + (f - sm->rstart[r]);
     const int j = items ? (int)items[q] : q;
     const float4 p = pos[j];
     uint32_t tag = (uint32_t)j;
     if (any_ex && orig[j] < (uint32_t)d.n_cp) tag |= 0x80000000u;
-    return make_float4(p.x + sm->rsx[lo], p.y + sm->rsy[lo], p.z + sm->rsz[lo], __uint_as_float(tag));
+    return make_float4(p.x + sm->rsx[r], p.y + sm->rsy[r], p.z + sm->rsz[r], __uint_as_float(tag));
 }
 
 // The group's candidate stream (ranges set up in sm) against every member's particle.
@@ -248,12 +246,13 @@ __device__ __forceinline__ void scan_stream(const PhysDev& d, const float4* __re
                                             const uint32_t* __restrict__ orig, const uint32_t* __restrict__ items,
                                             BuildSmem* sm, int total, bool mine, bool any_ex, int i, float4 pi,
                                             uint32_t oi, bool ex, int lane, int sub, int& cnt) {
-    float4 nxt = fetch_cand(d, sm, pos, orig, items, lane, total, any_ex);
+    int r = 0;
+    float4 nxt = fetch_cand(d, sm, pos, orig, items, lane, total, any_ex, r);
     for (int t0 = 0; t0 < total; t0 += 32) {
         __syncwarp();
         sm->cand[lane] = nxt;
         __syncwarp();
-        nxt = fetch_cand(d, sm, pos, orig, items, t0 + 32 + lane, total, any_ex);   // in flight during the tests
+        nxt = fetch_cand(d, sm, pos, orig, items, t0 + 32 + lane, total, any_ex, r);   // in flight during the tests
         uint32_t hm = 0u;
         if (mine) {
 #pragma unroll
@@ -266,25 +265,32 @@ __device__ __forceinline__ void scan_stream(const PhysDev& d, const float4* __re
                     dy = mimg(dy, d.L, d.invL);
                     dz = mimg(dz, d.L, d.invL);
                 }
-                hm |= (dx * dx + dy * dy + dz * dz < d.rlist2 ? 1u : 0u) << c;
+                const bool hit = dx * dx + dy * dy + dz * dz < d.rlist2 &&
+                                 (__float_as_uint(q.w) & 0x7fffffffu) != (uint32_t)i;   // not itself
+                hm |= (hit ? 1u : 0u) << c;
             }
-            // drop the particle itself and its bonded exclusions
-            for (uint32_t b = hm; b; b &= b - 1u) {
-                const int c = __ffs(b) - 1;
-                const uint32_t tag = __float_as_uint(sm->cand[c].w);
-                const uint32_t j = tag & 0x7fffffffu;
-                if (j == (uint32_t)i || (ex && (tag >> 31) && excluded(d, oi, orig[j]))) hm &= ~(1u << c);
-            }
+            if (ex)   // a compound particle drops its bonded exclusions
+                for (uint32_t b = hm; b; b &= b - 1u) {
+                    const int c = __ffs(b) - 1;
+                    const uint32_t tag = __float_as_uint(sm->cand[c].w);
+                    if ((tag >> 31) && excluded(d, oi, orig[tag & 0x7fffffffu])) hm &= ~(1u << c);
+                }
         }
-        uint32_t all = hm;   // the particle's hits (the 4 slices are lanes 4p .. 4p+3)
+        uint32_t all = hm;   // the particle's hits (its 4 slices are lanes 4p .. 4p+3)
         all |= __shfl_xor_sync(0xffffffffu, all, 1);
         all |= __shfl_xor_sync(0xffffffffu, all, 2);
-        for (uint32_t b = hm; b; b &= b - 1u) {
+        // hit of rank k goes to entry cnt + k; slice s writes ranks s, s + 4, ...
+        // (entry e of row i: word (e / 8 * n_pad + i) * 8 + e % 8, below 2^32
+        // because the list is smaller than 16 GB)
+        uint32_t b = all;
+        for (int k = 0; k < sub && b; k++) b &= b - 1u;
+        for (uint32_t e = (uint32_t)(cnt + sub); b; e += kBuildSlices) {
             const int c = __ffs(b) - 1;
-            const int k = cnt + __popc(all & ((1u << c) - 1u));
-            if (k < d.nl_cap)
-                d.nl[((size_t)(k / kGroup) * d.n_pad + (size_t)i) * kGroup + (k % kGroup)] =
+            if (e < (uint32_t)d.nl_cap)
+                d.nl[((e >> 3) * (uint32_t)d.n_pad + (uint32_t)i) * 8u + (e & 7u)] =
                     __float_as_uint(sm->cand[c].w) & 0x7fffffffu;
+#pragma unroll
+            for (int q = 0; q < kBuildSlices; q++) b &= b - 1u;
         }
         cnt += __popc(all);
     }
@@ -681,9 +687,10 @@ __device__ __forceinline__ void finish_sums(const PhysDev& d, int slot, cudaGrap
 
 // ------------------------------------------------------------------ the step ---
 // (lj_pair: physmath.cuh)
-// position loads in flight per lane in the mixed-precision pair loop: two
-// keep it at 48 registers (four: 56, one block fewer per SM)
-constexpr int kMixedGathers = 2;
+// position loads in flight per lane in the mixed-precision pair loop: the
+// mixed step kernel needs more than 48 registers either way (4 blocks of 256
+// per SM), and four in flight measured 71 against 79 us per flushed step
+constexpr int kMixedGathers = 4;
 
 // One lane's rows of its particle's Verlet list, GATHERS (4 or 2) position
 // loads in flight; MIXED: compensated sums every 8 pairs.

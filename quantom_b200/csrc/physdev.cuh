@@ -125,7 +125,13 @@ struct PhysHost {
     int n_s;
 };
 
-// returns 0 or a lima_status; device buffers are appended to `allocs`
+// Stream-ordered device allocations from a pool of the current device shared
+// by every context of the process; freed blocks stay cached in it, so a new
+// context reuses the memory of destroyed ones instead of mapping new memory.
+void* pool_alloc(size_t bytes, cudaStream_t s);   // nullptr on failure
+void pool_free(void* p, cudaStream_t s);
+
+// returns 0 or a lima_status; device buffers (from the pool) are appended to `allocs`
 int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>& allocs, std::string& msg);
 void phys_upload_state(const PhysHost& h, PhysDev& d, int cur, cudaStream_t s);
 void phys_rebuild(const PhysDev& d, int cur, cudaStream_t s);
@@ -134,7 +140,8 @@ void phys_rebuild_inplace(const PhysDev& d, const float4* pos, cudaStream_t s);
 void phys_prime(PhysDev& d, int cur, cudaStream_t s);
 // after a build: if a row overflowed the list capacity, grow the list to 1.25x
 // the longest row (the capacity starts from the box's mean density, which a
-// dense solute exceeds) and return true so the caller rebuilds; waits for s
+// dense solute exceeds) and return true so the caller rebuilds; waits for s.
+// allocs: the pool allocations of phys_setup (the list is one of them)
 bool phys_fit_list(PhysDev& d, cudaStream_t s, std::vector<void*>& allocs);
 // dynamic lists: the step graph of parity `cur` (the step kernel, which tail-launches
 // the rebuild when one is due); returns its kernel count, or -1 if the graph cannot be built
@@ -154,8 +161,17 @@ constexpr int kRebuildKernels = 6;
 int phys_step_kernels(const PhysDev& d, int cur, cudaStream_t s, bool energy = false, cudaEvent_t* ev = nullptr,
                       bool tail = false);
 void phys_energy_now(PhysDev& d, int cur, cudaStream_t s);
-void phys_read_compounds(const PhysDev& d, int cur, const lima_compound* comps, float4* pos_out, float4* prev_out);
-void phys_read_solvents(const PhysDev& d, int cur, float4* pos_out, float4* prev_out);
+// Host copy of the state in orig order (position and previous position, in
+// double), kept while the state it was read from is unchanged: `key` names
+// that state (the caller changes it whenever the state may have changed).
+struct PhysReadCache {
+    uint64_t key = ~0ull;
+    std::vector<double> x, xp;
+};
+void phys_read_compounds(const PhysDev& d, int cur, const lima_compound* comps, float4* pos_out, float4* prev_out,
+                         PhysReadCache& cache, uint64_t key);
+void phys_read_solvents(const PhysDev& d, int cur, float4* pos_out, float4* prev_out, PhysReadCache& cache,
+                        uint64_t key);
 void phys_read_forces(const PhysDev& d, const lima_compound* comps, float4* fc, float4* fs);
 // the Verlet list as CSR over orig ids (offsets[n + 1]; ids, nullable, sorted
 // ascending in each row); returns the total entry count

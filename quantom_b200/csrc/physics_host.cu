@@ -2,7 +2,9 @@
 // list rebuilds, step launches and readback (kernels in kernels_physics.cu).
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <stdexcept>
 #include <vector>
 
@@ -19,10 +21,64 @@ inline float host_int_as_float(int v) {
     return f;
 }
 
-template <typename T>
-T* dalloc(std::vector<void*>& allocs, size_t n) {
+// One device allocation carved into 256-byte aligned pieces: a pass with
+// base 0 sums the sizes, a second pass over the allocation hands out pointers.
+struct Arena {
+    uintptr_t base = 0;
+    size_t off = 0;
+    template <typename T>
+    T* take(size_t n) {
+        off = (off + 255) & ~static_cast<size_t>(255);
+        T* p = reinterpret_cast<T*>(base + off);
+        off += std::max<size_t>(n, 1) * sizeof(T);
+        return p;
+    }
+};
+
+}  // namespace
+
+void* pool_alloc(size_t bytes, cudaStream_t s) {
+    static std::mutex mu;
+    static std::vector<cudaMemPool_t> pools;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    cudaMemPool_t pool = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if ((int)pools.size() <= dev) pools.resize(dev + 1, nullptr);
+        if (!pools[dev]) {
+            cudaMemPoolProps props = {};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            if (cudaMemPoolCreate(&pools[dev], &props) != cudaSuccess) {
+                cudaGetLastError();
+                pools[dev] = nullptr;
+                return nullptr;
+            }
+            uint64_t keep = UINT64_MAX;   // freed blocks stay with the pool
+            cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        pool = pools[dev];
+    }
     void* p = nullptr;
-    if (cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) throw std::runtime_error("cudaMalloc failed");
+    if (cudaMallocFromPoolAsync(&p, std::max<size_t>(bytes, 1), pool, s) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return p;
+}
+
+void pool_free(void* p, cudaStream_t s) {
+    if (p) cudaFreeAsync(p, s);
+}
+
+namespace {
+
+template <typename T>
+T* dalloc(std::vector<void*>& allocs, size_t n, cudaStream_t s) {
+    void* p = pool_alloc(std::max<size_t>(n, 1) * sizeof(T), s);
+    if (!p) throw std::runtime_error("device allocation failed");
     allocs.push_back(p);
     return static_cast<T*>(p);
 }
@@ -87,8 +143,8 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
             const double ep = std::sqrt(std::max(0.0, (double)A.epsilon * (double)B.epsilon));
             tab[a * d.n_types + b] = make_float2((float)(sg * sg), (float)(4.0 * ep));
         }
-    // exclusions (LJ_Ignores -> orig ids)
-    std::vector<std::vector<uint32_t>> excl(d.n);
+    // exclusions (LJ_Ignores -> orig ids; solvents have none)
+    std::vector<std::vector<uint32_t>> excl(d.n_cp);
     for (int c = 0; c < h.n_c; c++)
         for (int t = 0; t < h.comps[c].n_particles; t++) {
             const lima_lj_ignores& ig = h.comps[c].lj_ignore_list[t];
@@ -103,8 +159,8 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
         }
     std::vector<uint32_t> eoff(d.n + 1, 0), eids;
     for (int i = 0; i < d.n; i++) {
-        eoff[i + 1] = eoff[i] + (uint32_t)excl[i].size();
-        eids.insert(eids.end(), excl[i].begin(), excl[i].end());
+        eoff[i + 1] = eoff[i] + (i < d.n_cp ? (uint32_t)excl[i].size() : 0u);
+        if (i < d.n_cp) eids.insert(eids.end(), excl[i].begin(), excl[i].end());
     }
     // bonded terms with orig ids (compounds, then bridges)
     std::vector<int4> bidx, aidx, didx;
@@ -192,51 +248,59 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
     d.nl_cap = std::min((d.n + kGroup - 1) / kGroup * kGroup, (int)((1.6 * expect + 96) / kGroup + 1) * kGroup);
     d.nl_cap = std::max(d.nl_cap, 4 * kGroup);
 
+    // every fixed-size buffer in one allocation; the list separately (it may grow)
+    auto carve = [&](Arena& a) {
+        for (int b = 0; b < 2; b++) d.pos[b] = a.take<float4>(d.n_pad);
+        d.vel = a.take<float4>(d.n_pad);
+        d.posc = a.take<float4>(d.n_pad);
+        d.velc = a.take<float4>(d.n_pad);
+        d.xref = a.take<float4>(d.n_pad);
+        d.force = a.take<float4>(d.n_pad);
+        for (int b = 0; b < 2; b++) d.pos_orig[b] = a.take<float4>(std::max(1, d.n_cp));
+        for (int b = 0; b < 2; b++) d.posc_orig[b] = a.take<float4>(std::max(1, d.n_cp));
+        d.orig_of_sorted = a.take<uint32_t>(d.n_pad);
+        d.sorted_of_orig = a.take<uint32_t>(d.n);
+        d.lj_table = a.take<float2>(tab.size());
+        d.cell_key = a.take<uint32_t>(d.n);
+        d.cell_rank = a.take<uint32_t>(d.n);
+        d.ccount = a.take<uint32_t>(d.n_cells);
+        d.order = a.take<uint32_t>(d.n);
+        d.cstart = a.take<uint32_t>((size_t)d.n_cells + 1);
+        for (int b = 0; b < 2; b++) d.pos_tmp[b] = a.take<float4>(d.n);
+        d.vel_tmp = a.take<float4>(d.n);
+        d.posc_tmp = a.take<float4>(d.n);
+        d.velc_tmp = a.take<float4>(d.n);
+        d.force_tmp = a.take<float4>(d.n);
+        d.orig_tmp = a.take<uint32_t>(d.n);
+        d.nl_cnt = a.take<uint32_t>(d.n_pad);
+        d.nl_need = a.take<int>(1);
+        d.excl_off = a.take<uint32_t>(eoff.size());
+        d.excl_ids = a.take<uint32_t>(eids.size());
+        d.bond_idx = a.take<int4>(bidx.size());
+        d.bond_par = a.take<float2>(bpar.size());
+        d.angle_idx = a.take<int4>(aidx.size());
+        d.angle_par = a.take<float2>(apar.size());
+        d.dih_idx = a.take<int4>(didx.size());
+        d.dih_par = a.take<float4>(dpar.size());
+        d.bterm_off = a.take<uint32_t>(boff.size());
+        d.bterm_slot = a.take<uint32_t>(bslot.size());
+        d.term_force = a.take<float4>(d.n_term_slots);
+        d.part = a.take<double>((size_t)step_blocks(d) * kRedStride);
+        d.bpart = a.take<double>((size_t)bonded_blocks(d) * 4);
+        d.done = a.take<unsigned int>(1);
+        d.e_last = a.take<double>(LIMA_E_COUNT);
+        d.lambda = a.take<float>(2);
+        d.err = a.take<int>(1);
+        d.need_rebuild = a.take<int>(1);
+        d.rebuild_count = a.take<unsigned long long>(1);
+    };
     try {
-        for (int b = 0; b < 2; b++) d.pos[b] = dalloc<float4>(allocs, d.n_pad);
-        d.vel = dalloc<float4>(allocs, d.n_pad);
-        d.posc = dalloc<float4>(allocs, d.n_pad);
-        d.velc = dalloc<float4>(allocs, d.n_pad);
-        d.xref = dalloc<float4>(allocs, d.n_pad);
-        d.force = dalloc<float4>(allocs, d.n_pad);
-        for (int b = 0; b < 2; b++) d.pos_orig[b] = dalloc<float4>(allocs, std::max(1, d.n_cp));
-        for (int b = 0; b < 2; b++) d.posc_orig[b] = dalloc<float4>(allocs, std::max(1, d.n_cp));
-        d.orig_of_sorted = dalloc<uint32_t>(allocs, d.n_pad);
-        d.sorted_of_orig = dalloc<uint32_t>(allocs, d.n);
-        d.lj_table = dalloc<float2>(allocs, tab.size());
-        d.cell_key = dalloc<uint32_t>(allocs, d.n);
-        d.cell_rank = dalloc<uint32_t>(allocs, d.n);
-        d.ccount = dalloc<uint32_t>(allocs, d.n_cells);
-        d.order = dalloc<uint32_t>(allocs, d.n);
-        d.cstart = dalloc<uint32_t>(allocs, (size_t)d.n_cells + 1);
-        for (int b = 0; b < 2; b++) d.pos_tmp[b] = dalloc<float4>(allocs, d.n);
-        d.vel_tmp = dalloc<float4>(allocs, d.n);
-        d.posc_tmp = dalloc<float4>(allocs, d.n);
-        d.velc_tmp = dalloc<float4>(allocs, d.n);
-        d.force_tmp = dalloc<float4>(allocs, d.n);
-        d.orig_tmp = dalloc<uint32_t>(allocs, d.n);
-        d.nl = dalloc<uint32_t>(allocs, (size_t)d.nl_cap * d.n_pad);
-        d.nl_cnt = dalloc<uint32_t>(allocs, d.n_pad);
-        d.nl_need = dalloc<int>(allocs, 1);
-        d.excl_off = dalloc<uint32_t>(allocs, eoff.size());
-        d.excl_ids = dalloc<uint32_t>(allocs, eids.size());
-        d.bond_idx = dalloc<int4>(allocs, bidx.size());
-        d.bond_par = dalloc<float2>(allocs, bpar.size());
-        d.angle_idx = dalloc<int4>(allocs, aidx.size());
-        d.angle_par = dalloc<float2>(allocs, apar.size());
-        d.dih_idx = dalloc<int4>(allocs, didx.size());
-        d.dih_par = dalloc<float4>(allocs, dpar.size());
-        d.bterm_off = dalloc<uint32_t>(allocs, boff.size());
-        d.bterm_slot = dalloc<uint32_t>(allocs, bslot.size());
-        d.term_force = dalloc<float4>(allocs, d.n_term_slots);
-        d.part = dalloc<double>(allocs, (size_t)step_blocks(d) * kRedStride);
-        d.bpart = dalloc<double>(allocs, (size_t)bonded_blocks(d) * 4);
-        d.done = dalloc<unsigned int>(allocs, 1);
-        d.e_last = dalloc<double>(allocs, LIMA_E_COUNT);
-        d.lambda = dalloc<float>(allocs, 2);
-        d.err = dalloc<int>(allocs, 1);
-        d.need_rebuild = dalloc<int>(allocs, 1);
-        d.rebuild_count = dalloc<unsigned long long>(allocs, 1);
+        Arena plan;
+        carve(plan);
+        Arena real;
+        real.base = reinterpret_cast<uintptr_t>(dalloc<uint8_t>(allocs, plan.off, s));
+        carve(real);
+        d.nl = dalloc<uint32_t>(allocs, (size_t)d.nl_cap * d.n_pad, s);
     } catch (const std::exception& e) {
         msg = std::string("device allocation failed: ") + e.what();
         return LIMA_ERR_CUDA;
@@ -271,17 +335,19 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
 // Host state (reference layout) -> device, in orig order (the next rebuild
 // sorts).  Half-step velocities from the Stormer pair: v = (x - x_prev)/dt.
 void phys_upload_state(const PhysHost& h, PhysDev& d, int cur, cudaStream_t s) {
-    std::vector<float4> pos(d.n_pad), vel(d.n_pad), zero(d.n_pad, make_float4(0, 0, 0, 0));
+    std::vector<float4> pos(d.n_pad), vel(d.n_pad);
     std::vector<uint32_t> ident(d.n_pad);
     const float L = d.L;
     auto wrap = [&](double x) {
-        x = std::fmod(x, (double)L);
-        if (x < 0) x += L;
+        if (!(x >= 0.0 && x < (double)L)) {   // most inputs are inside the box already
+            x = std::fmod(x, (double)L);
+            if (x < 0) x += L;
+        }
         float f = (float)x;
         if (f >= L) f = 0.f;
         return f;
     };
-    auto mimg = [&](double dd) { return dd - L * std::nearbyint(dd / L); };
+    auto mimg = [&](double dd) { return std::fabs(dd) <= 0.5 * L ? dd : dd - L * std::nearbyint(dd / L); };
     int k = 0;
     for (int c = 0; c < h.n_c; c++)
         for (int t = 0; t < h.comps[c].n_particles; t++, k++) {
@@ -306,10 +372,10 @@ void phys_upload_state(const PhysHost& h, PhysDev& d, int cur, cudaStream_t s) {
     for (int i = 0; i < d.n_pad; i++) ident[i] = i < d.n ? i : 0xffffffffu;
     cudaMemcpyAsync(d.pos[cur], pos.data(), sizeof(float4) * d.n_pad, cudaMemcpyHostToDevice, s);
     if (d.n_cp) cudaMemcpyAsync(d.pos_orig[cur], pos.data(), sizeof(float4) * d.n_cp, cudaMemcpyHostToDevice, s);
-    if (d.n_cp) cudaMemcpyAsync(d.posc_orig[cur], zero.data(), sizeof(float4) * d.n_cp, cudaMemcpyHostToDevice, s);
+    if (d.n_cp) cudaMemsetAsync(d.posc_orig[cur], 0, sizeof(float4) * d.n_cp, s);
     cudaMemcpyAsync(d.vel, vel.data(), sizeof(float4) * d.n_pad, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d.posc, zero.data(), sizeof(float4) * d.n_pad, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d.velc, zero.data(), sizeof(float4) * d.n_pad, cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(d.posc, 0, sizeof(float4) * d.n_pad, s);
+    cudaMemsetAsync(d.velc, 0, sizeof(float4) * d.n_pad, s);
     cudaMemcpyAsync(d.orig_of_sorted, ident.data(), sizeof(uint32_t) * d.n_pad, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(d.sorted_of_orig, ident.data(), sizeof(uint32_t) * d.n, cudaMemcpyHostToDevice, s);
     set_device_float(d.lambda, 1.f, s);
@@ -342,10 +408,10 @@ bool phys_fit_list(PhysDev& d, cudaStream_t s, std::vector<void*>& allocs) {
     cudaStreamSynchronize(s);
     if (!(err & ERR_BIT_PHYS_LIST_OVERFLOW) || need <= d.nl_cap) return false;
     const int cap = std::min((d.n + kGroup - 1) / kGroup * kGroup, ((need * 5 / 4 + 32) / kGroup + 1) * kGroup);
-    uint32_t* nl = dalloc<uint32_t>(allocs, (size_t)cap * d.n_pad);   // throws like the other allocations
+    uint32_t* nl = dalloc<uint32_t>(allocs, (size_t)cap * d.n_pad, s);   // throws like the other allocations
     for (auto it = allocs.begin(); it != allocs.end(); ++it)
         if (*it == d.nl) {
-            cudaFree(d.nl);
+            pool_free(d.nl, s);
             allocs.erase(it);
             break;
         }
@@ -509,10 +575,17 @@ void orig_state(const PhysDev& d, const Snapshot& sn, std::vector<double>& x, st
 
 // compound positions in the reference's convention: particle 0 in the box,
 // the others as the image nearest to it (Engine.cu:993-996)
-void phys_read_compounds(const PhysDev& d, int cur, const lima_compound* comps, float4* pos_out, float4* prev_out) {
-    Snapshot sn = snapshot(d, cur, false);
-    std::vector<double> x, xp;
-    orig_state(d, sn, x, xp);
+static void cached_orig_state(const PhysDev& d, int cur, PhysReadCache& cache, uint64_t key) {
+    if (cache.key == key && !cache.x.empty()) return;
+    orig_state(d, snapshot(d, cur, false), cache.x, cache.xp);
+    cache.key = key;
+}
+
+void phys_read_compounds(const PhysDev& d, int cur, const lima_compound* comps, float4* pos_out, float4* prev_out,
+                         PhysReadCache& cache, uint64_t key) {
+    cached_orig_state(d, cur, cache, key);
+    const std::vector<double>& x = cache.x;
+    const std::vector<double>& xp = cache.xp;
     const double L = d.L;
     int o = 0;
     for (int c = 0; c < d.n_c; c++) {
@@ -535,10 +608,11 @@ void phys_read_compounds(const PhysDev& d, int cur, const lima_compound* comps, 
     }
 }
 
-void phys_read_solvents(const PhysDev& d, int cur, float4* pos_out, float4* prev_out) {
-    Snapshot sn = snapshot(d, cur, false);
-    std::vector<double> x, xp;
-    orig_state(d, sn, x, xp);
+void phys_read_solvents(const PhysDev& d, int cur, float4* pos_out, float4* prev_out, PhysReadCache& cache,
+                        uint64_t key) {
+    cached_orig_state(d, cur, cache, key);
+    const std::vector<double>& x = cache.x;
+    const std::vector<double>& xp = cache.xp;
     for (int si = 0; si < d.n_s; si++) {
         const size_t o = 3 * (size_t)(d.n_cp + si);
         pos_out[si] = make_float4((float)x[o], (float)x[o + 1], (float)x[o + 2], 0.f);
