@@ -476,8 +476,11 @@ void lima_topology_destroy(lima_topology* topology);
    on `stream` (a cudaStream_t; NULL is the default stream) and the call returns
    without waiting.  The first call on a device looks up the array's address
    there (cudaGetSymbolAddress), so make it before any stream capture on that
-   device.  Every call on a device shares the one array: calls that overlap in
-   time, from other streams or host threads, race.  err (may be NULL) receives a
+   device.  The address is kept per device ordinal for the rest of the process:
+   it belongs to the device's primary context, so call this with the primary
+   context current, and not after cudaDeviceReset (which ends that context).
+   Every call on a device shares the one array: calls that overlap in time,
+   from other streams or host threads, race.  err (may be NULL) receives a
    message on failure. */
 lima_status lima_ss_nlist_noalloc(const lima_solvent* d_solvents, int n_solvents, float box_len, float cutoff,
                                   int capacity, uint32_t* d_ids, uint32_t* d_counts, int* d_overflow, void* stream,

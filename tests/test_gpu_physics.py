@@ -42,8 +42,13 @@ def _positions(E, eng, s):
 
 @functools.lru_cache(maxsize=2)
 def _system_and_fp64_forces(name, seed):
+    """The FP64 oracle at the positions the engine holds: the loader wraps every
+    coordinate into [0, L) and rounds it to FP32 (compound particles of bridged
+    chains start outside the box), which moves the forces of the raw input by up
+    to 3.9e-4 relative RMS; the bar is on the evaluation, not on that rounding."""
     s = make_named(name, seed)
-    F64, en64 = po.PhysSystem(s, rc=s.spec.cutoff, r_on=1.0).forces()
+    ps = po.PhysSystem(s, rc=s.spec.cutoff, r_on=1.0)
+    F64, en64 = ps.forces(_wrapped_f32(s).astype(np.float64))
     return s, F64, en64
 
 
@@ -59,12 +64,14 @@ def test_forces_and_energies_match_fp64(gpu, name, precision):
         tot = eng.compute_energies()
         fc, fs = eng.forces()
     F = _flat(s, fc, fs)
-    # Compound positions outside [0, L) are wrapped at load and rounded to FP32 (28 of
-    # small_bridged_dry's 192).  The FP64 oracle itself, evaluated at those rounded
-    # positions, differs from its forces at the raw ones by 3.9e-4 relative RMS in
-    # this stiff solvent-free box (1.7e-5 in small_bridged), so the bar is 1e-3 here.
-    tol = 1e-3 if name.endswith("_dry") else 5e-5
-    assert relrms(F, F64) < tol
+    # solvated_chains_258k: FP32 coordinates in a 20 nm box round at 1.9e-6 nm
+    # inside the FP32 arithmetic too (minimum images, differences): 5e-5.
+    # *_dry (no solvent): the forces are the stiff bonds' (k 2.5e8 J/(mol nm^2)),
+    # whose FP32 bond vectors at ~5 nm from the origin carry 2.4e-7 nm of
+    # rounding, ~60 J/(mol nm) against bond forces of ~1e6: measured 7.6e-5
+    tol = 5e-5 if name == "solvated_chains_258k" else (1e-4 if name.endswith("_dry") else 1e-5)
+    err = relrms(F, F64)
+    assert err < tol, err
     scale = abs(en64[0]) + abs(en64[3])
     assert abs(tot[E.E_LJ] - en64[0]) < 1e-5 * scale
     for k, q in ((E.E_BOND, 1), (E.E_ANGLE, 2), (E.E_DIHEDRAL, 3)):

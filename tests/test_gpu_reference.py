@@ -76,8 +76,8 @@ def test_matches_reference_fixtures(gpu, name):
 # 6lzm: the reference's own demo box (T4 lysozyme, 36 compounds, 35 bridges,
 # 5,000 waters) as its input path built it (tests/golden/golden_6lzm.npz);
 # *_dry: compounds (and bridges) with no solvent
-@pytest.mark.parametrize("name", ["tiny_chains", "small_bridged", "lj_solvent_4096", "solvated_chains_32k", "6lzm",
-                                  "tiny_chains_dry", "small_bridged_dry"])
+@pytest.mark.parametrize("name", ["tiny_chains", "small_bridged", "lj_solvent_4096", "lj_solvent_8192",
+                                  "solvated_chains_32k", "6lzm", "tiny_chains_dry", "small_bridged_dry"])
 def test_one_step_matches_oracle(gpu, name):
     E = gpu
     s = make_named(name, 7)
@@ -260,3 +260,54 @@ def test_invalid_box_is_rejected(gpu):
     with pytest.raises(E.LimaError) as ei:
         _engine(E, s)
     assert ei.value.status == E.ERR_ARGUMENT
+
+
+def test_reference_thermostat_schedule_matches_the_reference(gpu):
+    """100 steps with the reference thermostat against the reference's own step
+    code (oracle/_ref) driven by the reference's rule (Engine::hostMaster and
+    handleBoxtemp, Engine.cu:45-75, 362-393): after every 40th step the
+    temperature from the positions two steps apart (getBoxTemperature,
+    Engine.cu:314-359), lambda = clamp(310 / T, 0.9, 1.1) for the next step
+    only, none before step 20.  Two thermostat events (steps 40 and 80)."""
+    if not po.ref_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    E = gpu
+    s = S.make_system("tiny_chains", seed=6)
+    L = s.spec.box_len
+    ff = s.forcefield["particle_parameters"][0]
+    mass = np.concatenate([ff["mass"][s.compounds[c]["atom_types"][: s.compounds[c]["n_particles"]]]
+                           for c in range(s.n_compounds)] + [np.full(s.n_solvents, ff["mass"][0])]).astype(np.float64)
+
+    def flat(state):
+        _, st, sol = state
+        parts = [st[c]["positions"][: s.compounds[c]["n_particles"]] for c in range(s.n_compounds)]
+        return np.concatenate(parts + [sol["pos"]]).astype(np.float64)
+
+    ref = po.RefEngine(s)
+    ref.update_nlists()
+    lam, lams, snap = 1.0, [], {}
+    for k in range(1, 101):
+        ref.step(1, lam)
+        lam = 1.0
+        if k % 40 == 38:
+            snap[k] = flat(ref.state())
+        if k % 40 == 0:
+            d = flat(ref.state()) - snap[k - 2]
+            d -= L * np.round(d / L)
+            v = np.linalg.norm(d, axis=1) * 0.5 / s.spec.dt
+            T = (0.5 * mass * v * v).mean() * 2.0 / (3.0 * 8.3145)
+            lam = float(np.float32(min(max(310.0 / T, 0.9), 1.1))) if k > 20 else 1.0
+            lams.append(lam)
+    _, st_r, sol_r = ref.state()
+    ref.close()
+    assert any(abs(x - 1.0) > 1e-3 for x in lams)   # the thermostat acted
+    with _engine(E, s, thermostat=E.THERMOSTAT_REFERENCE, t_target=310.0) as eng:
+        eng.step(100)
+        st, _ = eng.compound_states()
+        sol = eng.solvents()
+    m = compound_mask(s)
+    dc = st["positions"][m].astype(np.float64) - st_r["positions"][m]
+    dc -= L * np.round(dc / L)
+    ds = sol["pos"].astype(np.float64) - sol_r["pos"]
+    ds -= L * np.round(ds / L)
+    assert np.abs(dc).max() < 1e-4 and np.abs(ds).max() < 1e-4

@@ -102,3 +102,25 @@ def test_wrapping_input_positions_to_fp32_moves_the_forces():
         out[name] = relrms(ps.forces(x32)[0], F)
     assert 1e-4 < out["small_bridged_dry"] < 1e-3
     assert out["small_bridged"] < 5e-5
+
+
+def test_lj_matches_the_reference_where_the_forms_coincide():
+    """Pins the oracle's LJ to the reference's calcLJForce (Engine.cu:475-522)
+    where the two functional forms coincide: one particle type (Lorentz-
+    Berthelot and the reference's arithmetic/geometric mixing agree), no
+    switch, and the physics cutoff equal to the reference's solvent list
+    radius 2 CUTOFF, inside which the reference sums the full LJ force.  The
+    reference's own step code (oracle/_ref) gives the forces of one step;
+    FP32 against FP64."""
+    if not po.ref_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    s = S.make_system("lj_solvent_4096", seed=21)
+    ref = po.RefEngine(s)
+    ref.update_nlists()
+    ref.step(1)
+    _, fs_ref = ref.forces()
+    ref.close()
+    rc = 2.0 * float(po.ref_cutoff_of(s))            # the reference's solvent-solvent list radius
+    F64, _ = po.PhysSystem(s, rc=rc, r_on=rc).forces()
+    err = np.sqrt(((fs_ref.astype(np.float64) - F64) ** 2).sum() / (F64 ** 2).sum())
+    assert err < 1e-5, err
