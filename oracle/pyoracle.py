@@ -93,6 +93,8 @@ def ref_lib():
         lib.ref_get_forces.argtypes = [vp, vp, vp]
         lib.ref_get_potE.restype = i
         lib.ref_get_potE.argtypes = [vp, vp]
+        lib.ref_get_log.restype = i
+        lib.ref_get_log.argtypes = [vp, vp, vp, vp, vp]
         lib.ref_get_step.restype = i
         lib.ref_get_step.argtypes = [vp]
         _ref = lib
@@ -171,6 +173,18 @@ class RefEngine:
         fs = np.zeros((s.n_solvents, 3), np.float32)
         self.lib.ref_get_forces(self.h, _p(fc) if s.n_compounds else None, _p(fs))
         return fc, fs
+
+    def log(self):
+        """The reference's logging buffers of its last step (traj_buffer,
+        potE_buffer, outdata, data_GAN), in its slot order."""
+        s = self.system
+        tpu = s.n_compounds * MAXP + s.n_solvents
+        pe = np.zeros(tpu, np.float64)
+        tr = np.zeros((tpu, 3), np.float32)
+        od = np.zeros(10, np.float32)
+        gan = np.zeros((max(s.n_compounds, 1), MAXP, 3, 3), np.float32)
+        self._check(self.lib.ref_get_log(self.h, _p(pe), _p(tr), _p(od), _p(gan)))
+        return {"potE": pe, "traj": tr, "logdata": od, "train": gan[: s.n_compounds]}
 
     def potE(self):
         s = self.system

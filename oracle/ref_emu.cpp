@@ -558,6 +558,26 @@ int ref_get_potE(void* h, double* out) {
     return 0;
 }
 
+// The reference's logging buffers of the most recent step: traj_buffer and
+// potE_buffer slot (step-1) % STEPS_PER_LOGTRANSFER (total_particles_upperbound
+// entries), outdata (10 floats) and data_GAN slot (step-1) %
+// STEPS_PER_TRAINDATATRANSFER (N_DATAGAN_VALUES Float3 per compound particle
+// slot); Engine.cu:1007-1040, 1136-1145.  Any output may be NULL.
+int ref_get_log(void* h, double* potE, float* traj, float* outdata, float* gan) {
+    auto* c = static_cast<RefCtx*>(h);
+    Box* box = c->sim->box;
+    if (box->step == 0) return -1;
+    const uint32_t tpu = box->total_particles_upperbound;
+    const size_t s_log = static_cast<size_t>((box->step - 1) % STEPS_PER_LOGTRANSFER);
+    const size_t s_gan = static_cast<size_t>((box->step - 1) % STEPS_PER_TRAINDATATRANSFER);
+    if (potE) std::memcpy(potE, box->potE_buffer + s_log * tpu, sizeof(double) * tpu);
+    if (traj) std::memcpy(traj, box->traj_buffer + s_log * tpu, sizeof(Float3) * tpu);
+    if (outdata) std::memcpy(outdata, box->outdata + s_log * 10, sizeof(float) * 10);
+    const size_t ng = static_cast<size_t>(N_DATAGAN_VALUES) * MAX_COMPOUND_PARTICLES * box->n_compounds;
+    if (gan) std::memcpy(gan, box->data_GAN + s_gan * ng, sizeof(Float3) * ng);
+    return 0;
+}
+
 int ref_get_step(void* h) { return static_cast<int>(static_cast<RefCtx*>(h)->sim->box->step); }
 
 }  // extern "C"

@@ -317,6 +317,8 @@ void ref_setup(lima_ctx* c) {
     d.force_c = c->dalloc<float4>(ncp);
     d.force_s = c->dalloc<float4>(ns);
     d.potE = c->dalloc<double>(ncp);
+    d.force_ljsol = c->dalloc<float4>(ncp);
+    cuda_ok(cudaMemsetAsync(d.force_ljsol, 0, sizeof(float4) * std::max<size_t>(ncp, 1), s), "memset");
     cuda_ok(cudaMemsetAsync(d.force_c, 0, sizeof(float4) * std::max<size_t>(ncp, 1), s), "memset");
     cuda_ok(cudaMemsetAsync(d.force_s, 0, sizeof(float4) * std::max(ns, 1), s), "memset");
     cuda_ok(cudaMemsetAsync(d.potE, 0, sizeof(double) * std::max<size_t>(ncp, 1), s), "memset");
@@ -444,6 +446,8 @@ void one_step(lima_ctx* c, cudaEvent_t* prof) {
             c->launches += lima::ref_step_kernels(d, c->cur, c->stream, prof ? prof + 2 : nullptr, &c->fork);
         }
         c->cur ^= 1;
+        if (c->log.on && (c->step % static_cast<uint64_t>(c->log.every)) == 0)
+            c->launches += lima::framelog_record_ref(c->log, d, c->cur, c->step, c->stream);
         c->step++;
         if (c->lambda_pending_reset) {
             lima::set_device_float(d.lambda, 1.f, c->stream);
@@ -1096,8 +1100,6 @@ lima_status lima_rdf(lima_ctx* c, int n_bins, float r_max, double* h) {
 lima_status lima_log_start(lima_ctx* c, const lima_log_params* p) {
     return guarded(c, [&] {
         need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
-        need(c->p.semantics == LIMA_SEMANTICS_PHYSICS, LIMA_ERR_UNSUPPORTED,
-             "the frame log records the physics semantics (the reference path is the parity path)");
         need(p != nullptr, LIMA_ERR_ARGUMENT, "null log params");
         need(p->every >= 1, LIMA_ERR_ARGUMENT, "log every must be >= 1");
         need(p->ring_frames >= 1 && p->ring_frames <= 65536, LIMA_ERR_ARGUMENT, "ring_frames outside 1..65536");
@@ -1108,7 +1110,7 @@ lima_status lima_log_start(lima_ctx* c, const lima_log_params* p) {
         for (const auto& cp : c->comps) np.push_back(cp.n_particles);
         std::string msg;
         int st = LIMA_OK;
-        lima::framelog_start(c->log, c->phys, np, *p, msg, st);
+        lima::framelog_start(c->log, static_cast<int>(c->sols.size()), np, *p, msg, st);
         if (st != LIMA_OK) fail(static_cast<lima_status>(st), msg);
         sync_checked(c);
     });
@@ -1157,6 +1159,71 @@ lima_status lima_log_read(lima_ctx* c, uint64_t first, uint64_t count, uint64_t*
     });
 }
 
+}  // extern "C"
+
+namespace {
+// Analyzer::analyzeEnergy (Analyzer.cu:33-207) on the recorded frames of a
+// reference-semantics run: for frame f with neighbours f - 1 and f + 1, per
+// particle the frame's potE and the kinetic energy of calcKineticEnergy
+// (Engine.cuh:32-45) over the positions two frames apart, with the solvent
+// mass for every particle as the reference's kernels use it; averaged over the
+// solvents and over the compound particles, and those two averages weighed by
+// their particle counts.  One Float3 per analysable frame (frames - 3, as the
+// reference analyses steps - 3); sums in double.
+std::vector<float> analyze_energy(lima_ctx* c, const lima::FrameLog& g) {
+    const size_t nf = g.steps.size(), slots = g.dev.n_slots, ntr = g.dev.n_train;
+    const int nc = static_cast<int>(c->comps.size()), ns = static_cast<int>(c->sols.size());
+    int ncp = 0;
+    for (const auto& cp : c->comps) ncp += cp.n_particles;
+    const double mass = c->ff.particle_parameters[LIMA_ATOMTYPE_SOL].mass;
+    const double dt = c->p.dt * static_cast<double>(g.every);
+    const float L = c->p.box_len, Lh = 0.5f * L;
+    auto ke = [&](const float* a, const float* b) {   // calcKineticEnergy(a, b): b moved into a's image
+        float bb[3];
+        for (int q = 0; q < 3; q++) {
+            bb[q] = b[q];
+            if (bb[q] - a[q] > Lh) bb[q] -= L;
+            else if (bb[q] - a[q] < -Lh) bb[q] += L;
+        }
+        const float dx = a[0] - bb[0], dy = a[1] - bb[1], dz = a[2] - bb[2];
+        const float vel = static_cast<float>(static_cast<double>(std::sqrt(dx * dx + dy * dy + dz * dz) * 0.5f) / dt);
+        return static_cast<float>(0.5 * mass * static_cast<double>(vel) * static_cast<double>(vel));
+    };
+    std::vector<float> out;
+    const size_t n_an = nf >= 4 ? nf - 3 : 0;
+    for (size_t k = 0; k < n_an; k++) {
+        const size_t f = k + 1;
+        const float* xm = &g.traj[(f - 1) * slots * 3];
+        const float* xp = &g.traj[(f + 1) * slots * 3];
+        const double* pe = &g.potE[f * slots];
+        double sol[3] = {0, 0, 0}, cmp[3] = {0, 0, 0};
+        for (int s = 0; s < ns; s++) {
+            const size_t i = ntr + s;
+            const double k_e = ke(&xp[3 * i], &xm[3 * i]);
+            sol[0] += pe[i];
+            sol[1] += k_e;
+            sol[2] += pe[i] + k_e;
+        }
+        for (int ci = 0; ci < nc; ci++)
+            for (int t = 0; t < c->comps[ci].n_particles; t++) {
+                const size_t i = static_cast<size_t>(ci) * LIMA_MAX_COMPOUND_PARTICLES + t;
+                const double k_e = ke(&xp[3 * i], &xm[3 * i]);
+                cmp[0] += pe[i];
+                cmp[1] += k_e;
+                cmp[2] += pe[i] + k_e;
+            }
+        const double n_tot = static_cast<double>(ns + ncp);
+        for (int q = 0; q < 3; q++) {
+            const double avg_s = ns ? sol[q] / ns : 0.0, avg_c = ncp ? cmp[q] / ncp : 0.0;
+            out.push_back(static_cast<float>((avg_s * ns + avg_c * ncp) / n_tot));
+        }
+    }
+    return out;
+}
+}  // namespace
+
+extern "C" {
+
 lima_status lima_log_write(lima_ctx* c, const char* dir) {
     return guarded(c, [&] {
         need(dir != nullptr, LIMA_ERR_ARGUMENT, "null directory");
@@ -1175,17 +1242,23 @@ lima_status lima_log_write(lima_ctx* c, const char* dir) {
         };
         // Environment.cpp:130: logging_data, 10 floats per step
         dump("logdata.bin", g.logdata.data(), g.logdata.size() * sizeof(float));
-        // Analyzer::analyzeEnergy (Analyzer.cu:177-183): per step the mean per particle of
-        // (potential, kinetic, total) energy as a Float3; here from the step's FP64 sums
-        const double n = static_cast<double>(c->phys.n);
-        std::vector<float> energy(nf * 3), temperature(nf);
-        for (size_t f = 0; f < nf; f++) {
-            const double* e = &g.energies[f * LIMA_E_COUNT];
-            const double pot = e[LIMA_E_LJ] + e[LIMA_E_BOND] + e[LIMA_E_ANGLE] + e[LIMA_E_DIHEDRAL];
-            energy[3 * f + 0] = static_cast<float>(pot / n);
-            energy[3 * f + 1] = static_cast<float>(e[LIMA_E_KINETIC] / n);
-            energy[3 * f + 2] = static_cast<float>(e[LIMA_E_TOTAL] / n);
-            temperature[f] = static_cast<float>(e[LIMA_E_TEMPERATURE]);
+        std::vector<float> energy, temperature(nf);
+        for (size_t f = 0; f < nf; f++) temperature[f] = static_cast<float>(g.energies[f * LIMA_E_COUNT + LIMA_E_TEMPERATURE]);
+        if (c->p.semantics == LIMA_SEMANTICS_PHYSICS) {
+            // Analyzer::analyzeEnergy (Analyzer.cu:177-183): per step the mean per particle of
+            // (potential, kinetic, total) energy as a Float3; here from the step's FP64 sums
+            const double n = static_cast<double>(c->phys.n);
+            energy.resize(nf * 3);
+            for (size_t f = 0; f < nf; f++) {
+                const double* e = &g.energies[f * LIMA_E_COUNT];
+                const double pot = e[LIMA_E_LJ] + e[LIMA_E_BOND] + e[LIMA_E_ANGLE] + e[LIMA_E_DIHEDRAL];
+                energy[3 * f + 0] = static_cast<float>(pot / n);
+                energy[3 * f + 1] = static_cast<float>(e[LIMA_E_KINETIC] / n);
+                energy[3 * f + 2] = static_cast<float>(e[LIMA_E_TOTAL] / n);
+            }
+        } else {
+            need(g.dev.traj && g.dev.potE, LIMA_ERR_STATE, "the energy analysis needs traj and potE frames");
+            energy = analyze_energy(c, g);
         }
         dump("energy.bin", energy.data(), energy.size() * sizeof(float));
         dump("temperature.bin", temperature.data(), temperature.size() * sizeof(float));

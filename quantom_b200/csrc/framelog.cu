@@ -16,6 +16,8 @@
 #include "framelog.cuh"
 #include "physkern.cuh"
 #include "physmath.cuh"
+#include "refdev.cuh"
+#include "refmath.cuh"
 
 namespace lima {
 namespace {
@@ -108,6 +110,82 @@ __global__ void __launch_bounds__(kTB) k_log_train(PhysDev d, FrameLogDev g, int
         t[0] = fx;
         t[1] = fy;
         t[2] = fz;
+    }
+}
+
+// ---- reference semantics -----------------------------------------------------
+// The reference's own per-step log, read from the state its step leaves
+// (positions after the integration, compound particles in the image of their
+// particle 0): traj_buffer and potE_buffer of every slot (Engine.cu:1007-1013,
+// 1136-1145; solvents log potE 0, as the reference computes none for them),
+// data_GAN of the compound slots (position, or (-1, -1, -1) past n_particles,
+// and the LJ force from solvents, Engine.cu:1030-1040) and the outdata line of
+// compound 0 particle 0 (speed and kinetic energy over the step, its potE and
+// |force|, Engine.cu:1016-1029).  `after`: the parity holding the positions
+// after the step.
+__global__ void __launch_bounds__(kTB) k_log_ref_frame(RefDev d, FrameLogDev g, int after, int r) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= g.n_slots) return;
+    const bool comp = k < g.n_train;
+    const float4 p = comp ? d.cpos[after][k] : d.spos[after][k - g.n_train];
+    if (g.traj) {
+        float* t = g.traj + ((size_t)r * g.n_slots + k) * 3;
+        t[0] = p.x;
+        t[1] = p.y;
+        t[2] = p.z;
+    }
+    if (g.potE) g.potE[(size_t)r * g.n_slots + k] = comp ? d.potE[k] : 0.0;
+    if (comp && g.train) {
+        const int c = k / LIMA_MAX_COMPOUND_PARTICLES, l = k % LIMA_MAX_COMPOUND_PARTICLES;
+        const bool live = l < d.comps[c].n_particles;
+        const float4 f = d.force_ljsol[k];
+        float* t = g.train + ((size_t)r * g.n_train + k) * (kTrainValues * 3);
+        t[0] = live ? p.x : -1.f;
+        t[1] = live ? p.y : -1.f;
+        t[2] = live ? p.z : -1.f;
+        t[3] = live ? f.x : 0.f;
+        t[4] = live ? f.y : 0.f;
+        t[5] = live ? f.z : 0.f;
+        for (int q = 6; q < kTrainValues * 3; q++) t[q] = 0.f;
+    }
+    if (k == 0 && g.logdata) {
+        float* l = g.logdata + (size_t)r * kLogDataFloats;
+        for (int q = 0; q < kLogDataFloats; q++) l[q] = 0.f;
+        if (g.n_train > 0) {
+            // Engine.cu:1016-1029: speed and kinetic energy from the position
+            // and the previous position (in its image), potE, |force|
+            refm::F3 a = refm::mk4(p), b = refm::mk4(d.cprev[0]);
+            refm::hyperpos(a, b, d.L, d.Lh);
+            const float dist = refm::len(refm::sub(a, b));
+            l[0] = dist / (float)d.dt;
+            const float vel = (float)((double)(dist * 0.5f) / d.dt);
+            l[1] = (float)(0.5 * (double)d.pp[d.comps[0].atom_types[0]].mass * (double)vel * (double)vel);
+            l[2] = (float)d.potE[0];
+            l[3] = refm::len(refm::mk4(d.force_c[0]));
+        }
+    }
+}
+
+// The frame's energies: the reference computes no LJ energy; its bonded
+// potE summed over the compound slots (fixed order, one block), as
+// lima_get_energies reports it, and the last reference-thermostat temperature.
+__global__ void __launch_bounds__(kTB) k_log_ref_energy(RefDev d, FrameLogDev g, int r) {
+    __shared__ double s_sum[kTB];
+    const int ncp = d.n_c * LIMA_MAX_COMPOUND_PARTICLES;
+    double a = 0.0;
+    for (int k = threadIdx.x; k < ncp; k += blockDim.x) a += d.potE[k];
+    s_sum[threadIdx.x] = a;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) s_sum[threadIdx.x] += s_sum[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && g.energies) {
+        double* e = g.energies + (size_t)r * LIMA_E_COUNT;
+        for (int q = 0; q < LIMA_E_COUNT; q++) e[q] = 0.0;
+        e[LIMA_E_BOND] = s_sum[0];
+        e[LIMA_E_TOTAL] = s_sum[0];
+        e[LIMA_E_TEMPERATURE] = *d.ke_accum;
     }
 }
 
@@ -266,8 +344,8 @@ void framelog_free(FrameLog& g) {
     g = FrameLog{};
 }
 
-void framelog_start(FrameLog& g, const PhysDev& d, const std::vector<int>& n_compound_particles,
-                    const lima_log_params& p, std::string& msg, int& status) {
+void framelog_start(FrameLog& g, int n_s, const std::vector<int>& n_compound_particles, const lima_log_params& p,
+                    std::string& msg, int& status) {
     framelog_free(g);
     status = LIMA_OK;
     const int n_c = (int)n_compound_particles.size();
@@ -275,14 +353,16 @@ void framelog_start(FrameLog& g, const PhysDev& d, const std::vector<int>& n_com
     v.flags = p.flags;
     v.ring = p.ring_frames;
     v.n_train = n_c * LIMA_MAX_COMPOUND_PARTICLES;
-    v.n_slots = v.n_train + d.n_s;
-    std::vector<uint32_t> slot(d.n);
+    v.n_slots = v.n_train + n_s;
+    int n = n_s;
+    for (int c = 0; c < n_c; c++) n += n_compound_particles[c];
+    std::vector<uint32_t> slot(std::max(n, 1));
     int o = 0;
     for (int c = 0; c < n_c; c++)
         for (int l = 0; l < n_compound_particles[c]; l++) slot[o++] = (uint32_t)(c * LIMA_MAX_COMPOUND_PARTICLES + l);
-    for (int s = 0; s < d.n_s; s++) slot[o++] = (uint32_t)(v.n_train + s);
+    for (int s = 0; s < n_s; s++) slot[o++] = (uint32_t)(v.n_train + s);
     const size_t f = (size_t)v.ring;
-    uint32_t* ref_slot = grow<uint32_t>(g.dallocs, d.n);
+    uint32_t* ref_slot = grow<uint32_t>(g.dallocs, slot.size());
     v.traj = (p.flags & LIMA_LOG_TRAJ) ? grow<float>(g.dallocs, f * v.n_slots * 3) : nullptr;
     v.potE = (p.flags & LIMA_LOG_POTE) ? grow<double>(g.dallocs, f * v.n_slots) : nullptr;
     v.train = (p.flags & LIMA_LOG_TRAIN) && n_c ? grow<float>(g.dallocs, f * v.n_train * kTrainValues * 3) : nullptr;
@@ -300,7 +380,7 @@ void framelog_start(FrameLog& g, const PhysDev& d, const std::vector<int>& n_com
         return;
     }
     v.ref_slot = ref_slot;
-    cudaMemcpy(ref_slot, slot.data(), sizeof(uint32_t) * d.n, cudaMemcpyHostToDevice);
+    cudaMemcpy(ref_slot, slot.data(), sizeof(uint32_t) * slot.size(), cudaMemcpyHostToDevice);
     if (v.traj) cudaMemset(v.traj, 0, f * v.n_slots * 3 * sizeof(float));
     if (v.potE) cudaMemset(v.potE, 0, f * v.n_slots * sizeof(double));
     if (v.train) {
@@ -335,6 +415,18 @@ int framelog_record(FrameLog& g, const PhysDev& d, int cur, uint64_t step, cudaS
     g.frames_logged++;
     if (g.in_ring == v.ring) drain(g, s);
     return launched;
+}
+
+int framelog_record_ref(FrameLog& g, const RefDev& d, int after, uint64_t step, cudaStream_t s) {
+    const FrameLogDev& v = g.dev;
+    const int r = g.in_ring;
+    k_log_ref_frame<<<(v.n_slots + kTB - 1) / kTB, kTB, 0, s>>>(d, v, after, r);
+    k_log_ref_energy<<<1, kTB, 0, s>>>(d, v, r);
+    g.ring_steps.push_back(step);
+    g.in_ring++;
+    g.frames_logged++;
+    if (g.in_ring == v.ring) drain(g, s);
+    return 2;
 }
 
 void framelog_flush(FrameLog& g, cudaStream_t s) {

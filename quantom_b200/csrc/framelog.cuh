@@ -1,4 +1,4 @@
-// Frame log of the physics path: the reference's on-device logging buffers
+// Frame log: the reference's on-device logging buffers
 // (Box::potE_buffer / traj_buffer / outdata / data_GAN, Engine.cu:1007-1047
 // and :1136-1145), its host offload (Engine::offloadLoggingData /
 // offloadTrainData, Engine.cu:290-310) and the per-step energies of its
@@ -22,6 +22,7 @@
 
 #include "lima_abi.h"
 #include "physdev.cuh"
+#include "refdev.cuh"
 
 namespace lima {
 
@@ -66,12 +67,14 @@ struct FrameLog {
     std::vector<uint64_t> buf_steps[2];
 };
 
-// sets up a ring for the loaded box; n_compound_particles[c] per compound
-void framelog_start(FrameLog& g, const PhysDev& d, const std::vector<int>& n_compound_particles,
-                    const lima_log_params& p, std::string& msg, int& status);
+// sets up a ring for the loaded box: n_s solvents, n_compound_particles[c] per compound
+void framelog_start(FrameLog& g, int n_s, const std::vector<int>& n_compound_particles, const lima_log_params& p,
+                    std::string& msg, int& status);
 void framelog_free(FrameLog& g);
 // after the energy variant of step `step` on parity `cur` (accumulator slot `cur`)
 int framelog_record(FrameLog& g, const PhysDev& d, int cur, uint64_t step, cudaStream_t s);
+// reference semantics: after step `step`, whose positions are in parity `after`
+int framelog_record_ref(FrameLog& g, const RefDev& d, int after, uint64_t step, cudaStream_t s);
 // every frame launched so far into the host store (waits for the stream)
 void framelog_flush(FrameLog& g, cudaStream_t s);
 

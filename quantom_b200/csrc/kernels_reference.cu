@@ -262,6 +262,7 @@ __global__ void __launch_bounds__(64) k_compound(RefDev d, int cur) {
         F3 acc = mk(0.f, 0.f, 0.f);
         for (int k = 0; k < nch; k++) acc = add(acc, mk4(d.cs_partial[((size_t)c * d.n_chunks + k) * kMaxCP + t]));
         force = add(force, acc);
+        d.force_ljsol[c * kMaxCP + t] = to4(acc);
     }
     __syncthreads();
     // integratePosition (Engine.cu:981-984)

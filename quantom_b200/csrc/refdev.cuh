@@ -65,6 +65,7 @@ struct RefDev {
     float4* force_c;         // [n_c*64]
     float4* force_s;         // [n_s]
     double* potE;            // [n_c*64] (solvent entries are always 0 in the reference)
+    float4* force_ljsol;     // [n_c*64] the LJ force from solvents (data_GAN value 1, Engine.cu:1034)
     float* lambda;           // thermostat scalar applied in the next step
     int* err;
     // reference thermostat (Engine::getBoxTemperature) scratch

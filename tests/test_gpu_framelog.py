@@ -1,13 +1,14 @@
-"""Frame log of the physics path (lima_log_*): the reference's logging buffers
+"""Frame log (lima_log_*): the reference's logging buffers
 (traj_buffer, potE_buffer, data_GAN, outdata: Engine.cu:1007-1047,
 1136-1145), their offload and the post-run energy analysis and output files
 (Environment.cpp:124-166, Analyzer.cu:33-207).
 
-Checked against a second engine stepped to the same steps (positions
-bit-identical, FP64 energies to 1e-9 relative), the FP64 oracle (LJ force
-from solvents on compound particles within 5e-5 relative RMS, the stated FP32
-force error), the per-particle energies summing to the FP64 totals, and the
-files read back in the reference's layouts.
+Physics semantics: checked against a second engine stepped to the same steps
+(positions bit-identical, FP64 energies to 1e-9 relative), the FP64 oracle
+(LJ force from solvents on compound particles within 5e-5 relative RMS, the
+stated FP32 force error), the per-particle energies summing to the FP64
+totals, and the files read back in the reference's layouts.  Reference
+semantics: checked frame by frame against the reference's own buffers.
 """
 import numpy as np
 import pytest
@@ -153,11 +154,81 @@ def test_stop_keeps_frames_and_stops_recording(gpu):
         assert eng.lib.lima_log_read(eng.h, 0, 1, None, None, None, buf.ctypes.data, None, None) == E.ERR_ARGUMENT
 
 
-def test_reference_semantics_refuses(gpu):
+def _analyze_energy(s, traj, potE, dt):
+    """Analyzer::analyzeEnergy (Analyzer.cu:33-207) restated over frames of
+    consecutive steps: per frame f (1 .. F-3) the particle's potE plus the
+    kinetic energy of calcKineticEnergy (Engine.cuh:32-45) over frames f-1 and
+    f+1 with the solvent mass, averaged over solvents and over compound
+    particles, the two averages weighed by their counts."""
+    L = s.spec.box_len
+    mass = float(s.forcefield["particle_parameters"][0]["mass"][0])
+    nc, ns = s.n_compounds, s.n_solvents
+    live = np.concatenate([np.arange(c * 64, c * 64 + s.compounds[c]["n_particles"]) for c in range(nc)] +
+                          [nc * 64 + np.arange(ns)]).astype(np.int64)
+    is_sol = live >= nc * 64
+    out = []
+    for f in range(1, len(traj) - 2):
+        a = traj[f + 1][live].astype(np.float64)
+        b = traj[f - 1][live].astype(np.float64)
+        d = a - b
+        d -= L * np.round(d / L)
+        vel = np.linalg.norm(d, axis=1) * 0.5 / dt
+        ke = 0.5 * mass * vel * vel
+        pe = potE[f][live]
+        row = []
+        for q in (pe, ke, pe + ke):
+            avg_s = q[is_sol].mean() if ns else 0.0
+            avg_c = q[~is_sol].mean() if (~is_sol).any() else 0.0
+            row.append((avg_s * ns + avg_c * (~is_sol).sum()) / len(live))
+        out.append(row)
+    return np.array(out)
+
+
+def test_reference_semantics_frames_match_the_reference(gpu, tmp_path):
+    """A reference-semantics run logged every step against the reference's own
+    logging buffers (oracle/_ref: traj_buffer, potE_buffer, outdata, data_GAN
+    of its step code, Engine.cu:1007-1047, 1136-1145) over the same 12 steps;
+    the frame ring (5 frames) wraps twice.  Positions within 1e-5 nm, potE
+    within 1e-6 relative, the solvent LJ force on compound particles within
+    1e-5 relative RMS, the outdata line within 1e-5 relative; energy.bin is
+    the Analyzer's central-difference product of the reference's frames."""
+    if not po.ref_available():
+        pytest.skip("reference build (oracle/_ref) not present")
     E = gpu
-    s = S.make_system("tiny_chains", seed=6)
+    s = S.make_system("tiny_chains", seed=4)
+    n_steps = 12
+    ref = po.RefEngine(s)
+    ref.update_nlists()
+    refl = []
+    for _ in range(n_steps):
+        ref.step(1)
+        refl.append(ref.log())
+    ref.close()
     p = E.default_params(box_len=s.spec.box_len, cutoff=s.spec.cutoff, dt=s.spec.dt)
     with E.Engine(s, p) as eng:
-        with pytest.raises(E.LimaError) as ei:
-            eng.log_start(1)
-        assert ei.value.status == E.ERR_UNSUPPORTED
+        eng.log_start(1, ring_frames=5, flags=E.LOG_TRAJ | E.LOG_POTE | E.LOG_TRAIN)
+        eng.step(n_steps)
+        fr = eng.log_read()
+        eng.log_write(tmp_path)
+    nc, ns = s.n_compounds, s.n_solvents
+    assert fr["steps"].tolist() == list(range(n_steps))
+    live = np.concatenate([np.arange(c * 64, c * 64 + s.compounds[c]["n_particles"]) for c in range(nc)] +
+                          [nc * 64 + np.arange(ns)]).astype(np.int64)
+    comp = live[live < nc * 64]
+    for k in range(n_steps):
+        r = refl[k]
+        assert np.abs(fr["traj"][k][live] - r["traj"][live]).max() < 1e-5, k
+        pe, pe_r = fr["potE"][k][: nc * 64], r["potE"][: nc * 64]
+        assert np.abs(pe - pe_r).max() <= 1e-6 * np.abs(pe_r).max(), k
+        assert not fr["potE"][k][nc * 64:].any()
+        tr, tr_r = fr["train"][k], r["train"]
+        assert np.abs(tr[:, :, 0].reshape(-1, 3)[comp] - tr_r[:, :, 0].reshape(-1, 3)[comp]).max() < 1e-5
+        pad = np.setdiff1d(np.arange(nc * 64), comp)
+        assert (tr[:, :, 0].reshape(-1, 3)[pad] == -1.0).all() and (tr_r[:, :, 0].reshape(-1, 3)[pad] == -1.0).all()
+        assert relrms(tr[:, :, 1].reshape(-1, 3)[comp], tr_r[:, :, 1].reshape(-1, 3)[comp]) < 1e-5
+        np.testing.assert_allclose(fr["logdata"][k][:4], r["logdata"][:4], rtol=1e-5)
+    en = np.fromfile(tmp_path / "energy.bin", np.float32).reshape(-1, 3)
+    want = _analyze_energy(s, np.array([r["traj"] for r in refl]), np.array([r["potE"] for r in refl]), s.spec.dt)
+    assert en.shape == want.shape == (n_steps - 3, 3)
+    np.testing.assert_allclose(en, want, rtol=1e-5)
+    np.testing.assert_array_equal(np.fromfile(tmp_path / "logdata.bin", np.float32).reshape(n_steps, 10), fr["logdata"])
