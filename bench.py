@@ -48,15 +48,22 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-sample-steps", type=int, default=2)
-    ap.add_argument("--mode", default="full", choices=["full", "kernels", "precision", "grad", "large", "6lzm"],
+    ap.add_argument("--mode", default="full",
+                    choices=["full", "kernels", "precision", "grad", "large", "large-fp64", "6lzm"],
                     help="kernels: only warm-up + K plain-FP32 steps (the command profiled with ncu); "
                          "precision: the NVE drift / force-error study of plain FP32 against mixed precision; "
                          "grad: the parameter-gradient study on the 8,192 LJ box; "
                          "large: the 258k solvated-chain box, mixed forward and adjoint gradients; "
+                         "large-fp64: central differences of the FP64 oracle loss at the start state and "
+                         "gradient that --mode large --grad-state saved (host only, no GPU); "
                          "6lzm: the reference's own demo box and settings, next to its published ms/step")
     ap.add_argument("--large-steps", type=int, default=10000, help="--mode large: mixed-precision forward steps")
     ap.add_argument("--nve-steps", type=int, default=50000, help="--mode precision: NVE steps per run")
     ap.add_argument("--eq-steps", type=int, default=5000, help="--mode precision: Berendsen equilibration steps")
+    ap.add_argument("--grad-state", default="",
+                    help="--mode large: save the gradient's start state, target and a 20-step adjoint gradient "
+                         "here (.npz); --mode large-fp64: read it")
+    ap.add_argument("--fd-workers", type=int, default=0, help="--mode large-fp64: host processes (0 = all cores)")
     ap.add_argument("--fp64-fd", action="store_true",
                     help="--mode grad: also central differences of the FP64 oracle loss (minutes of host time)")
     ap.add_argument("--semantics", default="physics", choices=["physics", "reference", "adjoint"],
@@ -648,16 +655,70 @@ def run_large(args):
                 fd.append((lp - lm) / (2 * h))
                 rel.append(abs(g[k] - fd[-1]) / max(abs(fd[-1]), 1e-300))
             fds[step], rels[step] = fd, rel
-        nt = (len(theta) - 3) // 2
-        names = [f"sigma[{t}]" for t in range(nt)] + [f"epsilon[{t}]" for t in range(nt)] + ["bond_k", "angle_k",
-                                                                                              "dihedral_k"]
+        names = eng.param_names()
         out["grad"] = {"n_steps": T, "checkpoint_every": C, "n_bins": nb, "w_energy": w_e, "w_rdf": w_r,
                        "target": "RDF-bin occupancy of the same box run with solvent sigma + 2 %",
                        "loss": L, "ms_forward_loss": t_loss, "ms_grad": t_grad, "grad_over_forward": t_grad / t_loss,
                        "params": names, "theta": theta.tolist(), "grad": g.tolist(),
                        "fd_fp32_gpu_h1e-3": fds[1e-3], "rel_err_vs_fd_h1e-3": rels[1e-3],
                        "fd_fp32_gpu_h1e-2": fds[1e-2], "rel_err_vs_fd_h1e-2": rels[1e-2]}
+        if args.grad_state:
+            # the FP64 pin: a 20-step unroll from the same state, gradient kept with the state
+            # for --mode large-fp64 (the oracle's loss costs ~20 s of host time per step here)
+            T64 = 20
+            L64, g64 = eng.grad(T64, C, nb, rmax, w_e, w_r, target)
+            np.savez(args.grad_state, forcefield=start.forcefield, compounds=start.compounds, states=start.states,
+                     solvents=start.solvents, bridges=start.bridges, target=target, theta=theta, grad=g64,
+                     loss=L64, names=np.array(names), n_steps=T64, checkpoint_every=C, n_bins=nb, r_max=rmax,
+                     w_energy=w_e, w_rdf=w_r, dt=spec.dt, cutoff=spec.cutoff, seed=args.seed)
+            out["grad"]["saved_for_fp64_check"] = {"path": args.grad_state, "n_steps": T64, "loss": L64}
     print(json.dumps(out), flush=True)
+
+
+def _fd64_one(job):
+    """One central difference of the FP64 oracle loss (a spawn-pool task)."""
+    from oracle import pyoracle as po
+    system, k, h, a = job
+    ps = po.PhysSystem(system, rc=a["cutoff"], r_on=1.0)
+    th = ps.params()
+    e = np.zeros(len(th))
+    e[k] = h
+    lp, _ = ps.with_params(th + e).loss(a["dt"], a["n_steps"], a["n_bins"], a["r_max"], a["w_energy"], a["w_rdf"],
+                                        a["target"])
+    lm, _ = ps.with_params(th - e).loss(a["dt"], a["n_steps"], a["n_bins"], a["r_max"], a["w_energy"], a["w_rdf"],
+                                        a["target"])
+    return (lp - lm) / (2 * h)
+
+
+def run_large_fp64(args):
+    """The 258k box's adjoint gradient (saved by --mode large --grad-state)
+    against central differences of the FP64 oracle loss (oracle/lima_oracle.c
+    orc_phys_loss) over the same unroll, every entry of theta, step 1e-4
+    relative (1e-4 rad for a zero phase); host processes only."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    from oracle import pyoracle as po
+    from quantom_b200 import systems as S
+    z = np.load(args.grad_state)
+    spec = S.CONFIGS[LARGE_WORKLOAD]
+    system = S.System(spec, int(z["seed"]), z["forcefield"], z["compounds"], z["states"], z["solvents"],
+                      z["bridges"])
+    a = {k: (z[k] if k == "target" else float(z[k])) for k in
+         ("target", "dt", "cutoff", "r_max", "w_energy", "w_rdf")}
+    a.update({k: int(z[k]) for k in ("n_steps", "n_bins")})
+    theta, g, names = z["theta"], z["grad"], [str(x) for x in z["names"]]
+    th64 = po.PhysSystem(system, rc=a["cutoff"], r_on=1.0).params()
+    steps = [1e-4 * abs(v) if v != 0.0 else 1e-4 for v in th64]
+    workers = args.fd_workers or os.cpu_count() or 1
+    t0 = time.perf_counter()
+    with ProcessPoolExecutor(workers, mp_context=mp.get_context("spawn")) as ex:
+        fd = np.array(list(ex.map(_fd64_one, [(system, k, steps[k], a) for k in range(len(th64))])))
+    rel = np.abs(g - fd) / np.maximum(np.abs(fd), 1e-300)
+    print(json.dumps({"mode": "large-fp64", "workload": LARGE_WORKLOAD, "n_steps": a["n_steps"],
+                      "theta_matches_oracle": bool(np.allclose(theta, th64, rtol=1e-6)), "params": names,
+                      "grad_adjoint_fp32": g.tolist(), "fd_fp64_oracle": fd.tolist(), "rel_err": rel.tolist(),
+                      "max_rel_err": float(rel.max()), "host_workers": workers,
+                      "host_s": time.perf_counter() - t0}), flush=True)
 
 
 # ------------------------------------------------------- the reference's demo --
@@ -1004,6 +1065,9 @@ def main():
         return
     if args.mode == "large":
         run_large(args)
+        return
+    if args.mode == "large-fp64":
+        run_large_fp64(args)
         return
     if args.mode == "6lzm":
         run_6lzm(args)

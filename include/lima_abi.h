@@ -291,12 +291,25 @@ lima_status lima_get_kernel_launches(lima_ctx* ctx, uint64_t* count);
 /* ------------------------------------------------------------------ */
 #define LIMA_LOSS_MAX_BINS 128
 
-/* Parameter vector theta, n = 2 * n_types + 3 entries:
-   [sigma_0 .. sigma_{n_types-1}, epsilon_0 .. epsilon_{n_types-1}, s_bond, s_angle, s_dihedral];
+/* Parameter vector theta, n = 2 * n_types + 3 + 2 * (n_bond_types + n_angle_types +
+   n_dihedral_types) entries:
+     [sigma_0 .. sigma_{n_types-1}, epsilon_0 .. epsilon_{n_types-1},
+      s_bond, s_angle, s_dihedral,
+      (r0, k) of every bond type, (theta0, k) of every angle type, (phi0, k) of every dihedral type]
    n_types = 1 + the largest atom type in the box, sigma in nm and epsilon in J/mol
-   (Lorentz-Berthelot mixing per pair), s_* scale every bond, angle and dihedral force
-   constant as loaded (1 = as loaded). */
+   (Lorentz-Berthelot mixing per pair).  A bonded term type is one distinct constant set
+   among the loaded terms of a kind (PairBond {b0, kb}, AngleBond {theta_0, k_theta},
+   DihedralBond {phi_0, k_phi, n}: Bodies.cuh:61-113), the types in ascending order of
+   (r0, k), (theta0, k), (phi0, k, n); every term of a type takes its r0 / theta0 / phi0,
+   and s_kind times its k as force constant (s_* = 1 as loaded).  The dihedral
+   multiplicity n is an integer and not a parameter. */
 lima_status lima_get_param_count(lima_ctx* ctx, int* n);
+/* counts[4] = {n_types, n_bond_types, n_angle_types, n_dihedral_types}. */
+lima_status lima_get_param_layout(lima_ctx* ctx, int* counts);
+/* The number of terms of a kind (0 bond, 1 angle, 2 dihedral) and, when type_of is not
+   NULL, the type of each, in load order: each compound's terms compound by compound,
+   then each bridge's terms. */
+lima_status lima_get_bonded_types(lima_ctx* ctx, int kind, int* n_terms, int* type_of);
 lima_status lima_get_params(lima_ctx* ctx, double* theta);
 lima_status lima_set_params(lima_ctx* ctx, const double* theta);
 

@@ -413,23 +413,54 @@ class PhysSystem:
         return F, en
 
     # -- trajectory loss (the quantity lima_loss / lima_grad evaluate) ---------
+    def term_types(self):
+        """Bonded term types as lima_get_params orders them: per kind the
+        distinct constant sets of the terms, (r0, k), (theta0, k), (phi0, k, n),
+        in ascending order; returns [(type constants (n_types, 2|3), type of
+        every term)] for bonds, angles, dihedrals."""
+        out = []
+        for keys, n in (((self.bond_r0, self.bond_k), self.n_bonds), ((self.angle_t0, self.angle_k), self.n_angles),
+                        ((self.dih_phi0, self.dih_k, self.dih_n.astype(np.float64)), self.n_dih)):
+            k = np.stack(keys, 1)[:n]
+            if n == 0:
+                out.append((np.zeros((0, k.shape[1])), np.zeros(0, np.int64)))
+                continue
+            u, inv = np.unique(k, axis=0, return_inverse=True)
+            out.append((u, inv.reshape(-1)))
+        return out
+
     def params(self):
         """theta in lima_get_params order: per-type sigma, per-type epsilon,
-        bond / angle / dihedral scales (1 = as built)."""
-        return np.concatenate([self.type_sigma, self.type_epsilon, [1.0, 1.0, 1.0]])
+        bond / angle / dihedral scales (1 = as built), then (r0, k) per bond
+        type, (theta0, k) per angle type, (phi0, k) per dihedral type."""
+        tt = [u[:, :2].reshape(-1) for u, _ in self.term_types()]
+        return np.concatenate([self.type_sigma, self.type_epsilon, [1.0, 1.0, 1.0], *tt])
 
     def with_params(self, theta):
-        """A copy whose per-type LJ parameters and bonded constants follow theta."""
+        """A copy whose per-type LJ parameters and bonded constants follow
+        theta: every term takes its type's r0 / theta0 / phi0 and the kind's
+        scale times its type's k."""
         import copy
+        theta = np.asarray(theta, np.float64)
         nt = self.n_types
         q = copy.copy(self)
-        q.type_sigma = np.asarray(theta[:nt], np.float64).copy()
-        q.type_epsilon = np.asarray(theta[nt:2 * nt], np.float64).copy()
+        q.type_sigma = theta[:nt].copy()
+        q.type_epsilon = theta[nt:2 * nt].copy()
         q.sigma = q.type_sigma[self.types]
         q.epsilon = q.type_epsilon[self.types]
-        q.bond_k = self.bond_k * theta[2 * nt]
-        q.angle_k = self.angle_k * theta[2 * nt + 1]
-        q.dih_k = self.dih_k * theta[2 * nt + 2]
+        o = 2 * nt + 3
+        for kind, ((u, inv), (c_name, k_name), n) in enumerate(zip(
+                self.term_types(), (("bond_r0", "bond_k"), ("angle_t0", "angle_k"), ("dih_phi0", "dih_k")),
+                (self.n_bonds, self.n_angles, self.n_dih))):
+            tv = theta[o:o + 2 * len(u)].reshape(-1, 2)
+            o += 2 * len(u)
+            c = getattr(self, c_name).copy()
+            k = getattr(self, k_name).copy()
+            if n:
+                c[:n] = tv[inv, 0]
+                k[:n] = tv[inv, 1] * theta[2 * nt + kind]
+            setattr(q, c_name, c)
+            setattr(q, k_name, k)
         return q
 
     def rdf(self, n_bins, r_max, x=None):

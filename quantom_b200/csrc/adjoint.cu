@@ -97,6 +97,7 @@ struct AdjArgs {
     float4* adj_term;
     const float* par;  // sigma[n_types], epsilon[n_types], scales
     double* gtheta;
+    double2* gterm;    // per bonded term: dL/dc, dL/dk (c = r0 | theta0 | phi0)
 };
 
 // --------------------------------------------------------------- loss pass --
@@ -201,6 +202,13 @@ __device__ __forceinline__ D3 sep(const PhysDev& d, float4 a, float4 wa, float4 
 __device__ __forceinline__ Dual cst(float v) { return {v, 0.f}; }
 
 // MODE 0: bonded energy of the state into *U_out.  MODE 1: adjoint contributions.
+// Every term's forces are F_q = g G_q: a scalar g that carries the constants
+// (bond: -k (r - r0); angle: k (theta - theta0); dihedral: dV/dphi =
+// -k n sin(n phi - phi0)) times directions G_q that depend on the positions
+// only.  The constants' derivatives of the loss at this state are then
+//   dL/dc = dt (dg/dc) sum_q w_q . G_q + le dE/dc     (c = r0 | theta0 | phi0, k)
+// and go to the term's own FP64 accumulator (one thread per term: no atomics,
+// the same order every run).
 template <int MODE>
 __global__ void __launch_bounds__(kAdjTB) k_adj_bonded(PhysDev d, const float4* __restrict__ po, AdjArgs a,
                                                        int hvp, double* U_out) {
@@ -208,24 +216,28 @@ __global__ void __launch_bounds__(kAdjTB) k_adj_bonded(PhysDev d, const float4* 
     const int nb = d.n_bonds, na = d.n_angles, nd = d.n_dih;
     const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
     auto W = [&](int orig) { return (MODE == 1 && hvp) ? a.wv[d.sorted_of_orig[orig]] : zero; };
-    int kind = -1, n_at = 0, slot0 = 0;
+    int n_at = 0, slot0 = 0;
+    bool live = false;
     int at[4] = {0, 0, 0, 0};
-    D3 F[4];
-    Dual E = cst(0.f);
+    D3 G[4];
+    Dual g = cst(0.f), E = cst(0.f);
+    float dg_dc = 0.f, dg_dk = 0.f, dE_dc = 0.f, dE_dk = 0.f;
     if (t < nb) {
-        kind = kParBond;
+        live = true;
         const int4 ix = d.bond_idx[t];
         const float2 par = d.bond_par[t];
         at[0] = ix.x, at[1] = ix.y, n_at = 2, slot0 = 2 * t;
         const D3 r = sep(d, po[ix.x], W(ix.x), po[ix.y], W(ix.y));
         const Dual rr = dsqrt(dot(r, r));
         const Dual dr = rr - cst(par.x);
-        const Dual f = (-par.y) * (dr / rr);   // F_j = f r
-        F[0] = -(f * r);
-        F[1] = f * r;
+        G[1] = (cst(1.f) / rr) * r;   // F_j = -k (r - r0) r / |r|
+        G[0] = -G[1];
+        g = (-par.y) * dr;
         E = (0.5f * par.y) * (dr * dr);
+        dg_dc = par.y, dg_dk = -dr.v;
+        dE_dc = -par.y * dr.v, dE_dk = 0.5f * dr.v * dr.v;
     } else if (t < nb + na) {
-        kind = kParAngle;
+        live = true;
         const int q = t - nb;
         const int4 ix = d.angle_idx[q];
         const float2 par = d.angle_par[q];
@@ -241,14 +253,16 @@ __global__ void __launch_bounds__(kAdjTB) k_adj_bonded(PhysDev d, const float4* 
         const Dual dth = th - cst(par.x);
         const Dual inuv = cst(1.f) / (nu * nv);
         const Dual cosv = cs * inuv;
-        const Dual s = dmaxf(sn * inuv, 1e-6f);
-        const Dual gk = (par.y * dth) / s;
-        F[0] = gk * (inuv * v - (cosv / uu) * u);
-        F[2] = gk * (inuv * u - (cosv / vv) * v);
-        F[1] = -(F[0] + F[2]);
+        const Dual is = cst(1.f) / dmaxf(sn * inuv, 1e-6f);
+        G[0] = is * (inuv * v - (cosv / uu) * u);
+        G[2] = is * (inuv * u - (cosv / vv) * v);
+        G[1] = -(G[0] + G[2]);
+        g = par.y * dth;
         E = (0.5f * par.y) * (dth * dth);
+        dg_dc = -par.y, dg_dk = dth.v;
+        dE_dc = -par.y * dth.v, dE_dk = 0.5f * dth.v * dth.v;
     } else if (t < nb + na + nd) {
-        kind = kParDihedral;
+        live = true;
         const int q = t - nb - na;
         const int4 ix = d.dih_idx[q];
         const float4 par = d.dih_par[q];
@@ -261,53 +275,51 @@ __global__ void __launch_bounds__(kAdjTB) k_adj_bonded(PhysDev d, const float4* 
         const Dual nb2 = dsqrt(b2b2);
         const Dual phi = datan2(nb2 * dot(b1, m2), dot(m1, m2));
         const Dual arg = par.z * phi - cst(par.x);
-        const Dual dVdphi = (-par.y * par.z) * dsin(arg);
-        const Dual gi = dVdphi * nb2 / m1m1, gl = -(dVdphi * nb2 / m2m2);
-        const D3 fi = gi * m1, fl = gl * m2;
+        const Dual sa = dsin(arg);
+        const D3 hi = (nb2 / m1m1) * m1, hl = -((nb2 / m2m2) * m2);
         const Dual p = dot(b1, b2) / b2b2, r = dot(b3, b2) / b2b2;
-        F[0] = fi;
-        F[1] = -fi - p * fi + r * fl;
-        F[2] = -fl + p * fi - r * fl;
-        F[3] = fl;
+        G[0] = hi;
+        G[1] = -hi - p * hi + r * hl;
+        G[2] = -hl + p * hi - r * hl;
+        G[3] = hl;
+        g = (-par.y * par.z) * sa;
         E = par.y * (cst(1.f) + dcos(arg));
+        const float ca = cosf(arg.v);
+        dg_dc = par.y * par.z * ca, dg_dk = -par.z * sa.v;
+        dE_dc = par.y * sa.v, dE_dk = 1.f + ca;
     }
     // reductions
-    double eu = 0.0, g[kParKinds] = {0.0, 0.0, 0.0};
-    if (kind >= 0) {
+    double eu = 0.0;
+    if (live) {
         if (MODE == 0) {
             eu = (double)E.v;
         } else {
-            const float scale = a.par[2 * a.n_types + kind];
-            const float inv_s = scale != 0.f ? 1.f / scale : 0.f;
-            float gd = 0.f;
+            float sg = 0.f;   // sum_q w_q . G_q
             for (int q = 0; q < n_at; q++) {
                 const float4 wq = W(at[q]);
-                const D3& f = F[q];
-                if (hvp) gd += wq.x * f.x.v + wq.y * f.y.v + wq.z * f.z.v;
+                const D3 f = g * G[q];
+                if (hvp) sg += wq.x * G[q].x.v + wq.y * G[q].y.v + wq.z * G[q].z.v;
                 const float4 o = make_float4((hvp ? a.dt * f.x.t : 0.f) - a.le * f.x.v,
                                              (hvp ? a.dt * f.y.t : 0.f) - a.le * f.y.v,
                                              (hvp ? a.dt * f.z.t : 0.f) - a.le * f.z.v, 0.f);
                 a.adj_term[slot0 + q] = o;
             }
-            g[kind] = (double)((a.dt * gd + a.le * E.v) * inv_s);   // F and E are linear in the scale
+            double2 acc = a.gterm[t];
+            acc.x += (double)(a.dt * dg_dc * sg + a.le * dE_dc);
+            acc.y += (double)(a.dt * dg_dk * sg + a.le * dE_dk);
+            a.gterm[t] = acc;
         }
     }
-    __shared__ double s_b[kAdjTB / 32][kParKinds + 1];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const double v0 = warp_sum_d(eu), v1 = warp_sum_d(g[0]), v2 = warp_sum_d(g[1]), v3 = warp_sum_d(g[2]);
-    if (lane == 0) {
-        s_b[w][0] = v0, s_b[w][1] = v1, s_b[w][2] = v2, s_b[w][3] = v3;
-    }
-    __syncthreads();
-    if (threadIdx.x <= kParKinds) {
-        double v = 0.0;
-        for (int q = 0; q < (int)(blockDim.x >> 5); q++) v += s_b[q][threadIdx.x];
-        if (v != 0.0) {
-            if (threadIdx.x == 0) {
-                if (MODE == 0) atomicAdd(U_out, v);
-            } else if (MODE == 1) {
-                atomicAdd(&a.gtheta[2 * a.n_types + threadIdx.x - 1], v);
-            }
+    if (MODE == 0) {
+        __shared__ double s_b[kAdjTB / 32];
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        const double v0 = warp_sum_d(eu);
+        if (lane == 0) s_b[w] = v0;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double v = 0.0;
+            for (int q = 0; q < (int)(blockDim.x >> 5); q++) v += s_b[q];
+            if (v != 0.0) atomicAdd(U_out, v);
         }
     }
 }
@@ -508,7 +520,10 @@ bool ensure(const PhysDev& d, AdjBuffers& A, std::vector<void*>& allocs, int n_c
         A.adj_term = grow<float4>(allocs, (size_t)std::max(d.n_term_slots, 1));
         A.gtheta = grow<double>(allocs, 2 * kMaxTypes + kParKinds);
         A.par = grow<float>(allocs, 2 * kMaxTypes + kParKinds);
-        if (!A.lam_x || !A.lam_v || !A.wv || !A.lam_xo || !A.lam_vo || !A.adj_term || !A.gtheta || !A.par)
+        A.cap_terms = std::max(d.n_bonds + d.n_angles + d.n_dih, 1);
+        A.gterm = grow<double2>(allocs, (size_t)A.cap_terms);
+        if (!A.lam_x || !A.lam_v || !A.wv || !A.lam_xo || !A.lam_vo || !A.adj_term || !A.gtheta || !A.par ||
+            !A.gterm)
             return false;
     }
     if (n_ckpt > A.cap_ckpt) {
@@ -545,6 +560,26 @@ int read_err(const PhysDev& d, cudaStream_t s) {
 }  // namespace
 
 // ------------------------------------------------------------- parameters --
+namespace {
+// Groups the loaded terms of one kind into types: the distinct constant sets
+// (c, k, n) in ascending order; type_of[t] is term t's type.
+void group_terms(const std::vector<float4>& terms, std::vector<int>& type_of, std::vector<float4>& type0) {
+    auto less = [](const float4& a, const float4& b) {
+        if (a.x != b.x) return a.x < b.x;
+        if (a.y != b.y) return a.y < b.y;
+        return a.z < b.z;
+    };
+    type0 = terms;
+    std::sort(type0.begin(), type0.end(), less);
+    type0.erase(std::unique(type0.begin(), type0.end(),
+                            [](const float4& a, const float4& b) { return a.x == b.x && a.y == b.y && a.z == b.z; }),
+                type0.end());
+    type_of.resize(terms.size());
+    for (size_t t = 0; t < terms.size(); t++)
+        type_of[t] = (int)(std::lower_bound(type0.begin(), type0.end(), terms[t], less) - type0.begin());
+}
+}  // namespace
+
 void phys_params_init(const PhysDev& d, const lima_forcefield& ff, PhysParams& pp, cudaStream_t s) {
     pp.n_types = d.n_types;
     pp.sigma.resize(d.n_types);
@@ -562,6 +597,19 @@ void phys_params_init(const PhysDev& d, const lima_forcefield& ff, PhysParams& p
         cudaMemcpyAsync(pp.angle0.data(), d.angle_par, sizeof(float2) * d.n_angles, cudaMemcpyDeviceToHost, s);
     if (d.n_dih) cudaMemcpyAsync(pp.dih0.data(), d.dih_par, sizeof(float4) * d.n_dih, cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
+    std::vector<float4> terms[kParKinds];
+    for (const float2& b : pp.bond0) terms[kParBond].push_back(make_float4(b.x, b.y, 0.f, 0.f));
+    for (const float2& a : pp.angle0) terms[kParAngle].push_back(make_float4(a.x, a.y, 0.f, 0.f));
+    for (const float4& q : pp.dih0) terms[kParDihedral].push_back(make_float4(q.x, q.y, q.z, 0.f));
+    for (int k = 0; k < kParKinds; k++) {
+        group_terms(terms[k], pp.type_of[k], pp.type0[k]);
+        pp.tc[k].resize(pp.type0[k].size());
+        pp.tk[k].resize(pp.type0[k].size());
+        for (size_t q = 0; q < pp.type0[k].size(); q++) {
+            pp.tc[k][q] = pp.type0[k][q].x;
+            pp.tk[k][q] = pp.type0[k][q].y;
+        }
+    }
 }
 
 void phys_params_get(const PhysParams& pp, double* theta) {
@@ -571,6 +619,12 @@ void phys_params_get(const PhysParams& pp, double* theta) {
         theta[nt + t] = pp.epsilon[t];
     }
     for (int k = 0; k < kParKinds; k++) theta[2 * nt + k] = pp.scale[k];
+    double* o = theta + 2 * nt + kParKinds;
+    for (int k = 0; k < kParKinds; k++)
+        for (size_t q = 0; q < pp.tc[k].size(); q++) {
+            *o++ = pp.tc[k][q];
+            *o++ = pp.tk[k][q];
+        }
 }
 
 int phys_params_set(PhysDev& d, PhysParams& pp, const double* theta, std::string& msg, cudaStream_t s) {
@@ -585,11 +639,24 @@ int phys_params_set(PhysDev& d, PhysParams& pp, const double* theta, std::string
             msg = "bonded scales must be finite and non-negative";
             return LIMA_ERR_ARGUMENT;
         }
+    const double* tt = theta + 2 * nt + kParKinds;
+    for (int k = 0, o = 0; k < kParKinds; k++)
+        for (size_t q = 0; q < pp.tc[k].size(); q++, o += 2)
+            if (!std::isfinite(tt[o]) || !std::isfinite(tt[o + 1]) || !(tt[o + 1] >= 0.0) ||
+                (k == kParBond && !(tt[o] > 0.0))) {
+                msg = "bonded type constants must be finite, force constants non-negative and bond lengths positive";
+                return LIMA_ERR_ARGUMENT;
+            }
     for (int t = 0; t < nt; t++) {
         pp.sigma[t] = theta[t];
         pp.epsilon[t] = theta[nt + t];
     }
     for (int k = 0; k < kParKinds; k++) pp.scale[k] = theta[2 * nt + k];
+    for (int k = 0, o = 0; k < kParKinds; k++)
+        for (size_t q = 0; q < pp.tc[k].size(); q++, o += 2) {
+            pp.tc[k][q] = tt[o];
+            pp.tk[k][q] = tt[o + 1];
+        }
     std::vector<float2> tab((size_t)nt * nt);
     for (int a = 0; a < nt; a++)
         for (int b = 0; b < nt; b++) {
@@ -597,11 +664,22 @@ int phys_params_set(PhysDev& d, PhysParams& pp, const double* theta, std::string
             const double ep = std::sqrt(pp.epsilon[a] * pp.epsilon[b]);
             tab[a * nt + b] = make_float2((float)(sg * sg), (float)(4.0 * ep));
         }
+    // every term takes its type's constants; the force constant times the kind's scale
     std::vector<float2> bp(pp.bond0), ap(pp.angle0);
     std::vector<float4> dp(pp.dih0);
-    for (auto& b : bp) b.y = (float)(b.y * pp.scale[kParBond]);
-    for (auto& q : ap) q.y = (float)(q.y * pp.scale[kParAngle]);
-    for (auto& q : dp) q.y = (float)(q.y * pp.scale[kParDihedral]);
+    for (size_t t = 0; t < bp.size(); t++) {
+        const int q = pp.type_of[kParBond][t];
+        bp[t] = make_float2((float)pp.tc[kParBond][q], (float)(pp.tk[kParBond][q] * pp.scale[kParBond]));
+    }
+    for (size_t t = 0; t < ap.size(); t++) {
+        const int q = pp.type_of[kParAngle][t];
+        ap[t] = make_float2((float)pp.tc[kParAngle][q], (float)(pp.tk[kParAngle][q] * pp.scale[kParAngle]));
+    }
+    for (size_t t = 0; t < dp.size(); t++) {
+        const int q = pp.type_of[kParDihedral][t];
+        dp[t].x = (float)pp.tc[kParDihedral][q];
+        dp[t].y = (float)(pp.tk[kParDihedral][q] * pp.scale[kParDihedral]);
+    }
     cudaMemcpyAsync(d.lj_table, tab.data(), sizeof(float2) * tab.size(), cudaMemcpyHostToDevice, s);
     if (!bp.empty()) cudaMemcpyAsync(d.bond_par, bp.data(), sizeof(float2) * bp.size(), cudaMemcpyHostToDevice, s);
     if (!ap.empty()) cudaMemcpyAsync(d.angle_par, ap.data(), sizeof(float2) * ap.size(), cudaMemcpyHostToDevice, s);
@@ -712,6 +790,7 @@ int adj_run(const PhysDev& d0, int cur, const PhysParams& pp, AdjBuffers& A, std
     cudaMemsetAsync(A.U, 0, sizeof(double) * (T + 1), s);
     cudaMemsetAsync(A.hist, 0, sizeof(double) * (size_t)(T + 1) * nb, s);
     cudaMemsetAsync(A.gtheta, 0, sizeof(double) * (2 * kMaxTypes + kParKinds), s);
+    cudaMemsetAsync(A.gterm, 0, sizeof(double2) * A.cap_terms, s);
     const int nt = pp.n_types;
     std::vector<float> par(2 * nt + kParKinds);
     for (int t = 0; t < nt; t++) {
@@ -775,6 +854,7 @@ int adj_run(const PhysDev& d0, int cur, const PhysParams& pp, AdjBuffers& A, std
         a.adj_term = A.adj_term;
         a.par = A.par;
         a.gtheta = A.gtheta;
+        a.gterm = A.gterm;
         const int pb = R.blocks_pair(), tbk = R.blocks_terms();
         for (int k = K - 1; k >= 0; k--) {
             const int n0 = k * C, len = std::min(C, T - n0);
@@ -831,8 +911,13 @@ int adj_run(const PhysDev& d0, int cur, const PhysParams& pp, AdjBuffers& A, std
     std::vector<double> U(T + 1), H((size_t)(T + 1) * nb);
     cudaMemcpyAsync(U.data(), A.U, sizeof(double) * (T + 1), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(H.data(), A.hist, sizeof(double) * H.size(), cudaMemcpyDeviceToHost, s);
-    std::vector<double> g(2 * nt + kParKinds, 0.0);
-    if (grad) cudaMemcpyAsync(g.data(), A.gtheta, sizeof(double) * g.size(), cudaMemcpyDeviceToHost, s);
+    std::vector<double> g(2 * nt, 0.0);
+    const int n_terms = d.n_bonds + d.n_angles + d.n_dih;
+    std::vector<double2> gt((size_t)n_terms);
+    if (grad) {
+        cudaMemcpyAsync(g.data(), A.gtheta, sizeof(double) * g.size(), cudaMemcpyDeviceToHost, s);
+        if (n_terms) cudaMemcpyAsync(gt.data(), A.gterm, sizeof(double2) * n_terms, cudaMemcpyDeviceToHost, s);
+    }
     const int err = read_err(d, s);
     // leave the state as found: restore the first checkpoint into the starting parity
     if (cur != start_cur) cur = start_cur;
@@ -854,8 +939,24 @@ int adj_run(const PhysDev& d0, int cur, const PhysParams& pp, AdjBuffers& A, std
         return LIMA_ERR_NUMERIC;
     }
     *loss = loss_of(U, H, target, T, nb, d.n, we, wr);
-    if (grad)
+    if (grad) {
         for (size_t q = 0; q < g.size(); q++) grad[q] = g[q];
+        // bonded constants: the terms' derivatives summed per type in term
+        // order; a term's force constant is s_kind * k_type
+        double* gs = grad + 2 * nt;
+        double* gty = gs + kParKinds;
+        for (int q = 0; q < kParKinds + 2 * pp.n_term_types(); q++) gs[q] = 0.0;
+        const int base[kParKinds] = {0, d.n_bonds, d.n_bonds + d.n_angles};
+        const int cnt[kParKinds] = {d.n_bonds, d.n_angles, d.n_dih};
+        for (int k = 0, off = 0; k < kParKinds; off += 2 * (int)pp.tc[k].size(), k++)
+            for (int t = 0; t < cnt[k]; t++) {
+                const double2 v = gt[base[k] + t];
+                const int q = pp.type_of[k][t];
+                gs[k] += v.y * pp.tk[k][q];
+                gty[off + 2 * q] += v.x;
+                gty[off + 2 * q + 1] += v.y * pp.scale[k];
+            }
+    }
     return LIMA_OK;
 }
 

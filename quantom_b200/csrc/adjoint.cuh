@@ -26,12 +26,25 @@ namespace lima {
 enum { kParBond = 0, kParAngle = 1, kParDihedral = 2, kParKinds = 3 };
 
 // Host copy of the differentiable parameters and of the bonded constants as loaded.
+// A bonded term type is one distinct constant set among the loaded terms of a
+// kind: (r0, k) of a bond, (theta0, k) of an angle, (phi0, k, n) of a
+// dihedral, in ascending order of that tuple.  The reference's force field
+// gives every term of one atom-type combination the same constants
+// (Bodies.cuh:61-113, filled per type by its force-field maker), so the
+// distinct sets are its bond / angle / dihedral types.
 struct PhysParams {
     int n_types = 0;
     std::vector<double> sigma, epsilon;      // per type
     double scale[kParKinds] = {1.0, 1.0, 1.0};
     std::vector<float2> bond0, angle0;       // (r0, k), (theta0, k) as loaded
     std::vector<float4> dih0;                // (phi0, k, n, 0) as loaded
+    std::vector<int> type_of[kParKinds];     // term -> its type, per kind
+    std::vector<float4> type0[kParKinds];    // the type's constants as loaded (c, k, n, 0)
+    std::vector<double> tc[kParKinds], tk[kParKinds];   // current c (r0 / theta0 / phi0) and k per type
+    int n_term_types() const {
+        return (int)(type0[kParBond].size() + type0[kParAngle].size() + type0[kParDihedral].size());
+    }
+    int count() const { return 2 * n_types + kParKinds + 2 * n_term_types(); }
 };
 
 // Device buffers of the loss / adjoint passes (grown on demand).
@@ -52,10 +65,16 @@ struct AdjBuffers {
     double* target = nullptr; // [cap_bins]
     double* gtheta = nullptr; // [2 * kMaxTypes + kParKinds]
     float* par = nullptr;     // [2 * kMaxTypes + kParKinds] current theta (float)
+    double2* gterm = nullptr; // [cap_terms] per bonded term: dL/d(r0 | theta0 | phi0), dL/dk of the term
+    int cap_terms = 0;
 };
 
 void phys_params_init(const PhysDev& d, const lima_forcefield& ff, PhysParams& pp, cudaStream_t s);
-// uploads theta into the LJ table and the bonded constants; returns a lima_status
+// theta layout (PhysParams::count() entries): sigma[n_types], epsilon[n_types],
+// s_bond, s_angle, s_dihedral, then (r0, k) per bond type, (theta0, k) per
+// angle type, (phi0, k) per dihedral type; a term's force constant is
+// s_kind * k of its type.  phys_params_set uploads theta into the LJ table and
+// the bonded constants and returns a lima_status.
 int phys_params_set(PhysDev& d, PhysParams& pp, const double* theta, std::string& msg, cudaStream_t s);
 void phys_params_get(const PhysParams& pp, double* theta);
 

@@ -1029,7 +1029,27 @@ lima_status lima_get_param_count(lima_ctx* c, int* n) {
     return guarded(c, [&] {
         need(n != nullptr, LIMA_ERR_ARGUMENT, "null count");
         need_physics(c);
-        *n = 2 * c->params.n_types + lima::kParKinds;
+        *n = c->params.count();
+    });
+}
+
+lima_status lima_get_param_layout(lima_ctx* c, int* counts) {
+    return guarded(c, [&] {
+        need(counts != nullptr, LIMA_ERR_ARGUMENT, "null counts");
+        need_physics(c);
+        counts[0] = c->params.n_types;
+        for (int k = 0; k < lima::kParKinds; k++) counts[1 + k] = static_cast<int>(c->params.tc[k].size());
+    });
+}
+
+lima_status lima_get_bonded_types(lima_ctx* c, int kind, int* n_terms, int* type_of) {
+    return guarded(c, [&] {
+        need(kind >= 0 && kind < lima::kParKinds, LIMA_ERR_ARGUMENT, "kind must be 0 (bond), 1 (angle) or 2 (dihedral)");
+        need(n_terms != nullptr, LIMA_ERR_ARGUMENT, "null count");
+        need_physics(c);
+        const auto& v = c->params.type_of[kind];
+        *n_terms = static_cast<int>(v.size());
+        if (type_of) std::copy(v.begin(), v.end(), type_of);
     });
 }
 

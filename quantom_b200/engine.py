@@ -101,6 +101,8 @@ def load_library():
         "lima_profile_steps": (i, [vp, i, vp]),
         "lima_get_rebuild_count": (i, [vp, ctypes.POINTER(ctypes.c_uint64)]),
         "lima_get_param_count": (i, [vp, ctypes.POINTER(i)]),
+        "lima_get_param_layout": (i, [vp, vp]),
+        "lima_get_bonded_types": (i, [vp, i, ctypes.POINTER(i), vp]),
         "lima_get_params": (i, [vp, vp]),
         "lima_set_params": (i, [vp, vp]),
         "lima_loss": (i, [vp, vp, ctypes.POINTER(d)]),
@@ -236,8 +238,35 @@ class Engine:
         self._check(self.lib.lima_get_param_count(self.h, ctypes.byref(n)))
         return int(n.value)
 
+    def param_layout(self) -> dict:
+        """Entry counts of theta: n_types, n_bond_types, n_angle_types, n_dihedral_types."""
+        c = np.zeros(4, np.int32)
+        self._check(self.lib.lima_get_param_layout(self.h, _ptr(c)))
+        return dict(zip(("n_types", "n_bond_types", "n_angle_types", "n_dihedral_types"), (int(x) for x in c)))
+
+    def param_names(self) -> list:
+        """A name for every entry of theta, in order."""
+        lay = self.param_layout()
+        nt = lay["n_types"]
+        names = [f"sigma[{t}]" for t in range(nt)] + [f"epsilon[{t}]" for t in range(nt)]
+        names += ["s_bond", "s_angle", "s_dihedral"]
+        for kind, c in (("bond", "r0"), ("angle", "theta0"), ("dihedral", "phi0")):
+            for q in range(lay[f"n_{kind}_types"]):
+                names += [f"{kind}[{q}].{c}", f"{kind}[{q}].k"]
+        return names
+
+    def bonded_types(self, kind: int) -> np.ndarray:
+        """Type of every term of a kind (0 bond, 1 angle, 2 dihedral), in load order."""
+        n = ctypes.c_int()
+        self._check(self.lib.lima_get_bonded_types(self.h, int(kind), ctypes.byref(n), None))
+        out = np.zeros(n.value, np.int32)
+        self._check(self.lib.lima_get_bonded_types(self.h, int(kind), ctypes.byref(n), _ptr(out)))
+        return out
+
     def get_params(self) -> np.ndarray:
-        """theta = [sigma per type, epsilon per type, bond, angle, dihedral scales]."""
+        """theta = [sigma per type, epsilon per type, bond / angle / dihedral scales,
+        (r0, k) per bond type, (theta0, k) per angle type, (phi0, k) per dihedral type]
+        (lima_get_params)."""
         th = np.zeros(self.param_count(), np.float64)
         self._check(self.lib.lima_get_params(self.h, _ptr(th)))
         return th
