@@ -643,7 +643,7 @@ def run_large(args):
         for step in (1e-3, 1e-2):
             fd, rel = [], []
             for k in range(len(theta)):
-                h = step * abs(theta[k])
+                h = step * abs(theta[k]) if theta[k] != 0.0 else step   # a zero phase: step in rad
                 tp = theta.copy()
                 tp[k] += h
                 eng.set_params(tp)

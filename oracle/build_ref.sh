@@ -25,6 +25,15 @@
 #      particle 0 after lane 0 wrapped it).  The host emulator runs threads one
 #      after another, so without the barriers it would resolve both races
 #      differently from the hardware.
+# The rasterizer (Quantom/Quantom/Rasterizer.cu + .cuh) is compiled in as well,
+# with two changes to the copy:
+#   6. the Rasterizer member functions render/getAllAtoms/sortAtoms/
+#      processAtoms (Rasterizer.cu:12-78: CUDA launch syntax, device
+#      allocations) are deleted; ref_emu.cpp's ref_render runs the same three
+#      kernels and the same merge sort in their order;
+#   7. the `1.8l` literal in processAtomsKernel (Rasterizer.cu:221) becomes
+#      `1.8`: CUDA device code has no long double and computes it in double,
+#      where the host compiler would use x87 extended precision.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 REF_ROOT="${LIMA_REF_ROOT:-/root/reference}"
@@ -38,7 +47,8 @@ mkdir -p "$OUT"
 TMP="$(mktemp -d /tmp/lima_ref_build.XXXXXX)"
 trap 'rm -rf "$TMP"' EXIT
 
-for f in Engine.cu Engine.cuh Bodies.cuh QuantomTypes.cuh Simulation.cuh Forcefield.cuh Filehandling.h; do
+for f in Engine.cu Engine.cuh Bodies.cuh QuantomTypes.cuh Simulation.cuh Forcefield.cuh Filehandling.h \
+         Rasterizer.cu Rasterizer.cuh; do
     cp "$SRC/$f" "$TMP/$f"
 done
 cp "$HERE/ref_shim/Constants.cuh" "$TMP/Constants.cuh"
@@ -67,6 +77,19 @@ sed -i -E '/^[[:space:]]*utility_buffer\[threadIdx\.x\] = Float3\((0\.f|0, 0, 0)
 n=$(grep -c 'applyHyperpos(&compound_state.positions\[0\], &compound_state.positions\[threadIdx.x\]);.*So all particles follows p0' "$TMP/Engine.cu" || true)
 [ "$n" = "1" ] || { echo "build_ref.sh: PBC hyperpos line not found" >&2; exit 1; }
 sed -i '/applyHyperpos(&compound_state.positions\[0\], &compound_state.positions\[threadIdx.x\]);.*So all particles follows p0/i\	__syncthreads();' "$TMP/Engine.cu"
+
+# 6. drop the Rasterizer member functions (signature to the first top-level closing brace)
+n=$(grep -cE '^[A-Za-z]+\*? Rasterizer::(render|getAllAtoms|sortAtoms|processAtoms)\(' "$TMP/Rasterizer.cu" || true)
+[ "$n" = "4" ] || { echo "build_ref.sh: expected 4 Rasterizer member functions, found $n" >&2; exit 1; }
+awk 'BEGIN{skip=0} /^[A-Za-z]+\*? Rasterizer::(render|getAllAtoms|sortAtoms|processAtoms)\(/{skip=1}
+     { if(!skip) print; else if ($0 ~ /^}/) skip=0 }' "$TMP/Rasterizer.cu" > "$TMP/Rasterizer.cu.new" &&
+    mv "$TMP/Rasterizer.cu.new" "$TMP/Rasterizer.cu"
+! grep -qE '<< ?<' "$TMP/Rasterizer.cu" || { echo "build_ref.sh: launch syntax left in Rasterizer.cu" >&2; exit 1; }
+
+# 7. the long double literal of processAtomsKernel
+n=$(grep -c ' \* 1\.8l;' "$TMP/Rasterizer.cu" || true)
+[ "$n" = "1" ] || { echo "build_ref.sh: expected one 1.8l literal, found $n" >&2; exit 1; }
+sed -i 's/ \* 1\.8l;/ * 1.8;/' "$TMP/Rasterizer.cu"
 
 CXX="${CXX:-g++}"
 "$CXX" -std=c++17 -O3 -march=x86-64-v3 -ffp-contract=off -fno-fast-math -pthread -fPIC -shared -w \

@@ -900,12 +900,14 @@ int orc_render_balls(int n, const float* pos, const unsigned char* kind, float L
         b.disable = t == RAS_NONE;
         src[i] = b;
     }
-    /* stable bottom-up merge sort by pos.y */
+    /* bottom-up merge sort by pos.y that takes the right run's element on a
+       tie, as the reference's merge (Rasterizer.cu:254-271): equal depths end
+       up in descending slot order */
     for (int w = 1; w < n; w *= 2) {
         for (int lo = 0; lo < n; lo += 2 * w) {
             int mid = lo + w < n ? lo + w : n, hi = lo + 2 * w < n ? lo + 2 * w : n;
             int a = lo, b = mid, k = lo;
-            while (a < mid && b < hi) tmp[k++] = (src[b].pos.y < src[a].pos.y) ? src[b++] : src[a++];
+            while (a < mid && b < hi) tmp[k++] = (src[a].pos.y < src[b].pos.y) ? src[a++] : src[b++];
             while (a < mid) tmp[k++] = src[a++];
             while (b < hi) tmp[k++] = src[b++];
         }

@@ -97,6 +97,8 @@ def ref_lib():
         lib.ref_get_log.argtypes = [vp, vp, vp, vp, vp]
         lib.ref_get_step.restype = i
         lib.ref_get_step.argtypes = [vp]
+        lib.ref_render.restype = i
+        lib.ref_render.argtypes = [vp, vp]
         _ref = lib
     return _ref
 
@@ -185,6 +187,15 @@ class RefEngine:
         gan = np.zeros((max(s.n_compounds, 1), MAXP, 3, 3), np.float32)
         self._check(self.lib.ref_get_log(self.h, _p(pe), _p(tr), _p(od), _p(gan)))
         return {"potE": pe, "traj": tr, "logdata": od, "train": gan[: s.n_compounds]}
+
+    def render(self):
+        """The reference Rasterizer's RenderBall list of the current box
+        (its three kernels and merge sort, Rasterizer.cu:12-293)."""
+        from quantom_b200 import layout as L
+        s = self.system
+        out = np.zeros(s.n_compounds * MAXP + s.n_solvents, L.RenderBall)
+        self._check(self.lib.ref_render(self.h, _p(out)))
+        return out
 
     def potE(self):
         s = self.system

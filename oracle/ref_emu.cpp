@@ -37,6 +37,7 @@
 
 #define private public
 #include "Engine.cu"
+#include "Rasterizer.cu"
 #undef private
 
 float BOX_LEN = 7.f;
@@ -579,5 +580,56 @@ int ref_get_log(void* h, double* potE, float* traj, float* outdata, float* gan) 
 }
 
 int ref_get_step(void* h) { return static_cast<int>(static_cast<RefCtx*>(h)->sim->box->step); }
+
+// The reference's RenderBall list of the current box, as Rasterizer::render
+// (Rasterizer.cu:12-27) makes it: loadCompoundatomsKernel over n_compounds
+// blocks of MAX_COMPOUND_PARTICLES threads, loadSolventatomsKernel over
+// ceil(n_solvents / 100) blocks of 100, processAtomsKernel over
+// ceil(upper / 64) blocks of 64 (upper = total_particles_upperbound,
+// BoxBuilder.cu:78), then mergeSortAPI over the first `upper` balls.  The
+// kernels have no barriers or shared memory, so their threads run one after
+// another.  The atom buffer is zero-filled where the reference leaves device
+// memory unset (positions of the empty compound slots, the padding up to a
+// whole block); its last block reads and writes past `upper`, so both
+// buffers are a whole number of blocks long.  `out` receives `upper` balls.
+int ref_render(void* h, void* out) {
+    auto* c = static_cast<RefCtx*>(h);
+    Simulation* sim = c->sim.get();
+    Box* box = sim->box;
+    const int nc = box->n_compounds, ns = box->n_solvents;
+    const int upper = nc * MAX_COMPOUND_PARTICLES + ns;
+    if (upper <= 0) return -1;
+    const int blocks = (int)ceil((float)upper / (float)RAS_THREADS_PER_BLOCK);
+    const size_t cap = (size_t)blocks * RAS_THREADS_PER_BLOCK;
+    RenderAtom* atoms = static_cast<RenderAtom*>(std::calloc(cap, sizeof(RenderAtom)));
+    RenderBall* balls = static_cast<RenderBall*>(std::calloc(cap, sizeof(RenderBall)));
+    if (!atoms || !balls) {
+        std::free(atoms);
+        std::free(balls);
+        return -1;
+    }
+    auto run = [](unsigned grid, unsigned block, auto&& body) {
+        blockDim = dim3(block, 1, 1);
+        gridDim = dim3(grid, 1, 1);
+        for (unsigned b = 0; b < grid; b++)
+            for (unsigned t = 0; t < block; t++) {
+                blockIdx = {b, 0, 0};
+                threadIdx = {t, 0, 0};
+                body();
+            }
+    };
+    if (nc > 0) run(nc, MAX_COMPOUND_PARTICLES, [&] { loadCompoundatomsKernel(box, atoms); });
+    if (ns > 0) {
+        const int sb = (int)ceil((float)ns / (float)THREADS_PER_LOADSOLVENTSATOMSKERNEL);
+        const int off = nc * MAX_COMPOUND_PARTICLES;
+        run(sb, THREADS_PER_LOADSOLVENTSATOMSKERNEL, [&] { loadSolventatomsKernel(box, atoms, off); });
+    }
+    run(blocks, RAS_THREADS_PER_BLOCK, [&] { processAtomsKernel(atoms, balls); });
+    mergeSortAPI(balls, upper);
+    std::memcpy(out, balls, sizeof(RenderBall) * (size_t)upper);
+    std::free(atoms);
+    std::free(balls);
+    return 0;
+}
 
 }  // extern "C"

@@ -9,8 +9,10 @@
 //   k_balls      per slot: atom type -> colour and radius, position ->
 //                normalised device coordinates (Rasterizer.cu:229-251); the
 //                depth key is the normalised y
-//   cub radix sort of the keys (stable), k_gather_balls into that order (the
-//                reference's host merge sort by pos.y, Rasterizer.cu:254-293)
+//   cub radix sort of the keys (stable, slots fed in reverse order so equal
+//                depths keep descending slot order), k_gather_balls into that
+//                order (the reference's host merge sort by pos.y,
+//                Rasterizer.cu:254-293)
 //   k_splat      one warp per ball over its pixel bounding box: each covered
 //                pixel keeps the smallest sorted index (atomicMin), i.e. the
 //                ball the display draws last (it draws from the back,
@@ -108,8 +110,11 @@ __global__ void k_balls(const float4* __restrict__ pos, const uint8_t* __restric
     b.disable = t == AT_NONE ? 1 : 0;
     b.pad[0] = b.pad[1] = b.pad[2] = 0;
     balls[i] = b;
-    keys[i] = b.pos.y;
-    vals[i] = (uint32_t)i;
+    // slots enter the stable sort in reverse order: equal depths come out in
+    // descending slot order, as the reference's merge, which takes the right
+    // half's ball on a tie (Rasterizer.cu:254-271), leaves them
+    keys[n - 1 - i] = b.pos.y;
+    vals[n - 1 - i] = (uint32_t)i;
 }
 
 __global__ void k_gather_balls(const lima_render_ball* __restrict__ in, const uint32_t* __restrict__ order, int n,

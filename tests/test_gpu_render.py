@@ -1,6 +1,9 @@
 """Headless rasterizer on the GPU (lima_render, lima_render_image) against
 the oracle's restatement of Rasterizer.cu and the display's shaded discs:
-ball lists and images bit-identical, in both semantics."""
+ball lists and images bit-identical, in both semantics.  The restatement's
+ball list is itself pinned to the reference's Rasterizer run on the host
+(tests/test_render_pin.py); here the GPU list is also compared with that
+reference run directly, on a box where most depths are tied."""
 import numpy as np
 import pytest
 
@@ -45,3 +48,29 @@ def test_ppm_file(gpu, tmp_path):
     E.save_ppm(tmp_path / "frame.ppm", img)
     data = (tmp_path / "frame.ppm").read_bytes()
     assert data.startswith(b"P6\n64 48\n255\n") and data[len(b"P6\n64 48\n255\n"):] == img.tobytes()
+
+
+def test_balls_match_reference_rasterizer(gpu):
+    """Reference semantics, the state as loaded and after 3 steps, and a
+    lattice box of tied depths: the GPU ball list equals the one the
+    reference's own Rasterizer kernels and merge sort make (oracle/_ref)."""
+    from test_render_pin import _lattice_box, FIELDS
+    if not po.ref_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    E = gpu
+    for s, steps in ((S.make_system("tiny_chains", seed=11), 0), (S.make_system("small_bridged", seed=11), 3),
+                     (_lattice_box(8, 4.0), 0)):
+        ref = po.RefEngine(s, n_threads=4)
+        if steps:
+            ref.update_nlists()
+            ref.step(steps)
+        want = ref.render()
+        ref.close()
+        with E.Engine(s, _params(E, s, "reference")) as eng:
+            eng.step(steps)
+            got = eng.render()
+        for f in FIELDS:
+            a, b = got[f], want[f]
+            if a.dtype.kind == "f":
+                a, b = a.view(np.uint32), b.view(np.uint32)
+            assert np.array_equal(a, b), (s.spec.name, f)

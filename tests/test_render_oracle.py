@@ -35,7 +35,7 @@ def test_empty_slot_is_disabled_at_the_origin():
     assert tuple(b["color"]) == (0xF2, 0xE5, 0xD9) and b["radius"] == F(0.25)
 
 
-def test_depth_sort_is_ascending_and_stable():
+def test_depth_sort_is_ascending_with_ties_in_descending_slot_order():
     rng = np.random.default_rng(3)
     pos = rng.uniform(0, 5, (500, 3)).astype(np.float32)
     pos[100:110, 1] = pos[50, 1]                           # 11 balls at one depth
@@ -46,8 +46,9 @@ def test_depth_sort_is_ascending_and_stable():
     y50 = F((np.float64(pos[50, 1]) / 5.0 - 0.5) * 1.8)
     tied = b[b["pos"][:, 1] == y50]
     assert len(tied) == 11
-    # slot order kept among equal depths: slot 50 first, then 100..109 by x
-    expect_x = [F((np.float64(pos[i, 0]) / 5.0 - 0.5) * 1.8) for i in [50] + list(range(100, 110))]
+    # equal depths in descending slot order (the reference's merge takes the right
+    # half's ball on a tie): slots 109..100, then slot 50
+    expect_x = [F((np.float64(pos[i, 0]) / 5.0 - 0.5) * 1.8) for i in list(range(109, 99, -1)) + [50]]
     assert tied["pos"][:, 0].tolist() == expect_x
 
 
