@@ -60,6 +60,9 @@ def parse():
     ap.add_argument("--large-steps", type=int, default=10000, help="--mode large: mixed-precision forward steps")
     ap.add_argument("--nve-steps", type=int, default=50000, help="--mode precision: NVE steps per run")
     ap.add_argument("--eq-steps", type=int, default=5000, help="--mode precision: Berendsen equilibration steps")
+    ap.add_argument("--replicas", type=int, default=1,
+                    help="--mode precision: independent NVE starts (each a further --replica-gap Berendsen steps on)")
+    ap.add_argument("--replica-gap", type=int, default=2500, help="--mode precision: steps between replica starts")
     ap.add_argument("--grad-state", default="",
                     help="--mode large: save the gradient's start state, target and a 20-step adjoint gradient "
                          "here (.npz); --mode large-fp64: read it")
@@ -360,9 +363,13 @@ def drift_fit(t, e):
 
 def run_precision(args):
     """Config-2 study on the 32k box: Berendsen equilibration, then NVE runs
-    of plain FP32 and mixed precision at dt 2 fs and 1 fs.  Drift = slope of
-    a linear fit of the total energy, per particle, in kT per ns.  Force error
-    = relative RMS against the FP64 oracle at the same positions."""
+    of plain FP32 and mixed precision at dt 2 fs and 1 fs from each of
+    --replicas starts (the equilibration continued --replica-gap steps
+    between starts).  Drift = slope of a linear fit of the total energy, per
+    particle, in kT per ns; per precision and dt the replicas' mean, with the
+    larger of two standard errors of that mean (the fits' errors combined,
+    and the replicas' scatter / sqrt(R) when R > 1).  Force error = relative
+    RMS against the FP64 oracle at the same positions."""
     from oracle import pyoracle as po
     from quantom_b200 import engine as E
     from quantom_b200 import systems as S
@@ -370,11 +377,16 @@ def run_precision(args):
     system = S.make_system(args.workload, seed=args.seed)
     n = system.n_particles
     kT = K_B * spec.temperature
+    R = max(1, args.replicas)
+    starts = []
     with E.Engine(system, physics_params(E, spec, E.PRECISION_FP32)) as eq:
         eq.step(args.eq_steps)
-        st, prev = eq.compound_states()
-        sol = eq.solvents()
-    start = with_state(system, st, prev, sol)
+        for r in range(R):
+            if r:
+                eq.step(args.replica_gap)
+            st, prev = eq.compound_states()
+            starts.append(with_state(system, st, prev, eq.solvents()))
+    start = starts[0]
 
     def force_errors(sys_x):
         F64, _ = po.PhysSystem(sys_x, rc=spec.cutoff, r_on=1.0).forces()
@@ -389,49 +401,71 @@ def run_precision(args):
         return out
 
     result = {"mode": "precision", "workload": args.workload, "particles": n, "eq_steps": args.eq_steps,
-              "nve_steps": args.nve_steps, "force_relrms_vs_fp64": {"start": force_errors(start)}, "runs": []}
+              "nve_steps": args.nve_steps, "replicas": R, "replica_gap_steps": args.replica_gap,
+              "force_relrms_vs_fp64": {"start": force_errors(start)}, "runs": []}
     block = 100
-    for dt_fs in (2.0, 1.0):
-        sys_dt = rescale_dt(start, dt_fs * 1e-6 / spec.dt)
-        for name, prec in (("fp32", E.PRECISION_FP32), ("mixed", E.PRECISION_MIXED)):
-            p = physics_params(E, spec, prec, dt=dt_fs * 1e-6)
-            p.thermostat = E.THERMOSTAT_NONE
-            t_ns, etot, temp = [], [], []
-            with E.Engine(sys_dt, p) as eng:
-                for b in range(args.nve_steps // block + 1):
-                    e = eng.compute_energies()
-                    t_ns.append(b * block * dt_fs * 1e-6)
-                    etot.append(e[E.E_TOTAL])
-                    temp.append(e[E.E_TEMPERATURE])
-                    if b < args.nve_steps // block:
-                        eng.step(block)
-                if dt_fs == 2.0 and name == "fp32":
-                    st2, prev2 = eng.compound_states()
-                    end = with_state(system, st2, prev2, eng.solvents())
-            t = np.asarray(t_ns)
-            et = np.asarray(etot)
-            slope, se, tau = drift_fit(t, et)
-            resid = et - np.polyval(np.polyfit(t, et, 1), t)
-            result["runs"].append({
-                "precision": name, "dt_fs": dt_fs, "simulated_ps": float(t[-1] * 1e3),
-                "drift_kT_per_particle_per_ns": slope / (n * kT),
-                "drift_stderr_kT_per_particle_per_ns": se / (n * kT),
-                "residual_autocorr_samples": tau,
-                "drift_J_per_mol_per_ns": slope,
-                "etot_fluct_rms_kT_per_particle": float(resid.std() / (n * kT)),
-                "temperature_mean_K": float(np.mean(temp)), "temperature_first_last_K": [temp[0], temp[-1]],
-            })
-            print(json.dumps(result["runs"][-1]), flush=True)
+    end = None
+    for r, start_r in enumerate(starts):
+        for dt_fs in (2.0, 1.0):
+            sys_dt = rescale_dt(start_r, dt_fs * 1e-6 / spec.dt)
+            for name, prec in (("fp32", E.PRECISION_FP32), ("mixed", E.PRECISION_MIXED)):
+                p = physics_params(E, spec, prec, dt=dt_fs * 1e-6)
+                p.thermostat = E.THERMOSTAT_NONE
+                t_ns, etot, temp = [], [], []
+                with E.Engine(sys_dt, p) as eng:
+                    for b in range(args.nve_steps // block + 1):
+                        e = eng.compute_energies()
+                        t_ns.append(b * block * dt_fs * 1e-6)
+                        etot.append(e[E.E_TOTAL])
+                        temp.append(e[E.E_TEMPERATURE])
+                        if b < args.nve_steps // block:
+                            eng.step(block)
+                    if r == 0 and dt_fs == 2.0 and name == "fp32":
+                        st2, prev2 = eng.compound_states()
+                        end = with_state(system, st2, prev2, eng.solvents())
+                t = np.asarray(t_ns)
+                et = np.asarray(etot)
+                slope, se, tau = drift_fit(t, et)
+                resid = et - np.polyval(np.polyfit(t, et, 1), t)
+                result["runs"].append({
+                    "replica": r, "precision": name, "dt_fs": dt_fs, "simulated_ps": float(t[-1] * 1e3),
+                    "drift_kT_per_particle_per_ns": slope / (n * kT),
+                    "drift_stderr_kT_per_particle_per_ns": se / (n * kT),
+                    "residual_autocorr_samples": tau,
+                    "drift_J_per_mol_per_ns": slope,
+                    "etot_fluct_rms_kT_per_particle": float(resid.std() / (n * kT)),
+                    "temperature_mean_K": float(np.mean(temp)), "temperature_first_last_K": [temp[0], temp[-1]],
+                })
+                print(json.dumps(result["runs"][-1]), flush=True)
     result["force_relrms_vs_fp64"]["after_nve_fp32_2fs"] = force_errors(end)
+    # Per precision and dt over the replicas: the signed mean drift, and the
+    # mean drift magnitude |slope|.  The FP32 energy wanders like a random
+    # walk whose sign differs between replicas, so the ratio is taken on the
+    # magnitudes; its standard errors are the larger of the fits' combined
+    # errors and the replicas' scatter / sqrt(R).
+    combined = {}
     for dt_fs in (2.0, 1.0):
-        r = {x["precision"]: x for x in result["runs"] if x["dt_fs"] == dt_fs}
-        f32, mx = r["fp32"], r["mixed"]
-        result[f"drift_ratio_fp32_over_mixed_{int(dt_fs)}fs"] = (
-            abs(f32["drift_kT_per_particle_per_ns"]) / max(abs(mx["drift_kT_per_particle_per_ns"]), 1e-30))
-        # lower bound: FP32 drift less 2 standard errors over mixed drift plus 2 standard errors
-        result[f"drift_ratio_lower_bound_2se_{int(dt_fs)}fs"] = (
-            max(abs(f32["drift_kT_per_particle_per_ns"]) - 2 * f32["drift_stderr_kT_per_particle_per_ns"], 0.0) /
-            (abs(mx["drift_kT_per_particle_per_ns"]) + 2 * mx["drift_stderr_kT_per_particle_per_ns"]))
+        for name in ("fp32", "mixed"):
+            runs = [x for x in result["runs"] if x["dt_fs"] == dt_fs and x["precision"] == name]
+            d = np.array([x["drift_kT_per_particle_per_ns"] for x in runs])
+            a = np.abs(d)
+            se_fit = math.sqrt(sum(x["drift_stderr_kT_per_particle_per_ns"] ** 2 for x in runs)) / len(runs)
+            se_scatter = float(d.std(ddof=1) / math.sqrt(len(d))) if len(d) > 1 else 0.0
+            se_abs_scatter = float(a.std(ddof=1) / math.sqrt(len(a))) if len(a) > 1 else 0.0
+            combined[(dt_fs, name)] = (float(a.mean()), max(se_fit, se_abs_scatter))
+            result.setdefault("combined", []).append({
+                "precision": name, "dt_fs": dt_fs, "replicas": len(runs),
+                "simulated_ps_total": float(sum(x["simulated_ps"] for x in runs)),
+                "drift_kT_per_particle_per_ns": float(d.mean()),
+                "drift_stderr": max(se_fit, se_scatter),
+                "drift_magnitude_kT_per_particle_per_ns": float(a.mean()),
+                "drift_magnitude_stderr": max(se_fit, se_abs_scatter),
+                "stderr_fits": se_fit, "stderr_replica_scatter": se_scatter,
+                "stderr_magnitude_replica_scatter": se_abs_scatter})
+        (d32, s32), (dmx, smx) = combined[(dt_fs, "fp32")], combined[(dt_fs, "mixed")]
+        result[f"drift_ratio_fp32_over_mixed_{int(dt_fs)}fs"] = d32 / max(dmx, 1e-30)
+        # lower bound: FP32 magnitude less 2 standard errors over mixed magnitude plus 2 standard errors
+        result[f"drift_ratio_lower_bound_2se_{int(dt_fs)}fs"] = max(d32 - 2 * s32, 0.0) / (dmx + 2 * smx)
     print(json.dumps(result), flush=True)
 
 

@@ -340,7 +340,7 @@ lima_status lima_grad(lima_ctx* ctx, const lima_loss_spec* spec, double* loss, d
 lima_status lima_rdf(lima_ctx* ctx, int n_bins, float r_max, double* h);
 
 /* ------------------------------------------------------------------ */
-/* Frame log (physics semantics).  Replaces the reference's logging      */
+/* Frame log (either semantics).  Replaces the reference's logging      */
 /* buffers written by the force kernels every step (Box::potE_buffer,   */
 /* traj_buffer, outdata, data_GAN: Engine.cu:1007-1047, 1136-1145),      */
 /* their host offload every 40 / 100 steps (Engine::hostMaster,          */
@@ -370,7 +370,15 @@ typedef struct {
    particle l at c*64 + l, solvent s at n_compounds*64 + s; empty compound
    slots are zero); train[n_compounds*64][3][3] float; energies[LIMA_E_COUNT]
    double; logdata[10] float (particle slot 0: speed, kinetic energy,
-   potential energy, |force|, then zeros). */
+   potential energy, |force|, then zeros).
+   Reference semantics records what the reference's step writes instead: the
+   positions after the step, the compound particles' potE of the step's
+   compound kernel (solvent slots 0), data_GAN (position or (-1, -1, -1), then
+   force_LJ_sol), the outdata line of compound 0 particle 0 and, as energies,
+   the bonded potE summed over the compound slots and the last thermostat
+   temperature; energy.bin then holds the Analyzer's central-difference
+   energies of frames 1 .. F-3, over frames `every` steps apart (the
+   reference records every step). */
 lima_status lima_log_start(lima_ctx* ctx, const lima_log_params* params);
 /* Stops recording; what was recorded stays readable. */
 lima_status lima_log_stop(lima_ctx* ctx);

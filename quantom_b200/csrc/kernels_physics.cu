@@ -692,7 +692,14 @@ __device__ __forceinline__ void finish_sums(const PhysDev& d, int slot, cudaGrap
 // per SM), and four in flight measured 71 against 79 us per flushed step
 constexpr int kMixedGathers = 4;
 
-// One lane's rows of its particle's Verlet list, GATHERS (4 or 2) position
+// Offset of a lane's m-th list entry from its first: with 8 lanes entry m is
+// in row m; with 4 lanes entries alternate between columns g and g + 4 of
+// one row.
+__device__ __forceinline__ uint32_t lane_entry(int m, uint32_t stride) {
+    return kStepLanes == 8 ? (uint32_t)m * stride : (uint32_t)(m >> 1) * stride + (uint32_t)(m & 1) * 4u;
+}
+
+// One lane's entries of its particle's Verlet list, GATHERS (4 or 2) position
 // loads in flight; MIXED: compensated sums every 8 pairs.
 template <bool MIXED, bool ENERGY, bool SWITCH, bool WRAP, int GATHERS = 4>
 __device__ __forceinline__ void pair_rows(const PhysDev& d, const float2* row, float4 pi, const float4* __restrict__ pos,
@@ -705,8 +712,8 @@ __device__ __forceinline__ void pair_rows(const PhysDev& d, const float2* row, f
         float px = 0.f, py = 0.f, pz = 0.f;
         if (GATHERS == 4) {
             for (; r + 3 < rend; r += 4) {
-                const uint32_t j0 = __ldg(nl + r * stride), j1 = __ldg(nl + (r + 1) * stride);
-                const uint32_t j2 = __ldg(nl + (r + 2) * stride), j3 = __ldg(nl + (r + 3) * stride);
+                const uint32_t j0 = __ldg(nl + lane_entry(r, stride)), j1 = __ldg(nl + lane_entry(r + 1, stride));
+                const uint32_t j2 = __ldg(nl + lane_entry(r + 2, stride)), j3 = __ldg(nl + lane_entry(r + 3, stride));
                 const float4 p0 = __ldg(pos + j0), p1 = __ldg(pos + j1), p2 = __ldg(pos + j2), p3 = __ldg(pos + j3);
                 lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p0, px, py, pz, e_i, w_i);
                 lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p1, px, py, pz, e_i, w_i);
@@ -715,14 +722,14 @@ __device__ __forceinline__ void pair_rows(const PhysDev& d, const float2* row, f
             }
         } else {
             for (; r + 1 < rend; r += 2) {
-                const uint32_t j0 = __ldg(nl + r * stride), j1 = __ldg(nl + (r + 1) * stride);
+                const uint32_t j0 = __ldg(nl + lane_entry(r, stride)), j1 = __ldg(nl + lane_entry(r + 1, stride));
                 const float4 p0 = __ldg(pos + j0), p1 = __ldg(pos + j1);
                 lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p0, px, py, pz, e_i, w_i);
                 lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p1, px, py, pz, e_i, w_i);
             }
         }
         for (; r < rend; r++) {
-            const uint32_t j0 = __ldg(nl + r * stride);
+            const uint32_t j0 = __ldg(nl + lane_entry(r, stride));
             lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, __ldg(pos + j0), px, py, pz, e_i, w_i);
         }
         if (MIXED) {
@@ -743,8 +750,8 @@ __device__ __forceinline__ void step_body(const PhysDev& d, int cur, int slot, c
     const int nt2 = d.n_types * d.n_types;
     for (int q = threadIdx.x; q < nt2; q += blockDim.x) s_tab[q] = d.lj_table[q];
     __syncthreads();
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) / kGroup;
-    const int g = threadIdx.x % kGroup;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) / kStepLanes;
+    const int g = threadIdx.x % kStepLanes;
     const bool active = i < d.n;
     // FP64 sums of this thread: kinetic energy, LJ energy, LJ virial
     double red[kRed] = {0.0, 0.0, 0.0};
@@ -756,7 +763,8 @@ __device__ __forceinline__ void step_body(const PhysDev& d, int cur, int slot, c
     const int cnt = active ? (int)d.nl_cnt[i] : 0;
     const uint32_t stride = (uint32_t)d.n_pad * kGroup;
     const uint32_t* __restrict__ nl = d.nl + (uint32_t)i * kGroup + g;
-    const int rows = cnt > g ? (cnt - g + kGroup - 1) / kGroup : 0;
+    // this lane's entries: g, g + kStepLanes, g + 2 kStepLanes, ... below cnt
+    const int rows = cnt > g ? (cnt - g + kStepLanes - 1) / kStepLanes : 0;
     // warps whose particles are all away from the box faces skip the minimum image
     if (__all_sync(0xffffffffu, !active || away_from_faces(d, pi)))
         pair_rows<MIXED, ENERGY, SWITCH, false, MIXED ? kMixedGathers : 4>(d, row, pi, pos, nl, stride, rows, fx, fy, fz,
@@ -764,9 +772,9 @@ __device__ __forceinline__ void step_body(const PhysDev& d, int cur, int slot, c
     else
         pair_rows<MIXED, ENERGY, SWITCH, true, MIXED ? kMixedGathers : 4>(d, row, pi, pos, nl, stride, rows, fx, fy, fz,
                                                                           cxx, cyy, czz, e_i, w_i);
-    // reduce the kGroup lanes of this particle (warp shuffles)
+    // reduce the kStepLanes lanes of this particle (warp shuffles)
 #pragma unroll
-    for (int o = kGroup / 2; o > 0; o >>= 1) {
+    for (int o = kStepLanes / 2; o > 0; o >>= 1) {
         if (MIXED) {
             const float ox = __shfl_xor_sync(0xffffffffu, fx, o), oy = __shfl_xor_sync(0xffffffffu, fy, o),
                         oz = __shfl_xor_sync(0xffffffffu, fz, o);

@@ -13,8 +13,14 @@ constexpr int kBuildWarps = 4;   // warps per block of the list build (8 particl
 constexpr int kMaxTypes = 32;    // LIMA_MAX_ATOM_TYPES
 constexpr int kScanThreads = 1024;
 
-// blocks of the step kernel (kGroup lanes per particle slot, n_pad a multiple of 32)
-__host__ __device__ inline int step_blocks(const PhysDev& d) { return (int)(((size_t)d.n_pad * kGroup + kTB - 1) / kTB); }
+// lanes per particle in the step kernel: 8 (one list column each) or 4 (two
+// columns each, columns g and g + 4 of every 8-entry row)
+constexpr int kStepLanes = 8;
+static_assert(kStepLanes == 8 || kStepLanes == 4, "the step kernel reads 8-entry list rows with 8 or 4 lanes");
+// blocks of the step kernel (kStepLanes lanes per particle slot, n_pad a multiple of 32)
+__host__ __device__ inline int step_blocks(const PhysDev& d) {
+    return (int)(((size_t)d.n_pad * kStepLanes + kTB - 1) / kTB);
+}
 // blocks of the bonded kernel (one thread per term)
 __host__ __device__ inline int bonded_blocks(const PhysDev& d) {
     const int nt = d.n_bonds + d.n_angles + d.n_dih;

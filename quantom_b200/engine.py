@@ -311,7 +311,7 @@ class Engine:
         self._check(self.lib.lima_get_rebuild_count(self.h, ctypes.byref(v)))
         return int(v.value)
 
-    # -- frame log (physics semantics) -------------------------------------
+    # -- frame log ---------------------------------------------------------
     def log_start(self, every: int, ring_frames: int = 64, flags: int = LOG_TRAJ | LOG_POTE | LOG_TRAIN):
         """Record the state of every `every`-th step: the reference's logging
         buffers (traj, potE, data_GAN, outdata) and per-step energies."""
