@@ -63,6 +63,7 @@ def parse():
     ap.add_argument("--replicas", type=int, default=1,
                     help="--mode precision: independent NVE starts (each a further --replica-gap Berendsen steps on)")
     ap.add_argument("--replica-gap", type=int, default=2500, help="--mode precision: steps between replica starts")
+    ap.add_argument("--dts", default="2,1", help="--mode precision: time steps in fs, comma-separated")
     ap.add_argument("--grad-state", default="",
                     help="--mode large: save the gradient's start state, target and a 20-step adjoint gradient "
                          "here (.npz); --mode large-fp64: read it")
@@ -405,8 +406,10 @@ def run_precision(args):
               "force_relrms_vs_fp64": {"start": force_errors(start)}, "runs": []}
     block = 100
     end = None
+    dts = [float(x) for x in args.dts.split(",")]
+    result["dts_fs"] = dts
     for r, start_r in enumerate(starts):
-        for dt_fs in (2.0, 1.0):
+        for dt_fs in dts:
             sys_dt = rescale_dt(start_r, dt_fs * 1e-6 / spec.dt)
             for name, prec in (("fp32", E.PRECISION_FP32), ("mixed", E.PRECISION_MIXED)):
                 p = physics_params(E, spec, prec, dt=dt_fs * 1e-6)
@@ -420,7 +423,7 @@ def run_precision(args):
                         temp.append(e[E.E_TEMPERATURE])
                         if b < args.nve_steps // block:
                             eng.step(block)
-                    if r == 0 and dt_fs == 2.0 and name == "fp32":
+                    if r == 0 and dt_fs == dts[0] and name == "fp32":
                         st2, prev2 = eng.compound_states()
                         end = with_state(system, st2, prev2, eng.solvents())
                 t = np.asarray(t_ns)
@@ -437,14 +440,14 @@ def run_precision(args):
                     "temperature_mean_K": float(np.mean(temp)), "temperature_first_last_K": [temp[0], temp[-1]],
                 })
                 print(json.dumps(result["runs"][-1]), flush=True)
-    result["force_relrms_vs_fp64"]["after_nve_fp32_2fs"] = force_errors(end)
+    result["force_relrms_vs_fp64"][f"after_nve_fp32_{dts[0]:g}fs"] = force_errors(end)
     # Per precision and dt over the replicas: the signed mean drift, and the
     # mean drift magnitude |slope|.  The FP32 energy wanders like a random
     # walk whose sign differs between replicas, so the ratio is taken on the
     # magnitudes; its standard errors are the larger of the fits' combined
     # errors and the replicas' scatter / sqrt(R).
     combined = {}
-    for dt_fs in (2.0, 1.0):
+    for dt_fs in dts:
         for name in ("fp32", "mixed"):
             runs = [x for x in result["runs"] if x["dt_fs"] == dt_fs and x["precision"] == name]
             d = np.array([x["drift_kT_per_particle_per_ns"] for x in runs])
@@ -452,7 +455,8 @@ def run_precision(args):
             se_fit = math.sqrt(sum(x["drift_stderr_kT_per_particle_per_ns"] ** 2 for x in runs)) / len(runs)
             se_scatter = float(d.std(ddof=1) / math.sqrt(len(d))) if len(d) > 1 else 0.0
             se_abs_scatter = float(a.std(ddof=1) / math.sqrt(len(a))) if len(a) > 1 else 0.0
-            combined[(dt_fs, name)] = (float(a.mean()), max(se_fit, se_abs_scatter))
+            combined[(dt_fs, name)] = (float(a.mean()), max(se_fit, se_abs_scatter), float(d.mean()),
+                                       max(se_fit, se_scatter))
             result.setdefault("combined", []).append({
                 "precision": name, "dt_fs": dt_fs, "replicas": len(runs),
                 "simulated_ps_total": float(sum(x["simulated_ps"] for x in runs)),
@@ -462,10 +466,13 @@ def run_precision(args):
                 "drift_magnitude_stderr": max(se_fit, se_abs_scatter),
                 "stderr_fits": se_fit, "stderr_replica_scatter": se_scatter,
                 "stderr_magnitude_replica_scatter": se_abs_scatter})
-        (d32, s32), (dmx, smx) = combined[(dt_fs, "fp32")], combined[(dt_fs, "mixed")]
+        (d32, s32, _, _), (dmx, smx, mmx, smm) = combined[(dt_fs, "fp32")], combined[(dt_fs, "mixed")]
         result[f"drift_ratio_fp32_over_mixed_{int(dt_fs)}fs"] = d32 / max(dmx, 1e-30)
         # lower bound: FP32 magnitude less 2 standard errors over mixed magnitude plus 2 standard errors
         result[f"drift_ratio_lower_bound_2se_{int(dt_fs)}fs"] = max(d32 - 2 * s32, 0.0) / (dmx + 2 * smx)
+        # the same against the mixed runs' systematic drift (their signed mean; its random part averages out)
+        result[f"drift_ratio_lower_bound_2se_vs_mixed_signed_mean_{int(dt_fs)}fs"] = (
+            max(d32 - 2 * s32, 0.0) / (abs(mmx) + 2 * smm))
     print(json.dumps(result), flush=True)
 
 
@@ -999,7 +1006,7 @@ def run_ours(args, ws, rank, local, pg):
     grad["fd_note"] = ("FP32 central differences are limited by the trajectories' rounding noise; against the FP64 "
                        "oracle's central differences (bench.py --mode grad --fp64-fd) the gradient agrees to "
                        "8.5e-8 (sigma) and 5.8e-7 (epsilon) relative")
-    # ---- roofline of the dominant kernel (pair + integrate) -----------------
+    # ---- roofline of the dominant kernel (k_step: pairs + integration) -------
     # The pair terms are bound by the FP32 pipe: 32 FLOP per unique pair within
     # r_c (minimum image 9, r^2 5, rcp 1, s^6 3, scalar force 5, vector force 3,
     # accumulation on both sides 6), pairs = N (4/3) pi r_c^3 rho / 2.  The peak
@@ -1021,9 +1028,9 @@ def run_ours(args, ws, rank, local, pg):
     compulsory = 80.0 * n
     list_len = (4.0 / 3.0) * math.pi * (spec.cutoff + SKIN) ** 3 * rho    # expected Verlet-list entries
     bytes_list = n * (80.0 + 4.0 * list_len)
-    traffic = ncu_traffic("k_pair_integrate", args.workload)
+    traffic = ncu_traffic("k_step", args.workload)
     roofline = {
-        "kernel": "k_pair_integrate", "bound": "fp32", "achieved": tflops, "peak": FP32_NOMINAL_TFLOPS,
+        "kernel": "k_step", "bound": "fp32", "achieved": tflops, "peak": FP32_NOMINAL_TFLOPS,
         "unit": "TFLOP/s", "frac": tflops / FP32_NOMINAL_TFLOPS, "traffic": traffic,
         "peak_source": "nominal, clock-derived (148 SMs x 128 lanes x 2 FLOP x 1.965 GHz); no measured FP32 figure",
         "kernel_ms": prof["pair"], "flops_per_launch": flops_pair, "unique_pairs_within_rc": pairs,
