@@ -49,10 +49,22 @@ def _stamp(cmd, src, headers) -> str:
     return h.hexdigest()
 
 
-def build(verbose: bool = False, force: bool = False) -> Path:
-    """Compile every source to _build/*.o and link the library.  An object is
-    recompiled when the content hash of its command, source and the headers
-    differs from the one recorded beside it, or always with force=True."""
+# Library variants: extra defines for some sources, linked with the default
+# objects of the others.  The staged variant reads the step kernel's list rows
+# through shared memory (bulk copies); the engine loads it when LIMA_B200_LIB
+# names it.
+VARIANTS = {"staged": {"kernels_physics.cu": ["-DLIMA_STAGED_LIST=1"]}}
+
+
+def variant_path(name: str) -> Path:
+    return PKG / f"liblima_b200_{name}.so"
+
+
+def build(verbose: bool = False, force: bool = False, variants=("staged",)) -> Path:
+    """Compile every source to _build/*.o and link the library (and the named
+    variants).  An object is recompiled when the content hash of its command,
+    source and the headers differs from the one recorded beside it, or always
+    with force=True."""
     BUILD.mkdir(exist_ok=True)
     srcs = sources()
     headers = [h for h in list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [ROOT / "include" / "lima_abi.h"]
@@ -60,17 +72,30 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     objs = []
     jobs = []
     nvcc = _nvcc()
-    for s in srcs:
-        o = BUILD / (s.name + ".o")
-        objs.append(o)
-        cmd = [nvcc, *ARCH, *NVCC_FLAGS, *PER_FILE.get(s.name, []), "-c", str(s), "-o", str(o)]
+    var_objs = {v: [] for v in variants}
+
+    def add(s, o, extra):
+        cmd = [nvcc, *ARCH, *NVCC_FLAGS, *PER_FILE.get(s.name, []), *extra, "-c", str(s), "-o", str(o)]
         if s.suffix == ".cpp":
-            cmd = [nvcc, *NVCC_FLAGS, "-x", "cu", *ARCH, "-c", str(s), "-o", str(o)]
+            cmd = [nvcc, *NVCC_FLAGS, *extra, "-x", "cu", *ARCH, "-c", str(s), "-o", str(o)]
         stamp_file = o.with_suffix(".o.sha256")
         stamp = _stamp(cmd, s, headers)
         if not force and o.exists() and stamp_file.exists() and stamp_file.read_text() == stamp:
-            continue
+            return
         jobs.append((cmd, stamp_file, stamp))
+
+    for s in srcs:
+        o = BUILD / (s.name + ".o")
+        objs.append(o)
+        add(s, o, [])
+        for v in variants:
+            extra = VARIANTS[v].get(s.name)
+            if extra:
+                ov = BUILD / (s.name + f".{v}.o")
+                add(s, ov, extra)
+                var_objs[v].append(ov)
+            else:
+                var_objs[v].append(o)
 
     def compile_one(job):
         cmd, stamp_file, stamp = job
@@ -80,12 +105,13 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         stamp_file.write_text(stamp)
     with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
         list(pool.map(compile_one, jobs))
-    tmp = OUT.with_suffix(".so.tmp")
-    cmd = [nvcc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudadevrt", "-lcudart", "-Xcompiler", "-fPIC"]
-    if verbose:
-        print(" ".join(cmd), flush=True)
-    subprocess.run(cmd, check=True)
-    os.replace(tmp, OUT)
+    for out, ol in [(OUT, objs)] + [(variant_path(v), var_objs[v]) for v in variants]:
+        tmp = out.with_suffix(".so.tmp")
+        cmd = [nvcc, *ARCH, "-shared", "-o", str(tmp), *map(str, ol), "-lcudadevrt", "-lcudart", "-Xcompiler", "-fPIC"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+        os.replace(tmp, out)
     return OUT
 
 

@@ -455,6 +455,44 @@ namespace {
 __device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
+// Bulk copies global -> shared memory completing on an mbarrier (the copy
+// engine, not the threads, moves the bytes).  Sources are this GPU's own
+// memory; there is no cluster multicast.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+// waits for the phase of `parity` to complete; false after the iteration limit
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    for (int it = 0; it < (1 << 20); it++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+// orders this thread's earlier generic-proxy shared accesses (after a block
+// barrier: the block's) before its following bulk-copy writes
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
 // lane 0 receives the warp's sum of v[0..K); then thread 0 adds the warps in
 // order into out[0..K) (fixed order)
 template <int K>
@@ -744,6 +782,102 @@ __device__ __forceinline__ void pair_rows(const PhysDev& d, const float2* row, f
     }
 }
 
+// One lane's entries of one staged group of list rows: entry q of the lane
+// at srow[q * kTB] (shared memory); MIXED: one compensated sum per group.
+template <bool MIXED, bool ENERGY, bool SWITCH, bool WRAP>
+__device__ __forceinline__ void pair_staged(const PhysDev& d, const float2* row, float4 pi,
+                                            const float4* __restrict__ pos, const uint32_t* srow, int nq, float& fx,
+                                            float& fy, float& fz, float& cxx, float& cyy, float& czz, float& e_i,
+                                            float& w_i) {
+    float px = 0.f, py = 0.f, pz = 0.f;
+    // staged ids are clamped into the position array (a wrong id stays a wrong force, not a stray read)
+    const uint32_t lim = (uint32_t)d.n_pad - 1u;
+    int q = 0;
+    for (; q + 3 < nq; q += 4) {
+        const uint32_t j0 = min(srow[q * kTB], lim), j1 = min(srow[(q + 1) * kTB], lim);
+        const uint32_t j2 = min(srow[(q + 2) * kTB], lim), j3 = min(srow[(q + 3) * kTB], lim);
+        const float4 p0 = __ldg(pos + j0), p1 = __ldg(pos + j1), p2 = __ldg(pos + j2), p3 = __ldg(pos + j3);
+        lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p0, px, py, pz, e_i, w_i);
+        lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p1, px, py, pz, e_i, w_i);
+        lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p2, px, py, pz, e_i, w_i);
+        lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p3, px, py, pz, e_i, w_i);
+    }
+    for (; q < nq; q++) lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, __ldg(pos + min(srow[q * kTB], lim)), px, py, pz, e_i, w_i);
+    if (MIXED) {
+        ds_add(fx, cxx, px);
+        ds_add(fy, cyy, py);
+        ds_add(fz, czz, pz);
+    } else {
+        fx += px;
+        fy += py;
+        fz += pz;
+    }
+}
+
+// The block's list rows through shared memory: row r of the block's 32
+// particles is one contiguous kilobyte of the blocked list (entry k of
+// particle i at ((k / 8) n_pad + i) 8 + k % 8, and lane t of the block reads
+// word t of each row), so each row is one bulk copy.  Groups of kStageRows
+// rows alternate between two buffers: thread 0 issues group s + 1 while the
+// block evaluates group s, and a block barrier after each group frees its
+// buffer for group s + 2.  Waits are bounded; one that runs out sets
+// ERR_BIT_TILE_TIMEOUT and ends the issuing, and thread 0 waits (bounded) for
+// the copies already issued before the block moves on.
+template <bool MIXED, bool ENERGY, bool SWITCH>
+__device__ __forceinline__ void pair_walk_staged(const PhysDev& d, const float2* row, float4 pi,
+                                                 const float4* __restrict__ pos, int rows, bool active, bool nowrap,
+                                                 float& fx, float& fy, float& fz, float& cxx, float& cyy, float& czz,
+                                                 float& e_i, float& w_i) {
+    __shared__ __align__(128) uint32_t s_stage[2][kStageRows][kTB];
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ int s_rows, s_fail;
+    if (threadIdx.x == 0) {
+        s_rows = 0;
+        s_fail = 0;
+        mbar_init(&s_bar[0], 1);
+        mbar_init(&s_bar[1], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    if (active && threadIdx.x % kStepLanes == 0) atomicMax(&s_rows, rows);
+    __syncthreads();
+    const int brows = s_rows;
+    const int nst = (brows + kStageRows - 1) / kStageRows;
+    // row 0 of this block's particles: particle i0 = blockIdx.x * 32, word i0 * 8
+    const uint32_t* src0 = d.nl + (size_t)blockIdx.x * kTB;
+    const size_t stride = (size_t)d.n_pad * kGroup;
+    int issued = 0;   // thread 0: groups issued
+    auto issue = [&](int st) {
+        const int r0 = st * kStageRows, nr = min(kStageRows, brows - r0);
+        uint64_t* bar = &s_bar[st & 1];
+        fence_proxy_async_smem();
+        mbar_expect_tx(bar, (uint32_t)(nr * kTB * sizeof(uint32_t)));
+        for (int q = 0; q < nr; q++)
+            bulk_g2s(&s_stage[st & 1][q][0], src0 + (size_t)(r0 + q) * stride, kTB * sizeof(uint32_t), bar);
+        issued = st + 1;
+    };
+    if (threadIdx.x == 0 && nst > 0) issue(0);
+    for (int st = 0; st < nst; st++) {
+        if (threadIdx.x == 0 && st + 1 < nst && !*(volatile int*)&s_fail) issue(st + 1);
+        const bool got = !*(volatile int*)&s_fail && mbar_wait_bounded(&s_bar[st & 1], (uint32_t)(st >> 1) & 1u);
+        if (!got && !*(volatile int*)&s_fail) {
+            s_fail = 1;
+            atomicOr(d.err, ERR_BIT_TILE_TIMEOUT);
+        }
+        const int nq = got ? max(0, min(kStageRows, rows - st * kStageRows)) : 0;
+        const uint32_t* srow = &s_stage[st & 1][0][threadIdx.x];
+        if (nowrap)
+            pair_staged<MIXED, ENERGY, SWITCH, false>(d, row, pi, pos, srow, nq, fx, fy, fz, cxx, cyy, czz, e_i, w_i);
+        else
+            pair_staged<MIXED, ENERGY, SWITCH, true>(d, row, pi, pos, srow, nq, fx, fy, fz, cxx, cyy, czz, e_i, w_i);
+        __syncthreads();
+    }
+    // after a timeout: the groups issued and not yet seen complete
+    if (threadIdx.x == 0 && s_fail)
+        for (int st = max(0, issued - 2); st < issued; st++) mbar_wait_bounded(&s_bar[st & 1], (uint32_t)(st >> 1) & 1u);
+    __syncthreads();
+}
+
 template <bool MIXED, bool ENERGY, bool INTEGRATE, bool SWITCH, bool TAIL>
 __device__ __forceinline__ void step_body(const PhysDev& d, int cur, int slot, cudaGraphExec_t tail) {
     extern __shared__ float2 s_tab[];
@@ -766,12 +900,18 @@ __device__ __forceinline__ void step_body(const PhysDev& d, int cur, int slot, c
     // this lane's entries: g, g + kStepLanes, g + 2 kStepLanes, ... below cnt
     const int rows = cnt > g ? (cnt - g + kStepLanes - 1) / kStepLanes : 0;
     // warps whose particles are all away from the box faces skip the minimum image
-    if (__all_sync(0xffffffffu, !active || away_from_faces(d, pi)))
-        pair_rows<MIXED, ENERGY, SWITCH, false, MIXED ? kMixedGathers : 4>(d, row, pi, pos, nl, stride, rows, fx, fy, fz,
-                                                                           cxx, cyy, czz, e_i, w_i);
-    else
-        pair_rows<MIXED, ENERGY, SWITCH, true, MIXED ? kMixedGathers : 4>(d, row, pi, pos, nl, stride, rows, fx, fy, fz,
-                                                                          cxx, cyy, czz, e_i, w_i);
+    const bool nowrap = __all_sync(0xffffffffu, !active || away_from_faces(d, pi));
+    if constexpr (kStagedList) {
+        pair_walk_staged<MIXED, ENERGY, SWITCH>(d, row, pi, pos, rows, active, nowrap, fx, fy, fz, cxx, cyy, czz, e_i,
+                                                w_i);
+    } else {
+        if (nowrap)
+            pair_rows<MIXED, ENERGY, SWITCH, false, MIXED ? kMixedGathers : 4>(d, row, pi, pos, nl, stride, rows, fx,
+                                                                               fy, fz, cxx, cyy, czz, e_i, w_i);
+        else
+            pair_rows<MIXED, ENERGY, SWITCH, true, MIXED ? kMixedGathers : 4>(d, row, pi, pos, nl, stride, rows, fx,
+                                                                              fy, fz, cxx, cyy, czz, e_i, w_i);
+    }
     // reduce the kStepLanes lanes of this particle (warp shuffles)
 #pragma unroll
     for (int o = kStepLanes / 2; o > 0; o >>= 1) {

@@ -17,6 +17,16 @@ constexpr int kScanThreads = 1024;
 // columns each, columns g and g + 4 of every 8-entry row)
 constexpr int kStepLanes = 8;
 static_assert(kStepLanes == 8 || kStepLanes == 4, "the step kernel reads 8-entry list rows with 8 or 4 lanes");
+// the step kernel reads its list rows from shared memory, staged by bulk
+// copies in groups of kStageRows rows (false: per-lane loads from the list).
+// Built into liblima_b200_staged.so (LIMA_STAGED_LIST=1) beside the default
+// library; it measured no faster on the 32k box.
+#ifndef LIMA_STAGED_LIST
+#define LIMA_STAGED_LIST 0
+#endif
+constexpr bool kStagedList = LIMA_STAGED_LIST != 0;
+constexpr int kStageRows = 8;
+static_assert(!kStagedList || kStepLanes == 8, "the staged list walk gives each lane one list column");
 // blocks of the step kernel (kStepLanes lanes per particle slot, n_pad a multiple of 32)
 __host__ __device__ inline int step_blocks(const PhysDev& d) {
     return (int)(((size_t)d.n_pad * kStepLanes + kTB - 1) / kTB);

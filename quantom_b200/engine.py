@@ -18,7 +18,8 @@ import numpy as np
 from . import layout as L
 
 _LIB = None
-LIB_PATH = Path(__file__).resolve().parent / "liblima_b200.so"
+# the library: LIMA_B200_LIB if set (e.g. a build variant), else the in-tree build
+LIB_PATH = Path(os.environ.get("LIMA_B200_LIB") or Path(__file__).resolve().parent / "liblima_b200.so")
 
 OK, ERR_ARGUMENT, ERR_CUDA, ERR_CAPACITY, ERR_STATE, ERR_NUMERIC, ERR_UNSUPPORTED = range(7)
 SEMANTICS_REFERENCE, SEMANTICS_PHYSICS = 0, 1
