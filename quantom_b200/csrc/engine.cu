@@ -98,6 +98,7 @@ struct lima_ctx {
     }
     ~lima_ctx() {
         lima::framelog_free(log);
+        lima::phys_read_cache_free(read_cache);
         lima::phys_free_rebuild(phys);
         for (auto& g : graph)
             if (g) cudaGraphExecDestroy(g);
@@ -805,7 +806,7 @@ lima_status lima_get_compound_states(lima_ctx* c, lima_compound_state* states, l
             cuda_ok(cudaMemcpy(hp.data(), c->ref.cpos[c->cur], sizeof(float4) * ncp, cudaMemcpyDeviceToHost), "D2H");
             cuda_ok(cudaMemcpy(hq.data(), c->ref.cprev, sizeof(float4) * ncp, cudaMemcpyDeviceToHost), "D2H");
         } else {
-            lima::phys_read_compounds(c->phys, c->cur, c->comps.data(), hp.data(), hq.data(), c->read_cache, c->state_version);
+            lima::phys_read_compounds(c->phys, c->cur, c->comps.data(), hp.data(), hq.data(), c->read_cache, c->state_version, c->stream);
         }
         for (int i = 0; i < nc; i++) {
             if (states) {
@@ -827,16 +828,16 @@ lima_status lima_get_solvents(lima_ctx* c, lima_solvent* sols) {
         need(sols != nullptr || c->sols.empty(), LIMA_ERR_ARGUMENT, "null solvent array");
         sync_checked(c);
         const int ns = static_cast<int>(c->sols.size());
-        std::vector<float4> a(ns), b(ns);
         if (c->p.semantics == LIMA_SEMANTICS_REFERENCE) {
+            std::vector<float4> a(ns), b(ns);
             cuda_ok(cudaMemcpy(a.data(), c->ref.spos[c->cur], sizeof(float4) * ns, cudaMemcpyDeviceToHost), "D2H");
             cuda_ok(cudaMemcpy(b.data(), c->ref.sprev[c->cur], sizeof(float4) * ns, cudaMemcpyDeviceToHost), "D2H");
+            for (int i = 0; i < ns; i++) {
+                sols[i].pos = lima_float3{a[i].x, a[i].y, a[i].z};
+                sols[i].pos_tsub1 = lima_float3{b[i].x, b[i].y, b[i].z};
+            }
         } else {
-            lima::phys_read_solvents(c->phys, c->cur, a.data(), b.data(), c->read_cache, c->state_version);
-        }
-        for (int i = 0; i < ns; i++) {
-            sols[i].pos = lima_float3{a[i].x, a[i].y, a[i].z};
-            sols[i].pos_tsub1 = lima_float3{b[i].x, b[i].y, b[i].z};
+            lima::phys_read_solvent_structs(c->phys, c->cur, sols, c->read_cache, c->state_version, c->stream);
         }
     });
 }
@@ -852,7 +853,7 @@ lima_status lima_get_positions(lima_ctx* c, float* cxyz, float* sxyz) {
             if (c->p.semantics == LIMA_SEMANTICS_REFERENCE)
                 cuda_ok(cudaMemcpy(hp.data(), c->ref.cpos[c->cur], sizeof(float4) * ncp, cudaMemcpyDeviceToHost), "D2H");
             else
-                lima::phys_read_compounds(c->phys, c->cur, c->comps.data(), hp.data(), hq.data(), c->read_cache, c->state_version);
+                lima::phys_read_compounds(c->phys, c->cur, c->comps.data(), hp.data(), hq.data(), c->read_cache, c->state_version, c->stream);
             for (int i = 0; i < nc; i++)
                 for (int t = 0; t < lima::kMaxCP; t++) {
                     const size_t k = static_cast<size_t>(i) * lima::kMaxCP + t;
@@ -866,7 +867,7 @@ lima_status lima_get_positions(lima_ctx* c, float* cxyz, float* sxyz) {
             if (c->p.semantics == LIMA_SEMANTICS_REFERENCE)
                 cuda_ok(cudaMemcpy(a.data(), c->ref.spos[c->cur], sizeof(float4) * ns, cudaMemcpyDeviceToHost), "D2H");
             else
-                lima::phys_read_solvents(c->phys, c->cur, a.data(), b.data(), c->read_cache, c->state_version);
+                lima::phys_read_solvents(c->phys, c->cur, a.data(), b.data(), c->read_cache, c->state_version, c->stream);
             for (int i = 0; i < ns; i++) {
                 sxyz[3 * i] = a[i].x;
                 sxyz[3 * i + 1] = a[i].y;
@@ -1130,7 +1131,7 @@ lima_status lima_log_start(lima_ctx* c, const lima_log_params* p) {
         for (const auto& cp : c->comps) np.push_back(cp.n_particles);
         std::string msg;
         int st = LIMA_OK;
-        lima::framelog_start(c->log, static_cast<int>(c->sols.size()), np, *p, msg, st);
+        lima::framelog_start(c->log, static_cast<int>(c->sols.size()), np, *p, c->stream, msg, st);
         if (st != LIMA_OK) fail(static_cast<lima_status>(st), msg);
         sync_checked(c);
     });

@@ -189,11 +189,12 @@ __global__ void __launch_bounds__(kTB) k_log_ref_energy(RefDev d, FrameLogDev g,
     }
 }
 
+// a device buffer of the frame log, from the process's stream-ordered pool
 template <typename T>
-T* grow(std::vector<void*>& allocs, size_t n) {
-    void* ptr = nullptr;
-    if (cudaMalloc(&ptr, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) return nullptr;
-    allocs.push_back(ptr);
+T* grow(FrameLog& g, size_t n) {
+    void* ptr = pool_alloc(std::max<size_t>(n, 1) * sizeof(T), g.stream);
+    if (!ptr) return nullptr;
+    g.dallocs.push_back(ptr);
     return static_cast<T*>(ptr);
 }
 
@@ -273,11 +274,8 @@ void absorb(FrameLog& g, int b) {
 bool ensure_pinned(FrameLog& g) {
     if (g.pinned[0]) return true;
     const size_t stride = (g.ring_bytes + 255) & ~static_cast<size_t>(255);
-    if (cudaMallocHost(&g.pinned[0], 2 * stride) != cudaSuccess) {
-        cudaGetLastError();
-        g.pinned[0] = nullptr;
-        return false;
-    }
+    g.pinned[0] = pinned_alloc(2 * stride);
+    if (!g.pinned[0]) return false;
     g.pinned[1] = static_cast<char*>(g.pinned[0]) + stride;
     for (int b = 0; b < 2; b++)
         if (cudaEventCreateWithFlags(&g.done[b], cudaEventDisableTiming) != cudaSuccess) {
@@ -332,9 +330,10 @@ void drain(FrameLog& g, cudaStream_t s) {
 void framelog_free(FrameLog& g) {
     for (int b = 0; b < 2; b++)
         if (g.pending[b] && g.done[b]) cudaEventSynchronize(g.done[b]);   // copies still in flight
-    for (void* p : g.dallocs) cudaFree(p);
+    for (void* p : g.dallocs) pool_free(p, g.stream);
+    if (!g.dallocs.empty()) cudaStreamSynchronize(g.stream);
     g.dallocs.clear();
-    if (g.pinned[0]) cudaFreeHost(g.pinned[0]);   // one allocation holds both staging rings
+    pinned_free(g.pinned[0]);   // one allocation holds both staging rings
     g.pinned[0] = g.pinned[1] = nullptr;
     for (auto& e : g.done)
         if (e) {
@@ -345,8 +344,9 @@ void framelog_free(FrameLog& g) {
 }
 
 void framelog_start(FrameLog& g, int n_s, const std::vector<int>& n_compound_particles, const lima_log_params& p,
-                    std::string& msg, int& status) {
+                    cudaStream_t s, std::string& msg, int& status) {
     framelog_free(g);
+    g.stream = s;
     status = LIMA_OK;
     const int n_c = (int)n_compound_particles.size();
     FrameLogDev& v = g.dev;
@@ -362,36 +362,41 @@ void framelog_start(FrameLog& g, int n_s, const std::vector<int>& n_compound_par
         for (int l = 0; l < n_compound_particles[c]; l++) slot[o++] = (uint32_t)(c * LIMA_MAX_COMPOUND_PARTICLES + l);
     for (int s = 0; s < n_s; s++) slot[o++] = (uint32_t)(v.n_train + s);
     const size_t f = (size_t)v.ring;
-    uint32_t* ref_slot = grow<uint32_t>(g.dallocs, slot.size());
-    v.traj = (p.flags & LIMA_LOG_TRAJ) ? grow<float>(g.dallocs, f * v.n_slots * 3) : nullptr;
-    v.potE = (p.flags & LIMA_LOG_POTE) ? grow<double>(g.dallocs, f * v.n_slots) : nullptr;
-    v.train = (p.flags & LIMA_LOG_TRAIN) && n_c ? grow<float>(g.dallocs, f * v.n_train * kTrainValues * 3) : nullptr;
-    v.energies = grow<double>(g.dallocs, f * LIMA_E_COUNT);
-    v.logdata = grow<float>(g.dallocs, f * kLogDataFloats);
+    uint32_t* ref_slot = grow<uint32_t>(g, slot.size());
+    v.traj = (p.flags & LIMA_LOG_TRAJ) ? grow<float>(g, f * v.n_slots * 3) : nullptr;
+    v.potE = (p.flags & LIMA_LOG_POTE) ? grow<double>(g, f * v.n_slots) : nullptr;
+    v.train = (p.flags & LIMA_LOG_TRAIN) && n_c ? grow<float>(g, f * v.n_train * kTrainValues * 3) : nullptr;
+    v.energies = grow<double>(g, f * LIMA_E_COUNT);
+    v.logdata = grow<float>(g, f * kLogDataFloats);
     const Sections R = sections(v, v.ring);
     g.ring_bytes = R.total;
     bool ok = ref_slot && v.energies && v.logdata && (!(p.flags & LIMA_LOG_TRAJ) || v.traj) &&
               (!(p.flags & LIMA_LOG_POTE) || v.potE) && (!(p.flags & LIMA_LOG_TRAIN) || !n_c || v.train);
     if (!ok) {
+        const cudaStream_t st = g.stream;
         framelog_free(g);
         cudaGetLastError();
+        g.stream = st;
         msg = "frame log: out of device memory for the ring";
         status = LIMA_ERR_CUDA;
         return;
     }
     v.ref_slot = ref_slot;
-    cudaMemcpy(ref_slot, slot.data(), sizeof(uint32_t) * slot.size(), cudaMemcpyHostToDevice);
-    if (v.traj) cudaMemset(v.traj, 0, f * v.n_slots * 3 * sizeof(float));
-    if (v.potE) cudaMemset(v.potE, 0, f * v.n_slots * sizeof(double));
+    // set-up copies in the engine's stream order; the host arrays live until the sync below
+    cudaMemcpyAsync(ref_slot, slot.data(), sizeof(uint32_t) * slot.size(), cudaMemcpyHostToDevice, s);
+    if (v.traj) cudaMemsetAsync(v.traj, 0, f * v.n_slots * 3 * sizeof(float), s);
+    if (v.potE) cudaMemsetAsync(v.potE, 0, f * v.n_slots * sizeof(double), s);
+    std::vector<float> pad;
     if (v.train) {
         // padding particles of a compound: position (-1, -1, -1) (Engine.cu:1036-1037), zero force
-        std::vector<float> pad((size_t)v.n_train * kTrainValues * 3, 0.f);
+        pad.assign((size_t)v.n_train * kTrainValues * 3, 0.f);
         for (int c = 0; c < n_c; c++)
             for (int l = n_compound_particles[c]; l < LIMA_MAX_COMPOUND_PARTICLES; l++)
                 for (int q = 0; q < 3; q++) pad[((size_t)c * LIMA_MAX_COMPOUND_PARTICLES + l) * kTrainValues * 3 + q] = -1.f;
         for (size_t r = 0; r < f; r++)
-            cudaMemcpy(v.train + r * pad.size(), pad.data(), sizeof(float) * pad.size(), cudaMemcpyHostToDevice);
+            cudaMemcpyAsync(v.train + r * pad.size(), pad.data(), sizeof(float) * pad.size(), cudaMemcpyHostToDevice, s);
     }
+    cudaStreamSynchronize(s);
     g.every = p.every;
     g.on = true;
 }

@@ -47,7 +47,8 @@ struct FrameLog {
     bool on = false;
     int every = 0;
     FrameLogDev dev{};
-    std::vector<void*> dallocs;
+    std::vector<void*> dallocs;     // device buffers from the process's stream-ordered pool
+    cudaStream_t stream = nullptr;  // the engine's stream (allocations, frees and copies)
     // pinned staging, two rings; pending[b] = frames copied into b not yet in the store
     void* pinned[2] = {nullptr, nullptr};
     size_t ring_bytes = 0;
@@ -69,7 +70,7 @@ struct FrameLog {
 
 // sets up a ring for the loaded box: n_s solvents, n_compound_particles[c] per compound
 void framelog_start(FrameLog& g, int n_s, const std::vector<int>& n_compound_particles, const lima_log_params& p,
-                    std::string& msg, int& status);
+                    cudaStream_t s, std::string& msg, int& status);
 void framelog_free(FrameLog& g);
 // after the energy variant of step `step` on parity `cur` (accumulator slot `cur`)
 int framelog_record(FrameLog& g, const PhysDev& d, int cur, uint64_t step, cudaStream_t s);

@@ -130,6 +130,11 @@ struct PhysHost {
 // context reuses the memory of destroyed ones instead of mapping new memory.
 void* pool_alloc(size_t bytes, cudaStream_t s);   // nullptr on failure
 void pool_free(void* p, cudaStream_t s);
+// Pinned host blocks from a process-wide cache: a freed block is kept and
+// handed to a later request of up to its size (cudaMallocHost costs about a
+// millisecond per call).
+void* pinned_alloc(size_t bytes);   // nullptr on failure
+void pinned_free(void* p);
 
 // returns 0 or a lima_status; device buffers (from the pool) are appended to `allocs`
 int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>& allocs, std::string& msg);
@@ -164,14 +169,24 @@ void phys_energy_now(PhysDev& d, int cur, cudaStream_t s);
 // Host copy of the state in orig order (position and previous position, in
 // double), kept while the state it was read from is unchanged: `key` names
 // that state (the caller changes it whenever the state may have changed).
+// The state in orig order as of one state version: per particle its position
+// (hi + lo) and previous position x - v dt in FP64, gathered on the device and
+// read back with one copy into pinned memory (buffers made by the first read).
 struct PhysReadCache {
     uint64_t key = ~0ull;
-    std::vector<double> x, xp;
+    double* host = nullptr;   // pinned [n][6]: x, y, z, then the previous position
+    double* dev = nullptr;    // device staging of the same (from the pool)
+    cudaStream_t stream = nullptr;
 };
+void phys_read_cache_free(PhysReadCache& cache);
+// both throw std::runtime_error when the buffers cannot be made
 void phys_read_compounds(const PhysDev& d, int cur, const lima_compound* comps, float4* pos_out, float4* prev_out,
-                         PhysReadCache& cache, uint64_t key);
+                         PhysReadCache& cache, uint64_t key, cudaStream_t s);
 void phys_read_solvents(const PhysDev& d, int cur, float4* pos_out, float4* prev_out, PhysReadCache& cache,
-                        uint64_t key);
+                        uint64_t key, cudaStream_t s);
+// the same straight into the reference's Solvent structs
+void phys_read_solvent_structs(const PhysDev& d, int cur, lima_solvent* out, PhysReadCache& cache, uint64_t key,
+                               cudaStream_t s);
 void phys_read_forces(const PhysDev& d, const lima_compound* comps, float4* fc, float4* fs);
 // the Verlet list as CSR over orig ids (offsets[n + 1]; ids, nullable, sorted
 // ascending in each row); returns the total entry count

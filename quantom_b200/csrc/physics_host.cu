@@ -4,8 +4,10 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <stdexcept>
+#include <unordered_map>
 #include <vector>
 
 #include "physdev.cuh"
@@ -71,6 +73,48 @@ void* pool_alloc(size_t bytes, cudaStream_t s) {
 
 void pool_free(void* p, cudaStream_t s) {
     if (p) cudaFreeAsync(p, s);
+}
+
+namespace {
+struct PinnedCache {
+    std::mutex mu;
+    std::multimap<size_t, void*> idle;       // freed blocks by size
+    std::unordered_map<void*, size_t> size;  // every block handed out
+};
+PinnedCache& pinned_cache() {
+    static PinnedCache* c = new PinnedCache();   // lives to process exit (blocks are reused, not returned)
+    return *c;
+}
+}  // namespace
+
+void* pinned_alloc(size_t bytes) {
+    bytes = std::max<size_t>(bytes, 1);
+    PinnedCache& c = pinned_cache();
+    {
+        std::lock_guard<std::mutex> lock(c.mu);
+        auto it = c.idle.lower_bound(bytes);
+        if (it != c.idle.end() && it->first <= 2 * bytes) {   // reuse a block of at most twice the size
+            void* p = it->second;
+            c.idle.erase(it);
+            return p;
+        }
+    }
+    void* p = nullptr;
+    if (cudaMallocHost(&p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(c.mu);
+    c.size[p] = bytes;
+    return p;
+}
+
+void pinned_free(void* p) {
+    if (!p) return;
+    PinnedCache& c = pinned_cache();
+    std::lock_guard<std::mutex> lock(c.mu);
+    auto it = c.size.find(p);
+    if (it != c.size.end()) c.idle.emplace(it->second, p);
 }
 
 namespace {
@@ -335,8 +379,19 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
 // Host state (reference layout) -> device, in orig order (the next rebuild
 // sorts).  Half-step velocities from the Stormer pair: v = (x - x_prev)/dt.
 void phys_upload_state(const PhysHost& h, PhysDev& d, int cur, cudaStream_t s) {
-    std::vector<float4> pos(d.n_pad), vel(d.n_pad);
-    std::vector<uint32_t> ident(d.n_pad);
+    // staged in one pinned block (pageable sources would each take a driver
+    // staging pass); plain host memory when no pinned block can be had
+    const size_t np = (size_t)d.n_pad;
+    const size_t bytes = np * (2 * sizeof(float4) + sizeof(uint32_t));
+    void* block = pinned_alloc(bytes);
+    std::vector<uint8_t> fallback;
+    if (!block) {
+        fallback.resize(bytes);
+        block = fallback.data();
+    }
+    float4* pos = static_cast<float4*>(block);
+    float4* vel = pos + np;
+    uint32_t* ident = reinterpret_cast<uint32_t*>(vel + np);
     const float L = d.L;
     auto wrap = [&](double x) {
         if (!(x >= 0.0 && x < (double)L)) {   // most inputs are inside the box already
@@ -370,18 +425,19 @@ void phys_upload_state(const PhysHost& h, PhysDev& d, int cur, cudaStream_t s) {
         vel[i] = make_float4(0, 0, 0, 0);
     }
     for (int i = 0; i < d.n_pad; i++) ident[i] = i < d.n ? i : 0xffffffffu;
-    cudaMemcpyAsync(d.pos[cur], pos.data(), sizeof(float4) * d.n_pad, cudaMemcpyHostToDevice, s);
-    if (d.n_cp) cudaMemcpyAsync(d.pos_orig[cur], pos.data(), sizeof(float4) * d.n_cp, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d.pos[cur], pos, sizeof(float4) * d.n_pad, cudaMemcpyHostToDevice, s);
+    if (d.n_cp) cudaMemcpyAsync(d.pos_orig[cur], pos, sizeof(float4) * d.n_cp, cudaMemcpyHostToDevice, s);
     if (d.n_cp) cudaMemsetAsync(d.posc_orig[cur], 0, sizeof(float4) * d.n_cp, s);
-    cudaMemcpyAsync(d.vel, vel.data(), sizeof(float4) * d.n_pad, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d.vel, vel, sizeof(float4) * d.n_pad, cudaMemcpyHostToDevice, s);
     cudaMemsetAsync(d.posc, 0, sizeof(float4) * d.n_pad, s);
     cudaMemsetAsync(d.velc, 0, sizeof(float4) * d.n_pad, s);
-    cudaMemcpyAsync(d.orig_of_sorted, ident.data(), sizeof(uint32_t) * d.n_pad, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d.sorted_of_orig, ident.data(), sizeof(uint32_t) * d.n, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d.orig_of_sorted, ident, sizeof(uint32_t) * d.n_pad, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d.sorted_of_orig, ident, sizeof(uint32_t) * d.n, cudaMemcpyHostToDevice, s);
     set_device_float(d.lambda, 1.f, s);
     set_device_float(d.lambda + 1, 1.f, s);
     cudaMemsetAsync(d.force, 0, sizeof(float4) * d.n_pad, s);
-    cudaStreamSynchronize(s);
+    cudaStreamSynchronize(s);   // the staging block is reused after this
+    if (fallback.empty()) pinned_free(block);
 }
 
 void phys_rebuild(const PhysDev& d, int cur, cudaStream_t s) {
@@ -554,46 +610,70 @@ Snapshot snapshot(const PhysDev& d, int cur, bool want_force) {
     }
     return sn;
 }
-// per orig id: position (hi + lo) and previous position x - v dt
-void orig_state(const PhysDev& d, const Snapshot& sn, std::vector<double>& x, std::vector<double>& xp) {
-    x.assign(3 * (size_t)d.n, 0.0);
-    xp.assign(3 * (size_t)d.n, 0.0);
-    const bool mixed = !sn.posc.empty();
-    for (int k = 0; k < d.n; k++) {
-        const uint32_t o = sn.orig[k];
-        const float4 p = sn.pos[k], v = sn.vel[k];
-        double px = p.x, py = p.y, pz = p.z, vx = v.x, vy = v.y, vz = v.z;
-        if (mixed) {
-            px += sn.posc[k].x; py += sn.posc[k].y; pz += sn.posc[k].z;
-            vx += sn.velc[k].x; vy += sn.velc[k].y; vz += sn.velc[k].z;
-        }
-        x[3 * o] = px; x[3 * o + 1] = py; x[3 * o + 2] = pz;
-        xp[3 * o] = px - vx * d.dt; xp[3 * o + 1] = py - vy * d.dt; xp[3 * o + 2] = pz - vz * d.dt;
+}  // namespace
+
+namespace {
+// per sorted slot: the particle's position and previous position x - v dt
+// (hi + lo in mixed precision) in FP64 at its orig id
+__global__ void k_orig_state(PhysDev d, int cur, double* __restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= d.n) return;
+    const uint32_t o = d.orig_of_sorted[k];
+    const float4 p = d.pos[cur][k], v = d.vel[k];
+    double px = p.x, py = p.y, pz = p.z, vx = v.x, vy = v.y, vz = v.z;
+    if (d.precision == LIMA_PRECISION_MIXED) {
+        const float4 pc = d.posc[k], vc = d.velc[k];
+        px += pc.x; py += pc.y; pz += pc.z;
+        vx += vc.x; vy += vc.y; vz += vc.z;
     }
+    double* r = out + 6 * (size_t)o;
+    r[0] = px; r[1] = py; r[2] = pz;
+    r[3] = px - vx * d.dt; r[4] = py - vy * d.dt; r[5] = pz - vz * d.dt;
 }
 }  // namespace
 
-// compound positions in the reference's convention: particle 0 in the box,
-// the others as the image nearest to it (Engine.cu:993-996)
-static void cached_orig_state(const PhysDev& d, int cur, PhysReadCache& cache, uint64_t key) {
-    if (cache.key == key && !cache.x.empty()) return;
-    orig_state(d, snapshot(d, cur, false), cache.x, cache.xp);
+void phys_read_cache_free(PhysReadCache& cache) {
+    pinned_free(cache.host);
+    if (cache.dev) {
+        pool_free(cache.dev, cache.stream);
+        cudaStreamSynchronize(cache.stream);
+    }
+    cache = PhysReadCache{};
+}
+
+// the orig-ordered state of version `key` in cache.host (one gather kernel and one copy)
+static void cached_orig_state(const PhysDev& d, int cur, PhysReadCache& cache, uint64_t key, cudaStream_t s) {
+    if (cache.key == key && cache.host) return;
+    const size_t bytes = sizeof(double) * 6 * (size_t)std::max(d.n, 1);
+    if (!cache.host) {
+        cache.stream = s;
+        cache.dev = static_cast<double*>(pool_alloc(bytes, s));
+        cache.host = cache.dev ? static_cast<double*>(pinned_alloc(bytes)) : nullptr;
+        if (!cache.host) {
+            phys_read_cache_free(cache);
+            throw std::runtime_error("cannot allocate the readback buffers");
+        }
+    }
+    k_orig_state<<<(d.n + 255) / 256, 256, 0, s>>>(d, cur, cache.dev);
+    cudaMemcpyAsync(cache.host, cache.dev, bytes, cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) throw std::runtime_error("the state readback failed");
     cache.key = key;
 }
 
+// compound positions in the reference's convention: particle 0 in the box,
+// the others as the image nearest to it (Engine.cu:993-996)
 void phys_read_compounds(const PhysDev& d, int cur, const lima_compound* comps, float4* pos_out, float4* prev_out,
-                         PhysReadCache& cache, uint64_t key) {
-    cached_orig_state(d, cur, cache, key);
-    const std::vector<double>& x = cache.x;
-    const std::vector<double>& xp = cache.xp;
+                         PhysReadCache& cache, uint64_t key, cudaStream_t s) {
+    cached_orig_state(d, cur, cache, key, s);
+    const double* h = cache.host;
     const double L = d.L;
     int o = 0;
     for (int c = 0; c < d.n_c; c++) {
         const int n = comps[c].n_particles;
-        const double* p0 = &x[3 * (size_t)o];
+        const double* p0 = &h[6 * (size_t)o];
         for (int t = 0; t < n; t++) {
-            const double* pt = &x[3 * (size_t)(o + t)];
-            const double* qt = &xp[3 * (size_t)(o + t)];
+            const double* pt = &h[6 * (size_t)(o + t)];
+            const double* qt = pt + 3;
             double q[3], r[3];
             for (int k = 0; k < 3; k++) {
                 double dd = pt[k] - p0[k];
@@ -609,14 +689,22 @@ void phys_read_compounds(const PhysDev& d, int cur, const lima_compound* comps, 
 }
 
 void phys_read_solvents(const PhysDev& d, int cur, float4* pos_out, float4* prev_out, PhysReadCache& cache,
-                        uint64_t key) {
-    cached_orig_state(d, cur, cache, key);
-    const std::vector<double>& x = cache.x;
-    const std::vector<double>& xp = cache.xp;
+                        uint64_t key, cudaStream_t s) {
+    cached_orig_state(d, cur, cache, key, s);
     for (int si = 0; si < d.n_s; si++) {
-        const size_t o = 3 * (size_t)(d.n_cp + si);
-        pos_out[si] = make_float4((float)x[o], (float)x[o + 1], (float)x[o + 2], 0.f);
-        prev_out[si] = make_float4((float)xp[o], (float)xp[o + 1], (float)xp[o + 2], 0.f);
+        const double* r = &cache.host[6 * (size_t)(d.n_cp + si)];
+        pos_out[si] = make_float4((float)r[0], (float)r[1], (float)r[2], 0.f);
+        prev_out[si] = make_float4((float)r[3], (float)r[4], (float)r[5], 0.f);
+    }
+}
+
+void phys_read_solvent_structs(const PhysDev& d, int cur, lima_solvent* out, PhysReadCache& cache, uint64_t key,
+                               cudaStream_t s) {
+    cached_orig_state(d, cur, cache, key, s);
+    for (int si = 0; si < d.n_s; si++) {
+        const double* r = &cache.host[6 * (size_t)(d.n_cp + si)];
+        out[si].pos = lima_float3{(float)r[0], (float)r[1], (float)r[2]};
+        out[si].pos_tsub1 = lima_float3{(float)r[3], (float)r[4], (float)r[5]};
     }
 }
 
