@@ -1133,6 +1133,28 @@ void launch_build_list(const PhysDev& d, const float4* pos, const uint32_t* orig
                                                                                     mixed ? 1 : 0);
 }
 
+namespace {
+__global__ void k_orig_state(PhysDev d, int cur, double* __restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= d.n) return;
+    const uint32_t o = d.orig_of_sorted[k];
+    const float4 p = d.pos[cur][k], v = d.vel[k];
+    double px = p.x, py = p.y, pz = p.z, vx = v.x, vy = v.y, vz = v.z;
+    if (d.precision == LIMA_PRECISION_MIXED) {
+        const float4 pc = d.posc[k], vc = d.velc[k];
+        px += pc.x; py += pc.y; pz += pc.z;
+        vx += vc.x; vy += vc.y; vz += vc.z;
+    }
+    double* r = out + 6 * (size_t)o;
+    r[0] = px; r[1] = py; r[2] = pz;
+    r[3] = px - vx * d.dt; r[4] = py - vy * d.dt; r[5] = pz - vz * d.dt;
+}
+}  // namespace
+
+void launch_orig_state(const PhysDev& d, int cur, double* out, cudaStream_t s) {
+    k_orig_state<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d, cur, out);
+}
+
 void launch_bonded(const PhysDev& d, int cur, bool energy, cudaStream_t s) {
     const int nb = bonded_blocks(d);
     const bool mixed = d.precision == LIMA_PRECISION_MIXED;

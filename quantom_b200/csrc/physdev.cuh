@@ -171,10 +171,11 @@ void phys_energy_now(PhysDev& d, int cur, cudaStream_t s);
 // that state (the caller changes it whenever the state may have changed).
 // The state in orig order as of one state version: per particle its position
 // (hi + lo) and previous position x - v dt in FP64, gathered on the device and
-// read back with one copy into pinned memory (buffers made by the first read).
+// read back with one copy (buffers made by the first read).
 struct PhysReadCache {
     uint64_t key = ~0ull;
-    double* host = nullptr;   // pinned [n][6]: x, y, z, then the previous position
+    double* host = nullptr;   // [n][6]: x, y, z, then the previous position
+    bool pinned = false;      // host is a pinned block (else plain memory)
     double* dev = nullptr;    // device staging of the same (from the pool)
     cudaStream_t stream = nullptr;
 };

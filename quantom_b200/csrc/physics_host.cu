@@ -612,28 +612,9 @@ Snapshot snapshot(const PhysDev& d, int cur, bool want_force) {
 }
 }  // namespace
 
-namespace {
-// per sorted slot: the particle's position and previous position x - v dt
-// (hi + lo in mixed precision) in FP64 at its orig id
-__global__ void k_orig_state(PhysDev d, int cur, double* __restrict__ out) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= d.n) return;
-    const uint32_t o = d.orig_of_sorted[k];
-    const float4 p = d.pos[cur][k], v = d.vel[k];
-    double px = p.x, py = p.y, pz = p.z, vx = v.x, vy = v.y, vz = v.z;
-    if (d.precision == LIMA_PRECISION_MIXED) {
-        const float4 pc = d.posc[k], vc = d.velc[k];
-        px += pc.x; py += pc.y; pz += pc.z;
-        vx += vc.x; vy += vc.y; vz += vc.z;
-    }
-    double* r = out + 6 * (size_t)o;
-    r[0] = px; r[1] = py; r[2] = pz;
-    r[3] = px - vx * d.dt; r[4] = py - vy * d.dt; r[5] = pz - vz * d.dt;
-}
-}  // namespace
-
 void phys_read_cache_free(PhysReadCache& cache) {
-    pinned_free(cache.host);
+    if (cache.pinned) pinned_free(cache.host);
+    else delete[] cache.host;
     if (cache.dev) {
         pool_free(cache.dev, cache.stream);
         cudaStreamSynchronize(cache.stream);
@@ -642,19 +623,27 @@ void phys_read_cache_free(PhysReadCache& cache) {
 }
 
 // the orig-ordered state of version `key` in cache.host (one gather kernel and one copy)
+// The first state read of a context lands in plain host memory (one copy);
+// a context that reads again, at a later state, moves to a pinned block.
 static void cached_orig_state(const PhysDev& d, int cur, PhysReadCache& cache, uint64_t key, cudaStream_t s) {
     if (cache.key == key && cache.host) return;
-    const size_t bytes = sizeof(double) * 6 * (size_t)std::max(d.n, 1);
-    if (!cache.host) {
+    const size_t n6 = 6 * (size_t)std::max(d.n, 1);
+    const size_t bytes = sizeof(double) * n6;
+    if (!cache.dev) {
         cache.stream = s;
         cache.dev = static_cast<double*>(pool_alloc(bytes, s));
-        cache.host = cache.dev ? static_cast<double*>(pinned_alloc(bytes)) : nullptr;
-        if (!cache.host) {
-            phys_read_cache_free(cache);
-            throw std::runtime_error("cannot allocate the readback buffers");
+        if (!cache.dev) throw std::runtime_error("cannot allocate the readback buffer");
+    }
+    if (!cache.host) {
+        cache.host = new double[n6];
+    } else if (!cache.pinned) {
+        if (double* p = static_cast<double*>(pinned_alloc(bytes))) {
+            delete[] cache.host;
+            cache.host = p;
+            cache.pinned = true;
         }
     }
-    k_orig_state<<<(d.n + 255) / 256, 256, 0, s>>>(d, cur, cache.dev);
+    launch_orig_state(d, cur, cache.dev, s);
     cudaMemcpyAsync(cache.host, cache.dev, bytes, cudaMemcpyDeviceToHost, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) throw std::runtime_error("the state readback failed");
     cache.key = key;
