@@ -215,7 +215,8 @@ lima_status lima_step(lima_ctx* ctx, int n_steps);
 lima_status lima_synchronize(lima_ctx* ctx);
 
 /* State readback in the reference layout (Box::compound_state_array,
-   Compound::prev_positions, Box::solvents). */
+   Compound::prev_positions, Box::solvents); compound slots past a compound's
+   n_particles are zero in both arrays.  Either compound array may be NULL. */
 lima_status lima_get_compound_states(lima_ctx* ctx, lima_compound_state* states, lima_float3* prev_positions);
 lima_status lima_get_solvents(lima_ctx* ctx, lima_solvent* solvents);
 /* The same positions as flat float arrays, for callers that do not use the

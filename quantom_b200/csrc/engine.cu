@@ -82,11 +82,8 @@ struct lima_ctx {
     uint64_t launches = 0;     // kernels of this library launched by this context
     int graph_kernels = 0;     // kernels in one replay of a step graph
     lima::FrameLog log;        // physics: frames recorded every log.every steps
-    // physics readbacks: the orig-ordered state of the last read, kept until the
-    // state changes (state_version names the state; every call that may change
-    // it moves it on)
-    lima::PhysReadCache read_cache;
-    uint64_t state_version = 0;
+    // physics readbacks: device copies of the reference's state structs (pool)
+    void* read_stage = nullptr;
     lima::RenderBuf render;    // headless rasterizer buffers (allocated by the first lima_render)
 
     template <typename T>
@@ -98,7 +95,6 @@ struct lima_ctx {
     }
     ~lima_ctx() {
         lima::framelog_free(log);
-        lima::phys_read_cache_free(read_cache);
         lima::phys_free_rebuild(phys);
         for (auto& g : graph)
             if (g) cudaGraphExecDestroy(g);
@@ -429,7 +425,6 @@ void ref_nlist_now(lima_ctx* c) {
 // the four per-kernel-group events of ref_step_kernels / phys_step_kernels;
 // with prof the step is launched directly instead of through the graph.
 void one_step(lima_ctx* c, cudaEvent_t* prof) {
-    c->state_version++;
     const int period = std::max(1, c->p.nlist_period);
     const bool rebuild = c->step > 0 && c->step - c->last_nlist_step >= static_cast<uint64_t>(period);
     // profiling a dynamic list: the host reads the rebuild request before the first event
@@ -795,28 +790,60 @@ lima_status lima_set_thermostat_scalar(lima_ctx* c, float scalar) {
     });
 }
 
+namespace {
+// physics semantics: device copies of the reference's state structs (one pool
+// block per context, made by the first read)
+struct PhysStage {
+    lima_compound_state* states;
+    lima_float3* prev;
+    lima_solvent* sols;
+};
+PhysStage phys_stage(lima_ctx* c) {
+    const size_t nc = c->comps.size(), ns = c->sols.size();
+    const size_t b_states = (nc * sizeof(lima_compound_state) + 255) & ~size_t(255);
+    const size_t b_prev = (nc * lima::kMaxCP * sizeof(lima_float3) + 255) & ~size_t(255);
+    if (!c->read_stage) {
+        c->read_stage = lima::pool_alloc(b_states + b_prev + ns * sizeof(lima_solvent), c->stream);
+        need(c->read_stage != nullptr, LIMA_ERR_CUDA, "cannot allocate the readback buffer");
+        c->pool_allocs.push_back(c->read_stage);
+    }
+    uint8_t* b = static_cast<uint8_t*>(c->read_stage);
+    return {reinterpret_cast<lima_compound_state*>(b), reinterpret_cast<lima_float3*>(b + b_states),
+            reinterpret_cast<lima_solvent*>(b + b_states + b_prev)};
+}
+}  // namespace
+
 lima_status lima_get_compound_states(lima_ctx* c, lima_compound_state* states, lima_float3* prev) {
     return guarded(c, [&] {
         need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
         sync_checked(c);
         const int nc = static_cast<int>(c->comps.size());
         const size_t ncp = static_cast<size_t>(nc) * lima::kMaxCP;
-        std::vector<float4> hp(ncp), hq(ncp);
-        if (c->p.semantics == LIMA_SEMANTICS_REFERENCE) {
-            cuda_ok(cudaMemcpy(hp.data(), c->ref.cpos[c->cur], sizeof(float4) * ncp, cudaMemcpyDeviceToHost), "D2H");
-            cuda_ok(cudaMemcpy(hq.data(), c->ref.cprev, sizeof(float4) * ncp, cudaMemcpyDeviceToHost), "D2H");
-        } else {
-            lima::phys_read_compounds(c->phys, c->cur, c->comps.data(), hp.data(), hq.data(), c->read_cache, c->state_version, c->stream);
+        if (c->p.semantics == LIMA_SEMANTICS_PHYSICS) {
+            // one kernel writes the structs on the device; one copy each into the caller's arrays
+            if (nc == 0 || (!states && !prev)) return;
+            const PhysStage st = phys_stage(c);
+            lima::launch_read_compounds(c->phys, c->cur, states ? st.states : nullptr, prev ? st.prev : nullptr,
+                                        c->stream);
+            if (states)
+                cudaMemcpyAsync(states, st.states, sizeof(lima_compound_state) * nc, cudaMemcpyDeviceToHost, c->stream);
+            if (prev) cudaMemcpyAsync(prev, st.prev, sizeof(lima_float3) * ncp, cudaMemcpyDeviceToHost, c->stream);
+            sync_checked(c);
+            return;
         }
+        std::vector<float4> hp(ncp), hq(ncp);
+        cuda_ok(cudaMemcpy(hp.data(), c->ref.cpos[c->cur], sizeof(float4) * ncp, cudaMemcpyDeviceToHost), "D2H");
+        cuda_ok(cudaMemcpy(hq.data(), c->ref.cprev, sizeof(float4) * ncp, cudaMemcpyDeviceToHost), "D2H");
         for (int i = 0; i < nc; i++) {
             if (states) {
                 std::memset(&states[i], 0, sizeof(lima_compound_state));
                 states[i].n_particles = c->comps[i].n_particles;
             }
-            for (int t = 0; t < c->comps[i].n_particles; t++) {
+            for (int t = 0; t < lima::kMaxCP; t++) {
+                const bool live = t < c->comps[i].n_particles;
                 const float4 a = hp[i * lima::kMaxCP + t], b = hq[i * lima::kMaxCP + t];
-                if (states) states[i].positions[t] = lima_float3{a.x, a.y, a.z};
-                if (prev) prev[i * lima::kMaxCP + t] = lima_float3{b.x, b.y, b.z};
+                if (states && live) states[i].positions[t] = lima_float3{a.x, a.y, a.z};
+                if (prev) prev[i * lima::kMaxCP + t] = live ? lima_float3{b.x, b.y, b.z} : lima_float3{0.f, 0.f, 0.f};
             }
         }
     });
@@ -828,16 +855,20 @@ lima_status lima_get_solvents(lima_ctx* c, lima_solvent* sols) {
         need(sols != nullptr || c->sols.empty(), LIMA_ERR_ARGUMENT, "null solvent array");
         sync_checked(c);
         const int ns = static_cast<int>(c->sols.size());
-        if (c->p.semantics == LIMA_SEMANTICS_REFERENCE) {
-            std::vector<float4> a(ns), b(ns);
-            cuda_ok(cudaMemcpy(a.data(), c->ref.spos[c->cur], sizeof(float4) * ns, cudaMemcpyDeviceToHost), "D2H");
-            cuda_ok(cudaMemcpy(b.data(), c->ref.sprev[c->cur], sizeof(float4) * ns, cudaMemcpyDeviceToHost), "D2H");
-            for (int i = 0; i < ns; i++) {
-                sols[i].pos = lima_float3{a[i].x, a[i].y, a[i].z};
-                sols[i].pos_tsub1 = lima_float3{b[i].x, b[i].y, b[i].z};
-            }
-        } else {
-            lima::phys_read_solvent_structs(c->phys, c->cur, sols, c->read_cache, c->state_version, c->stream);
+        if (ns == 0) return;
+        if (c->p.semantics == LIMA_SEMANTICS_PHYSICS) {
+            const PhysStage st = phys_stage(c);
+            lima::launch_read_solvents(c->phys, c->cur, st.sols, c->stream);
+            cudaMemcpyAsync(sols, st.sols, sizeof(lima_solvent) * ns, cudaMemcpyDeviceToHost, c->stream);
+            sync_checked(c);
+            return;
+        }
+        std::vector<float4> a(ns), b(ns);
+        cuda_ok(cudaMemcpy(a.data(), c->ref.spos[c->cur], sizeof(float4) * ns, cudaMemcpyDeviceToHost), "D2H");
+        cuda_ok(cudaMemcpy(b.data(), c->ref.sprev[c->cur], sizeof(float4) * ns, cudaMemcpyDeviceToHost), "D2H");
+        for (int i = 0; i < ns; i++) {
+            sols[i].pos = lima_float3{a[i].x, a[i].y, a[i].z};
+            sols[i].pos_tsub1 = lima_float3{b[i].x, b[i].y, b[i].z};
         }
     });
 }
@@ -848,12 +879,23 @@ lima_status lima_get_positions(lima_ctx* c, float* cxyz, float* sxyz) {
         sync_checked(c);
         const int nc = static_cast<int>(c->comps.size()), ns = static_cast<int>(c->sols.size());
         const size_t ncp = static_cast<size_t>(nc) * lima::kMaxCP;
-        std::vector<float4> hp(ncp), hq(ncp), a(ns), b(ns);
-        if (cxyz) {
-            if (c->p.semantics == LIMA_SEMANTICS_REFERENCE)
+        const bool phys = c->p.semantics == LIMA_SEMANTICS_PHYSICS;
+        if (cxyz && nc > 0) {
+            std::vector<float4> hp(ncp);
+            if (phys) {
+                // the same values lima_get_compound_states gives
+                std::vector<lima_compound_state> st(nc);
+                const PhysStage g = phys_stage(c);
+                lima::launch_read_compounds(c->phys, c->cur, g.states, nullptr, c->stream);
+                cudaMemcpyAsync(st.data(), g.states, sizeof(lima_compound_state) * nc, cudaMemcpyDeviceToHost, c->stream);
+                sync_checked(c);
+                for (size_t k = 0; k < ncp; k++) {
+                    const lima_float3 v = st[k / lima::kMaxCP].positions[k % lima::kMaxCP];
+                    hp[k] = make_float4(v.x, v.y, v.z, 0.f);
+                }
+            } else {
                 cuda_ok(cudaMemcpy(hp.data(), c->ref.cpos[c->cur], sizeof(float4) * ncp, cudaMemcpyDeviceToHost), "D2H");
-            else
-                lima::phys_read_compounds(c->phys, c->cur, c->comps.data(), hp.data(), hq.data(), c->read_cache, c->state_version, c->stream);
+            }
             for (int i = 0; i < nc; i++)
                 for (int t = 0; t < lima::kMaxCP; t++) {
                     const size_t k = static_cast<size_t>(i) * lima::kMaxCP + t;
@@ -864,14 +906,25 @@ lima_status lima_get_positions(lima_ctx* c, float* cxyz, float* sxyz) {
                 }
         }
         if (sxyz && ns > 0) {
-            if (c->p.semantics == LIMA_SEMANTICS_REFERENCE)
+            if (phys) {
+                std::vector<lima_solvent> sv(ns);
+                const PhysStage g = phys_stage(c);
+                lima::launch_read_solvents(c->phys, c->cur, g.sols, c->stream);
+                cudaMemcpyAsync(sv.data(), g.sols, sizeof(lima_solvent) * ns, cudaMemcpyDeviceToHost, c->stream);
+                sync_checked(c);
+                for (int i = 0; i < ns; i++) {
+                    sxyz[3 * i] = sv[i].pos.x;
+                    sxyz[3 * i + 1] = sv[i].pos.y;
+                    sxyz[3 * i + 2] = sv[i].pos.z;
+                }
+            } else {
+                std::vector<float4> a(ns);
                 cuda_ok(cudaMemcpy(a.data(), c->ref.spos[c->cur], sizeof(float4) * ns, cudaMemcpyDeviceToHost), "D2H");
-            else
-                lima::phys_read_solvents(c->phys, c->cur, a.data(), b.data(), c->read_cache, c->state_version, c->stream);
-            for (int i = 0; i < ns; i++) {
-                sxyz[3 * i] = a[i].x;
-                sxyz[3 * i + 1] = a[i].y;
-                sxyz[3 * i + 2] = a[i].z;
+                for (int i = 0; i < ns; i++) {
+                    sxyz[3 * i] = a[i].x;
+                    sxyz[3 * i + 1] = a[i].y;
+                    sxyz[3 * i + 2] = a[i].z;
+                }
             }
         }
     });
@@ -880,7 +933,6 @@ lima_status lima_get_positions(lima_ctx* c, float* cxyz, float* sxyz) {
 lima_status lima_set_state(lima_ctx* c, const lima_compound_state* states, const lima_float3* prev,
                            const lima_solvent* sols) {
     return guarded(c, [&] {
-        c->state_version++;
         need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
         sync_checked(c);
         const int nc = static_cast<int>(c->comps.size()), ns = static_cast<int>(c->sols.size());
@@ -997,7 +1049,6 @@ lima_status lima_get_energies(lima_ctx* c, double* totals, double* per_particle)
 
 lima_status lima_build_nlist(lima_ctx* c) {
     return guarded(c, [&] {
-        c->state_version++;
         need(c->finished, LIMA_ERR_STATE, "lima_finish_box has not run");
         if (c->p.semantics == LIMA_SEMANTICS_REFERENCE) {
             ref_nlist_now(c);
@@ -1064,7 +1115,6 @@ lima_status lima_get_params(lima_ctx* c, double* theta) {
 
 lima_status lima_set_params(lima_ctx* c, const double* theta) {
     return guarded(c, [&] {
-        c->state_version++;
         need(theta != nullptr, LIMA_ERR_ARGUMENT, "null parameter vector");
         need_physics(c);
         sync_checked(c);
@@ -1080,7 +1130,6 @@ lima_status lima_set_params(lima_ctx* c, const double* theta) {
 
 lima_status lima_loss(lima_ctx* c, const lima_loss_spec* spec, double* loss) {
     return guarded(c, [&] {
-        c->state_version++;
         need(spec != nullptr && loss != nullptr, LIMA_ERR_ARGUMENT, "null spec or output");
         need_gradable(c);
         sync_checked(c);
@@ -1094,7 +1143,6 @@ lima_status lima_loss(lima_ctx* c, const lima_loss_spec* spec, double* loss) {
 
 lima_status lima_grad(lima_ctx* c, const lima_loss_spec* spec, double* loss, double* grad) {
     return guarded(c, [&] {
-        c->state_version++;
         need(spec != nullptr && loss != nullptr && grad != nullptr, LIMA_ERR_ARGUMENT, "null spec or output");
         need_gradable(c);
         sync_checked(c);

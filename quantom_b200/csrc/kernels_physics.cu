@@ -1134,25 +1134,70 @@ void launch_build_list(const PhysDev& d, const float4* pos, const uint32_t* orig
 }
 
 namespace {
-__global__ void k_orig_state(PhysDev d, int cur, double* __restrict__ out) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= d.n) return;
-    const uint32_t o = d.orig_of_sorted[k];
-    const float4 p = d.pos[cur][k], v = d.vel[k];
-    double px = p.x, py = p.y, pz = p.z, vx = v.x, vy = v.y, vz = v.z;
+// position and half-step velocity of orig id o in FP64 (hi + lo)
+__device__ __forceinline__ void state_of_orig(const PhysDev& d, int cur, uint32_t o, double* x, double* v) {
+    const uint32_t k = d.sorted_of_orig[o];
+    const float4 p = d.pos[cur][k], w = d.vel[k];
+    x[0] = p.x; x[1] = p.y; x[2] = p.z;
+    v[0] = w.x; v[1] = w.y; v[2] = w.z;
     if (d.precision == LIMA_PRECISION_MIXED) {
-        const float4 pc = d.posc[k], vc = d.velc[k];
-        px += pc.x; py += pc.y; pz += pc.z;
-        vx += vc.x; vy += vc.y; vz += vc.z;
+        const float4 pc = d.posc[k], wc = d.velc[k];
+        x[0] += pc.x; x[1] += pc.y; x[2] += pc.z;
+        v[0] += wc.x; v[1] += wc.y; v[2] += wc.z;
     }
-    double* r = out + 6 * (size_t)o;
-    r[0] = px; r[1] = py; r[2] = pz;
-    r[3] = px - vx * d.dt; r[4] = py - vy * d.dt; r[5] = pz - vz * d.dt;
+}
+
+// one thread per compound slot (c, t)
+__global__ void k_read_compounds(PhysDev d, int cur, lima_compound_state* __restrict__ states,
+                                 lima_float3* __restrict__ prev) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= d.n_c * LIMA_MAX_COMPOUND_PARTICLES) return;
+    const int c = q / LIMA_MAX_COMPOUND_PARTICLES, t = q % LIMA_MAX_COMPOUND_PARTICLES;
+    const uint32_t b = d.cp_base[c];
+    const int n = (int)(d.cp_base[c + 1] - b);
+    lima_float3 a = {0.f, 0.f, 0.f}, r = {0.f, 0.f, 0.f};
+    if (t < n) {
+        double x[3], v[3], x0[3], vv[3];
+        state_of_orig(d, cur, b + t, x, v);
+        state_of_orig(d, cur, b, x0, vv);
+        const double L = d.L;
+        double qq[3];
+        for (int k = 0; k < 3; k++) {
+            double dd = x[k] - x0[k];
+            dd -= L * nearbyint(dd / L);
+            qq[k] = t == 0 ? x[k] : x0[k] + dd;
+        }
+        a = lima_float3{(float)qq[0], (float)qq[1], (float)qq[2]};
+        r = lima_float3{(float)(qq[0] - v[0] * d.dt), (float)(qq[1] - v[1] * d.dt), (float)(qq[2] - v[2] * d.dt)};
+    }
+    if (states) {
+        states[c].positions[t] = a;
+        if (t == 0) {
+            // the count and the struct's padding bytes
+            uint32_t* tail = reinterpret_cast<uint32_t*>(&states[c].n_particles);
+            *tail = (uint32_t)n;
+        }
+    }
+    if (prev) prev[q] = r;
+}
+
+__global__ void k_read_solvents(PhysDev d, int cur, lima_solvent* __restrict__ out) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= d.n_s) return;
+    double x[3], v[3];
+    state_of_orig(d, cur, (uint32_t)(d.n_cp + s), x, v);
+    out[s].pos = lima_float3{(float)x[0], (float)x[1], (float)x[2]};
+    out[s].pos_tsub1 = lima_float3{(float)(x[0] - v[0] * d.dt), (float)(x[1] - v[1] * d.dt), (float)(x[2] - v[2] * d.dt)};
 }
 }  // namespace
 
-void launch_orig_state(const PhysDev& d, int cur, double* out, cudaStream_t s) {
-    k_orig_state<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d, cur, out);
+void launch_read_compounds(const PhysDev& d, int cur, lima_compound_state* states, lima_float3* prev, cudaStream_t s) {
+    const int n = d.n_c * LIMA_MAX_COMPOUND_PARTICLES;
+    if (n > 0) k_read_compounds<<<(n + kTB - 1) / kTB, kTB, 0, s>>>(d, cur, states, prev);
+}
+
+void launch_read_solvents(const PhysDev& d, int cur, lima_solvent* out, cudaStream_t s) {
+    if (d.n_s > 0) k_read_solvents<<<(d.n_s + kTB - 1) / kTB, kTB, 0, s>>>(d, cur, out);
 }
 
 void launch_bonded(const PhysDev& d, int cur, bool energy, cudaStream_t s) {

@@ -69,6 +69,7 @@ struct PhysDev {
     float4* posc_orig[2];       // [n_cp] their low parts (mixed precision)
     uint32_t* orig_of_sorted;   // [n]
     uint32_t* sorted_of_orig;   // [n]
+    uint32_t* cp_base;          // [n_c + 1] orig id of each compound's particle 0 (n_cp at the end)
     float2* lj_table;           // [n_types^2] (sigma^2, 4 eps), Lorentz-Berthelot
     // cell grid and the counting sort by cell (stable: ascending slot inside a cell)
     int m;                      // cells per dimension
@@ -169,25 +170,13 @@ void phys_energy_now(PhysDev& d, int cur, cudaStream_t s);
 // Host copy of the state in orig order (position and previous position, in
 // double), kept while the state it was read from is unchanged: `key` names
 // that state (the caller changes it whenever the state may have changed).
-// The state in orig order as of one state version: per particle its position
-// (hi + lo) and previous position x - v dt in FP64, gathered on the device and
-// read back with one copy (buffers made by the first read).
-struct PhysReadCache {
-    uint64_t key = ~0ull;
-    double* host = nullptr;   // [n][6]: x, y, z, then the previous position
-    bool pinned = false;      // host is a pinned block (else plain memory)
-    double* dev = nullptr;    // device staging of the same (from the pool)
-    cudaStream_t stream = nullptr;
-};
-void phys_read_cache_free(PhysReadCache& cache);
-// both throw std::runtime_error when the buffers cannot be made
-void phys_read_compounds(const PhysDev& d, int cur, const lima_compound* comps, float4* pos_out, float4* prev_out,
-                         PhysReadCache& cache, uint64_t key, cudaStream_t s);
-void phys_read_solvents(const PhysDev& d, int cur, float4* pos_out, float4* prev_out, PhysReadCache& cache,
-                        uint64_t key, cudaStream_t s);
-// the same straight into the reference's Solvent structs
-void phys_read_solvent_structs(const PhysDev& d, int cur, lima_solvent* out, PhysReadCache& cache, uint64_t key,
-                               cudaStream_t s);
+// The state in the reference's layout, straight into device copies of its
+// structs: every compound slot (particle 0 in the box, the others in the image
+// nearest to it, Engine.cu:993-996; previous position x - v dt in the same
+// image; empty slots zero) and every solvent (position, previous position).
+// Either compound output may be null.
+void launch_read_compounds(const PhysDev& d, int cur, lima_compound_state* states, lima_float3* prev, cudaStream_t s);
+void launch_read_solvents(const PhysDev& d, int cur, lima_solvent* out, cudaStream_t s);
 void phys_read_forces(const PhysDev& d, const lima_compound* comps, float4* fc, float4* fs);
 // the Verlet list as CSR over orig ids (offsets[n + 1]; ids, nullable, sorted
 // ascending in each row); returns the total entry count

@@ -304,6 +304,7 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
         for (int b = 0; b < 2; b++) d.posc_orig[b] = a.take<float4>(std::max(1, d.n_cp));
         d.orig_of_sorted = a.take<uint32_t>(d.n_pad);
         d.sorted_of_orig = a.take<uint32_t>(d.n);
+        d.cp_base = a.take<uint32_t>((size_t)h.n_c + 1);
         d.lj_table = a.take<float2>(tab.size());
         d.cell_key = a.take<uint32_t>(d.n);
         d.cell_rank = a.take<uint32_t>(d.n);
@@ -352,6 +353,8 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
     auto up = [&](void* dst, const void* src, size_t bytes) {
         if (bytes) cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
     };
+    std::vector<uint32_t> cbase(base.begin(), base.end());
+    up(d.cp_base, cbase.data(), sizeof(uint32_t) * cbase.size());
     up(d.lj_table, tab.data(), sizeof(float2) * tab.size());
     up(d.excl_off, eoff.data(), sizeof(uint32_t) * eoff.size());
     up(d.excl_ids, eids.data(), sizeof(uint32_t) * eids.size());
@@ -611,91 +614,6 @@ Snapshot snapshot(const PhysDev& d, int cur, bool want_force) {
     return sn;
 }
 }  // namespace
-
-void phys_read_cache_free(PhysReadCache& cache) {
-    if (cache.pinned) pinned_free(cache.host);
-    else delete[] cache.host;
-    if (cache.dev) {
-        pool_free(cache.dev, cache.stream);
-        cudaStreamSynchronize(cache.stream);
-    }
-    cache = PhysReadCache{};
-}
-
-// the orig-ordered state of version `key` in cache.host (one gather kernel and one copy)
-// The first state read of a context lands in plain host memory (one copy);
-// a context that reads again, at a later state, moves to a pinned block.
-static void cached_orig_state(const PhysDev& d, int cur, PhysReadCache& cache, uint64_t key, cudaStream_t s) {
-    if (cache.key == key && cache.host) return;
-    const size_t n6 = 6 * (size_t)std::max(d.n, 1);
-    const size_t bytes = sizeof(double) * n6;
-    if (!cache.dev) {
-        cache.stream = s;
-        cache.dev = static_cast<double*>(pool_alloc(bytes, s));
-        if (!cache.dev) throw std::runtime_error("cannot allocate the readback buffer");
-    }
-    if (!cache.host) {
-        cache.host = new double[n6];
-    } else if (!cache.pinned) {
-        if (double* p = static_cast<double*>(pinned_alloc(bytes))) {
-            delete[] cache.host;
-            cache.host = p;
-            cache.pinned = true;
-        }
-    }
-    launch_orig_state(d, cur, cache.dev, s);
-    cudaMemcpyAsync(cache.host, cache.dev, bytes, cudaMemcpyDeviceToHost, s);
-    if (cudaStreamSynchronize(s) != cudaSuccess) throw std::runtime_error("the state readback failed");
-    cache.key = key;
-}
-
-// compound positions in the reference's convention: particle 0 in the box,
-// the others as the image nearest to it (Engine.cu:993-996)
-void phys_read_compounds(const PhysDev& d, int cur, const lima_compound* comps, float4* pos_out, float4* prev_out,
-                         PhysReadCache& cache, uint64_t key, cudaStream_t s) {
-    cached_orig_state(d, cur, cache, key, s);
-    const double* h = cache.host;
-    const double L = d.L;
-    int o = 0;
-    for (int c = 0; c < d.n_c; c++) {
-        const int n = comps[c].n_particles;
-        const double* p0 = &h[6 * (size_t)o];
-        for (int t = 0; t < n; t++) {
-            const double* pt = &h[6 * (size_t)(o + t)];
-            const double* qt = pt + 3;
-            double q[3], r[3];
-            for (int k = 0; k < 3; k++) {
-                double dd = pt[k] - p0[k];
-                dd -= L * std::nearbyint(dd / L);
-                q[k] = t == 0 ? pt[k] : p0[k] + dd;
-                r[k] = q[k] - (pt[k] - qt[k]);
-            }
-            pos_out[c * 64 + t] = make_float4((float)q[0], (float)q[1], (float)q[2], 0.f);
-            prev_out[c * 64 + t] = make_float4((float)r[0], (float)r[1], (float)r[2], 0.f);
-        }
-        o += n;
-    }
-}
-
-void phys_read_solvents(const PhysDev& d, int cur, float4* pos_out, float4* prev_out, PhysReadCache& cache,
-                        uint64_t key, cudaStream_t s) {
-    cached_orig_state(d, cur, cache, key, s);
-    for (int si = 0; si < d.n_s; si++) {
-        const double* r = &cache.host[6 * (size_t)(d.n_cp + si)];
-        pos_out[si] = make_float4((float)r[0], (float)r[1], (float)r[2], 0.f);
-        prev_out[si] = make_float4((float)r[3], (float)r[4], (float)r[5], 0.f);
-    }
-}
-
-void phys_read_solvent_structs(const PhysDev& d, int cur, lima_solvent* out, PhysReadCache& cache, uint64_t key,
-                               cudaStream_t s) {
-    cached_orig_state(d, cur, cache, key, s);
-    for (int si = 0; si < d.n_s; si++) {
-        const double* r = &cache.host[6 * (size_t)(d.n_cp + si)];
-        out[si].pos = lima_float3{(float)r[0], (float)r[1], (float)r[2]};
-        out[si].pos_tsub1 = lima_float3{(float)r[3], (float)r[4], (float)r[5]};
-    }
-}
 
 void phys_read_forces(const PhysDev& d, const lima_compound* comps, float4* fc, float4* fs) {
     Snapshot sn = snapshot(d, 0, true);

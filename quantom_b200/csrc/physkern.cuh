@@ -38,9 +38,6 @@ __host__ __device__ inline int bonded_blocks(const PhysDev& d) {
 }
 
 // the counting sort of the slots by the cell of `pos`: cell_key, cstart, order
-// per sorted slot: position and previous position x - v dt (hi + lo) in FP64
-// at the particle's orig id, out[orig][6]
-void launch_orig_state(const PhysDev& d, int cur, double* out, cudaStream_t s);
 void launch_sort(const PhysDev& d, const float4* pos, cudaStream_t s);
 // every per-slot array into cell order in the tmp arrays, reference positions
 void launch_permute(const PhysDev& d, int cur, bool mixed, cudaStream_t s);
