@@ -293,7 +293,26 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
     d.nl_cap = std::max(d.nl_cap, 4 * kGroup);
 
     // every fixed-size buffer in one allocation; the list separately (it may grow)
+    // the topology arrays first and together: the host builds their image
+    // with the same offsets and uploads it in one copy
+    auto carve_topology = [&](Arena& a) {
+        d.cp_base = a.take<uint32_t>((size_t)h.n_c + 1);
+        d.lj_table = a.take<float2>(tab.size());
+        d.excl_off = a.take<uint32_t>(eoff.size());
+        d.excl_ids = a.take<uint32_t>(eids.size());
+        d.bond_idx = a.take<int4>(bidx.size());
+        d.bond_par = a.take<float2>(bpar.size());
+        d.angle_idx = a.take<int4>(aidx.size());
+        d.angle_par = a.take<float2>(apar.size());
+        d.dih_idx = a.take<int4>(didx.size());
+        d.dih_par = a.take<float4>(dpar.size());
+        d.bterm_off = a.take<uint32_t>(boff.size());
+        d.bterm_slot = a.take<uint32_t>(bslot.size());
+    };
+    size_t topo_bytes = 0;
     auto carve = [&](Arena& a) {
+        carve_topology(a);
+        topo_bytes = a.off;
         for (int b = 0; b < 2; b++) d.pos[b] = a.take<float4>(d.n_pad);
         d.vel = a.take<float4>(d.n_pad);
         d.posc = a.take<float4>(d.n_pad);
@@ -304,8 +323,6 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
         for (int b = 0; b < 2; b++) d.posc_orig[b] = a.take<float4>(std::max(1, d.n_cp));
         d.orig_of_sorted = a.take<uint32_t>(d.n_pad);
         d.sorted_of_orig = a.take<uint32_t>(d.n);
-        d.cp_base = a.take<uint32_t>((size_t)h.n_c + 1);
-        d.lj_table = a.take<float2>(tab.size());
         d.cell_key = a.take<uint32_t>(d.n);
         d.cell_rank = a.take<uint32_t>(d.n);
         d.ccount = a.take<uint32_t>(d.n_cells);
@@ -319,16 +336,6 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
         d.orig_tmp = a.take<uint32_t>(d.n);
         d.nl_cnt = a.take<uint32_t>(d.n_pad);
         d.nl_need = a.take<int>(1);
-        d.excl_off = a.take<uint32_t>(eoff.size());
-        d.excl_ids = a.take<uint32_t>(eids.size());
-        d.bond_idx = a.take<int4>(bidx.size());
-        d.bond_par = a.take<float2>(bpar.size());
-        d.angle_idx = a.take<int4>(aidx.size());
-        d.angle_par = a.take<float2>(apar.size());
-        d.dih_idx = a.take<int4>(didx.size());
-        d.dih_par = a.take<float4>(dpar.size());
-        d.bterm_off = a.take<uint32_t>(boff.size());
-        d.bterm_slot = a.take<uint32_t>(bslot.size());
         d.term_force = a.take<float4>(d.n_term_slots);
         d.part = a.take<double>((size_t)step_blocks(d) * kRedStride);
         d.bpart = a.take<double>((size_t)bonded_blocks(d) * 4);
@@ -350,22 +357,28 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
         msg = std::string("device allocation failed: ") + e.what();
         return LIMA_ERR_CUDA;
     }
-    auto up = [&](void* dst, const void* src, size_t bytes) {
-        if (bytes) cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
-    };
-    std::vector<uint32_t> cbase(base.begin(), base.end());
-    up(d.cp_base, cbase.data(), sizeof(uint32_t) * cbase.size());
-    up(d.lj_table, tab.data(), sizeof(float2) * tab.size());
-    up(d.excl_off, eoff.data(), sizeof(uint32_t) * eoff.size());
-    up(d.excl_ids, eids.data(), sizeof(uint32_t) * eids.size());
-    up(d.bond_idx, bidx.data(), sizeof(int4) * bidx.size());
-    up(d.bond_par, bpar.data(), sizeof(float2) * bpar.size());
-    up(d.angle_idx, aidx.data(), sizeof(int4) * aidx.size());
-    up(d.angle_par, apar.data(), sizeof(float2) * apar.size());
-    up(d.dih_idx, didx.data(), sizeof(int4) * didx.size());
-    up(d.dih_par, dpar.data(), sizeof(float4) * dpar.size());
-    up(d.bterm_off, boff.data(), sizeof(uint32_t) * boff.size());
-    up(d.bterm_slot, bslot.data(), sizeof(uint32_t) * bslot.size());
+    // the topology image: each array at the offset its device copy has
+    {
+        std::vector<uint8_t> img(topo_bytes, 0);
+        const uintptr_t dev0 = reinterpret_cast<uintptr_t>(d.cp_base);
+        auto put = [&](const void* dst, const void* src, size_t bytes) {
+            if (bytes) std::memcpy(img.data() + (reinterpret_cast<uintptr_t>(dst) - dev0), src, bytes);
+        };
+        std::vector<uint32_t> cbase(base.begin(), base.end());
+        put(d.cp_base, cbase.data(), sizeof(uint32_t) * cbase.size());
+        put(d.lj_table, tab.data(), sizeof(float2) * tab.size());
+        put(d.excl_off, eoff.data(), sizeof(uint32_t) * eoff.size());
+        put(d.excl_ids, eids.data(), sizeof(uint32_t) * eids.size());
+        put(d.bond_idx, bidx.data(), sizeof(int4) * bidx.size());
+        put(d.bond_par, bpar.data(), sizeof(float2) * bpar.size());
+        put(d.angle_idx, aidx.data(), sizeof(int4) * aidx.size());
+        put(d.angle_par, apar.data(), sizeof(float2) * apar.size());
+        put(d.dih_idx, didx.data(), sizeof(int4) * didx.size());
+        put(d.dih_par, dpar.data(), sizeof(float4) * dpar.size());
+        put(d.bterm_off, boff.data(), sizeof(uint32_t) * boff.size());
+        put(d.bterm_slot, bslot.data(), sizeof(uint32_t) * bslot.size());
+        cudaMemcpyAsync(d.cp_base, img.data(), topo_bytes, cudaMemcpyHostToDevice, s);   // pageable: copied at the call
+    }
     cudaMemsetAsync(d.ccount, 0, sizeof(uint32_t) * d.n_cells, s);
     cudaMemsetAsync(d.done, 0, sizeof(unsigned int), s);
     cudaMemsetAsync(d.e_last, 0, sizeof(double) * LIMA_E_COUNT, s);
