@@ -455,6 +455,7 @@ namespace {
 __device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
+#if LIMA_STAGED_LIST
 // Bulk copies global -> shared memory completing on an mbarrier (the copy
 // engine, not the threads, moves the bytes).  Sources are this GPU's own
 // memory; there is no cluster multicast.
@@ -492,6 +493,7 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                  "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
 }
+#endif  // LIMA_STAGED_LIST
 
 // lane 0 receives the warp's sum of v[0..K); then thread 0 adds the warps in
 // order into out[0..K) (fixed order)
@@ -728,7 +730,9 @@ __device__ __forceinline__ void finish_sums(const PhysDev& d, int slot, cudaGrap
 // position loads in flight per lane in the mixed-precision pair loop: the
 // mixed step kernel needs more than 48 registers either way (4 blocks of 256
 // per SM), and four in flight measured 71 against 79 us per flushed step
+#if !LIMA_STAGED_LIST
 constexpr int kMixedGathers = 4;
+#endif
 
 // Offset of a lane's m-th list entry from its first: with 8 lanes entry m is
 // in row m; with 4 lanes entries alternate between columns g and g + 4 of
@@ -782,6 +786,7 @@ __device__ __forceinline__ void pair_rows(const PhysDev& d, const float2* row, f
     }
 }
 
+#if LIMA_STAGED_LIST
 // One lane's entries of one staged group of list rows: entry q of the lane
 // at srow[q * kTB] (shared memory); MIXED: one compensated sum per group.
 template <bool MIXED, bool ENERGY, bool SWITCH, bool WRAP>
@@ -877,6 +882,7 @@ __device__ __forceinline__ void pair_walk_staged(const PhysDev& d, const float2*
         for (int st = max(0, issued - 2); st < issued; st++) mbar_wait_bounded(&s_bar[st & 1], (uint32_t)(st >> 1) & 1u);
     __syncthreads();
 }
+#endif  // LIMA_STAGED_LIST
 
 template <bool MIXED, bool ENERGY, bool INTEGRATE, bool SWITCH, bool TAIL>
 __device__ __forceinline__ void step_body(const PhysDev& d, int cur, int slot, cudaGraphExec_t tail) {
@@ -901,17 +907,18 @@ __device__ __forceinline__ void step_body(const PhysDev& d, int cur, int slot, c
     const int rows = cnt > g ? (cnt - g + kStepLanes - 1) / kStepLanes : 0;
     // warps whose particles are all away from the box faces skip the minimum image
     const bool nowrap = __all_sync(0xffffffffu, !active || away_from_faces(d, pi));
-    if constexpr (kStagedList) {
-        pair_walk_staged<MIXED, ENERGY, SWITCH>(d, row, pi, pos, rows, active, nowrap, fx, fy, fz, cxx, cyy, czz, e_i,
-                                                w_i);
-    } else {
-        if (nowrap)
-            pair_rows<MIXED, ENERGY, SWITCH, false, MIXED ? kMixedGathers : 4>(d, row, pi, pos, nl, stride, rows, fx,
-                                                                               fy, fz, cxx, cyy, czz, e_i, w_i);
-        else
-            pair_rows<MIXED, ENERGY, SWITCH, true, MIXED ? kMixedGathers : 4>(d, row, pi, pos, nl, stride, rows, fx,
-                                                                              fy, fz, cxx, cyy, czz, e_i, w_i);
-    }
+#if LIMA_STAGED_LIST
+    (void)nl;
+    (void)stride;
+    pair_walk_staged<MIXED, ENERGY, SWITCH>(d, row, pi, pos, rows, active, nowrap, fx, fy, fz, cxx, cyy, czz, e_i, w_i);
+#else
+    if (nowrap)
+        pair_rows<MIXED, ENERGY, SWITCH, false, MIXED ? kMixedGathers : 4>(d, row, pi, pos, nl, stride, rows, fx, fy,
+                                                                           fz, cxx, cyy, czz, e_i, w_i);
+    else
+        pair_rows<MIXED, ENERGY, SWITCH, true, MIXED ? kMixedGathers : 4>(d, row, pi, pos, nl, stride, rows, fx, fy,
+                                                                          fz, cxx, cyy, czz, e_i, w_i);
+#endif
     // reduce the kStepLanes lanes of this particle (warp shuffles)
 #pragma unroll
     for (int o = kStepLanes / 2; o > 0; o >>= 1) {
