@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(kAdjTB) k_loss_pairs(PhysDev d, const float4* 
         const int ti = __float_as_int(pi.w);
         const int cnt = (int)d.nl_cnt[i];
         for (int k = g; k < cnt; k += kGroup) {
-            const uint32_t j = d.nl[nl_at(d, i, k)];
+            const uint32_t j = nl_load(d, nl_at(d, i, k));
             const float4 pj = pos[j];
             const float dx = mimg_a(pi.x - pj.x, d.L, d.invL), dy = mimg_a(pi.y - pj.y, d.L, d.invL),
                         dz = mimg_a(pi.z - pj.z, d.L, d.invL);
@@ -369,7 +369,7 @@ __global__ void __launch_bounds__(kAdjTB) k_adj_pair(PhysDev d, const float4* __
         const float eps_a = s_par[nt + ti];
         const int cnt = (int)d.nl_cnt[i];
         for (int k = g; k < cnt; k += kGroup) {
-            const uint32_t j = d.nl[nl_at(d, i, k)];
+            const uint32_t j = nl_load(d, nl_at(d, i, k));
             const float4 pj = pos[j];
             const float dx = mimg_a(pi.x - pj.x, d.L, d.invL), dy = mimg_a(pi.y - pj.y, d.L, d.invL),
                         dz = mimg_a(pi.z - pj.z, d.L, d.invL);

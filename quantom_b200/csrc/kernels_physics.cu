@@ -287,8 +287,8 @@ __device__ __forceinline__ void scan_stream(const PhysDev& d, const float4* __re
         for (uint32_t e = (uint32_t)(cnt + sub); b; e += kBuildSlices) {
             const int c = __ffs(b) - 1;
             if (e < (uint32_t)d.nl_cap)
-                d.nl[((e >> 3) * (uint32_t)d.n_pad + (uint32_t)i) * 8u + (e & 7u)] =
-                    __float_as_uint(sm->cand[c].w) & 0x7fffffffu;
+                nl_store(d, ((e >> 3) * (uint32_t)d.n_pad + (uint32_t)i) * 8u + (e & 7u),
+                         __float_as_uint(sm->cand[c].w) & 0x7fffffffu);
 #pragma unroll
             for (int q = 0; q < kBuildSlices; q++) b &= b - 1u;
         }
@@ -743,9 +743,9 @@ __device__ __forceinline__ uint32_t lane_entry(int m, uint32_t stride) {
 
 // One lane's entries of its particle's Verlet list, GATHERS (4 or 2) position
 // loads in flight; MIXED: compensated sums every 8 pairs.
-template <bool MIXED, bool ENERGY, bool SWITCH, bool WRAP, int GATHERS = 4>
+template <bool MIXED, bool ENERGY, bool SWITCH, bool WRAP, int GATHERS, typename ID>
 __device__ __forceinline__ void pair_rows(const PhysDev& d, const float2* row, float4 pi, const float4* __restrict__ pos,
-                                          const uint32_t* __restrict__ nl, uint32_t stride, int rows, float& fx,
+                                          const ID* __restrict__ nl, uint32_t stride, int rows, float& fx,
                                           float& fy, float& fz, float& cxx, float& cyy, float& czz, float& e_i,
                                           float& w_i) {
     int r = 0;
@@ -754,8 +754,10 @@ __device__ __forceinline__ void pair_rows(const PhysDev& d, const float2* row, f
         float px = 0.f, py = 0.f, pz = 0.f;
         if (GATHERS == 4) {
             for (; r + 3 < rend; r += 4) {
-                const uint32_t j0 = __ldg(nl + lane_entry(r, stride)), j1 = __ldg(nl + lane_entry(r + 1, stride));
-                const uint32_t j2 = __ldg(nl + lane_entry(r + 2, stride)), j3 = __ldg(nl + lane_entry(r + 3, stride));
+                const uint32_t j0 = (uint32_t)__ldg(nl + lane_entry(r, stride));
+                const uint32_t j1 = (uint32_t)__ldg(nl + lane_entry(r + 1, stride));
+                const uint32_t j2 = (uint32_t)__ldg(nl + lane_entry(r + 2, stride));
+                const uint32_t j3 = (uint32_t)__ldg(nl + lane_entry(r + 3, stride));
                 const float4 p0 = __ldg(pos + j0), p1 = __ldg(pos + j1), p2 = __ldg(pos + j2), p3 = __ldg(pos + j3);
                 lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p0, px, py, pz, e_i, w_i);
                 lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p1, px, py, pz, e_i, w_i);
@@ -764,14 +766,15 @@ __device__ __forceinline__ void pair_rows(const PhysDev& d, const float2* row, f
             }
         } else {
             for (; r + 1 < rend; r += 2) {
-                const uint32_t j0 = __ldg(nl + lane_entry(r, stride)), j1 = __ldg(nl + lane_entry(r + 1, stride));
+                const uint32_t j0 = (uint32_t)__ldg(nl + lane_entry(r, stride));
+                const uint32_t j1 = (uint32_t)__ldg(nl + lane_entry(r + 1, stride));
                 const float4 p0 = __ldg(pos + j0), p1 = __ldg(pos + j1);
                 lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p0, px, py, pz, e_i, w_i);
                 lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p1, px, py, pz, e_i, w_i);
             }
         }
         for (; r < rend; r++) {
-            const uint32_t j0 = __ldg(nl + lane_entry(r, stride));
+            const uint32_t j0 = (uint32_t)__ldg(nl + lane_entry(r, stride));
             lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, __ldg(pos + j0), px, py, pz, e_i, w_i);
         }
         if (MIXED) {
@@ -884,7 +887,7 @@ __device__ __forceinline__ void pair_walk_staged(const PhysDev& d, const float2*
 }
 #endif  // LIMA_STAGED_LIST
 
-template <bool MIXED, bool ENERGY, bool INTEGRATE, bool SWITCH, bool TAIL>
+template <bool MIXED, bool ENERGY, bool INTEGRATE, bool SWITCH, bool TAIL, typename ID>
 __device__ __forceinline__ void step_body(const PhysDev& d, int cur, int slot, cudaGraphExec_t tail) {
     extern __shared__ float2 s_tab[];
     const int nt2 = d.n_types * d.n_types;
@@ -902,7 +905,7 @@ __device__ __forceinline__ void step_body(const PhysDev& d, int cur, int slot, c
     float e_i = 0.f, w_i = 0.f;
     const int cnt = active ? (int)d.nl_cnt[i] : 0;
     const uint32_t stride = (uint32_t)d.n_pad * kGroup;
-    const uint32_t* __restrict__ nl = d.nl + (uint32_t)i * kGroup + g;
+    const ID* __restrict__ nl = reinterpret_cast<const ID*>(d.nl) + (uint32_t)i * kGroup + g;
     // this lane's entries: g, g + kStepLanes, g + 2 kStepLanes, ... below cnt
     const int rows = cnt > g ? (cnt - g + kStepLanes - 1) / kStepLanes : 0;
     // warps whose particles are all away from the box faces skip the minimum image
@@ -913,11 +916,11 @@ __device__ __forceinline__ void step_body(const PhysDev& d, int cur, int slot, c
     pair_walk_staged<MIXED, ENERGY, SWITCH>(d, row, pi, pos, rows, active, nowrap, fx, fy, fz, cxx, cyy, czz, e_i, w_i);
 #else
     if (nowrap)
-        pair_rows<MIXED, ENERGY, SWITCH, false, MIXED ? kMixedGathers : 4>(d, row, pi, pos, nl, stride, rows, fx, fy,
-                                                                           fz, cxx, cyy, czz, e_i, w_i);
+        pair_rows<MIXED, ENERGY, SWITCH, false, MIXED ? kMixedGathers : 4, ID>(d, row, pi, pos, nl, stride, rows, fx, fy,
+                                                                               fz, cxx, cyy, czz, e_i, w_i);
     else
-        pair_rows<MIXED, ENERGY, SWITCH, true, MIXED ? kMixedGathers : 4>(d, row, pi, pos, nl, stride, rows, fx, fy,
-                                                                          fz, cxx, cyy, czz, e_i, w_i);
+        pair_rows<MIXED, ENERGY, SWITCH, true, MIXED ? kMixedGathers : 4, ID>(d, row, pi, pos, nl, stride, rows, fx, fy,
+                                                                              fz, cxx, cyy, czz, e_i, w_i);
 #endif
     // reduce the kStepLanes lanes of this particle (warp shuffles)
 #pragma unroll
@@ -1064,13 +1067,14 @@ __device__ __forceinline__ void step_body(const PhysDev& d, int cur, int slot, c
 
 // FP32: at most 48 registers, 5 blocks of 256 per SM.  Mixed keeps the
 // compiler's own choice (a 5-block bound slowed it).
-template <bool ENERGY, bool INTEGRATE, bool SWITCH, bool TAIL>
+// ID: the list's slot-id type (uint16_t when the slots fit, else uint32_t).
+template <bool ENERGY, bool INTEGRATE, bool SWITCH, bool TAIL, typename ID>
 __global__ void __launch_bounds__(kTB, 5) k_step(PhysDev d, int cur, int slot, cudaGraphExec_t tail) {
-    step_body<false, ENERGY, INTEGRATE, SWITCH, TAIL>(d, cur, slot, tail);
+    step_body<false, ENERGY, INTEGRATE, SWITCH, TAIL, ID>(d, cur, slot, tail);
 }
-template <bool ENERGY, bool INTEGRATE, bool SWITCH, bool TAIL>
+template <bool ENERGY, bool INTEGRATE, bool SWITCH, bool TAIL, typename ID>
 __global__ void __launch_bounds__(kTB) k_step_mixed(PhysDev d, int cur, int slot, cudaGraphExec_t tail) {
-    step_body<true, ENERGY, INTEGRATE, SWITCH, TAIL>(d, cur, slot, tail);
+    step_body<true, ENERGY, INTEGRATE, SWITCH, TAIL, ID>(d, cur, slot, tail);
 }
 
 // ---------------------------------------------------------------- launchers --
@@ -1095,17 +1099,25 @@ void launch_programmatic(K kernel, const PhysDev& d, int cur, int slot, cudaGrap
     cudaLaunchKernelEx(&cfg, kernel, d, cur, slot, tail);
 }
 
-template <bool MIXED, bool ENERGY, bool INTEGRATE, bool TAIL>
-void step_variant(const PhysDev& d, int cur, int slot, cudaGraphExec_t tail, cudaStream_t s) {
+template <bool MIXED, bool ENERGY, bool INTEGRATE, bool TAIL, typename ID>
+void step_variant_id(const PhysDev& d, int cur, int slot, cudaGraphExec_t tail, cudaStream_t s) {
     const size_t smem = sizeof(float2) * d.n_types * d.n_types;
     if (MIXED && d.use_switch)
-        launch_programmatic(k_step_mixed<ENERGY, INTEGRATE, true, TAIL>, d, cur, slot, tail, smem, s);
+        launch_programmatic(k_step_mixed<ENERGY, INTEGRATE, true, TAIL, ID>, d, cur, slot, tail, smem, s);
     else if (MIXED)
-        launch_programmatic(k_step_mixed<ENERGY, INTEGRATE, false, TAIL>, d, cur, slot, tail, smem, s);
+        launch_programmatic(k_step_mixed<ENERGY, INTEGRATE, false, TAIL, ID>, d, cur, slot, tail, smem, s);
     else if (d.use_switch)
-        launch_programmatic(k_step<ENERGY, INTEGRATE, true, TAIL>, d, cur, slot, tail, smem, s);
+        launch_programmatic(k_step<ENERGY, INTEGRATE, true, TAIL, ID>, d, cur, slot, tail, smem, s);
     else
-        launch_programmatic(k_step<ENERGY, INTEGRATE, false, TAIL>, d, cur, slot, tail, smem, s);
+        launch_programmatic(k_step<ENERGY, INTEGRATE, false, TAIL, ID>, d, cur, slot, tail, smem, s);
+}
+
+template <bool MIXED, bool ENERGY, bool INTEGRATE, bool TAIL>
+void step_variant(const PhysDev& d, int cur, int slot, cudaGraphExec_t tail, cudaStream_t s) {
+    if (d.nl16)
+        step_variant_id<MIXED, ENERGY, INTEGRATE, TAIL, uint16_t>(d, cur, slot, tail, s);
+    else
+        step_variant_id<MIXED, ENERGY, INTEGRATE, TAIL, uint32_t>(d, cur, slot, tail, s);
 }
 
 template <bool MIXED, bool ENERGY, bool INTEGRATE>
@@ -1132,6 +1144,8 @@ void launch_permute(const PhysDev& d, int cur, bool mixed, cudaStream_t s) {
 void launch_set_xref(const PhysDev& d, const float4* pos, cudaStream_t s) {
     k_set_xref<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d, pos);
 }
+
+bool list_ids_16bit(int n_pad) { return !kStagedList && n_pad <= 65536; }
 
 void launch_build_list(const PhysDev& d, const float4* pos, const uint32_t* orig, const uint32_t* items, int copy_cur,
                        bool mixed, cudaStream_t s) {

@@ -17,7 +17,8 @@
 //   posc/velc       low parts of pos/vel (mixed precision)
 //   xref[n_pad]     positions at the last rebuild (list validity check)
 //   force[n_pad]    total force of the last evaluation, w = per-particle potential energy
-//   nl[cap][n_pad]  Verlet list of sorted slots, entry k of particle i at
+//   nl[cap][n_pad]  Verlet list of sorted slots (uint16 ids when n_pad <= 65536,
+//                   else uint32), entry k of particle i at
 //                   ((k / kGroup) * n_pad + i) * kGroup + k % kGroup: the
 //                   kGroup lanes of one particle read kGroup consecutive
 //                   entries and consecutive particles follow each other
@@ -82,6 +83,7 @@ struct PhysDev {
     float4* pos_tmp[2]; float4* vel_tmp; float4* posc_tmp; float4* velc_tmp; float4* force_tmp; uint32_t* orig_tmp;
     // Verlet list (tile-local indices)
     uint32_t* nl; uint32_t* nl_cnt; int nl_cap;
+    int nl16;                   // 1: nl holds uint16 slot ids (half the bytes per step), 0: uint32
     int* nl_need;               // largest row length a build found beyond nl_cap (0: none)
     // dynamic lists (nlist_period <= 0): the step kernel's last block sees
     // that a particle moved more than skin/2 since the last build and

@@ -291,6 +291,7 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
     const double expect = 4.0 / 3.0 * M_PI * (double)d.rlist * d.rlist * d.rlist * rho;
     d.nl_cap = std::min((d.n + kGroup - 1) / kGroup * kGroup, (int)((1.6 * expect + 96) / kGroup + 1) * kGroup);
     d.nl_cap = std::max(d.nl_cap, 4 * kGroup);
+    d.nl16 = list_ids_16bit(d.n_pad) ? 1 : 0;
 
     // every fixed-size buffer in one allocation; the list separately (it may grow)
     // the topology arrays first and together: the host builds their image
@@ -352,7 +353,7 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
         Arena real;
         real.base = reinterpret_cast<uintptr_t>(dalloc<uint8_t>(allocs, plan.off, s));
         carve(real);
-        d.nl = dalloc<uint32_t>(allocs, (size_t)d.nl_cap * d.n_pad, s);
+        d.nl = reinterpret_cast<uint32_t*>(dalloc<uint8_t>(allocs, (size_t)d.nl_cap * d.n_pad * nl_entry_bytes(d), s));
     } catch (const std::exception& e) {
         msg = std::string("device allocation failed: ") + e.what();
         return LIMA_ERR_CUDA;
@@ -480,7 +481,7 @@ bool phys_fit_list(PhysDev& d, cudaStream_t s, std::vector<void*>& allocs) {
     cudaStreamSynchronize(s);
     if (!(err & ERR_BIT_PHYS_LIST_OVERFLOW) || need <= d.nl_cap) return false;
     const int cap = std::min((d.n + kGroup - 1) / kGroup * kGroup, ((need * 5 / 4 + 32) / kGroup + 1) * kGroup);
-    uint32_t* nl = dalloc<uint32_t>(allocs, (size_t)cap * d.n_pad, s);   // throws like the other allocations
+    uint32_t* nl = reinterpret_cast<uint32_t*>(dalloc<uint8_t>(allocs, (size_t)cap * d.n_pad * nl_entry_bytes(d), s));   // throws like the other allocations
     for (auto it = allocs.begin(); it != allocs.end(); ++it)
         if (*it == d.nl) {
             pool_free(d.nl, s);
@@ -645,7 +646,13 @@ uint32_t phys_read_list(const PhysDev& d, uint32_t* offsets, uint32_t* ids) {
     std::vector<uint32_t> cnt(d.n), orig(d.n), nl((size_t)d.nl_cap * d.n_pad);
     cudaMemcpy(cnt.data(), d.nl_cnt, sizeof(uint32_t) * d.n, cudaMemcpyDeviceToHost);
     cudaMemcpy(orig.data(), d.orig_of_sorted, sizeof(uint32_t) * d.n, cudaMemcpyDeviceToHost);
-    cudaMemcpy(nl.data(), d.nl, sizeof(uint32_t) * nl.size(), cudaMemcpyDeviceToHost);
+    if (d.nl16) {
+        std::vector<uint16_t> n16(nl.size());
+        cudaMemcpy(n16.data(), d.nl, sizeof(uint16_t) * n16.size(), cudaMemcpyDeviceToHost);
+        std::copy(n16.begin(), n16.end(), nl.begin());
+    } else {
+        cudaMemcpy(nl.data(), d.nl, sizeof(uint32_t) * nl.size(), cudaMemcpyDeviceToHost);
+    }
     std::vector<uint32_t> by_orig(d.n);
     for (int k = 0; k < d.n; k++) by_orig[orig[k]] = (uint32_t)k;
     uint32_t pos = 0;

@@ -27,6 +27,22 @@ static_assert(kStepLanes == 8 || kStepLanes == 4, "the step kernel reads 8-entry
 constexpr bool kStagedList = LIMA_STAGED_LIST != 0;
 constexpr int kStageRows = 8;
 static_assert(!kStagedList || kStepLanes == 8, "the staged list walk gives each lane one list column");
+// list entry `idx` (a word index of the blocked layout) in either id width
+__device__ __forceinline__ uint32_t nl_load(const PhysDev& d, size_t idx) {
+    return d.nl16 ? (uint32_t)reinterpret_cast<const uint16_t*>(d.nl)[idx] : d.nl[idx];
+}
+__device__ __forceinline__ void nl_store(const PhysDev& d, size_t idx, uint32_t j) {
+    if (d.nl16)
+        reinterpret_cast<uint16_t*>(d.nl)[idx] = (uint16_t)j;
+    else
+        d.nl[idx] = j;
+}
+// whether the step kernels of this library take 16-bit list ids for n_pad
+// slots: whenever they fit, except in the staged variant (32-bit rows)
+bool list_ids_16bit(int n_pad);
+// bytes of one list entry
+__host__ __device__ inline size_t nl_entry_bytes(const PhysDev& d) { return d.nl16 ? 2 : 4; }
+
 // blocks of the step kernel (kStepLanes lanes per particle slot, n_pad a multiple of 32)
 __host__ __device__ inline int step_blocks(const PhysDev& d) {
     return (int)(((size_t)d.n_pad * kStepLanes + kTB - 1) / kTB);
