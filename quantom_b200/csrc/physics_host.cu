@@ -395,11 +395,14 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
 
 // Host state (reference layout) -> device, in orig order (the next rebuild
 // sorts).  Half-step velocities from the Stormer pair: v = (x - x_prev)/dt.
+// Positions are wrapped into [0, L) in double and rounded to FP32; mixed
+// precision keeps what the rounding dropped (of the position and of the
+// velocity) in the low words, so its state starts at the input itself.
 void phys_upload_state(const PhysHost& h, PhysDev& d, int cur, cudaStream_t s) {
     // staged in one pinned block (pageable sources would each take a driver
     // staging pass); plain host memory when no pinned block can be had
     const size_t np = (size_t)d.n_pad;
-    const size_t bytes = np * (2 * sizeof(float4) + sizeof(uint32_t));
+    const size_t bytes = np * (4 * sizeof(float4) + sizeof(uint32_t));
     void* block = pinned_alloc(bytes);
     std::vector<uint8_t> fallback;
     if (!block) {
@@ -408,46 +411,61 @@ void phys_upload_state(const PhysHost& h, PhysDev& d, int cur, cudaStream_t s) {
     }
     float4* pos = static_cast<float4*>(block);
     float4* vel = pos + np;
-    uint32_t* ident = reinterpret_cast<uint32_t*>(vel + np);
+    float4* posc = vel + np;
+    float4* velc = posc + np;
+    uint32_t* ident = reinterpret_cast<uint32_t*>(velc + np);
     const float L = d.L;
-    auto wrap = [&](double x) {
+    const bool mixed = d.precision == LIMA_PRECISION_MIXED;
+    // the coordinate in [0, L) as FP32 plus its rounding residual (hi + lo = x mod L)
+    auto wrap = [&](double x, float& lo) {
         if (!(x >= 0.0 && x < (double)L)) {   // most inputs are inside the box already
             x = std::fmod(x, (double)L);
             if (x < 0) x += L;
         }
         float f = (float)x;
-        if (f >= L) f = 0.f;
+        if (f >= L) {   // rounded up onto the face: the image at 0
+            f = 0.f;
+            x -= L;
+        }
+        lo = mixed ? (float)(x - (double)f) : 0.f;
+        return f;
+    };
+    auto split = [&](double v, float& lo) {
+        const float f = (float)v;
+        lo = mixed ? (float)(v - (double)f) : 0.f;
         return f;
     };
     auto mimg = [&](double dd) { return std::fabs(dd) <= 0.5 * L ? dd : dd - L * std::nearbyint(dd / L); };
+    auto put = [&](int k, const lima_float3& x, const lima_float3& xp, int type, float im) {
+        float lx, ly, lz, ux, uy, uz;
+        const float px = wrap(x.x, lx), py = wrap(x.y, ly), pz = wrap(x.z, lz);
+        pos[k] = make_float4(px, py, pz, host_int_as_float(type));
+        posc[k] = make_float4(lx, ly, lz, 0.f);
+        const float vx = split(mimg((double)x.x - xp.x) / d.dt, ux), vy = split(mimg((double)x.y - xp.y) / d.dt, uy),
+                    vz = split(mimg((double)x.z - xp.z) / d.dt, uz);
+        vel[k] = make_float4(vx, vy, vz, im);
+        velc[k] = make_float4(ux, uy, uz, 0.f);
+    };
     int k = 0;
     for (int c = 0; c < h.n_c; c++)
         for (int t = 0; t < h.comps[c].n_particles; t++, k++) {
-            const lima_float3 x = h.states[c].positions[t], xp = h.comps[c].prev_positions[t];
             const int type = h.comps[c].atom_types[t];
-            pos[k] = make_float4(wrap(x.x), wrap(x.y), wrap(x.z), host_int_as_float(type));
-            const float im = 1.f / h.ff->particle_parameters[type].mass;
-            vel[k] = make_float4((float)(mimg((double)x.x - xp.x) / d.dt), (float)(mimg((double)x.y - xp.y) / d.dt),
-                                 (float)(mimg((double)x.z - xp.z) / d.dt), im);
+            put(k, h.states[c].positions[t], h.comps[c].prev_positions[t], type,
+                1.f / h.ff->particle_parameters[type].mass);
         }
     const float im_sol = 1.f / h.ff->particle_parameters[LIMA_ATOMTYPE_SOL].mass;
-    for (int si = 0; si < h.n_s; si++, k++) {
-        const lima_float3 x = h.sols[si].pos, xp = h.sols[si].pos_tsub1;
-        pos[k] = make_float4(wrap(x.x), wrap(x.y), wrap(x.z), host_int_as_float(LIMA_ATOMTYPE_SOL));
-        vel[k] = make_float4((float)(mimg((double)x.x - xp.x) / d.dt), (float)(mimg((double)x.y - xp.y) / d.dt),
-                             (float)(mimg((double)x.z - xp.z) / d.dt), im_sol);
-    }
+    for (int si = 0; si < h.n_s; si++, k++) put(k, h.sols[si].pos, h.sols[si].pos_tsub1, LIMA_ATOMTYPE_SOL, im_sol);
     for (int i = d.n; i < d.n_pad; i++) {
         pos[i] = make_float4(0, 0, 0, host_int_as_float(0));
-        vel[i] = make_float4(0, 0, 0, 0);
+        vel[i] = posc[i] = velc[i] = make_float4(0, 0, 0, 0);
     }
     for (int i = 0; i < d.n_pad; i++) ident[i] = i < d.n ? i : 0xffffffffu;
     cudaMemcpyAsync(d.pos[cur], pos, sizeof(float4) * d.n_pad, cudaMemcpyHostToDevice, s);
     if (d.n_cp) cudaMemcpyAsync(d.pos_orig[cur], pos, sizeof(float4) * d.n_cp, cudaMemcpyHostToDevice, s);
-    if (d.n_cp) cudaMemsetAsync(d.posc_orig[cur], 0, sizeof(float4) * d.n_cp, s);
+    if (d.n_cp) cudaMemcpyAsync(d.posc_orig[cur], posc, sizeof(float4) * d.n_cp, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(d.vel, vel, sizeof(float4) * d.n_pad, cudaMemcpyHostToDevice, s);
-    cudaMemsetAsync(d.posc, 0, sizeof(float4) * d.n_pad, s);
-    cudaMemsetAsync(d.velc, 0, sizeof(float4) * d.n_pad, s);
+    cudaMemcpyAsync(d.posc, posc, sizeof(float4) * d.n_pad, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d.velc, velc, sizeof(float4) * d.n_pad, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(d.orig_of_sorted, ident, sizeof(uint32_t) * d.n_pad, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(d.sorted_of_orig, ident, sizeof(uint32_t) * d.n, cudaMemcpyHostToDevice, s);
     set_device_float(d.lambda, 1.f, s);

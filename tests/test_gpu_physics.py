@@ -41,14 +41,16 @@ def _positions(E, eng, s):
 
 
 @functools.lru_cache(maxsize=2)
-def _system_and_fp64_forces(name, seed):
-    """The FP64 oracle at the positions the engine holds: the loader wraps every
-    coordinate into [0, L) and rounds it to FP32 (compound particles of bridged
-    chains start outside the box), which moves the forces of the raw input by up
-    to 3.9e-4 relative RMS; the bar is on the evaluation, not on that rounding."""
+def _system_and_fp64_forces(name, seed, raw=False):
+    """The FP64 oracle at the positions the engine holds.  Plain FP32: the
+    loader wraps every coordinate into [0, L) and rounds it to FP32 (compound
+    particles of bridged chains start outside the box), which moves the forces
+    of the raw input by up to 3.9e-4 relative RMS; the bar is on the
+    evaluation, not on that rounding.  Mixed precision (raw=True) keeps the
+    rounding residual in its low words, so its state is the input itself."""
     s = make_named(name, seed)
     ps = po.PhysSystem(s, rc=s.spec.cutoff, r_on=1.0)
-    F64, en64 = ps.forces(_wrapped_f32(s).astype(np.float64))
+    F64, en64 = ps.forces() if raw else ps.forces(_wrapped_f32(s).astype(np.float64))
     return s, F64, en64
 
 
@@ -59,7 +61,7 @@ def _system_and_fp64_forces(name, seed):
                                   "solvated_chains_258k", "6lzm", "small_bridged_dry"])
 def test_forces_and_energies_match_fp64(gpu, name, precision):
     E = gpu
-    s, F64, en64 = _system_and_fp64_forces(name, 7)
+    s, F64, en64 = _system_and_fp64_forces(name, 7, raw=precision == E.PRECISION_MIXED)
     with E.Engine(s, _params(E, s, precision=precision)) as eng:
         tot = eng.compute_energies()
         fc, fs = eng.forces()
@@ -163,8 +165,9 @@ def test_deterministic_with_berendsen_and_rebuilds(gpu, precision):
 
 @pytest.mark.parametrize("precision", [0, 1])
 def test_dynamic_list_trajectory_matches_fp64(gpu, precision):
-    """nlist_period 0: rebuilds decided on the device (conditional node of the
-    step graph) leave the trajectory on the FP64 oracle's."""
+    """nlist_period 0: rebuilds decided and launched on the device (the step
+    kernel's tail launch of the rebuild graph) leave the trajectory on the
+    FP64 oracle's."""
     E = gpu
     s = S.make_system("small_chains", seed=3)
     ps = po.PhysSystem(s, rc=s.spec.cutoff, r_on=1.0)
