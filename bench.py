@@ -556,19 +556,34 @@ def grad_study(E, S, device=0, fd=True, fp64_fd=False):
                     rel.append(abs(g[k] - fdv[-1]) / abs(fdv[-1]))
                 out.update({"fd_fp32_gpu" + key: fdv, "rel_err_vs_fd_fp32_gpu" + key: rel})
     if fp64_fd:
+        # central differences of the FP64 oracle loss at the specified step (1e-4
+        # relative), the four losses in parallel host processes
+        import multiprocessing as mp
+        from concurrent.futures import ProcessPoolExecutor
         from oracle import pyoracle as po
+        t0 = time.perf_counter()
         ps = po.PhysSystem(start, rc=spec.cutoff, r_on=1.0)
         th64 = ps.params()
-        fdv, rel = [], []
+        jobs, hs = [], []
         for k in (0, 1):
             h = 1e-4 * abs(th64[k])
-            e = np.eye(len(th64))[k]
-            lp, _ = ps.with_params(th64 + h * e).loss(spec.dt, T, nb, rmax, w_e, w_r, target)
-            lm, _ = ps.with_params(th64 - h * e).loss(spec.dt, T, nb, rmax, w_e, w_r, target)
-            fdv.append((lp - lm) / (2 * h))
-            rel.append(abs(g[k] - fdv[-1]) / abs(fdv[-1]))
-        out.update({"fd_fp64_oracle": fdv, "rel_err_vs_fd_fp64": rel})
+            hs.append(h)
+            for sign in (1.0, -1.0):
+                e = np.zeros(len(th64))
+                e[k] = sign * h
+                jobs.append((ps, th64 + e, spec.dt, T, nb, rmax, w_e, w_r, target))
+        with ProcessPoolExecutor(min(4, os.cpu_count() or 1), mp_context=mp.get_context("spawn")) as ex:
+            losses = list(ex.map(_fp64_loss, jobs))
+        fdv = [(losses[2 * k] - losses[2 * k + 1]) / (2 * hs[k]) for k in (0, 1)]
+        rel = [abs(g[k] - fdv[k]) / abs(fdv[k]) for k in (0, 1)]
+        out.update({"fd_fp64_oracle": fdv, "rel_err_vs_fd_fp64": rel, "fd_fp64_host_s": time.perf_counter() - t0})
     return out
+
+
+def _fp64_loss(job):
+    """One FP64 oracle loss (a spawn-pool task of the gradient check)."""
+    ps, theta, dt, T, nb, rmax, w_e, w_r, target = job
+    return ps.with_params(theta).loss(dt, T, nb, rmax, w_e, w_r, target)[0]
 
 
 def run_grad(args):
@@ -999,13 +1014,14 @@ def run_ours(args, ws, rank, local, pg):
     if rank != 0:
         return
     # ---- parameter gradients (config 3), cost relative to the forward loss ---
-    grad = grad_study(E, S, device=local, fd=True, fp64_fd=False)
+    grad = grad_study(E, S, device=local, fd=True, fp64_fd=True)
     grad = {k: grad[k] for k in ("workload", "n_steps", "checkpoint_every", "ms_forward_loss", "ms_grad",
-                                 "grad_over_forward", "grad", "fd_fp32_gpu", "rel_err_vs_fd_fp32_gpu",
-                                 "fd_fp32_gpu_h1e-3", "rel_err_vs_fd_fp32_gpu_h1e-3")}
-    grad["fd_note"] = ("FP32 central differences are limited by the trajectories' rounding noise; against the FP64 "
-                       "oracle's central differences (bench.py --mode grad --fp64-fd) the gradient agrees to "
-                       "8.5e-8 (sigma) and 5.8e-7 (epsilon) relative")
+                                 "grad_over_forward", "grad", "fd_fp64_oracle", "rel_err_vs_fd_fp64",
+                                 "fd_fp64_host_s", "fd_fp32_gpu", "rel_err_vs_fd_fp32_gpu", "fd_fp32_gpu_h1e-3",
+                                 "rel_err_vs_fd_fp32_gpu_h1e-3")}
+    grad["fd_note"] = ("rel_err_vs_fd_fp64: against central differences of the FP64 oracle loss at the specified "
+                       "step (1e-4 relative), the check the target names; the FP32 central differences of the "
+                       "GPU loss beside it carry the FP32 trajectories' rounding noise")
     # ---- roofline of the dominant kernel (k_step: pairs + integration) -------
     # The pair terms are bound by the FP32 pipe: 32 FLOP per unique pair within
     # r_c (minimum image 9, r^2 5, rcp 1, s^6 3, scalar force 5, vector force 3,
