@@ -32,7 +32,7 @@ constexpr int kListEpoch = 10;
 __device__ __forceinline__ float mimg_a(float d, float L, float invL) { return d - L * rintf(d * invL); }
 
 __device__ __forceinline__ uint32_t nl_at(const PhysDev& d, int i, int k) {
-    return ((uint32_t)(k / kGroup) * (uint32_t)d.n_pad + (uint32_t)i) * kGroup + (uint32_t)(k % kGroup);
+    return nl_word((uint32_t)d.n_pad, (uint32_t)i, (uint32_t)k);
 }
 
 __device__ __forceinline__ double warp_sum_d(double v) {

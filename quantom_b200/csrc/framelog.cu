@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(kTB) k_log_train(PhysDev d, FrameLogDev g, int
         const float2* row = &s_tab[__float_as_int(pi.w) * d.n_types];
         const int cnt = (int)d.nl_cnt[i];
         for (int k = lane; k < cnt; k += kGroup) {
-            const uint32_t j = nl_load(d, ((uint32_t)(k / kGroup) * (uint32_t)d.n_pad + (uint32_t)i) * kGroup + k % kGroup);
+            const uint32_t j = nl_load(d, nl_word((uint32_t)d.n_pad, (uint32_t)i, (uint32_t)k));
             if (d.orig_of_sorted[j] < (uint32_t)d.n_cp) continue;   // solvent neighbours only
             lj_pair<false, SWITCH>(d, row, pi, pos[j], fx, fy, fz, e, w);
         }

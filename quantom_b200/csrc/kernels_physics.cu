@@ -280,15 +280,14 @@ __device__ __forceinline__ void scan_stream(const PhysDev& d, const float4* __re
         all |= __shfl_xor_sync(0xffffffffu, all, 1);
         all |= __shfl_xor_sync(0xffffffffu, all, 2);
         // hit of rank k goes to entry cnt + k; slice s writes ranks s, s + 4, ...
-        // (entry e of row i: word (e / 8 * n_pad + i) * 8 + e % 8, below 2^32
-        // because the list is smaller than 16 GB)
+        // (entry e of particle i at nl_word, below 2^32 because the list is
+        // smaller than 16 GB)
         uint32_t b = all;
         for (int k = 0; k < sub && b; k++) b &= b - 1u;
         for (uint32_t e = (uint32_t)(cnt + sub); b; e += kBuildSlices) {
             const int c = __ffs(b) - 1;
             if (e < (uint32_t)d.nl_cap)
-                nl_store(d, ((e >> 3) * (uint32_t)d.n_pad + (uint32_t)i) * 8u + (e & 7u),
-                         __float_as_uint(sm->cand[c].w) & 0x7fffffffu);
+                nl_store(d, nl_word((uint32_t)d.n_pad, (uint32_t)i, e), __float_as_uint(sm->cand[c].w) & 0x7fffffffu);
 #pragma unroll
             for (int q = 0; q < kBuildSlices; q++) b &= b - 1u;
         }
@@ -727,56 +726,78 @@ __device__ __forceinline__ void finish_sums(const PhysDev& d, int slot, cudaGrap
 
 // ------------------------------------------------------------------ the step ---
 // (lj_pair: physmath.cuh)
-// position loads in flight per lane in the mixed-precision pair loop: the
-// mixed step kernel needs more than 48 registers either way (4 blocks of 256
-// per SM), and four in flight measured 71 against 79 us per flushed step
-#if !LIMA_STAGED_LIST
-constexpr int kMixedGathers = 4;
-#endif
+// The four ids of one chunk column (nl_word): one 8-byte load of 16-bit ids
+// or one 16-byte load of 32-bit ids.
+template <typename ID>
+struct ChunkIds;
+template <>
+struct ChunkIds<uint16_t> {
+    using V = uint2;
+    static __device__ __forceinline__ void split(V v, uint32_t& a, uint32_t& b, uint32_t& c, uint32_t& e) {
+        a = v.x & 0xffffu;
+        b = v.x >> 16;
+        c = v.y & 0xffffu;
+        e = v.y >> 16;
+    }
+};
+template <>
+struct ChunkIds<uint32_t> {
+    using V = uint4;
+    static __device__ __forceinline__ void split(V v, uint32_t& a, uint32_t& b, uint32_t& c, uint32_t& e) {
+        a = v.x;
+        b = v.y;
+        c = v.z;
+        e = v.w;
+    }
+};
 
-// Offset of a lane's m-th list entry from its first: with 8 lanes entry m is
-// in row m; with 4 lanes entries alternate between columns g and g + 4 of
-// one row.
-__device__ __forceinline__ uint32_t lane_entry(int m, uint32_t stride) {
-    return kStepLanes == 8 ? (uint32_t)m * stride : (uint32_t)(m >> 1) * stride + (uint32_t)(m & 1) * 4u;
-}
-
-// One lane's entries of its particle's Verlet list, GATHERS (4 or 2) position
-// loads in flight; MIXED: compensated sums every 8 pairs.
-template <bool MIXED, bool ENERGY, bool SWITCH, bool WRAP, int GATHERS, typename ID>
+// One lane's entries of its particle's Verlet list: `rows` entries, four per
+// chunk column (col: the lane's column of chunk 0; cstride: vectors between
+// chunks), each chunk one vector load and four position gathers in flight.
+// In the last, partial chunk the words past the lane's count are not ids
+// (the gathers for them re-read the first entry and are not evaluated).
+// MIXED: compensated sums every two chunks (8 pairs).
+template <bool MIXED, bool ENERGY, bool SWITCH, bool WRAP, typename ID>
 __device__ __forceinline__ void pair_rows(const PhysDev& d, const float2* row, float4 pi, const float4* __restrict__ pos,
-                                          const ID* __restrict__ nl, uint32_t stride, int rows, float& fx,
-                                          float& fy, float& fz, float& cxx, float& cyy, float& czz, float& e_i,
-                                          float& w_i) {
-    int r = 0;
-    while (r < rows) {
-        const int rend = MIXED ? min(rows, r + 8) : rows;
+                                          const typename ChunkIds<ID>::V* __restrict__ col, uint32_t cstride, int rows,
+                                          float& fx, float& fy, float& fz, float& cxx, float& cyy, float& czz,
+                                          float& e_i, float& w_i) {
+    const int full = rows >> 2, tail = rows & 3;
+    uint32_t off = 0;
+    int c = 0;
+    while (c < full) {
+        const int cend = MIXED ? min(full, c + 2) : full;
         float px = 0.f, py = 0.f, pz = 0.f;
-        if (GATHERS == 4) {
-            for (; r + 3 < rend; r += 4) {
-                const uint32_t j0 = (uint32_t)__ldg(nl + lane_entry(r, stride));
-                const uint32_t j1 = (uint32_t)__ldg(nl + lane_entry(r + 1, stride));
-                const uint32_t j2 = (uint32_t)__ldg(nl + lane_entry(r + 2, stride));
-                const uint32_t j3 = (uint32_t)__ldg(nl + lane_entry(r + 3, stride));
-                const float4 p0 = __ldg(pos + j0), p1 = __ldg(pos + j1), p2 = __ldg(pos + j2), p3 = __ldg(pos + j3);
-                lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p0, px, py, pz, e_i, w_i);
-                lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p1, px, py, pz, e_i, w_i);
-                lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p2, px, py, pz, e_i, w_i);
-                lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p3, px, py, pz, e_i, w_i);
-            }
+        for (; c < cend; c++, off += cstride) {
+            uint32_t j0, j1, j2, j3;
+            ChunkIds<ID>::split(__ldg(col + off), j0, j1, j2, j3);
+            const float4 p0 = __ldg(pos + j0), p1 = __ldg(pos + j1), p2 = __ldg(pos + j2), p3 = __ldg(pos + j3);
+            lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p0, px, py, pz, e_i, w_i);
+            lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p1, px, py, pz, e_i, w_i);
+            lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p2, px, py, pz, e_i, w_i);
+            lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p3, px, py, pz, e_i, w_i);
+        }
+        if (MIXED) {
+            ds_add(fx, cxx, px);
+            ds_add(fy, cyy, py);
+            ds_add(fz, czz, pz);
         } else {
-            for (; r + 1 < rend; r += 2) {
-                const uint32_t j0 = (uint32_t)__ldg(nl + lane_entry(r, stride));
-                const uint32_t j1 = (uint32_t)__ldg(nl + lane_entry(r + 1, stride));
-                const float4 p0 = __ldg(pos + j0), p1 = __ldg(pos + j1);
-                lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p0, px, py, pz, e_i, w_i);
-                lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p1, px, py, pz, e_i, w_i);
-            }
+            fx += px;
+            fy += py;
+            fz += pz;
         }
-        for (; r < rend; r++) {
-            const uint32_t j0 = (uint32_t)__ldg(nl + lane_entry(r, stride));
-            lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, __ldg(pos + j0), px, py, pz, e_i, w_i);
-        }
+    }
+    if (tail) {
+        uint32_t j0, j1, j2, j3;
+        ChunkIds<ID>::split(__ldg(col + off), j0, j1, j2, j3);
+        const float4 p0 = __ldg(pos + j0);
+        const float4 p1 = __ldg(pos + (tail > 1 ? j1 : j0));
+        const float4 p2 = __ldg(pos + (tail > 2 ? j2 : j0));
+        float px = 0.f, py = 0.f, pz = 0.f;
+        lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p0, px, py, pz, e_i, w_i);
+        if (tail > 1) lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p1, px, py, pz, e_i, w_i);
+        if (tail > 2) lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p2, px, py, pz, e_i, w_i);
+        (void)j3;
         if (MIXED) {
             ds_add(fx, cxx, px);
             ds_add(fy, cyy, py);
@@ -790,8 +811,12 @@ __device__ __forceinline__ void pair_rows(const PhysDev& d, const float2* row, f
 }
 
 #if LIMA_STAGED_LIST
-// One lane's entries of one staged group of list rows: entry q of the lane
-// at srow[q * kTB] (shared memory); MIXED: one compensated sum per group.
+// One lane's entries of one staged group of list chunks: entry q of the lane
+// at srow[(q / 4) * kChunkWords + q % 4] (shared memory; srow = the lane's
+// column of the group's first chunk); MIXED: one compensated sum per group.
+constexpr int kStageChunks = kStageRows / 4;   // list chunks per staged group
+constexpr int kChunkWords = kTB * 4;           // words of one chunk of a block's 32 particles
+__device__ __forceinline__ int staged_at(int q) { return (q >> 2) * kChunkWords + (q & 3); }
 template <bool MIXED, bool ENERGY, bool SWITCH, bool WRAP>
 __device__ __forceinline__ void pair_staged(const PhysDev& d, const float2* row, float4 pi,
                                             const float4* __restrict__ pos, const uint32_t* srow, int nq, float& fx,
@@ -802,15 +827,16 @@ __device__ __forceinline__ void pair_staged(const PhysDev& d, const float2* row,
     const uint32_t lim = (uint32_t)d.n_pad - 1u;
     int q = 0;
     for (; q + 3 < nq; q += 4) {
-        const uint32_t j0 = min(srow[q * kTB], lim), j1 = min(srow[(q + 1) * kTB], lim);
-        const uint32_t j2 = min(srow[(q + 2) * kTB], lim), j3 = min(srow[(q + 3) * kTB], lim);
+        const uint32_t j0 = min(srow[staged_at(q)], lim), j1 = min(srow[staged_at(q + 1)], lim);
+        const uint32_t j2 = min(srow[staged_at(q + 2)], lim), j3 = min(srow[staged_at(q + 3)], lim);
         const float4 p0 = __ldg(pos + j0), p1 = __ldg(pos + j1), p2 = __ldg(pos + j2), p3 = __ldg(pos + j3);
         lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p0, px, py, pz, e_i, w_i);
         lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p1, px, py, pz, e_i, w_i);
         lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p2, px, py, pz, e_i, w_i);
         lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p3, px, py, pz, e_i, w_i);
     }
-    for (; q < nq; q++) lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, __ldg(pos + min(srow[q * kTB], lim)), px, py, pz, e_i, w_i);
+    for (; q < nq; q++)
+        lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, __ldg(pos + min(srow[staged_at(q)], lim)), px, py, pz, e_i, w_i);
     if (MIXED) {
         ds_add(fx, cxx, px);
         ds_add(fy, cyy, py);
@@ -822,13 +848,12 @@ __device__ __forceinline__ void pair_staged(const PhysDev& d, const float2* row,
     }
 }
 
-// The block's list rows through shared memory: row r of the block's 32
-// particles is one contiguous kilobyte of the blocked list (entry k of
-// particle i at ((k / 8) n_pad + i) 8 + k % 8, and lane t of the block reads
-// word t of each row), so each row is one bulk copy.  Groups of kStageRows
-// rows alternate between two buffers: thread 0 issues group s + 1 while the
-// block evaluates group s, and a block barrier after each group frees its
-// buffer for group s + 2.  Waits are bounded; one that runs out sets
+// The block's list chunks through shared memory: chunk q of the block's 32
+// particles is four contiguous kilobytes of the list (nl_word: lane t of the
+// block reads words 4t .. 4t + 3 of each chunk), so each chunk is one bulk
+// copy.  Groups of kStageChunks chunks (kStageRows rows) alternate between
+// two buffers: thread 0 issues group s + 1 while the block evaluates group
+// s, and a block barrier after each group frees its buffer for group s + 2.  Waits are bounded; one that runs out sets
 // ERR_BIT_TILE_TIMEOUT and ends the issuing, and thread 0 waits (bounded) for
 // the copies already issued before the block moves on.
 template <bool MIXED, bool ENERGY, bool SWITCH>
@@ -836,7 +861,7 @@ __device__ __forceinline__ void pair_walk_staged(const PhysDev& d, const float2*
                                                  const float4* __restrict__ pos, int rows, bool active, bool nowrap,
                                                  float& fx, float& fy, float& fz, float& cxx, float& cyy, float& czz,
                                                  float& e_i, float& w_i) {
-    __shared__ __align__(128) uint32_t s_stage[2][kStageRows][kTB];
+    __shared__ __align__(128) uint32_t s_stage[2][kStageChunks][kChunkWords];
     __shared__ __align__(8) uint64_t s_bar[2];
     __shared__ int s_rows, s_fail;
     if (threadIdx.x == 0) {
@@ -849,19 +874,19 @@ __device__ __forceinline__ void pair_walk_staged(const PhysDev& d, const float2*
     __syncthreads();
     if (active && threadIdx.x % kStepLanes == 0) atomicMax(&s_rows, rows);
     __syncthreads();
-    const int brows = s_rows;
-    const int nst = (brows + kStageRows - 1) / kStageRows;
-    // row 0 of this block's particles: particle i0 = blockIdx.x * 32, word i0 * 8
-    const uint32_t* src0 = d.nl + (size_t)blockIdx.x * kTB;
-    const size_t stride = (size_t)d.n_pad * kGroup;
+    const int bchunks = (s_rows + 3) / 4;
+    const int nst = (bchunks + kStageChunks - 1) / kStageChunks;
+    // chunk 0 of this block's particles: particle i0 = blockIdx.x * 32, word i0 * 32
+    const uint32_t* src0 = d.nl + (size_t)blockIdx.x * kChunkWords;
+    const size_t stride = (size_t)d.n_pad * kListChunk;   // words between chunks
     int issued = 0;   // thread 0: groups issued
     auto issue = [&](int st) {
-        const int r0 = st * kStageRows, nr = min(kStageRows, brows - r0);
+        const int c0 = st * kStageChunks, nc = min(kStageChunks, bchunks - c0);
         uint64_t* bar = &s_bar[st & 1];
         fence_proxy_async_smem();
-        mbar_expect_tx(bar, (uint32_t)(nr * kTB * sizeof(uint32_t)));
-        for (int q = 0; q < nr; q++)
-            bulk_g2s(&s_stage[st & 1][q][0], src0 + (size_t)(r0 + q) * stride, kTB * sizeof(uint32_t), bar);
+        mbar_expect_tx(bar, (uint32_t)(nc * kChunkWords * sizeof(uint32_t)));
+        for (int q = 0; q < nc; q++)
+            bulk_g2s(&s_stage[st & 1][q][0], src0 + (size_t)(c0 + q) * stride, kChunkWords * sizeof(uint32_t), bar);
         issued = st + 1;
     };
     if (threadIdx.x == 0 && nst > 0) issue(0);
@@ -873,7 +898,7 @@ __device__ __forceinline__ void pair_walk_staged(const PhysDev& d, const float2*
             atomicOr(d.err, ERR_BIT_TILE_TIMEOUT);
         }
         const int nq = got ? max(0, min(kStageRows, rows - st * kStageRows)) : 0;
-        const uint32_t* srow = &s_stage[st & 1][0][threadIdx.x];
+        const uint32_t* srow = &s_stage[st & 1][0][threadIdx.x * 4];
         if (nowrap)
             pair_staged<MIXED, ENERGY, SWITCH, false>(d, row, pi, pos, srow, nq, fx, fy, fz, cxx, cyy, czz, e_i, w_i);
         else
@@ -904,23 +929,23 @@ __device__ __forceinline__ void step_body(const PhysDev& d, int cur, int slot, c
     float fx = 0.f, fy = 0.f, fz = 0.f, cxx = 0.f, cyy = 0.f, czz = 0.f;
     float e_i = 0.f, w_i = 0.f;
     const int cnt = active ? (int)d.nl_cnt[i] : 0;
-    const uint32_t stride = (uint32_t)d.n_pad * kGroup;
-    const ID* __restrict__ nl = reinterpret_cast<const ID*>(d.nl) + (uint32_t)i * kGroup + g;
-    // this lane's entries: g, g + kStepLanes, g + 2 kStepLanes, ... below cnt
+    // this lane's entries: g, g + 8, g + 16, ... below cnt
     const int rows = cnt > g ? (cnt - g + kStepLanes - 1) / kStepLanes : 0;
     // warps whose particles are all away from the box faces skip the minimum image
     const bool nowrap = __all_sync(0xffffffffu, !active || away_from_faces(d, pi));
 #if LIMA_STAGED_LIST
-    (void)nl;
-    (void)stride;
     pair_walk_staged<MIXED, ENERGY, SWITCH>(d, row, pi, pos, rows, active, nowrap, fx, fy, fz, cxx, cyy, czz, e_i, w_i);
 #else
+    // the lane's column of chunk 0 (nl_word with k = g), chunks n_pad * 8 vectors apart
+    using V = typename ChunkIds<ID>::V;
+    const V* __restrict__ col = reinterpret_cast<const V*>(d.nl) + (uint32_t)i * kGroup + g;
+    const uint32_t cstride = (uint32_t)d.n_pad * kGroup;
     if (nowrap)
-        pair_rows<MIXED, ENERGY, SWITCH, false, MIXED ? kMixedGathers : 4, ID>(d, row, pi, pos, nl, stride, rows, fx, fy,
-                                                                               fz, cxx, cyy, czz, e_i, w_i);
+        pair_rows<MIXED, ENERGY, SWITCH, false, ID>(d, row, pi, pos, col, cstride, rows, fx, fy, fz, cxx, cyy, czz, e_i,
+                                                    w_i);
     else
-        pair_rows<MIXED, ENERGY, SWITCH, true, MIXED ? kMixedGathers : 4, ID>(d, row, pi, pos, nl, stride, rows, fx, fy,
-                                                                              fz, cxx, cyy, czz, e_i, w_i);
+        pair_rows<MIXED, ENERGY, SWITCH, true, ID>(d, row, pi, pos, col, cstride, rows, fx, fy, fz, cxx, cyy, czz, e_i,
+                                                   w_i);
 #endif
     // reduce the kStepLanes lanes of this particle (warp shuffles)
 #pragma unroll

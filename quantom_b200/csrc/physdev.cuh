@@ -18,10 +18,11 @@
 //   xref[n_pad]     positions at the last rebuild (list validity check)
 //   force[n_pad]    total force of the last evaluation, w = per-particle potential energy
 //   nl[cap][n_pad]  Verlet list of sorted slots (uint16 ids when n_pad <= 65536,
-//                   else uint32), entry k of particle i at
-//                   ((k / kGroup) * n_pad + i) * kGroup + k % kGroup: the
-//                   kGroup lanes of one particle read kGroup consecutive
-//                   entries and consecutive particles follow each other
+//                   else uint32), entry k of particle i at word
+//                   ((k / 32) * n_pad + i) * 32 + (k % 8) * 4 + (k / 8) % 4
+//                   (nl_word): lane g of a particle's 8 reads entries
+//                   g, g + 8, g + 16, g + 24 as one vector, and consecutive
+//                   particles follow each other
 //   term_force      one float4 per (term, atom) of every bonded term; gathered
 //                   per particle through bterm_off/bterm_slot (CSR over orig)
 //   part[blocks][4] per-block FP64 partial sums of the last step kernel; the

@@ -289,8 +289,8 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
     d.n_cells = d.m * d.m * d.m;
     const double rho = d.n / ((double)d.L * d.L * d.L);
     const double expect = 4.0 / 3.0 * M_PI * (double)d.rlist * d.rlist * d.rlist * rho;
-    d.nl_cap = std::min((d.n + kGroup - 1) / kGroup * kGroup, (int)((1.6 * expect + 96) / kGroup + 1) * kGroup);
-    d.nl_cap = std::max(d.nl_cap, 4 * kGroup);
+    d.nl_cap = std::min(nl_round_cap(d.n), nl_round_cap((int)(1.6 * expect + 96)));
+    d.nl_cap = std::max(d.nl_cap, kListChunk);
     d.nl16 = list_ids_16bit(d.n_pad) ? 1 : 0;
 
     // every fixed-size buffer in one allocation; the list separately (it may grow)
@@ -498,7 +498,7 @@ bool phys_fit_list(PhysDev& d, cudaStream_t s, std::vector<void*>& allocs) {
     cudaMemcpyAsync(&need, d.nl_need, sizeof(int), cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
     if (!(err & ERR_BIT_PHYS_LIST_OVERFLOW) || need <= d.nl_cap) return false;
-    const int cap = std::min((d.n + kGroup - 1) / kGroup * kGroup, ((need * 5 / 4 + 32) / kGroup + 1) * kGroup);
+    const int cap = std::min(nl_round_cap(d.n), nl_round_cap(need * 5 / 4 + 32));
     uint32_t* nl = reinterpret_cast<uint32_t*>(dalloc<uint8_t>(allocs, (size_t)cap * d.n_pad * nl_entry_bytes(d), s));   // throws like the other allocations
     for (auto it = allocs.begin(); it != allocs.end(); ++it)
         if (*it == d.nl) {
@@ -680,7 +680,7 @@ uint32_t phys_read_list(const PhysDev& d, uint32_t* offsets, uint32_t* ids) {
         if (ids) {
             std::vector<uint32_t> row(cnt[k]);
             for (uint32_t e = 0; e < cnt[k]; e++)
-                row[e] = orig[nl[((size_t)(e / kGroup) * d.n_pad + k) * kGroup + e % kGroup]];
+                row[e] = orig[nl[nl_word((uint32_t)d.n_pad, k, e)]];
             std::sort(row.begin(), row.end());
             std::copy(row.begin(), row.end(), ids + pos);
         }

@@ -13,10 +13,9 @@ constexpr int kBuildWarps = 4;   // warps per block of the list build (8 particl
 constexpr int kMaxTypes = 32;    // LIMA_MAX_ATOM_TYPES
 constexpr int kScanThreads = 1024;
 
-// lanes per particle in the step kernel: 8 (one list column each) or 4 (two
-// columns each, columns g and g + 4 of every 8-entry row)
+// lanes per particle in the step kernel: one list column each
 constexpr int kStepLanes = 8;
-static_assert(kStepLanes == 8 || kStepLanes == 4, "the step kernel reads 8-entry list rows with 8 or 4 lanes");
+static_assert(kStepLanes == kGroup, "the step kernel gives each lane one list column");
 // the step kernel reads its list rows from shared memory, staged by bulk
 // copies in groups of kStageRows rows (false: per-lane loads from the list).
 // Built into liblima_b200_staged.so (LIMA_STAGED_LIST=1) beside the default
@@ -26,8 +25,21 @@ static_assert(kStepLanes == 8 || kStepLanes == 4, "the step kernel reads 8-entry
 #endif
 constexpr bool kStagedList = LIMA_STAGED_LIST != 0;
 constexpr int kStageRows = 8;
-static_assert(!kStagedList || kStepLanes == 8, "the staged list walk gives each lane one list column");
-// list entry `idx` (a word index of the blocked layout) in either id width
+// Verlet-list layout: entry k of particle slot i is column k % 8 of row k / 8,
+// and a particle's rows come in chunks of kListChunk / 8 = 4: column g of
+// chunk q holds rows 4q .. 4q + 3 in consecutive words, so the lane that owns
+// column g reads its next four entries with one 8-byte (16-bit ids) or
+// 16-byte (32-bit ids) load, and the 32 words of one chunk of consecutive
+// particles follow each other.  The capacity per particle is a multiple of
+// kListChunk.
+constexpr int kListChunk = 32;
+static_assert(kGroup == 8 && kListChunk == 4 * kGroup, "chunks of four 8-entry rows");
+__host__ __device__ inline uint32_t nl_word(uint32_t n_pad, uint32_t i, uint32_t k) {
+    return ((k >> 5) * n_pad + i) * 32u + (k & 7u) * 4u + ((k >> 3) & 3u);
+}
+// list capacity per particle: `want` entries rounded up to whole chunks
+__host__ __device__ inline int nl_round_cap(int want) { return (want + kListChunk - 1) / kListChunk * kListChunk; }
+// list entry `idx` (a word index of the layout above) in either id width
 __device__ __forceinline__ uint32_t nl_load(const PhysDev& d, size_t idx) {
     return d.nl16 ? (uint32_t)reinterpret_cast<const uint16_t*>(d.nl)[idx] : d.nl[idx];
 }

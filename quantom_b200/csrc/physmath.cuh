@@ -18,6 +18,15 @@ __device__ __forceinline__ bool away_from_faces(const PhysDev& d, float4 p) {
     return p.x >= m && p.x <= hi && p.y >= m && p.y <= hi && p.z >= m && p.z <= hi;
 }
 
+// 1/x by the special-function unit's approximate reciprocal (PTX
+// rcp.approx.ftz.f32, relative error within 2^-23); x is a squared pair
+// distance, positive and far from the denormal and overflow ranges.
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // One pair, branch-free: out-of-cutoff pairs contribute zero through a
 // select, the switch is evaluated for every pair (S = 1, S' = 0 below r_on).
 // WRAP false: i is away_from_faces, the plain difference is the minimum image.
@@ -29,7 +38,7 @@ __device__ __forceinline__ void lj_pair(const PhysDev& d, const float2* __restri
     const float dz = WRAP ? mimg(pj.z - pi.z, d.L, d.invL) : pj.z - pi.z;
     const float r2 = dx * dx + dy * dy + dz * dz;
     const float2 tab = row[__float_as_int(pj.w)];
-    const float inv = __fdividef(1.f, r2);
+    const float inv = rcp_approx(r2);
     const float sr2 = tab.x * inv;
     const float sr6 = sr2 * sr2 * sr2;
     float fr = 6.f * tab.y * inv * sr6 * (2.f * sr6 - 1.f);   // F_j / r_vec
