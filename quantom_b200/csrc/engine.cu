@@ -67,9 +67,10 @@ struct lima_ctx {
     lima::RefDev ref{};
     lima::PhysDev phys{};
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    // physics with dynamic lists: [parity][energy] step graphs with a conditional rebuild
-    cudaGraphExec_t dgraph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
-    int dgraph_kernels[2] = {0, 0};
+    // physics with dynamic lists: [parity][plain, energy, energy + frame log]
+    // step graphs, each with the rebuild as a device tail launch
+    cudaGraphExec_t dgraph[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+    int dgraph_kernels[3] = {0, 0, 0};
     uint64_t host_rebuilds = 0;   // list builds launched by the host (creation, set_state, build_nlist, ...)
     // physics: differentiable parameters and the loss / adjoint buffers
     lima::PhysParams params;
@@ -422,6 +423,17 @@ void ref_nlist_now(lima_ctx* c) {
 }
 
 // One step.  prof (nullable): [0] before any list rebuild, [1] after it, then
+// the frame-log kernels of a logged step, captured into its step graph
+struct LogCapture {
+    const lima::FrameLog* log;
+    const lima::PhysDev* d;
+    int cur;
+};
+int capture_frame_log(void* ctx, cudaStream_t s) {
+    const LogCapture* lc = static_cast<const LogCapture*>(ctx);
+    return lima::framelog_launch(*lc->log, *lc->d, lc->cur, s);
+}
+
 // the four per-kernel-group events of ref_step_kernels / phys_step_kernels;
 // with prof the step is launched directly instead of through the graph.
 void one_step(lima_ctx* c, cudaEvent_t* prof) {
@@ -468,14 +480,20 @@ void one_step(lima_ctx* c, cudaEvent_t* prof) {
         const bool logged = c->log.on && (c->step % static_cast<uint64_t>(c->log.every)) == 0;
         const bool energy = logged || (c->p.energy_period > 0 && (c->step % c->p.energy_period) == 0);
         if (!prof) {
-            cudaGraphExec_t& g = c->dgraph[c->cur][energy ? 1 : 0];
+            // a logged step records its frame inside the step graph (the frame
+            // kernels take their ring position from the device)
+            const int v = logged ? 2 : (energy ? 1 : 0);
+            cudaGraphExec_t& g = c->dgraph[c->cur][v];
             if (!g) {   // instantiated on first use: a short run pays only for the variants it steps
-                const int k = lima::phys_capture_dynamic(c->phys, c->cur, energy, c->stream, &g);
+                LogCapture lc{&c->log, &c->phys, c->cur};
+                const int k = lima::phys_capture_dynamic(c->phys, c->cur, energy, c->stream, &g,
+                                                         logged ? capture_frame_log : nullptr, &lc);
                 need(k > 0, LIMA_ERR_CUDA, "cannot build the step graph of a dynamic pair list");
-                c->dgraph_kernels[energy ? 1 : 0] = k;
+                c->dgraph_kernels[v] = k;
             }
             cuda_ok(cudaGraphLaunch(g, c->stream), "cudaGraphLaunch");
-            c->launches += c->dgraph_kernels[energy ? 1 : 0];
+            c->launches += c->dgraph_kernels[v];
+            if (logged) lima::framelog_note(c->log, c->step, c->stream);
         } else {   // profiling: the same kernels launched directly, the rebuild decided on the host
             if (dyn_rebuild) {
                 lima::phys_rebuild(c->phys, c->cur, c->stream);
@@ -486,7 +504,7 @@ void one_step(lima_ctx* c, cudaEvent_t* prof) {
             c->launches += lima::phys_step_kernels(c->phys, c->cur, c->stream, energy, prof + 2);
             cuda_ok(cudaEventRecord(prof[5], c->stream), "cudaEventRecord");
         }
-        if (logged) c->launches += lima::framelog_record(c->log, c->phys, c->cur, c->step, c->stream);
+        if (logged && prof) c->launches += lima::framelog_record(c->log, c->phys, c->cur, c->step, c->stream);
         c->cur ^= 1;
         c->step++;
     } else {
@@ -1175,6 +1193,12 @@ lima_status lima_log_start(lima_ctx* c, const lima_log_params* p) {
         need((p->flags & ~(LIMA_LOG_TRAJ | LIMA_LOG_POTE | LIMA_LOG_TRAIN)) == 0, LIMA_ERR_ARGUMENT,
              "unknown log flags");
         sync_checked(c);
+        // the logged-step graphs hold the old log's buffers
+        for (auto& row : c->dgraph)
+            if (row[2]) {
+                cudaGraphExecDestroy(row[2]);
+                row[2] = nullptr;
+            }
         std::vector<int> np;
         for (const auto& cp : c->comps) np.push_back(cp.n_particles);
         std::string msg;

@@ -22,13 +22,13 @@
 namespace lima {
 namespace {
 
-__global__ void __launch_bounds__(kTB) k_log_frame(PhysDev d, FrameLogDev g, int cur, int r) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k == 0 && g.energies) {   // the step kernel's FP64 totals of the logged step
-        double* e = g.energies + (size_t)r * LIMA_E_COUNT;
-        for (int q = 0; q < LIMA_E_COUNT; q++) e[q] = d.e_last[q];
-    }
-    if (k >= d.n) return;
+// the ring position of the frame being written
+__device__ __forceinline__ int ring_pos(const FrameLogDev& g) {
+    return (int)(__ldcg(g.frame_ctr) % (unsigned long long)g.ring);
+}
+
+// one particle's entries of frame r
+__device__ __forceinline__ void log_frame_particle(const PhysDev& d, const FrameLogDev& g, int cur, int r, int k) {
     const uint32_t o = d.orig_of_sorted[k];
     const uint32_t slot = g.ref_slot[o];
     float4 p = d.pos[cur][k];
@@ -77,8 +77,28 @@ __global__ void __launch_bounds__(kTB) k_log_frame(PhysDev d, FrameLogDev g, int
     }
 }
 
+__global__ void __launch_bounds__(kTB) k_log_frame(PhysDev d, FrameLogDev g, int cur) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = ring_pos(g);
+    if (k == 0 && g.energies) {   // the step kernel's FP64 totals of the logged step
+        double* e = g.energies + (size_t)r * LIMA_E_COUNT;
+        for (int q = 0; q < LIMA_E_COUNT; q++) e[q] = d.e_last[q];
+    }
+    if (k < d.n) log_frame_particle(d, g, cur, r, k);
+    // the last block to finish moves the ring on (every block has read r)
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(g.blocks_done, 1u) == gridDim.x - 1u) {
+            *g.blocks_done = 0u;
+            *g.frame_ctr += 1ull;
+        }
+    }
+}
+
 template <bool SWITCH>
-__global__ void __launch_bounds__(kTB) k_log_train(PhysDev d, FrameLogDev g, int cur, int r) {
+__global__ void __launch_bounds__(kTB) k_log_train(PhysDev d, FrameLogDev g, int cur) {
+    const int r = ring_pos(g);   // k_log_frame of the same frame runs after this kernel
     extern __shared__ float2 s_tab[];
     const int nt2 = d.n_types * d.n_types;
     for (int q = threadIdx.x; q < nt2; q += blockDim.x) s_tab[q] = d.lj_table[q];
@@ -306,6 +326,7 @@ void drain_sync(FrameLog& g, cudaStream_t s) {
     g.steps.insert(g.steps.end(), g.ring_steps.begin(), g.ring_steps.end());
     g.ring_steps.clear();
     g.in_ring = 0;
+    cudaMemsetAsync(v.frame_ctr, 0, sizeof(unsigned long long), s);
 }
 
 // the frames in the device ring -> the next pinned buffer (absorbing what it held first)
@@ -323,6 +344,7 @@ void drain(FrameLog& g, cudaStream_t s) {
     g.ring_steps.clear();
     g.in_ring = 0;
     g.next_buf ^= 1;
+    cudaMemsetAsync(g.dev.frame_ctr, 0, sizeof(unsigned long long), s);   // after the copy, in stream order
 }
 
 }  // namespace
@@ -368,10 +390,13 @@ void framelog_start(FrameLog& g, int n_s, const std::vector<int>& n_compound_par
     v.train = (p.flags & LIMA_LOG_TRAIN) && n_c ? grow<float>(g, f * v.n_train * kTrainValues * 3) : nullptr;
     v.energies = grow<double>(g, f * LIMA_E_COUNT);
     v.logdata = grow<float>(g, f * kLogDataFloats);
+    v.frame_ctr = grow<unsigned long long>(g, 1);
+    v.blocks_done = grow<unsigned int>(g, 1);
     const Sections R = sections(v, v.ring);
     g.ring_bytes = R.total;
-    bool ok = ref_slot && v.energies && v.logdata && (!(p.flags & LIMA_LOG_TRAJ) || v.traj) &&
-              (!(p.flags & LIMA_LOG_POTE) || v.potE) && (!(p.flags & LIMA_LOG_TRAIN) || !n_c || v.train);
+    bool ok = ref_slot && v.energies && v.logdata && v.frame_ctr && v.blocks_done &&
+              (!(p.flags & LIMA_LOG_TRAJ) || v.traj) && (!(p.flags & LIMA_LOG_POTE) || v.potE) &&
+              (!(p.flags & LIMA_LOG_TRAIN) || !n_c || v.train);
     if (!ok) {
         const cudaStream_t st = g.stream;
         framelog_free(g);
@@ -384,6 +409,8 @@ void framelog_start(FrameLog& g, int n_s, const std::vector<int>& n_compound_par
     v.ref_slot = ref_slot;
     // set-up copies in the engine's stream order; the host arrays live until the sync below
     cudaMemcpyAsync(ref_slot, slot.data(), sizeof(uint32_t) * slot.size(), cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(v.frame_ctr, 0, sizeof(unsigned long long), s);
+    cudaMemsetAsync(v.blocks_done, 0, sizeof(unsigned int), s);
     if (v.traj) cudaMemsetAsync(v.traj, 0, f * v.n_slots * 3 * sizeof(float), s);
     if (v.potE) cudaMemsetAsync(v.potE, 0, f * v.n_slots * sizeof(double), s);
     std::vector<float> pad;
@@ -401,24 +428,32 @@ void framelog_start(FrameLog& g, int n_s, const std::vector<int>& n_compound_par
     g.on = true;
 }
 
-int framelog_record(FrameLog& g, const PhysDev& d, int cur, uint64_t step, cudaStream_t s) {
+int framelog_launch(const FrameLog& g, const PhysDev& d, int cur, cudaStream_t s) {
     const FrameLogDev& v = g.dev;
-    const int r = g.in_ring;
-    k_log_frame<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d, v, cur, r);
     int launched = 1;
-    if (v.train && d.n_cp > 0) {
+    if (v.train && d.n_cp > 0) {   // before k_log_frame, which moves the ring position on
         const int nb = (int)(((size_t)d.n_cp * kGroup + kTB - 1) / kTB);
         const size_t smem = sizeof(float2) * d.n_types * d.n_types;
         if (d.use_switch)
-            k_log_train<true><<<nb, kTB, smem, s>>>(d, v, cur, r);
+            k_log_train<true><<<nb, kTB, smem, s>>>(d, v, cur);
         else
-            k_log_train<false><<<nb, kTB, smem, s>>>(d, v, cur, r);
+            k_log_train<false><<<nb, kTB, smem, s>>>(d, v, cur);
         launched++;
     }
+    k_log_frame<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d, v, cur);
+    return launched;
+}
+
+void framelog_note(FrameLog& g, uint64_t step, cudaStream_t s) {
     g.ring_steps.push_back(step);
     g.in_ring++;
     g.frames_logged++;
-    if (g.in_ring == v.ring) drain(g, s);
+    if (g.in_ring == g.dev.ring) drain(g, s);
+}
+
+int framelog_record(FrameLog& g, const PhysDev& d, int cur, uint64_t step, cudaStream_t s) {
+    const int launched = framelog_launch(g, d, cur, s);
+    framelog_note(g, step, s);
     return launched;
 }
 

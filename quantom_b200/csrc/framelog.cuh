@@ -41,6 +41,11 @@ struct FrameLogDev {
     float* train;           // [ring][n_train][3 values][3]
     double* energies;       // [ring][LIMA_E_COUNT]
     float* logdata;         // [ring][10]
+    // physics: frames written to the ring since its last drain; the kernels of
+    // a frame write at ring position frame_ctr % ring, and the last block of
+    // k_log_frame advances it (so a captured step graph can log)
+    unsigned long long* frame_ctr;
+    unsigned int* blocks_done;
 };
 
 struct FrameLog {
@@ -74,6 +79,11 @@ void framelog_start(FrameLog& g, int n_s, const std::vector<int>& n_compound_par
 void framelog_free(FrameLog& g);
 // after the energy variant of step `step` on parity `cur` (accumulator slot `cur`)
 int framelog_record(FrameLog& g, const PhysDev& d, int cur, uint64_t step, cudaStream_t s);
+// the two halves of framelog_record: the frame's kernels (stream-ordered, also
+// inside a graph capture) and the host's record of the frame (ring position,
+// drain when the ring is full)
+int framelog_launch(const FrameLog& g, const PhysDev& d, int cur, cudaStream_t s);
+void framelog_note(FrameLog& g, uint64_t step, cudaStream_t s);
 // reference semantics: after step `step`, whose positions are in parity `after`
 int framelog_record_ref(FrameLog& g, const RefDev& d, int after, uint64_t step, cudaStream_t s);
 // every frame launched so far into the host store (waits for the stream)

@@ -725,7 +725,7 @@ __device__ __forceinline__ void finish_sums(const PhysDev& d, int slot, cudaGrap
 }  // namespace
 
 // ------------------------------------------------------------------ the step ---
-// (lj_pair: physmath.cuh)
+// (lj_pair_step: physmath.cuh)
 // The four ids of one chunk column (nl_word): one 8-byte load of 16-bit ids
 // or one 16-byte load of 32-bit ids.
 template <typename ID>
@@ -756,8 +756,9 @@ struct ChunkIds<uint32_t> {
 // chunks), each chunk one vector load and four position gathers in flight.
 // In the last, partial chunk the words past the lane's count are not ids
 // (the gathers for them re-read the first entry and are not evaluated).
-// MIXED: compensated sums every two chunks (8 pairs).
-template <bool MIXED, bool ENERGY, bool SWITCH, bool WRAP, typename ID>
+// MIXED: compensated sums every two chunks (8 pairs).  WM: the axes that take
+// the minimum image.
+template <bool MIXED, bool ENERGY, bool SWITCH, int WM, typename ID>
 __device__ __forceinline__ void pair_rows(const PhysDev& d, const float2* row, float4 pi, const float4* __restrict__ pos,
                                           const typename ChunkIds<ID>::V* __restrict__ col, uint32_t cstride, int rows,
                                           float& fx, float& fy, float& fz, float& cxx, float& cyy, float& czz,
@@ -772,10 +773,10 @@ __device__ __forceinline__ void pair_rows(const PhysDev& d, const float2* row, f
             uint32_t j0, j1, j2, j3;
             ChunkIds<ID>::split(__ldg(col + off), j0, j1, j2, j3);
             const float4 p0 = __ldg(pos + j0), p1 = __ldg(pos + j1), p2 = __ldg(pos + j2), p3 = __ldg(pos + j3);
-            lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p0, px, py, pz, e_i, w_i);
-            lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p1, px, py, pz, e_i, w_i);
-            lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p2, px, py, pz, e_i, w_i);
-            lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p3, px, py, pz, e_i, w_i);
+            lj_pair_step<ENERGY, SWITCH, WM>(d, row, pi, p0, px, py, pz, e_i, w_i);
+            lj_pair_step<ENERGY, SWITCH, WM>(d, row, pi, p1, px, py, pz, e_i, w_i);
+            lj_pair_step<ENERGY, SWITCH, WM>(d, row, pi, p2, px, py, pz, e_i, w_i);
+            lj_pair_step<ENERGY, SWITCH, WM>(d, row, pi, p3, px, py, pz, e_i, w_i);
         }
         if (MIXED) {
             ds_add(fx, cxx, px);
@@ -794,9 +795,9 @@ __device__ __forceinline__ void pair_rows(const PhysDev& d, const float2* row, f
         const float4 p1 = __ldg(pos + (tail > 1 ? j1 : j0));
         const float4 p2 = __ldg(pos + (tail > 2 ? j2 : j0));
         float px = 0.f, py = 0.f, pz = 0.f;
-        lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p0, px, py, pz, e_i, w_i);
-        if (tail > 1) lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p1, px, py, pz, e_i, w_i);
-        if (tail > 2) lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p2, px, py, pz, e_i, w_i);
+        lj_pair_step<ENERGY, SWITCH, WM>(d, row, pi, p0, px, py, pz, e_i, w_i);
+        if (tail > 1) lj_pair_step<ENERGY, SWITCH, WM>(d, row, pi, p1, px, py, pz, e_i, w_i);
+        if (tail > 2) lj_pair_step<ENERGY, SWITCH, WM>(d, row, pi, p2, px, py, pz, e_i, w_i);
         (void)j3;
         if (MIXED) {
             ds_add(fx, cxx, px);
@@ -817,7 +818,7 @@ __device__ __forceinline__ void pair_rows(const PhysDev& d, const float2* row, f
 constexpr int kStageChunks = kStageRows / 4;   // list chunks per staged group
 constexpr int kChunkWords = kTB * 4;           // words of one chunk of a block's 32 particles
 __device__ __forceinline__ int staged_at(int q) { return (q >> 2) * kChunkWords + (q & 3); }
-template <bool MIXED, bool ENERGY, bool SWITCH, bool WRAP>
+template <bool MIXED, bool ENERGY, bool SWITCH, int WM>
 __device__ __forceinline__ void pair_staged(const PhysDev& d, const float2* row, float4 pi,
                                             const float4* __restrict__ pos, const uint32_t* srow, int nq, float& fx,
                                             float& fy, float& fz, float& cxx, float& cyy, float& czz, float& e_i,
@@ -830,13 +831,13 @@ __device__ __forceinline__ void pair_staged(const PhysDev& d, const float2* row,
         const uint32_t j0 = min(srow[staged_at(q)], lim), j1 = min(srow[staged_at(q + 1)], lim);
         const uint32_t j2 = min(srow[staged_at(q + 2)], lim), j3 = min(srow[staged_at(q + 3)], lim);
         const float4 p0 = __ldg(pos + j0), p1 = __ldg(pos + j1), p2 = __ldg(pos + j2), p3 = __ldg(pos + j3);
-        lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p0, px, py, pz, e_i, w_i);
-        lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p1, px, py, pz, e_i, w_i);
-        lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p2, px, py, pz, e_i, w_i);
-        lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, p3, px, py, pz, e_i, w_i);
+        lj_pair_step<ENERGY, SWITCH, WM>(d, row, pi, p0, px, py, pz, e_i, w_i);
+        lj_pair_step<ENERGY, SWITCH, WM>(d, row, pi, p1, px, py, pz, e_i, w_i);
+        lj_pair_step<ENERGY, SWITCH, WM>(d, row, pi, p2, px, py, pz, e_i, w_i);
+        lj_pair_step<ENERGY, SWITCH, WM>(d, row, pi, p3, px, py, pz, e_i, w_i);
     }
     for (; q < nq; q++)
-        lj_pair<ENERGY, SWITCH, WRAP>(d, row, pi, __ldg(pos + min(srow[staged_at(q)], lim)), px, py, pz, e_i, w_i);
+        lj_pair_step<ENERGY, SWITCH, WM>(d, row, pi, __ldg(pos + min(srow[staged_at(q)], lim)), px, py, pz, e_i, w_i);
     if (MIXED) {
         ds_add(fx, cxx, px);
         ds_add(fy, cyy, py);
@@ -858,7 +859,7 @@ __device__ __forceinline__ void pair_staged(const PhysDev& d, const float2* row,
 // the copies already issued before the block moves on.
 template <bool MIXED, bool ENERGY, bool SWITCH>
 __device__ __forceinline__ void pair_walk_staged(const PhysDev& d, const float2* row, float4 pi,
-                                                 const float4* __restrict__ pos, int rows, bool active, bool nowrap,
+                                                 const float4* __restrict__ pos, int rows, bool active, unsigned wm,
                                                  float& fx, float& fy, float& fz, float& cxx, float& cyy, float& czz,
                                                  float& e_i, float& w_i) {
     __shared__ __align__(128) uint32_t s_stage[2][kStageChunks][kChunkWords];
@@ -899,10 +900,16 @@ __device__ __forceinline__ void pair_walk_staged(const PhysDev& d, const float2*
         }
         const int nq = got ? max(0, min(kStageRows, rows - st * kStageRows)) : 0;
         const uint32_t* srow = &s_stage[st & 1][0][threadIdx.x * 4];
-        if (nowrap)
-            pair_staged<MIXED, ENERGY, SWITCH, false>(d, row, pi, pos, srow, nq, fx, fy, fz, cxx, cyy, czz, e_i, w_i);
-        else
-            pair_staged<MIXED, ENERGY, SWITCH, true>(d, row, pi, pos, srow, nq, fx, fy, fz, cxx, cyy, czz, e_i, w_i);
+#define LIMA_STAGED_CALL(WM) \
+    pair_staged<MIXED, ENERGY, SWITCH, WM>(d, row, pi, pos, srow, nq, fx, fy, fz, cxx, cyy, czz, e_i, w_i)
+        switch (wm) {
+            case 0: LIMA_STAGED_CALL(0); break;
+            case 1: LIMA_STAGED_CALL(1); break;
+            case 2: LIMA_STAGED_CALL(2); break;
+            case 4: LIMA_STAGED_CALL(4); break;
+            default: LIMA_STAGED_CALL(7); break;
+        }
+#undef LIMA_STAGED_CALL
         __syncthreads();
     }
     // after a timeout: the groups issued and not yet seen complete
@@ -914,9 +921,13 @@ __device__ __forceinline__ void pair_walk_staged(const PhysDev& d, const float2*
 
 template <bool MIXED, bool ENERGY, bool INTEGRATE, bool SWITCH, bool TAIL, typename ID>
 __device__ __forceinline__ void step_body(const PhysDev& d, int cur, int slot, cudaGraphExec_t tail) {
+    // the LJ table as lj_pair_step reads it: (sigma^2, 24 eps)
     extern __shared__ float2 s_tab[];
     const int nt2 = d.n_types * d.n_types;
-    for (int q = threadIdx.x; q < nt2; q += blockDim.x) s_tab[q] = d.lj_table[q];
+    for (int q = threadIdx.x; q < nt2; q += blockDim.x) {
+        const float2 t = d.lj_table[q];
+        s_tab[q] = make_float2(t.x, 6.f * t.y);
+    }
     __syncthreads();
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) / kStepLanes;
     const int g = threadIdx.x % kStepLanes;
@@ -931,21 +942,26 @@ __device__ __forceinline__ void step_body(const PhysDev& d, int cur, int slot, c
     const int cnt = active ? (int)d.nl_cnt[i] : 0;
     // this lane's entries: g, g + 8, g + 16, ... below cnt
     const int rows = cnt > g ? (cnt - g + kStepLanes - 1) / kStepLanes : 0;
-    // warps whose particles are all away from the box faces skip the minimum image
-    const bool nowrap = __all_sync(0xffffffffu, !active || away_from_faces(d, pi));
+    // the axes that take the minimum image: those on which some particle of the
+    // warp lies within r_c of a face (one axis alone, or all three)
+    const unsigned wm = __reduce_or_sync(0xffffffffu, active ? face_axes(d, pi) : 0u);
 #if LIMA_STAGED_LIST
-    pair_walk_staged<MIXED, ENERGY, SWITCH>(d, row, pi, pos, rows, active, nowrap, fx, fy, fz, cxx, cyy, czz, e_i, w_i);
+    pair_walk_staged<MIXED, ENERGY, SWITCH>(d, row, pi, pos, rows, active, wm, fx, fy, fz, cxx, cyy, czz, e_i, w_i);
 #else
     // the lane's column of chunk 0 (nl_word with k = g), chunks n_pad * 8 vectors apart
     using V = typename ChunkIds<ID>::V;
     const V* __restrict__ col = reinterpret_cast<const V*>(d.nl) + (uint32_t)i * kGroup + g;
     const uint32_t cstride = (uint32_t)d.n_pad * kGroup;
-    if (nowrap)
-        pair_rows<MIXED, ENERGY, SWITCH, false, ID>(d, row, pi, pos, col, cstride, rows, fx, fy, fz, cxx, cyy, czz, e_i,
-                                                    w_i);
-    else
-        pair_rows<MIXED, ENERGY, SWITCH, true, ID>(d, row, pi, pos, col, cstride, rows, fx, fy, fz, cxx, cyy, czz, e_i,
-                                                   w_i);
+#define LIMA_ROWS_CALL(WM) \
+    pair_rows<MIXED, ENERGY, SWITCH, WM, ID>(d, row, pi, pos, col, cstride, rows, fx, fy, fz, cxx, cyy, czz, e_i, w_i)
+    switch (wm) {
+        case 0: LIMA_ROWS_CALL(0); break;
+        case 1: LIMA_ROWS_CALL(1); break;
+        case 2: LIMA_ROWS_CALL(2); break;
+        case 4: LIMA_ROWS_CALL(4); break;
+        default: LIMA_ROWS_CALL(7); break;
+    }
+#undef LIMA_ROWS_CALL
 #endif
     // reduce the kStepLanes lanes of this particle (warp shuffles)
 #pragma unroll

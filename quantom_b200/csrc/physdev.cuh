@@ -55,6 +55,7 @@ struct PhysDev {
     int n_cp;           // compound particles
     int n_c, n_s;
     float L, invL, rc, rc2, rlist, rlist2, ron2, inv_sw_d, half_skin2;   // inv_sw_d = 1/(rc^2 - r_on^2)
+    float sw_c0, sw_k10;        // rc^2 inv_sw_d and 10 inv_sw_d (the step kernel's switch)
     int use_switch;
     double dt;
     int precision;      // lima_precision
@@ -153,8 +154,12 @@ void phys_prime(PhysDev& d, int cur, cudaStream_t s);
 // allocs: the pool allocations of phys_setup (the list is one of them)
 bool phys_fit_list(PhysDev& d, cudaStream_t s, std::vector<void*>& allocs);
 // dynamic lists: the step graph of parity `cur` (the step kernel, which tail-launches
-// the rebuild when one is due); returns its kernel count, or -1 if the graph cannot be built
-int phys_capture_dynamic(const PhysDev& d, int cur, bool energy, cudaStream_t s, cudaGraphExec_t* out);
+// the rebuild when one is due); returns its kernel count, or -1 if the graph cannot be built.
+// extra (nullable): more kernels for the same graph, launched into the
+// capturing stream after the step (the frame log of a logged step), returning
+// how many it launched
+int phys_capture_dynamic(const PhysDev& d, int cur, bool energy, cudaStream_t s, cudaGraphExec_t* out,
+                         int (*extra)(void*, cudaStream_t) = nullptr, void* extra_ctx = nullptr);
 bool phys_rebuild_pending(const PhysDev& d, cudaStream_t s);
 unsigned long long phys_device_rebuilds(const PhysDev& d, cudaStream_t s);
 // the device-launchable rebuild graphs of both parities (after the list capacity is final)

@@ -159,6 +159,8 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
     const float ron = d.use_switch ? p.switch_on : p.cutoff;
     d.ron2 = ron * ron;
     d.inv_sw_d = d.use_switch ? 1.f / (d.rc2 - d.ron2) : 0.f;
+    d.sw_c0 = d.rc2 * d.inv_sw_d;
+    d.sw_k10 = 10.f * d.inv_sw_d;
     d.dt = p.dt;
     d.precision = p.precision;
     d.thermostat = p.thermostat;
@@ -578,9 +580,11 @@ void phys_free_rebuild(PhysDev& d) {
     }
 }
 
-// The step graph of a dynamic list: the step kernel alone, with the rebuild
-// of the next parity as its tail launch.
-int phys_capture_dynamic(const PhysDev& d, int cur, bool energy, cudaStream_t s, cudaGraphExec_t* out) {
+// The step graph of a dynamic list: the bonded and step kernels (and the
+// `extra` kernels), with the rebuild of the next parity as the step kernel's
+// tail launch, which runs after the whole graph.
+int phys_capture_dynamic(const PhysDev& d, int cur, bool energy, cudaStream_t s, cudaGraphExec_t* out,
+                         int (*extra)(void*, cudaStream_t), void* extra_ctx) {
     *out = nullptr;
     if (!d.rebuild_exec[cur ^ 1]) return -1;
     cudaGraph_t g = nullptr;
@@ -588,7 +592,8 @@ int phys_capture_dynamic(const PhysDev& d, int cur, bool energy, cudaStream_t s,
         cudaGetLastError();
         return -1;
     }
-    const int k = phys_step_kernels(d, cur, s, energy, nullptr, true);
+    int k = phys_step_kernels(d, cur, s, energy, nullptr, true);
+    if (extra) k += extra(extra_ctx, s);
     if (cudaStreamEndCapture(s, &g) != cudaSuccess || !g) {
         end_open_capture(s);
         return -1;
