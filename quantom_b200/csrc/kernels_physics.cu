@@ -757,21 +757,28 @@ struct ChunkIds<uint32_t> {
 // In the last, partial chunk the words past the lane's count are not ids
 // (the gathers for them re-read the first entry and are not evaluated).
 // MIXED: compensated sums every two chunks (8 pairs).  WM: the axes that take
-// the minimum image.
+// the minimum image.  The plain FP32 walk loads each chunk's ids one chunk
+// ahead (the mixed walk, and the energies of an unswitched cutoff, have no
+// registers to spare for it).
 template <bool MIXED, bool ENERGY, bool SWITCH, int WM, typename ID>
 __device__ __forceinline__ void pair_rows(const PhysDev& d, const float2* row, float4 pi, const float4* __restrict__ pos,
                                           const typename ChunkIds<ID>::V* __restrict__ col, uint32_t cstride, int rows,
                                           float& fx, float& fy, float& fz, float& cxx, float& cyy, float& czz,
                                           float& e_i, float& w_i) {
+    constexpr bool kAhead = !MIXED && (SWITCH || !ENERGY);
     const int full = rows >> 2, tail = rows & 3;
+    const int nch = full + (tail ? 1 : 0);
     uint32_t off = 0;
     int c = 0;
+    typename ChunkIds<ID>::V nxt{};
+    if (kAhead && nch > 0) nxt = __ldg(col);
     while (c < full) {
         const int cend = MIXED ? min(full, c + 2) : full;
         float px = 0.f, py = 0.f, pz = 0.f;
         for (; c < cend; c++, off += cstride) {
             uint32_t j0, j1, j2, j3;
-            ChunkIds<ID>::split(__ldg(col + off), j0, j1, j2, j3);
+            ChunkIds<ID>::split(kAhead ? nxt : __ldg(col + off), j0, j1, j2, j3);
+            if (kAhead && c + 1 < nch) nxt = __ldg(col + off + cstride);
             const float4 p0 = __ldg(pos + j0), p1 = __ldg(pos + j1), p2 = __ldg(pos + j2), p3 = __ldg(pos + j3);
             lj_pair_step<ENERGY, SWITCH, WM>(d, row, pi, p0, px, py, pz, e_i, w_i);
             lj_pair_step<ENERGY, SWITCH, WM>(d, row, pi, p1, px, py, pz, e_i, w_i);
@@ -790,7 +797,7 @@ __device__ __forceinline__ void pair_rows(const PhysDev& d, const float2* row, f
     }
     if (tail) {
         uint32_t j0, j1, j2, j3;
-        ChunkIds<ID>::split(__ldg(col + off), j0, j1, j2, j3);
+        ChunkIds<ID>::split(kAhead ? nxt : __ldg(col + off), j0, j1, j2, j3);
         const float4 p0 = __ldg(pos + j0);
         const float4 p1 = __ldg(pos + (tail > 1 ? j1 : j0));
         const float4 p2 = __ldg(pos + (tail > 2 ? j2 : j0));
@@ -952,6 +959,17 @@ __device__ __forceinline__ void step_body(const PhysDev& d, int cur, int slot, c
     using V = typename ChunkIds<ID>::V;
     const V* __restrict__ col = reinterpret_cast<const V*>(d.nl) + (uint32_t)i * kGroup + g;
     const uint32_t cstride = (uint32_t)d.n_pad * kGroup;
+    {   // the warp's list chunks into L2 at once: chunk q of its 4 particles is
+        // 4 x 32 contiguous ids, one bulk prefetch per lane q (no completion to wait for)
+        const int wch = ((int)__reduce_max_sync(0xffffffffu, (unsigned)rows) + 3) / 4;
+        const int lane = threadIdx.x & 31;
+        if (lane < wch) {
+            const uint32_t i0 = (blockIdx.x * blockDim.x + (threadIdx.x & ~31u)) / kStepLanes;
+            const char* a = reinterpret_cast<const char*>(d.nl) + ((size_t)lane * d.n_pad + i0) * kListChunk * sizeof(ID);
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((unsigned)(4 * kListChunk * sizeof(ID)))
+                         : "memory");
+        }
+    }
 #define LIMA_ROWS_CALL(WM) \
     pair_rows<MIXED, ENERGY, SWITCH, WM, ID>(d, row, pi, pos, col, cstride, rows, fx, fy, fz, cxx, cyy, czz, e_i, w_i)
     switch (wm) {

@@ -56,6 +56,7 @@ struct PhysDev {
     int n_c, n_s;
     float L, invL, rc, rc2, rlist, rlist2, ron2, inv_sw_d, half_skin2;   // inv_sw_d = 1/(rc^2 - r_on^2)
     float sw_c0, sw_k10;        // rc^2 inv_sw_d and 10 inv_sw_d (the step kernel's switch)
+    float inv_rc2;              // 1 / rc^2
     int use_switch;
     double dt;
     int precision;      // lima_precision

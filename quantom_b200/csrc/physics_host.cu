@@ -161,6 +161,7 @@ int phys_setup(const PhysHost& h, PhysDev& d, cudaStream_t s, std::vector<void*>
     d.inv_sw_d = d.use_switch ? 1.f / (d.rc2 - d.ron2) : 0.f;
     d.sw_c0 = d.rc2 * d.inv_sw_d;
     d.sw_k10 = 10.f * d.inv_sw_d;
+    d.inv_rc2 = 1.f / d.rc2;
     d.dt = p.dt;
     d.precision = p.precision;
     d.thermostat = p.thermostat;

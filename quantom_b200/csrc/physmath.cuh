@@ -108,8 +108,8 @@ __device__ __forceinline__ void lj_pair_step(const PhysDev& d, const float2* __r
         fr = t2 * z;
     } else {
         const bool in = r2 < d.rc2;
-        if (ENERGY) {
-            const float src2 = tab.x / d.rc2, src6 = src2 * src2 * src2;
+        if (ENERGY) {   // shifted to zero at r_c
+            const float src2 = tab.x * d.inv_rc2, src6 = src2 * src2 * src2;
             v = in ? (v6 - tab.y * (src6 * src6 - src6)) * (1.f / 6.f) : 0.f;
         }
         fr = in ? fr : 0.f;
