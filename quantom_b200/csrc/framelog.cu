@@ -5,7 +5,10 @@
 //                the particle; compound particles also their position into
 //                the train record (data_GAN value 0); thread 0 the frame's
 //                FP64 energies from the step's accumulator slot and the
-//                reference's 10-float log line of particle 0 (outdata)
+//                reference's 10-float log line of particle 0 (outdata).
+//                With no per-particle array logged, one block writes the
+//                energies and that line.  Its last block moves the device
+//                ring position on, so a step graph can hold the frame.
 //   k_log_train  8 lanes per compound particle over its Verlet list: the LJ
 //                force from solvent neighbours only (data_GAN value 1,
 //                Engine.cu:1034 force_LJ_sol), reduced with warp shuffles
@@ -77,10 +80,13 @@ __device__ __forceinline__ void log_frame_particle(const PhysDev& d, const Frame
     }
 }
 
-__global__ void __launch_bounds__(kTB) k_log_frame(PhysDev d, FrameLogDev g, int cur) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+// per_particle 0 (no per-particle arrays logged): one block, whose thread 0
+// writes the energies and the log line of particle 0
+__global__ void __launch_bounds__(kTB) k_log_frame(PhysDev d, FrameLogDev g, int cur, int per_particle) {
+    const int k = per_particle ? (int)(blockIdx.x * blockDim.x + threadIdx.x)
+                               : (threadIdx.x == 0 ? (int)d.sorted_of_orig[0] : d.n);
     const int r = ring_pos(g);
-    if (k == 0 && g.energies) {   // the step kernel's FP64 totals of the logged step
+    if (blockIdx.x == 0 && threadIdx.x == 0 && g.energies) {   // the step kernel's FP64 totals of the logged step
         double* e = g.energies + (size_t)r * LIMA_E_COUNT;
         for (int q = 0; q < LIMA_E_COUNT; q++) e[q] = d.e_last[q];
     }
@@ -440,7 +446,9 @@ int framelog_launch(const FrameLog& g, const PhysDev& d, int cur, cudaStream_t s
             k_log_train<false><<<nb, kTB, smem, s>>>(d, v, cur);
         launched++;
     }
-    k_log_frame<<<(d.n + kTB - 1) / kTB, kTB, 0, s>>>(d, v, cur);
+    const bool per_particle = v.traj || v.potE || v.train;
+    k_log_frame<<<per_particle ? (d.n + kTB - 1) / kTB : 1, per_particle ? kTB : 32, 0, s>>>(d, v, cur,
+                                                                                         per_particle ? 1 : 0);
     return launched;
 }
 
