@@ -1043,7 +1043,8 @@ def run_ours(args, ws, rank, local, pg):
     tflops = flops_pair / t_pair / 1e12
     compulsory = 80.0 * n
     list_len = (4.0 / 3.0) * math.pi * (spec.cutoff + SKIN) ** 3 * rho    # expected Verlet-list entries
-    bytes_list = n * (80.0 + 4.0 * list_len)
+    id_bytes = 2.0 if n <= 65536 else 4.0    # the list's slot ids are 16-bit while the slots fit
+    bytes_list = n * (80.0 + id_bytes * list_len)
     traffic = ncu_traffic("k_step", args.workload)
     roofline = {
         "kernel": "k_step", "bound": "fp32", "achieved": tflops, "peak": FP32_NOMINAL_TFLOPS,
@@ -1056,8 +1057,8 @@ def run_ours(args, ws, rank, local, pg):
                 "traffic_over_compulsory": (traffic / compulsory) if traffic else None,
                 "list_inclusive": {"bytes_per_launch": bytes_list, "achieved_gbs": bytes_list / t_pair / 1e9,
                                    "frac": bytes_list / t_pair / 1e9 / hbm,
-                                   "note": "counts the 4-byte Verlet-list entries (an implementation choice, "
-                                           "not algorithmic bytes)"}},
+                                   "note": f"counts the {int(id_bytes)}-byte Verlet-list entries (an "
+                                           "implementation choice, not algorithmic bytes)"}},
         "step": {"ms": ms_step, "frac_fp32": flops_pair / (ms_step * 1e-3) / 1e12 / FP32_NOMINAL_TFLOPS},
     }
     cpu = None
