@@ -457,7 +457,7 @@ __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;"
 #if LIMA_STAGED_LIST
 // Bulk copies global -> shared memory completing on an mbarrier (the copy
 // engine, not the threads, moves the bytes).  Sources are this GPU's own
-// memory; there is no cluster multicast.
+// memory, and each copy lands in the issuing block's shared memory only.
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
