@@ -154,6 +154,31 @@ def test_stop_keeps_frames_and_stops_recording(gpu):
         assert eng.lib.lima_log_read(eng.h, 0, 1, None, None, None, buf.ctypes.data, None, None) == E.ERR_ARGUMENT
 
 
+def test_energy_only_frames_and_reads_during_the_run(gpu):
+    """A log of energies and the log line only (one block per frame) read part
+    way through the run, which drains the device ring early, gives the same
+    frames as a full log read once at the end: the frame kernels take their
+    ring position from the device, inside the logged step's graph."""
+    E = gpu
+    s = S.make_system("tiny_chains", seed=8)
+    with E.Engine(s, _params(E, s)) as eng:
+        eng.log_start(1, ring_frames=4, flags=0)
+        eng.step(6)                      # the ring wraps once; two frames wait in it
+        first = eng.log_read()
+        eng.step(7)
+        assert eng.log_count() == 13
+        late = eng.log_read(6)
+    with E.Engine(s, _params(E, s)) as ref:
+        ref.log_start(1, ring_frames=64, flags=E.LOG_TRAJ | E.LOG_POTE | E.LOG_TRAIN)
+        ref.step(13)
+        full = ref.log_read()
+    assert first["steps"].tolist() == list(range(6)) and late["steps"].tolist() == list(range(6, 13))
+    for key in ("energies", "logdata"):
+        got = np.concatenate([first[key], late[key]])
+        np.testing.assert_array_equal(got, full[key])
+    assert "traj" not in first and "potE" not in first
+
+
 def _analyze_energy(s, traj, potE, dt):
     """Analyzer::analyzeEnergy (Analyzer.cu:33-207) restated over frames of
     consecutive steps: per frame f (1 .. F-3) the particle's potE plus the
