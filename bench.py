@@ -895,7 +895,7 @@ def metric_name(workload):
 
 
 def workload_text(workload, spec, n, ws):
-    """What the workload is, in BASELINE's terms and where it departs from them."""
+    """What the workload is, in the benchmark's terms and where it departs from them."""
     if workload != WORKLOAD:
         return workload
     return (f"{workload}: 16 chains x 64 (4 LJ types, harmonic bonds/angles, periodic dihedrals, one compound per "

@@ -4,7 +4,7 @@
 // sources to a temporary directory and puts this file in place of the
 // original, so that:
 //  * BOX_LEN / BOX_LEN_HALF / CUTOFF become runtime globals (set through the
-//    oracle's C API) instead of constexpr values — every BASELINE workload has
+//    oracle's C API) instead of constexpr values — every benchmark box has
 //    its own box length and cutoff;
 //  * the neighbour-list capacities are raised so a host run never overflows
 //    (NeighborList::addId calls exit(1) on overflow, Bodies.cuh:215-245);

@@ -2,7 +2,7 @@
 // reference's solvent placement (BoxBuilder::solvateBox/spaceAvailable,
 // Quantom/Quantom/BoxBuilder.cu:194-218, 440-461).  The reference rejects a
 // candidate solvent closer than a minimum distance to anything already placed.
-// Near the packing fractions the BASELINE workloads ask for (phi ~ 0.377 at
+// Near the packing fractions of the benchmark boxes (phi ~ 0.377 at
 // 0.28 nm) sequential rejection approaches the random-sequential-addition
 // jamming limit and needs ~1e9 trials, so this builder samples the same target
 // — positions uniform in the box conditioned on no pair closer than d_min —
